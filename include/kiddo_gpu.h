@@ -1,0 +1,199 @@
+/*
+ * kiddo_gpu.h — C ABI of the B200 batched query engine for kiddo's
+ * ImmutableKdTree (KdTree<A, u32, Eytzinger, VecOfArenas<A,u32,K,32>, K, 32>).
+ *
+ * The engine takes the reference builder's own layout — the Eytzinger stem
+ * array, the VecOfArenas leaf arena bytes and the (offset, len) leaf extents —
+ * uploads it unchanged to HBM and answers whole batches of queries with CUDA
+ * kernels for sm_100a.  Results are bit-identical to the reference's scalar
+ * `.execute()` path on the same tree and queries.
+ *
+ * Conventions
+ *  - Every entry point returns a kgpu_status; nothing aborts or throws across
+ *    the ABI.  kgpu_last_error() gives a message for the calling thread.
+ *  - Host arrays passed in are borrowed for the duration of the call only.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    With KGPU_FLAG_HOST_BUFFERS clear, query inputs and outputs are device
+ *    pointers and the call is asynchronous on `stream`.  With the flag set
+ *    they are host pointers (pinned or pageable); the library stages them
+ *    through HBM on `stream` and returns after the results are back.
+ *  - Trees are immutable after creation; a tree handle may be queried from
+ *    several host threads on different streams at once.
+ *
+ * Reference surface replaced (paths relative to the kiddo repository root):
+ *   KdTree::query(&q) -> QueryBuilder ... .execute()   src/kd_tree/query/builder.rs:2318-2331, :1693
+ *   the per-family execute impls                         src/kd_tree/query/builder.rs:4444-5419
+ *   KdTreeAccessor (layout read access)                  src/traits/kd_tree.rs:15-46
+ */
+#ifndef KIDDO_GPU_H
+#define KIDDO_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KGPU_ABI_VERSION 1u
+
+typedef enum kgpu_status {
+  KGPU_OK = 0,
+  KGPU_EINVAL = 1,        /* invalid argument (bad handle, size, box <= 0, k == 0 ...) */
+  KGPU_EUNSUPPORTED = 2,  /* layout or option this engine does not handle */
+  KGPU_ENOMEM = 3,        /* device or host allocation failed */
+  KGPU_ECUDA = 4,         /* a CUDA runtime call failed */
+  KGPU_ETIMEDOUT = 5,     /* a bounded device wait gave up */
+  KGPU_EOVERFLOW = 6,     /* result capacity or a size limit exceeded */
+  KGPU_ENOTREADY = 7
+} kgpu_status;
+
+typedef enum kgpu_dtype { KGPU_F32 = 0, KGPU_F64 = 1 } kgpu_dtype;
+
+typedef enum kgpu_stem_strategy {
+  KGPU_STEM_EYTZINGER = 0, /* src/stem_strategy/eytzinger/mod.rs */
+  KGPU_STEM_DONNELLY = 1   /* src/stem_strategy/donnelly/core.rs (not accepted yet) */
+} kgpu_stem_strategy;
+
+typedef enum kgpu_resolution {
+  KGPU_RES_ARITHMETIC = 0, /* OwnedStemLeafResolution::Arithmetic, stem_leaf_resolution.rs:28-68 */
+  KGPU_RES_MAPPED = 1,
+  KGPU_RES_PRISTINE = 2
+} kgpu_resolution;
+
+typedef enum kgpu_metric {
+  KGPU_SQUARED_EUCLIDEAN = 0, /* src/dist/squared_euclidean/mod.rs:21-40 */
+  KGPU_MANHATTAN = 1          /* src/dist/manhattan/mod.rs:21-48 */
+} kgpu_metric;
+
+typedef enum kgpu_family {
+  KGPU_NEAREST_ONE = 0,        /* .nearest_one::<D>()                 builder.rs:4444 */
+  KGPU_APPROX_NEAREST_ONE = 1, /* .nearest_one::<D>().approx()        builder.rs:4502 */
+  KGPU_NEAREST_N = 2,          /* .nearest_n::<D>(k)                  builder.rs:4629/:4706 */
+  KGPU_NEAREST_N_WITHIN = 3,   /* .nearest_n::<D>(k).within(r)        builder.rs:4783/:4874 */
+  KGPU_WITHIN = 4,             /* .within::<D>(r)                     builder.rs:4965 */
+  KGPU_WITHIN_UNSORTED = 5,    /* .within::<D>(r).unsorted()          builder.rs:5048 */
+  KGPU_BEST_N_WITHIN = 6       /* .best_n_within::<D>(r, n)           builder.rs:5419 */
+} kgpu_family;
+
+/* Query flags */
+#define KGPU_FLAG_HOST_BUFFERS 0x1u  /* queries/outputs are host pointers */
+#define KGPU_FLAG_SPATIAL_ORDER 0x2u /* process queries in Morton order (same results) */
+
+/* Layout of one ImmutableKdTree as the reference stores it
+ * (src/kd_tree/mod.rs:221-241, src/leaf_strategy/vec_of_arenas.rs:60-69). */
+typedef struct kgpu_tree_desc {
+  uint32_t abi_version;      /* KGPU_ABI_VERSION */
+  int32_t dtype;             /* kgpu_dtype of the axis type A */
+  uint32_t dims;             /* K, 1..4 */
+  uint32_t item_size;        /* sizeof(T); 4 (u32) */
+  uint32_t bucket_size;      /* B; 32 */
+  int32_t stem_strategy;     /* kgpu_stem_strategy */
+  uint32_t block_height;     /* Donnelly BH; 0 for Eytzinger */
+  int32_t resolution;        /* kgpu_resolution */
+  const void* stems;         /* stem_count values of type A, Eytzinger order, +inf = no split */
+  uint64_t stem_count;
+  const uint8_t* leaf_bytes; /* VecOfArenas arena: tiles 32/8/4/2/1, K columns then items */
+  uint64_t leaf_bytes_len;
+  const uint64_t* leaf_extents; /* leaf_count pairs (byte offset, len) */
+  uint64_t leaf_count;
+  int32_t max_stem_level;    /* KdTree::max_stem_level, -1 for a stemless tree */
+  uint32_t reserved0;
+  uint64_t size;             /* number of points */
+  uint64_t max_leaf_len;
+} kgpu_tree_desc;
+
+typedef struct kgpu_query_desc {
+  uint32_t abi_version;   /* KGPU_ABI_VERSION */
+  int32_t family;         /* kgpu_family */
+  int32_t metric;         /* kgpu_metric */
+  uint32_t max_qty;       /* k for nearest_n*, n for best_n_within (1..32) */
+  double radius;          /* metric units (squared distance for SquaredEuclidean); cast to A */
+  int32_t exclusive;      /* .exclusive_boundaries(): strict `< radius` */
+  int32_t sorted;         /* 1 = default sorted output, 0 = .unsorted() */
+  const void* periodic_box; /* host pointer to K values of A, or NULL (Cartesian) */
+  uint32_t flags;         /* KGPU_FLAG_* */
+  uint32_t reserved0;
+} kgpu_query_desc;
+
+typedef struct kgpu_layout kgpu_layout; /* host-side tree layout built by this library */
+typedef struct kgpu_tree kgpu_tree;     /* device-resident tree */
+
+/* ---- errors ------------------------------------------------------------ */
+const char* kgpu_last_error(void);
+const char* kgpu_status_string(int32_t status);
+uint32_t kgpu_abi_version(void);
+
+/* ---- host construction -------------------------------------------------
+ * Builds the ImmutableKdTree layout with the reference's soft-bucket bulk
+ * construction (src/kd_tree/construction.rs:413-539, 868-968, 1089-1175;
+ * VecOfArenas::append_leaf src/leaf_strategy/vec_of_arenas.rs:292-323).
+ * Replaces KdTree::new_from_slice (items NULL: item = source index,
+ * construction.rs:278-303) and KdTree::new_from_entries (construction.rs:403-409).
+ * `points` is n rows of `dims` values of `dtype`.  Points inside a leaf are
+ * stored in ascending source index. */
+int32_t kgpu_layout_build(int32_t dtype, uint32_t dims, const void* points,
+                          const uint32_t* items, uint64_t n, int32_t nthreads,
+                          kgpu_layout** out);
+/* Fills `desc` with pointers into the layout's own storage (valid until free). */
+int32_t kgpu_layout_describe(const kgpu_layout* layout, kgpu_tree_desc* desc);
+int32_t kgpu_layout_free(kgpu_layout* layout);
+
+/* ---- device trees --------------------------------------------------------
+ * Upload a layout (one the reference built, or kgpu_layout_build's) to the
+ * current CUDA device.  Stems and arena bytes are copied unchanged; extents
+ * are re-encoded as 32-bit (offset / 8, len) pairs. */
+int32_t kgpu_tree_create(const kgpu_tree_desc* desc, void* stream, kgpu_tree** out);
+int32_t kgpu_tree_destroy(kgpu_tree* tree);
+/* info[0..7] = dtype, dims, size, leaf_count, max_stem_level, stem_count,
+ *              leaf_bytes_len, device bytes held */
+int32_t kgpu_tree_info(const kgpu_tree* tree, int64_t* info);
+
+/* ---- fixed-size families --------------------------------------------------
+ * KGPU_NEAREST_ONE, KGPU_APPROX_NEAREST_ONE: out_dists/out_items hold nq
+ * entries.  KGPU_NEAREST_N, KGPU_NEAREST_N_WITHIN, KGPU_BEST_N_WITHIN: they
+ * hold nq * max_qty entries, row-major; out_counts[nq] (may be NULL) receives
+ * the number of valid entries per query; unused slots hold +inf and
+ * 0xFFFFFFFF.  A periodic box is accepted for the nearest families
+ * (src/kd_tree/query/periodic.rs:156-214, :682-791).
+ * Output order: nearest_n sorted by (distance, traversal arrival);
+ * .unsorted() keeps arrival order while fewer than k were found (ThresholdVec
+ * into_vec, results/result_collection.rs:136-215); best_n_within ascending
+ * (item, arrival). */
+int32_t kgpu_query(kgpu_tree* tree, const kgpu_query_desc* desc, const void* queries,
+                   uint64_t nq, void* out_dists, uint32_t* out_items, uint32_t* out_counts,
+                   void* stream);
+
+/* ---- radius families (KGPU_WITHIN, KGPU_WITHIN_UNSORTED) ---------------
+ * Two phases with caller-owned memory:
+ *  1. kgpu_query_radius_count writes offsets[0..nq] (exclusive prefix of the
+ *     per-query hit counts; offsets[nq] = total).
+ *  2. kgpu_query_radius_fill writes total hits into out_dists/out_items at
+ *     those offsets: sorted = stable by distance over traversal order
+ *     (Vec::sort, results/result_collection.rs:1313-1316); unsorted =
+ *     traversal order (within_unsorted.rs:133-157).
+ * Both accept a periodic box. */
+int32_t kgpu_query_radius_count(kgpu_tree* tree, const kgpu_query_desc* desc,
+                                const void* queries, uint64_t nq, uint64_t* offsets,
+                                void* stream);
+int32_t kgpu_query_radius_fill(kgpu_tree* tree, const kgpu_query_desc* desc,
+                               const void* queries, uint64_t nq, const uint64_t* offsets,
+                               void* out_dists, uint32_t* out_items, void* stream);
+
+/* ---- traversal statistics ----------------------------------------------
+ * Runs the query's traversal (for the radius families: the counting pass)
+ * with counters and writes the totals over the batch to stats[0..2]:
+ * stem visits, leaf visits, points scanned — the quantities of
+ * src/test_utils/exact_query_stats.rs:23-60.  Outputs are discarded.
+ * Synchronous; for sizing and for the algorithmic-bytes roofline model. */
+int32_t kgpu_query_stats(kgpu_tree* tree, const kgpu_query_desc* desc, const void* queries,
+                         uint64_t nq, uint64_t* stats, void* stream);
+
+/* ---- accounting --------------------------------------------------------
+ * Number of CUDA kernels this library has launched in the process so far
+ * (all threads).  Lets a caller count the launches inside a timed region. */
+uint64_t kgpu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KIDDO_GPU_H */

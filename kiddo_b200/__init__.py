@@ -1,0 +1,448 @@
+"""kiddo_b200 — a batched B200 query engine for kiddo's ImmutableKdTree.
+
+Host-side mirror of the reference's fluent query surface
+(``KdTree::query(&q) -> QueryBuilder -> .execute()``,
+src/kd_tree/query/builder.rs:2318-2331, :1546-1565, :1693) with a batched
+``.execute_gpu()`` terminal.  Everything below the builder runs in
+``libkiddo_gpu.so`` (CUDA, sm_100a) through the C ABI of include/kiddo_gpu.h.
+
+    tree = ImmutableKdTree.new_from_slice(points)          # construction.rs:278-303
+    res = tree.query(queries).nearest_n(SquaredEuclidean, 16).execute_gpu()
+    res.distances, res.items, res.counts
+
+Query families and modifiers follow builder.rs:1994-2077:
+``nearest_one``, ``.approx()``, ``nearest_n``, ``nearest_n(...).within(r)``,
+``within``, ``.unsorted()``, ``best_n_within``, ``.exclusive_boundaries()``,
+``periodic_boundary_condition(box)`` (chosen before the query type).
+Radii are in metric units (squared distance for SquaredEuclidean), exactly as
+the reference's ``within::<SquaredEuclidean<_>>(radius)``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _capi as C
+from ._capi import KiddoGpuError, launch_count
+
+__all__ = ["ImmutableKdTree", "GpuTree", "SquaredEuclidean", "Manhattan", "KiddoGpuError",
+           "NearestOneResult", "NearestNResult", "WithinResult", "launch_count"]
+
+
+class SquaredEuclidean:
+    """dist/squared_euclidean/mod.rs:21-40 — radius in squared units."""
+    code = C.SQUARED_EUCLIDEAN
+
+
+class Manhattan:
+    """dist/manhattan/mod.rs:21-48."""
+    code = C.MANHATTAN
+
+
+def _metric_code(m) -> int:
+    if m in (SquaredEuclidean, "sqeuclidean", "squared_euclidean"):
+        return C.SQUARED_EUCLIDEAN
+    if m in (Manhattan, "manhattan"):
+        return C.MANHATTAN
+    raise TypeError(f"unsupported metric {m!r} (SquaredEuclidean or Manhattan)")
+
+
+def _vp(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+def _is_torch_cuda(x) -> bool:
+    try:
+        import torch
+        return isinstance(x, torch.Tensor) and x.is_cuda
+    except ImportError:
+        return False
+
+
+class ImmutableKdTree:
+    """Host copy of an ImmutableKdTree<A, K> layout (stems, arena, extents).
+
+    Built with the reference's soft construction by ``kgpu_layout_build``, or
+    wrapped around a layout the reference itself produced (``from_layout``).
+    """
+
+    def __init__(self, desc: C.TreeDesc, keepalive, dtype, dims):
+        self._desc = desc
+        self._keep = keepalive
+        self.dtype = np.dtype(dtype)
+        self.dims = int(dims)
+        self._gpu: Optional[GpuTree] = None
+
+    # ---- construction (construction.rs:278-303, 403-409) -------------------
+    @classmethod
+    def new_from_slice(cls, points, threads: int = 0) -> "ImmutableKdTree":
+        return cls._build(points, None, threads)
+
+    @classmethod
+    def new_from_entries(cls, items, points, threads: int = 0) -> "ImmutableKdTree":
+        return cls._build(points, np.ascontiguousarray(items, dtype=np.uint32), threads)
+
+    @classmethod
+    def _build(cls, points, items, threads):
+        pts = np.ascontiguousarray(points)
+        if pts.dtype not in (np.float32, np.float64) or pts.ndim != 2:
+            raise TypeError("points must be a 2-D float32 or float64 array")
+        n, k = pts.shape
+        if items is not None and items.shape[0] != n:
+            raise ValueError("items and points differ in length")
+        L = C.lib()
+        h = ctypes.c_void_p()
+        C.check(L.kgpu_layout_build(C.F32 if pts.dtype == np.float32 else C.F64, k, _vp(pts),
+                                    _vp(items), n, threads, ctypes.byref(h)))
+        holder = _LayoutHandle(h)
+        desc = C.TreeDesc()
+        C.check(L.kgpu_layout_describe(h, ctypes.byref(desc)))
+        return cls(desc, holder, pts.dtype, k)
+
+    @classmethod
+    def from_layout(cls, dtype, dims, stems, leaf_bytes, extents, max_stem_level, size,
+                    max_leaf_len) -> "ImmutableKdTree":
+        """Wrap the reference's own layout arrays (KdTreeAccessor, traits/kd_tree.rs:15-46)."""
+        dt = np.dtype(dtype)
+        stems = np.ascontiguousarray(stems, dtype=dt)
+        lb = np.ascontiguousarray(leaf_bytes, dtype=np.uint8)
+        ex = np.ascontiguousarray(extents, dtype=np.uint64).reshape(-1, 2)
+        d = C.TreeDesc()
+        d.abi_version = C.ABI_VERSION
+        d.dtype = C.F32 if dt == np.float32 else C.F64
+        d.dims = dims
+        d.item_size = 4
+        d.bucket_size = 32
+        d.stem_strategy = C.STEM_EYTZINGER
+        d.resolution = C.RES_ARITHMETIC
+        d.stems = stems.ctypes.data if stems.size else None
+        d.stem_count = stems.size
+        d.leaf_bytes = lb.ctypes.data if lb.size else None
+        d.leaf_bytes_len = lb.size
+        d.leaf_extents = ex.ctypes.data if ex.size else None
+        d.leaf_count = ex.shape[0]
+        d.max_stem_level = int(max_stem_level)
+        d.size = int(size)
+        d.max_leaf_len = int(max_leaf_len)
+        return cls(d, (stems, lb, ex), dt, dims)
+
+    # ---- KdTreeAccessor -----------------------------------------------------
+    def size(self) -> int:
+        return int(self._desc.size)
+
+    def leaf_count(self) -> int:
+        return int(self._desc.leaf_count)
+
+    def max_stem_level(self) -> int:
+        return int(self._desc.max_stem_level)
+
+    def max_leaf_len(self) -> int:
+        return int(self._desc.max_leaf_len)
+
+    def stems(self) -> np.ndarray:
+        n = int(self._desc.stem_count)
+        if n == 0:
+            return np.empty(0, dtype=self.dtype)
+        buf = (ctypes.c_char * (n * self.dtype.itemsize)).from_address(self._desc.stems)
+        return np.frombuffer(buf, dtype=self.dtype).copy()
+
+    def leaf_bytes(self) -> np.ndarray:
+        n = int(self._desc.leaf_bytes_len)
+        if n == 0:
+            return np.empty(0, dtype=np.uint8)
+        buf = (ctypes.c_char * n).from_address(self._desc.leaf_bytes)
+        return np.frombuffer(buf, dtype=np.uint8).copy()
+
+    def leaf_extents(self) -> np.ndarray:
+        n = int(self._desc.leaf_count)
+        if n == 0:
+            return np.empty((0, 2), dtype=np.uint64)
+        buf = (ctypes.c_char * (n * 16)).from_address(self._desc.leaf_extents)
+        return np.frombuffer(buf, dtype=np.uint64).reshape(n, 2).copy()
+
+    # ---- device -------------------------------------------------------------
+    def to_gpu(self, stream=None) -> "GpuTree":
+        if self._gpu is None:
+            self._gpu = GpuTree(self, stream)
+        return self._gpu
+
+    def query(self, queries) -> "QueryBuilder":
+        """KdTree::query (builder.rs:2318-2331), batched: rows of `queries`."""
+        return self.to_gpu().query(queries)
+
+
+class _LayoutHandle:
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        if self.h and C._lib is not None:
+            C._lib.kgpu_layout_free(self.h)
+            self.h = None
+
+
+class GpuTree:
+    """A tree resident in HBM (kgpu_tree_create)."""
+
+    def __init__(self, host: ImmutableKdTree, stream=None):
+        L = C.lib()
+        self.host = host
+        self.dtype = host.dtype
+        self.dims = host.dims
+        h = ctypes.c_void_p()
+        C.check(L.kgpu_tree_create(ctypes.byref(host._desc), _stream_ptr(stream), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and C._lib is not None:
+            C._lib.kgpu_tree_destroy(self._h)
+            self._h = None
+
+    def info(self):
+        a = np.zeros(8, dtype=np.int64)
+        C.check(C.lib().kgpu_tree_info(self._h, _vp(a)))
+        return dict(zip(["dtype", "dims", "size", "leaf_count", "max_stem_level", "stem_count",
+                         "leaf_bytes_len", "device_bytes"], a.tolist()))
+
+    def query(self, queries) -> "QueryBuilder":
+        return QueryBuilder(self, queries)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+@dataclass
+class NearestOneResult:
+    distances: object
+    items: object
+
+
+@dataclass
+class NearestNResult:
+    distances: object
+    items: object
+    counts: object
+
+
+@dataclass
+class WithinResult:
+    offsets: object
+    distances: object
+    items: object
+
+    def __len__(self):
+        return len(self.offsets) - 1
+
+    def __getitem__(self, i):
+        a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+        return self.distances[a:b], self.items[a:b]
+
+
+class QueryBuilder:
+    """Runtime mirror of the typestate QueryBuilder (builder.rs:1373-1398)."""
+
+    def __init__(self, tree: GpuTree, queries):
+        self.tree = tree
+        self.queries = queries
+        self.family = None
+        self.metric = None
+        self.max_qty = 0
+        self.radius = None
+        self.exclusive = False
+        self.sorted = True
+        self.box = None
+        self.spatial_order = False
+        self.stream = None
+
+    # ---- space --------------------------------------------------------------
+    def periodic_boundary_condition(self, box_size) -> "QueryBuilder":
+        if self.family is not None:
+            raise TypeError("periodic_boundary_condition must be chosen before the query type")
+        box = np.ascontiguousarray(box_size, dtype=self.tree.dtype).reshape(-1)
+        if box.size != self.tree.dims:
+            raise ValueError("box_size must have one entry per axis")
+        if not np.all(box > 0):
+            raise ValueError("periodic box sizes must be strictly positive")
+        self.box = box
+        return self
+
+    # ---- query type -----------------------------------------------------------
+    def nearest_one(self, metric) -> "QueryBuilder":
+        self._set_family(C.NEAREST_ONE, metric)
+        return self
+
+    def nearest_n(self, metric, max_qty: int) -> "QueryBuilder":
+        if int(max_qty) < 1:
+            raise ValueError("max_qty must be non-zero (NonZeroUsize)")
+        self._set_family(C.NEAREST_N, metric)
+        self.max_qty = int(max_qty)
+        return self
+
+    def within(self, *args) -> "QueryBuilder":
+        """``within(metric, radius)`` selects a radius query;
+        ``nearest_n(...).within(radius)`` bounds a k-NN query."""
+        if self.family == C.NEAREST_N and len(args) == 1:
+            self.family = C.NEAREST_N_WITHIN
+            self.radius = float(args[0])
+            return self
+        if len(args) != 2:
+            raise TypeError("within(metric, radius) or nearest_n(metric, k).within(radius)")
+        self._set_family(C.WITHIN, args[0])
+        self.radius = float(args[1])
+        return self
+
+    def best_n_within(self, metric, radius, max_qty: int) -> "QueryBuilder":
+        if self.box is not None:
+            raise TypeError("best_n_within is Cartesian-only")
+        if int(max_qty) < 1:
+            raise ValueError("max_qty must be non-zero")
+        self._set_family(C.BEST_N_WITHIN, metric)
+        self.radius = float(radius)
+        self.max_qty = int(max_qty)
+        return self
+
+    # ---- options ---------------------------------------------------------------
+    def approx(self) -> "QueryBuilder":
+        if self.family != C.NEAREST_ONE or self.box is not None:
+            raise TypeError("approx() is available only after a Cartesian nearest_one()")
+        self.family = C.APPROX_NEAREST_ONE
+        return self
+
+    def unsorted(self) -> "QueryBuilder":
+        if self.family not in (C.WITHIN, C.NEAREST_N, C.NEAREST_N_WITHIN):
+            raise TypeError("unsorted() applies to within and nearest_n queries")
+        self.sorted = False
+        if self.family == C.WITHIN:
+            self.family = C.WITHIN_UNSORTED
+        return self
+
+    def exclusive_boundaries(self) -> "QueryBuilder":
+        if self.family not in (C.WITHIN, C.WITHIN_UNSORTED, C.NEAREST_N_WITHIN, C.BEST_N_WITHIN):
+            raise TypeError("exclusive_boundaries() applies to radius-bounded queries")
+        self.exclusive = True
+        return self
+
+    def with_spatial_order(self, on: bool = True) -> "QueryBuilder":
+        """Process the batch in a cache-friendly order (identical results)."""
+        self.spatial_order = bool(on)
+        return self
+
+    def on_stream(self, stream) -> "QueryBuilder":
+        self.stream = stream
+        return self
+
+    def _set_family(self, fam, metric):
+        if self.family is not None:
+            raise TypeError("query type already chosen")
+        self.family = fam
+        self.metric = _metric_code(metric)
+
+    # ---- terminal ---------------------------------------------------------------
+    def _desc(self, host: bool) -> C.QueryDesc:
+        d = C.QueryDesc()
+        d.abi_version = C.ABI_VERSION
+        d.family = self.family
+        d.metric = self.metric
+        d.max_qty = self.max_qty
+        d.radius = float(self.radius) if self.radius is not None else float("inf")
+        d.exclusive = int(self.exclusive)
+        d.sorted = int(self.sorted)
+        d.periodic_box = self.box.ctypes.data if self.box is not None else None
+        d.flags = (C.FLAG_HOST_BUFFERS if host else 0) | (
+            C.FLAG_SPATIAL_ORDER if self.spatial_order else 0)
+        return d
+
+    def traversal_stats(self):
+        """[stem visits, leaf visits, points scanned] over the batch
+        (exact_query_stats.rs:23-60), measured by the GPU traversal."""
+        if self.family is None:
+            raise TypeError("choose a query type first")
+        q = np.ascontiguousarray(self.queries, dtype=self.tree.dtype).reshape(-1, self.tree.dims)
+        out = np.zeros(3, dtype=np.uint64)
+        d = self._desc(True)
+        C.check(C.lib().kgpu_query_stats(self.tree._h, ctypes.byref(d), _vp(q), q.shape[0],
+                                         _vp(out), _stream_ptr(self.stream)))
+        return out
+
+    def execute_gpu(self):
+        if self.family is None:
+            raise TypeError("choose a query type before execute_gpu()")
+        if _is_torch_cuda(self.queries):
+            return self._execute_device()
+        return self._execute_host()
+
+    def _execute_host(self):
+        L = C.lib()
+        q = np.ascontiguousarray(self.queries, dtype=self.tree.dtype)
+        if q.ndim == 1:
+            q = q.reshape(1, -1)
+        if q.shape[1] != self.tree.dims:
+            raise ValueError("query dimensionality does not match the tree")
+        nq = q.shape[0]
+        d = self._desc(True)
+        st = _stream_ptr(self.stream)
+        if self.family in (C.WITHIN, C.WITHIN_UNSORTED):
+            off = np.empty(nq + 1, dtype=np.uint64)
+            C.check(L.kgpu_query_radius_count(self.tree._h, ctypes.byref(d), _vp(q), nq, _vp(off),
+                                              st))
+            total = int(off[-1])
+            dist = np.empty(total, dtype=self.tree.dtype)
+            items = np.empty(total, dtype=np.uint32)
+            C.check(L.kgpu_query_radius_fill(self.tree._h, ctypes.byref(d), _vp(q), nq, _vp(off),
+                                             _vp(dist), _vp(items), st))
+            return WithinResult(off, dist, items)
+        w = 1 if self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE) else self.max_qty
+        dist = np.empty((nq, w), dtype=self.tree.dtype)
+        items = np.empty((nq, w), dtype=np.uint32)
+        counts = np.empty(nq, dtype=np.uint32)
+        C.check(L.kgpu_query(self.tree._h, ctypes.byref(d), _vp(q), nq, _vp(dist), _vp(items),
+                             _vp(counts), st))
+        if w == 1 and self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE):
+            return NearestOneResult(dist[:, 0], items[:, 0])
+        return NearestNResult(dist, items, counts)
+
+    def _execute_device(self):
+        import torch
+        L = C.lib()
+        tdt = torch.float32 if self.tree.dtype == np.float32 else torch.float64
+        q = self.queries
+        if q.dtype != tdt:
+            raise TypeError("device queries must match the tree dtype")
+        q = q.contiguous()
+        nq = q.shape[0]
+        d = self._desc(False)
+        stream = self.stream if self.stream is not None else torch.cuda.current_stream(q.device)
+        st = _stream_ptr(stream)
+        dev = q.device
+        if self.family in (C.WITHIN, C.WITHIN_UNSORTED):
+            off = torch.empty(nq + 1, dtype=torch.int64, device=dev)
+            C.check(L.kgpu_query_radius_count(self.tree._h, ctypes.byref(d),
+                                              ctypes.c_void_p(q.data_ptr()), nq,
+                                              ctypes.c_void_p(off.data_ptr()), st))
+            total = int(off[-1].item())
+            dist = torch.empty(max(total, 1), dtype=tdt, device=dev)
+            items = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+            C.check(L.kgpu_query_radius_fill(self.tree._h, ctypes.byref(d),
+                                             ctypes.c_void_p(q.data_ptr()), nq,
+                                             ctypes.c_void_p(off.data_ptr()),
+                                             ctypes.c_void_p(dist.data_ptr()),
+                                             ctypes.c_void_p(items.data_ptr()), st))
+            return WithinResult(off, dist[:total], items[:total])
+        w = 1 if self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE) else self.max_qty
+        dist = torch.empty((nq, w), dtype=tdt, device=dev)
+        items = torch.empty((nq, w), dtype=torch.int32, device=dev)
+        counts = torch.empty(nq, dtype=torch.int32, device=dev)
+        C.check(L.kgpu_query(self.tree._h, ctypes.byref(d), ctypes.c_void_p(q.data_ptr()), nq,
+                             ctypes.c_void_p(dist.data_ptr()), ctypes.c_void_p(items.data_ptr()),
+                             ctypes.c_void_p(counts.data_ptr()), st))
+        if self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE):
+            return NearestOneResult(dist[:, 0], items[:, 0])
+        return NearestNResult(dist, items, counts)

@@ -1,0 +1,552 @@
+// kgpu_api.cu — the extern "C" entry points declared in include/kiddo_gpu.h.
+//
+// Validation, upload of the reference layout, host staging, and the
+// count -> scan -> fill -> sort pipeline of the radius families.  Every entry
+// point returns a status; no C++ exception or CUDA error escapes the ABI.
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/kiddo_gpu.h"
+#include "kgpu_internal.h"
+#include "kgpu_launch.h"
+
+namespace kgpu {
+
+std::atomic<uint64_t> g_launches{0};
+
+namespace {
+thread_local std::string t_last_error;
+}
+
+int set_error(int status, const std::string& msg) {
+  t_last_error = msg;
+  return status;
+}
+
+static int cuda_fail(cudaError_t e, const char* what) {
+  return set_error(KGPU_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int sm_count() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static std::mutex mu;
+  static std::vector<int> cache;
+  std::lock_guard<std::mutex> g(mu);
+  if (dev >= int(cache.size())) cache.resize(dev + 1, 0);
+  if (cache[dev] == 0) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cache[dev] = n > 0 ? n : 1;
+  }
+  return cache[dev];
+}
+
+namespace {
+
+size_t leaf_encoded_bytes(uint64_t len, int K, size_t sa) {
+  size_t total = 0;
+  while (len) {
+    uint64_t w = len >= 32 ? 32 : len >= 8 ? 8 : len >= 4 ? 4 : len >= 2 ? 2 : 1;
+    total += size_t(w) * (K * sa + 4);
+    len -= w;
+  }
+  return total;
+}
+
+// RAII device buffer allocated on a stream (stream-ordered allocator).
+struct DevBuf {
+  void* p = nullptr;
+  cudaStream_t s = nullptr;
+  cudaError_t alloc(size_t bytes, cudaStream_t st) {
+    s = st;
+    if (bytes == 0) bytes = 16;
+    return cudaMallocAsync(&p, bytes, st);
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, s);
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_family);
+
+}  // namespace
+}  // namespace kgpu
+
+struct kgpu_tree {
+  kgpu::DeviceTree dt;
+};
+
+using namespace kgpu;
+
+extern "C" {
+
+const char* kgpu_last_error(void) { return t_last_error.c_str(); }
+
+const char* kgpu_status_string(int32_t s) {
+  switch (s) {
+    case KGPU_OK: return "ok";
+    case KGPU_EINVAL: return "invalid argument";
+    case KGPU_EUNSUPPORTED: return "unsupported layout or option";
+    case KGPU_ENOMEM: return "out of memory";
+    case KGPU_ECUDA: return "CUDA error";
+    case KGPU_ETIMEDOUT: return "device wait timed out";
+    case KGPU_EOVERFLOW: return "capacity overflow";
+    case KGPU_ENOTREADY: return "not ready";
+  }
+  return "unknown status";
+}
+
+uint32_t kgpu_abi_version(void) { return KGPU_ABI_VERSION; }
+
+uint64_t kgpu_launch_count(void) { return g_launches.load(); }
+
+// ---- host construction ----------------------------------------------------
+int32_t kgpu_layout_build(int32_t dtype, uint32_t dims, const void* points, const uint32_t* items,
+                          uint64_t n, int32_t nthreads, kgpu_layout** out) {
+  if (!out) return set_error(KGPU_EINVAL, "out is NULL");
+  *out = nullptr;
+  auto* lay = new (std::nothrow) kgpu_layout();
+  if (!lay) return set_error(KGPU_ENOMEM, "host allocation failed");
+  int st = build_layout_any(lay->L, dtype, int(dims), points, items, n, nthreads);
+  if (st != KGPU_OK) {
+    delete lay;
+    return st;
+  }
+  *out = lay;
+  return KGPU_OK;
+}
+
+int32_t kgpu_layout_describe(const kgpu_layout* lay, kgpu_tree_desc* d) {
+  if (!lay || !d) return set_error(KGPU_EINVAL, "NULL argument");
+  const Layout& L = lay->L;
+  std::memset(d, 0, sizeof(*d));
+  d->abi_version = KGPU_ABI_VERSION;
+  d->dtype = L.dtype;
+  d->dims = uint32_t(L.dims);
+  d->item_size = 4;
+  d->bucket_size = 32;
+  d->stem_strategy = KGPU_STEM_EYTZINGER;
+  d->block_height = 0;
+  d->resolution = KGPU_RES_ARITHMETIC;
+  const size_t sa = L.dtype == KGPU_F64 ? 8 : 4;
+  d->stems = L.stems_bytes.empty() ? nullptr : L.stems_bytes.data();
+  d->stem_count = L.stems_bytes.size() / sa;
+  d->leaf_bytes = L.leaf_bytes.empty() ? nullptr : L.leaf_bytes.data();
+  d->leaf_bytes_len = L.leaf_bytes.size();
+  d->leaf_extents = L.extents.empty() ? nullptr : L.extents.data();
+  d->leaf_count = L.extents.size() / 2;
+  d->max_stem_level = L.max_stem_level;
+  d->size = L.size;
+  d->max_leaf_len = L.max_leaf_len;
+  return KGPU_OK;
+}
+
+int32_t kgpu_layout_free(kgpu_layout* lay) {
+  delete lay;
+  return KGPU_OK;
+}
+
+// ---- device trees -----------------------------------------------------------
+int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out) {
+  if (!d || !out) return set_error(KGPU_EINVAL, "NULL argument");
+  *out = nullptr;
+  if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
+  if (d->dtype != KGPU_F32 && d->dtype != KGPU_F64)
+    return set_error(KGPU_EINVAL, "dtype must be KGPU_F32 or KGPU_F64");
+  if (d->dims < 1 || d->dims > uint32_t(kMaxDims))
+    return set_error(KGPU_EUNSUPPORTED, "dims must be 1..4");
+  if (d->item_size != 4) return set_error(KGPU_EUNSUPPORTED, "only u32 items (ImmutableKdTree)");
+  if (d->bucket_size != 32) return set_error(KGPU_EUNSUPPORTED, "only bucket size 32");
+  if (d->stem_strategy != KGPU_STEM_EYTZINGER)
+    return set_error(KGPU_EUNSUPPORTED, "only the Eytzinger stem strategy is accepted");
+  if (d->resolution != KGPU_RES_ARITHMETIC)
+    return set_error(KGPU_EUNSUPPORTED,
+                     "only arithmetic stem/leaf resolution (soft immutable trees) is accepted");
+  if (d->max_stem_level < -1 || d->max_stem_level > kMaxStemLevel)
+    return set_error(KGPU_EUNSUPPORTED, "max_stem_level must be -1..30");
+  const size_t sa = d->dtype == KGPU_F64 ? 8 : 4;
+  const int K = int(d->dims);
+  const uint64_t expect_leaves =
+      d->max_stem_level >= 0 ? (uint64_t(1) << (d->max_stem_level + 1)) : (d->size ? 1 : 0);
+  if (d->leaf_count != expect_leaves)
+    return set_error(KGPU_EINVAL, "leaf_count does not match max_stem_level (arithmetic layout)");
+  if (d->max_stem_level >= 0 && d->stem_count < (uint64_t(1) << (d->max_stem_level + 1)))
+    return set_error(KGPU_EINVAL, "stem array shorter than 2^(max_stem_level+1)");
+  if (d->leaf_count && (!d->leaf_extents || !d->leaf_bytes))
+    return set_error(KGPU_EINVAL, "leaf arrays are NULL");
+  if (d->max_stem_level >= 0 && !d->stems) return set_error(KGPU_EINVAL, "stems is NULL");
+  if (d->leaf_bytes_len / 8 >= (uint64_t(1) << 32))
+    return set_error(KGPU_EOVERFLOW, "leaf arena larger than 32 GiB");
+  // extents -> (offset / 8, len), validated against the arena
+  std::vector<uint32_t> ex;
+  try {
+    ex.resize(2 * d->leaf_count);
+  } catch (const std::bad_alloc&) {
+    return set_error(KGPU_ENOMEM, "host allocation failed");
+  }
+  uint64_t total = 0;
+  for (uint64_t l = 0; l < d->leaf_count; ++l) {
+    const uint64_t off = d->leaf_extents[2 * l], len = d->leaf_extents[2 * l + 1];
+    if (off % 8) return set_error(KGPU_EINVAL, "leaf offset not 8-byte aligned");
+    if (len > 1024) return set_error(KGPU_EINVAL, "leaf longer than 1024 points");
+    if (off + leaf_encoded_bytes(len, K, sa) > d->leaf_bytes_len)
+      return set_error(KGPU_EINVAL, "leaf extent outside the arena");
+    ex[2 * l] = uint32_t(off / 8);
+    ex[2 * l + 1] = uint32_t(len);
+    total += len;
+  }
+  if (total != d->size) return set_error(KGPU_EINVAL, "sum of leaf lengths != size");
+
+  auto* t = new (std::nothrow) kgpu_tree();
+  if (!t) return set_error(KGPU_ENOMEM, "host allocation failed");
+  DeviceTree& dt = t->dt;
+  dt.dtype = d->dtype;
+  dt.dims = K;
+  cudaGetDevice(&dt.device);
+  dt.max_stem_level = d->max_stem_level;
+  dt.leaf_count = uint32_t(d->leaf_count);
+  dt.size = d->size;
+  dt.stem_count = d->stem_count;
+  dt.leaf_bytes_len = d->leaf_bytes_len;
+  dt.max_leaf_len = d->max_leaf_len;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t stem_bytes = std::max<size_t>(16, d->stem_count * sa);
+  const size_t arena_bytes = std::max<size_t>(16, d->leaf_bytes_len + 16);
+  const size_t ex_bytes = std::max<size_t>(16, ex.size() * 4);
+  cudaError_t e;
+  if ((e = cudaMalloc(&dt.stems, stem_bytes)) != cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&dt.arena), arena_bytes)) != cudaSuccess ||
+      (e = cudaMalloc(&dt.extents, ex_bytes)) != cudaSuccess) {
+    cudaFree(dt.stems);
+    cudaFree(dt.arena);
+    cudaFree(dt.extents);
+    delete t;
+    if (e == cudaErrorMemoryAllocation) return set_error(KGPU_ENOMEM, "device allocation failed");
+    return cuda_fail(e, "cudaMalloc");
+  }
+  dt.device_bytes = stem_bytes + arena_bytes + ex_bytes;
+  if (d->stem_count) e = cudaMemcpyAsync(dt.stems, d->stems, d->stem_count * sa, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && d->leaf_bytes_len)
+    e = cudaMemcpyAsync(dt.arena, d->leaf_bytes, d->leaf_bytes_len, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !ex.empty())
+    e = cudaMemcpyAsync(dt.extents, ex.data(), ex.size() * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // `ex` is a local
+  if (e != cudaSuccess) {
+    kgpu_tree_destroy(t);
+    return cuda_fail(e, "uploading the tree");
+  }
+  *out = t;
+  return KGPU_OK;
+}
+
+int32_t kgpu_tree_destroy(kgpu_tree* t) {
+  if (!t) return KGPU_OK;
+  cudaFree(t->dt.stems);
+  cudaFree(t->dt.arena);
+  cudaFree(t->dt.extents);
+  delete t;
+  return KGPU_OK;
+}
+
+int32_t kgpu_tree_info(const kgpu_tree* t, int64_t* info) {
+  if (!t || !info) return set_error(KGPU_EINVAL, "NULL argument");
+  const DeviceTree& d = t->dt;
+  info[0] = d.dtype;
+  info[1] = d.dims;
+  info[2] = int64_t(d.size);
+  info[3] = int64_t(d.leaf_count);
+  info[4] = d.max_stem_level;
+  info[5] = int64_t(d.stem_count);
+  info[6] = int64_t(d.leaf_bytes_len);
+  info[7] = int64_t(d.device_bytes);
+  return KGPU_OK;
+}
+
+}  // extern "C"
+
+namespace kgpu {
+namespace {
+
+int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_family) {
+  if (!t || !d) return set_error(KGPU_EINVAL, "NULL argument");
+  if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
+  if (d->metric != KGPU_SQUARED_EUCLIDEAN && d->metric != KGPU_MANHATTAN)
+    return set_error(KGPU_EINVAL, "unknown metric");
+  const int f = d->family;
+  if (radius_family) {
+    if (f != KGPU_WITHIN && f != KGPU_WITHIN_UNSORTED)
+      return set_error(KGPU_EINVAL, "family is not a radius family");
+  } else {
+    if (f != KGPU_NEAREST_ONE && f != KGPU_APPROX_NEAREST_ONE && f != KGPU_NEAREST_N &&
+        f != KGPU_NEAREST_N_WITHIN && f != KGPU_BEST_N_WITHIN)
+      return set_error(KGPU_EINVAL, "family is not a fixed-size family");
+    if (f == KGPU_NEAREST_N || f == KGPU_NEAREST_N_WITHIN || f == KGPU_BEST_N_WITHIN) {
+      if (d->max_qty == 0) return set_error(KGPU_EINVAL, "max_qty must be >= 1");
+      if (d->max_qty > uint32_t(kMaxK))
+        return set_error(KGPU_EUNSUPPORTED, "max_qty above 32 is not supported");
+    }
+  }
+  if (d->periodic_box) {
+    if (f == KGPU_BEST_N_WITHIN || f == KGPU_APPROX_NEAREST_ONE)
+      return set_error(KGPU_EINVAL, "periodic boundaries apply to nearest_one, nearest_n and within");
+    return set_error(KGPU_EUNSUPPORTED, "periodic boundary conditions are not enabled in this build");
+  }
+  return KGPU_OK;
+}
+
+template <typename A>
+cudaError_t run_fixed(const DeviceTree& dt, QueryLaunch& q) { return launch_fixed<A>(dt, q); }
+
+int out_width(const kgpu_query_desc* d) {
+  return (d->family == KGPU_NEAREST_ONE || d->family == KGPU_APPROX_NEAREST_ONE)
+             ? 1
+             : int(d->max_qty);
+}
+
+}  // namespace
+}  // namespace kgpu
+
+extern "C" {
+
+int32_t kgpu_query(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, uint64_t nq,
+                   void* out_dists, uint32_t* out_items, uint32_t* out_counts, void* stream) {
+  int st = check_query_desc(t, d, false);
+  if (st != KGPU_OK) return st;
+  if (nq == 0) return KGPU_OK;
+  if (!queries || !out_dists || !out_items) return set_error(KGPU_EINVAL, "NULL buffer");
+  const DeviceTree& dt = t->dt;
+  const size_t sa = dt.dtype == KGPU_F64 ? 8 : 4;
+  const int w = out_width(d);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  QueryLaunch q;
+  q.family = d->family;
+  q.metric = d->metric;
+  q.k = w;
+  q.radius = (d->family == KGPU_NEAREST_N) ? __builtin_inf() : d->radius;
+  q.exclusive = d->exclusive != 0;
+  q.sorted = d->sorted != 0;
+  q.nq = nq;
+  const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
+  DevBuf bq, bd, bi, bc;
+  cudaError_t e = cudaSuccess;
+  if (host) {
+    const size_t qbytes = nq * dt.dims * sa;
+    if ((e = bq.alloc(qbytes, s)) != cudaSuccess || (e = bd.alloc(nq * w * sa, s)) != cudaSuccess ||
+        (e = bi.alloc(nq * w * 4, s)) != cudaSuccess ||
+        (out_counts && (e = bc.alloc(nq * 4, s)) != cudaSuccess))
+      return e == cudaErrorMemoryAllocation ? set_error(KGPU_ENOMEM, "device allocation failed")
+                                            : cuda_fail(e, "cudaMallocAsync");
+    if ((e = cudaMemcpyAsync(bq.p, queries, qbytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_fail(e, "copying queries to the device");
+    q.queries = bq.p;
+    q.out_d = bd.p;
+    q.out_i = bi.as<uint32_t>();
+    q.out_c = out_counts ? bc.as<uint32_t>() : nullptr;
+  } else {
+    q.queries = queries;
+    q.out_d = out_dists;
+    q.out_i = out_items;
+    q.out_c = out_counts;
+  }
+  q.stream = s;
+  e = dt.dtype == KGPU_F64 ? run_fixed<double>(dt, q) : run_fixed<float>(dt, q);
+  if (e != cudaSuccess) return cuda_fail(e, "launching the query kernel");
+  if (host) {
+    if ((e = cudaMemcpyAsync(out_dists, bd.p, nq * w * sa, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(out_items, bi.p, nq * w * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (out_counts &&
+         (e = cudaMemcpyAsync(out_counts, bc.p, nq * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess))
+      return cuda_fail(e, "copying results to the host");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "query execution");
+  }
+  return KGPU_OK;
+}
+
+int32_t kgpu_query_radius_count(kgpu_tree* t, const kgpu_query_desc* d, const void* queries,
+                                uint64_t nq, uint64_t* offsets, void* stream) {
+  int st = check_query_desc(t, d, true);
+  if (st != KGPU_OK) return st;
+  if (!offsets) return set_error(KGPU_EINVAL, "offsets is NULL");
+  if (nq > 0 && !queries) return set_error(KGPU_EINVAL, "queries is NULL");
+  const DeviceTree& dt = t->dt;
+  const size_t sa = dt.dtype == KGPU_F64 ? 8 : 4;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
+  DevBuf bq, boff, btmp;
+  cudaError_t e;
+  QueryLaunch q;
+  q.family = d->family;
+  q.metric = d->metric;
+  q.radius = d->radius;
+  q.exclusive = d->exclusive != 0;
+  q.sorted = d->family == KGPU_WITHIN && d->sorted != 0;
+  q.nq = nq;
+  q.stream = s;
+  uint64_t* doff = offsets;
+  if (host) {
+    if ((e = bq.alloc(nq * dt.dims * sa, s)) != cudaSuccess ||
+        (e = boff.alloc((nq + 1) * 8, s)) != cudaSuccess)
+      return set_error(KGPU_ENOMEM, "device allocation failed");
+    if (nq && (e = cudaMemcpyAsync(bq.p, queries, nq * dt.dims * sa, cudaMemcpyHostToDevice, s)) !=
+                  cudaSuccess)
+      return cuda_fail(e, "copying queries to the device");
+    q.queries = bq.p;
+    doff = boff.as<uint64_t>();
+  } else {
+    q.queries = queries;
+  }
+  if ((e = btmp.alloc(scan_tmp_bytes(nq), s)) != cudaSuccess)
+    return set_error(KGPU_ENOMEM, "device allocation failed");
+  if (nq) {
+    e = dt.dtype == KGPU_F64 ? launch_within_count<double>(dt, q, doff)
+                             : launch_within_count<float>(dt, q, doff);
+    if (e != cudaSuccess) return cuda_fail(e, "launching the counting kernel");
+  }
+  e = launch_exclusive_scan(doff, doff, nq, btmp.p, s);
+  if (e != cudaSuccess) return cuda_fail(e, "launching the scan");
+  if (host) {
+    if ((e = cudaMemcpyAsync(offsets, doff, (nq + 1) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return cuda_fail(e, "copying offsets to the host");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "radius count");
+  }
+  return KGPU_OK;
+}
+
+int32_t kgpu_query_radius_fill(kgpu_tree* t, const kgpu_query_desc* d, const void* queries,
+                               uint64_t nq, const uint64_t* offsets, void* out_dists,
+                               uint32_t* out_items, void* stream) {
+  int st = check_query_desc(t, d, true);
+  if (st != KGPU_OK) return st;
+  if (!offsets) return set_error(KGPU_EINVAL, "offsets is NULL");
+  if (nq == 0) return KGPU_OK;
+  if (!queries) return set_error(KGPU_EINVAL, "queries is NULL");
+  const DeviceTree& dt = t->dt;
+  const size_t sa = dt.dtype == KGPU_F64 ? 8 : 4;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
+  const bool sorted = d->family == KGPU_WITHIN && d->sorted != 0;
+  uint64_t total = 0;
+  cudaError_t e;
+  if (host) {
+    total = offsets[nq];
+  } else {
+    if ((e = cudaMemcpyAsync(&total, offsets + nq, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+      return cuda_fail(e, "reading the hit total");
+  }
+  if (total == 0) return KGPU_OK;
+  if (!out_dists || !out_items) return set_error(KGPU_EINVAL, "NULL output buffer");
+  DevBuf bq, boff, bd, bi, sd, si;
+  QueryLaunch q;
+  q.family = d->family;
+  q.metric = d->metric;
+  q.radius = d->radius;
+  q.exclusive = d->exclusive != 0;
+  q.sorted = sorted;
+  q.nq = nq;
+  q.stream = s;
+  const uint64_t* doff = offsets;
+  if (host) {
+    if ((e = bq.alloc(nq * dt.dims * sa, s)) != cudaSuccess ||
+        (e = boff.alloc((nq + 1) * 8, s)) != cudaSuccess ||
+        (e = bd.alloc(total * sa, s)) != cudaSuccess || (e = bi.alloc(total * 4, s)) != cudaSuccess)
+      return set_error(KGPU_ENOMEM, "device allocation failed");
+    if ((e = cudaMemcpyAsync(bq.p, queries, nq * dt.dims * sa, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(boff.p, offsets, (nq + 1) * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_fail(e, "copying inputs to the device");
+    q.queries = bq.p;
+    doff = boff.as<uint64_t>();
+    q.out_d = bd.p;
+    q.out_i = bi.as<uint32_t>();
+  } else {
+    q.queries = queries;
+    q.out_d = out_dists;
+    q.out_i = out_items;
+  }
+  e = dt.dtype == KGPU_F64 ? launch_within_fill<double>(dt, q, doff)
+                           : launch_within_fill<float>(dt, q, doff);
+  if (e != cudaSuccess) return cuda_fail(e, "launching the fill kernel");
+  if (sorted) {
+    if ((e = sd.alloc(total * sa, s)) != cudaSuccess || (e = si.alloc(total * 4, s)) != cudaSuccess)
+      return set_error(KGPU_ENOMEM, "device allocation failed");
+    e = dt.dtype == KGPU_F64
+            ? launch_seg_sort<double>(doff, nq, static_cast<double*>(q.out_d), q.out_i,
+                                      sd.as<double>(), si.as<uint32_t>(), s)
+            : launch_seg_sort<float>(doff, nq, static_cast<float*>(q.out_d), q.out_i,
+                                     sd.as<float>(), si.as<uint32_t>(), s);
+    if (e != cudaSuccess) return cuda_fail(e, "launching the segmented sort");
+  }
+  if (host) {
+    if ((e = cudaMemcpyAsync(out_dists, q.out_d, total * sa, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(out_items, q.out_i, total * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return cuda_fail(e, "copying results to the host");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "radius fill");
+  }
+  return KGPU_OK;
+}
+
+int32_t kgpu_query_stats(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, uint64_t nq,
+                         uint64_t* stats, void* stream) {
+  if (!t || !d || !stats) return set_error(KGPU_EINVAL, "NULL argument");
+  const bool radius = d->family == KGPU_WITHIN || d->family == KGPU_WITHIN_UNSORTED;
+  int st = check_query_desc(t, d, radius);
+  if (st != KGPU_OK) return st;
+  stats[0] = stats[1] = stats[2] = 0;
+  if (nq == 0) return KGPU_OK;
+  if (!queries) return set_error(KGPU_EINVAL, "queries is NULL");
+  const DeviceTree& dt = t->dt;
+  const size_t sa = dt.dtype == KGPU_F64 ? 8 : 4;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
+  const int w = radius ? 1 : out_width(d);
+  DevBuf bq, bd, bi, bst;
+  cudaError_t e;
+  if ((e = bd.alloc(radius ? (nq + 1) * 8 : nq * w * sa, s)) != cudaSuccess ||
+      (e = bi.alloc(nq * w * 4, s)) != cudaSuccess || (e = bst.alloc(3 * 8, s)) != cudaSuccess)
+    return set_error(KGPU_ENOMEM, "device allocation failed");
+  const void* dq = queries;
+  if (host) {
+    if ((e = bq.alloc(nq * dt.dims * sa, s)) != cudaSuccess)
+      return set_error(KGPU_ENOMEM, "device allocation failed");
+    if ((e = cudaMemcpyAsync(bq.p, queries, nq * dt.dims * sa, cudaMemcpyHostToDevice, s)) !=
+        cudaSuccess)
+      return cuda_fail(e, "copying queries to the device");
+    dq = bq.p;
+  }
+  if ((e = cudaMemsetAsync(bst.p, 0, 24, s)) != cudaSuccess) return cuda_fail(e, "memset");
+  QueryLaunch q;
+  q.family = d->family;
+  q.metric = d->metric;
+  q.k = w;
+  q.radius = (d->family == KGPU_NEAREST_N) ? __builtin_inf() : d->radius;
+  q.exclusive = d->exclusive != 0;
+  q.sorted = d->sorted != 0;
+  q.nq = nq;
+  q.queries = dq;
+  q.out_d = bd.p;
+  q.out_i = bi.as<uint32_t>();
+  q.stats = bst.as<unsigned long long>();
+  q.stream = s;
+  if (radius)
+    e = dt.dtype == KGPU_F64 ? launch_within_count<double>(dt, q, bd.as<uint64_t>())
+                             : launch_within_count<float>(dt, q, bd.as<uint64_t>());
+  else
+    e = dt.dtype == KGPU_F64 ? run_fixed<double>(dt, q) : run_fixed<float>(dt, q);
+  if (e != cudaSuccess) return cuda_fail(e, "launching the query kernel");
+  if ((e = cudaMemcpyAsync(stats, bst.p, 24, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess)
+    return cuda_fail(e, "reading statistics");
+  return KGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,562 @@
+// kgpu_device.cuh — device building blocks of the query engine (sm_100a).
+//
+// One warp answers one query.  Every lane keeps an identical copy of the
+// query's scalar traversal state (stem index, level, per-axis offsets, rd,
+// the pending-far bitmask) so the descent needs no shuffles; the per-level
+// continuation records of kiddo's arithmetic traversal
+// (kd_tree/orchestrator/mod.rs:388-603: restore frame {old_off, has_far} and
+// far frame {stem, far_off, rd}) live in registers of the lane whose index is
+// the level ("per-lane register stacks").  The 32 lanes then scan a leaf's
+// points side by side: lane i reads point i of the VecOfArenas tile, so the
+// column loads of a 32-wide tile are one coalesced transaction per axis.
+//
+// All distance and rectangle-distance arithmetic uses the explicitly rounded
+// intrinsics (__fadd_rn/__fsub_rn/__fmul_rn and the double forms), in the
+// reference's order, so no multiply-add is ever contracted; the translation
+// unit is also compiled with -fmad=false.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kgpu {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// exactly rounded scalar helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float abs_val(float a) { return fabsf(a); }
+__device__ __forceinline__ double abs_val(double a) { return fabs(a); }
+
+template <typename A> __device__ __forceinline__ A inf_of();
+template <> __device__ __forceinline__ float inf_of<float>() { return __int_as_float(0x7f800000); }
+template <> __device__ __forceinline__ double inf_of<double>() {
+  return __longlong_as_double(0x7ff0000000000000ll);
+}
+
+__device__ __forceinline__ float shfl(float v, int src) { return __shfl_sync(FULL, v, src); }
+__device__ __forceinline__ double shfl(double v, int src) { return __shfl_sync(FULL, v, src); }
+__device__ __forceinline__ uint32_t shfl(uint32_t v, int src) { return __shfl_sync(FULL, v, src); }
+__device__ __forceinline__ float shfl_up(float v, int d) { return __shfl_up_sync(FULL, v, d); }
+__device__ __forceinline__ double shfl_up(double v, int d) { return __shfl_up_sync(FULL, v, d); }
+__device__ __forceinline__ uint32_t shfl_up(uint32_t v, int d) { return __shfl_up_sync(FULL, v, d); }
+
+// ---------------------------------------------------------------------------
+// Metrics (dist/distance_metric_core.rs:12-105)
+// ---------------------------------------------------------------------------
+struct SqEuclidean {
+  // dist1(a, b) = (a - b)^2   (dist/squared_euclidean/mod.rs:35-38)
+  template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
+    const A d = sub_rn(a, b);
+    return mul_rn(d, d);
+  }
+  // (rd - dist1(old, 0)) + dist1(new, 0)   (distance_metric_core.rs:86-96)
+  template <typename A> __device__ __forceinline__ static A rect(A rd, A old_off, A new_off) {
+    return add_rn(sub_rn(rd, mul_rn(old_off, old_off)), mul_rn(new_off, new_off));
+  }
+};
+
+struct Manhattan {
+  // |a - b|   (dist/manhattan/mod.rs:35-38)
+  template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
+    return abs_val(sub_rn(a, b));
+  }
+  // (rd - old) + new   (dist/manhattan/mod.rs:40-48)
+  template <typename A> __device__ __forceinline__ static A rect(A rd, A old_off, A new_off) {
+    return add_rn(sub_rn(rd, old_off), new_off);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Tree view and the VecOfArenas tile addressing (leaf_view/mod.rs:19-41, 491-505)
+// ---------------------------------------------------------------------------
+template <typename A>
+struct TreeView {
+  const A* __restrict__ stems;
+  const uint8_t* __restrict__ arena;
+  const uint2* __restrict__ extents;  // (byte offset / 8, len)
+  int max_stem_level;
+  uint32_t leaf_count;
+  uint64_t size;
+  uint64_t stem_count;
+};
+
+// Byte offset inside the leaf, tile width and index in tile of point p of a
+// leaf of `len` points laid out as tiles of 32, then 8, then 4, 2, 1.
+template <typename A, int K>
+__device__ __forceinline__ void tile_slot(uint32_t len, uint32_t p, uint32_t& off, uint32_t& w,
+                                          uint32_t& i) {
+  constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
+  const uint32_t n32 = len >> 5;
+  if (p < (n32 << 5)) {
+    w = 32; i = p & 31; off = (p >> 5) * (32 * per);
+    return;
+  }
+  uint32_t base = n32 * (32 * per);
+  const uint32_t r = len & 31;
+  uint32_t pp = p - (n32 << 5);
+  const uint32_t n8 = r >> 3;
+  if (pp < (n8 << 3)) {
+    w = 8; i = pp & 7; off = base + (pp >> 3) * (8 * per);
+    return;
+  }
+  base += n8 * (8 * per);
+  pp -= n8 << 3;
+  const uint32_t r7 = r & 7;
+  if (r7 & 4) {
+    if (pp < 4) { w = 4; i = pp; off = base; return; }
+    base += 4 * per; pp -= 4;
+  }
+  if (r7 & 2) {
+    if (pp < 2) { w = 2; i = pp; off = base; return; }
+    base += 2 * per; pp -= 2;
+  }
+  w = 1; i = 0; off = base;
+}
+
+template <typename A, int K>
+__device__ __forceinline__ void load_point(const uint8_t* __restrict__ leaf, uint32_t len,
+                                           uint32_t p, A (&c)[K], uint32_t& item) {
+  uint32_t off, w, i;
+  tile_slot<A, K>(len, p, off, w, i);
+  const A* col = reinterpret_cast<const A*>(leaf + off);
+#pragma unroll
+  for (int d = 0; d < K; ++d) c[d] = __ldg(col + d * w + i);
+  item = __ldg(reinterpret_cast<const uint32_t*>(leaf + off + K * w * sizeof(A)) + i);
+}
+
+// acc = ((0 + dist1(c0, q0)) + dist1(c1, q1)) + ...   (combine_component order)
+template <typename M, typename A, int K>
+__device__ __forceinline__ A point_dist(const A (&c)[K], const A (&q)[K]) {
+  A acc = A(0);
+#pragma unroll
+  for (int d = 0; d < K; ++d) acc = add_rn(acc, M::template dist1<A>(c[d], q[d]));
+  return acc;
+}
+
+template <typename A, int K>
+__device__ __forceinline__ A sel(const A (&v)[K], int d) {
+  A r = v[0];
+#pragma unroll
+  for (int j = 1; j < K; ++j)
+    if (d == j) r = v[j];
+  return r;
+}
+template <typename A, int K>
+__device__ __forceinline__ void put(A (&v)[K], int d, A x) {
+#pragma unroll
+  for (int j = 0; j < K; ++j)
+    if (d == j) v[j] = x;
+}
+
+// ---------------------------------------------------------------------------
+// The arithmetic traversal, one warp per query.
+// Policy interface:
+//   A max_dist() const;                       QueryContext::max_dist
+//   static constexpr bool kPruneOnEqual;      QueryContext::prune_on_equal_max_dist
+//   bool unbounded_start() const;             QueryContext::initial_bound_is_unbounded
+//   uint32_t leaf(const TreeView<A>&, uint32_t leaf_idx, const A (&q)[K], int lane);
+//     scans one leaf and returns its length.
+// ---------------------------------------------------------------------------
+// Per-query traversal counters (the counters of test_utils/exact_query_stats.rs:23-60):
+// stem visits, leaf visits, points scanned.
+struct TravStats {
+  uint32_t stems = 0, leaves = 0, points = 0;
+};
+
+template <typename A, int K, typename M, typename P>
+__device__ __forceinline__ void warp_arith_query(const TreeView<A>& tv, const A (&q)[K], P& pol,
+                                                 int lane, TravStats& st) {
+  if (tv.size == 0) return;
+  const A INF = inf_of<A>();
+  const int msl = tv.max_stem_level;
+  A off[K];
+#pragma unroll
+  for (int d = 0; d < K; ++d) off[d] = A(0);
+  uint32_t stem_idx = 1;
+  int level = 0;
+  int dim = 0;
+  A rd = A(0);
+  uint32_t has_far = 0;             // bit L: a far frame is pending for level L
+  A s_old = A(0), s_far = A(0), s_rd = A(0);  // this lane's level-`lane` records
+
+  // arithmetic_descend_to_leaf (orchestrator/mod.rs:520-603)
+  auto descend = [&](bool check_bound) -> uint32_t {
+    while (level <= msl) {
+      ++st.stems;
+      const A pivot = __ldg(tv.stems + stem_idx);
+      const A oo = sel(off, dim);
+      const uint32_t bit = 1u << level;
+      if (pivot < INF) {
+        const A qd = sel(q, dim);
+        const bool is_right = qd >= pivot;
+        const A new_off = abs_val(sub_rn(qd, pivot));
+        const A rd_far = M::template rect<A>(rd, oo, new_off);
+        const bool cand = !check_bound || !(rd_far > pol.max_dist());
+        if (lane == level) { s_old = oo; s_far = new_off; s_rd = rd_far; }
+        has_far = cand ? (has_far | bit) : (has_far & ~bit);
+        stem_idx = stem_idx * 2u + (is_right ? 1u : 0u);
+      } else {
+        if (lane == level) s_old = oo;
+        has_far &= ~bit;
+        stem_idx = stem_idx * 2u;
+      }
+      ++level;
+      dim = (dim + 1 == K) ? 0 : dim + 1;
+    }
+    return stem_idx & ~(1u << level);  // Eytzinger leaf_idx (eytzinger/mod.rs:115-118)
+  };
+
+  st.points += pol.leaf(tv, descend(!pol.unbounded_start()), q, lane);
+  ++st.leaves;
+
+  // continuation loop (orchestrator/mod.rs:450-515)
+  int cur = level;  // stem_idx is the path node at level `cur`
+  for (;;) {
+    bool resumed = false;
+    while (cur > 0) {
+      const int L = cur - 1;
+      const int d = dim == 0 ? K - 1 : dim - 1;
+      dim = d;
+      const A old = shfl(s_old, L);
+      put(off, d, old);
+      const uint32_t bit = 1u << L;
+      if (has_far & bit) {
+        has_far &= ~bit;
+        const A frd = shfl(s_rd, L);
+        const A md = pol.max_dist();
+        const bool prune = frd > md || (P::kPruneOnEqual && frd == md);
+        if (!prune) {
+          put(off, d, shfl(s_far, L));
+          rd = frd;
+          stem_idx ^= 1u;  // the sibling at level L + 1
+          level = cur;
+          dim = d + 1 == K ? 0 : d + 1;
+          st.points += pol.leaf(tv, descend(true), q, lane);
+          ++st.leaves;
+          cur = level;
+          resumed = true;
+          break;
+        }
+      }
+      stem_idx >>= 1;
+      cur = L;
+    }
+    if (!resumed) break;
+  }
+}
+
+// Straight descent for approx (traits/stem_strategy.rs:182-200).
+template <typename A, int K>
+__device__ __forceinline__ uint32_t straight_leaf(const TreeView<A>& tv, const A (&q)[K]) {
+  uint32_t stem_idx = 1;
+  int level = 0, dim = 0;
+  while (level <= tv.max_stem_level) {
+    const A pivot = __ldg(tv.stems + stem_idx);
+    stem_idx = stem_idx * 2u + (sel(q, dim) >= pivot ? 1u : 0u);
+    ++level;
+    dim = dim + 1 == K ? 0 : dim + 1;
+  }
+  return stem_idx & ~(1u << level);
+}
+
+// ---------------------------------------------------------------------------
+// Leaf scans
+// ---------------------------------------------------------------------------
+
+// nearest_one leaf kernel (leaf_view_chunked/nearest_one/fallback.rs:69-104):
+// sequential `if dist < best` over tile order == first minimum of the leaf
+// when it beats the incoming best.  Lanes take points lane, lane+32, ...
+template <typename A, int K, typename M>
+__device__ __forceinline__ uint32_t scan_nearest_one(const TreeView<A>& tv, uint32_t leaf,
+                                                 const A (&q)[K], int lane, A& best,
+                                                 uint32_t& best_item) {
+  const uint2 ex = __ldg(tv.extents + leaf);
+  const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+  const uint32_t len = ex.y;
+  const A INF = inf_of<A>();
+  for (uint32_t b = 0; b < len; b += 32) {
+    const uint32_t p = b + lane;
+    A dd = INF;
+    uint32_t it = 0;
+    if (p < len) {
+      A c[K];
+      load_point<A, K>(base, len, p, c, it);
+      dd = point_dist<M, A, K>(c, q);
+    }
+    A m = dd;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const A other = __shfl_xor_sync(FULL, m, o);
+      m = other < m ? other : m;
+    }
+    if (m < best) {
+      const uint32_t hit = __ballot_sync(FULL, p < len && dd == m);
+      const int src = __ffs(hit) - 1;
+      best = m;
+      best_item = shfl(it, src);
+    }
+  }
+  return len;
+}
+
+// NearestOne policy (kd_tree/query/nearest_one.rs:321-352)
+template <typename A, int K, typename M>
+struct NearestOnePolicy {
+  static constexpr bool kPruneOnEqual = true;
+  A best;
+  uint32_t item;
+  __device__ NearestOnePolicy() : best(inf_of<A>()), item(0) {}
+  __device__ __forceinline__ A max_dist() const { return best; }
+  __device__ __forceinline__ bool unbounded_start() const { return true; }
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
+                                           int lane) {
+    return scan_nearest_one<A, K, M>(tv, l, q, lane, best, item);
+  }
+};
+
+// Top-k list in lanes 0..k-1 sorted by (distance, arrival): the
+// ThresholdVecResultCollection of result_collection.rs:136-215 with a stable
+// fill sort.  Pruning bound = min(k-th distance once full, radius)
+// (nearest_n_within.rs:461-468); leaf filter `<=` or `<` against the bound at
+// leaf entry (leaf_view_chunked/nearest_n_within/fallback.rs:37-95).
+template <typename A, int K, typename M, bool kExclusive>
+struct NearestNPolicy {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A ld;           // lane j: j-th distance
+  uint32_t li;    // lane j: j-th item
+  uint32_t lseq;  // lane j: arrival number of the j-th entry
+  int n;          // entries held (uniform)
+  int k;
+  A radius;
+  A kth;          // ld of lane k-1 once full (uniform)
+  uint32_t seq;   // arrivals so far (uniform)
+  __device__ NearestNPolicy(int k_, A r)
+      : ld(inf_of<A>()), li(0xffffffffu), lseq(0), n(0), k(k_), radius(r), kth(inf_of<A>()),
+        seq(0) {}
+  __device__ __forceinline__ A max_dist() const {
+    return (n == k && kth < radius) ? kth : radius;
+  }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+
+  __device__ __forceinline__ void insert(A cd, uint32_t ci, int lane) {
+    const uint32_t le = __ballot_sync(FULL, lane < n && !(ld > cd));
+    const int pos = __popc(le);
+    const A up_d = shfl_up(ld, 1);
+    const uint32_t up_i = shfl_up(li, 1);
+    const uint32_t up_s = shfl_up(lseq, 1);
+    if (lane > pos) { ld = up_d; li = up_i; lseq = up_s; }
+    if (lane == pos) { ld = cd; li = ci; lseq = seq; }
+    ++seq;
+    if (n < k) ++n;
+    kth = shfl(ld, k - 1);
+  }
+
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
+                                           int lane) {
+    const uint2 ex = __ldg(tv.extents + l);
+    const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+    const uint32_t len = ex.y;
+    const A bound = max_dist();
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t p = b + lane;
+      A dd = inf_of<A>();
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < len) {
+        A c[K];
+        load_point<A, K>(base, len, p, c, it);
+        dd = point_dist<M, A, K>(c, q);
+        pass = kExclusive ? (dd < bound) : (dd <= bound);
+      }
+      uint32_t mask = __ballot_sync(FULL, pass);
+      if (n == k) mask &= __ballot_sync(FULL, dd < kth);
+      while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const A cd = shfl(dd, src);
+        const uint32_t ci = shfl(it, src);
+        insert(cd, ci, lane);
+        if (n == k) mask &= __ballot_sync(FULL, dd < kth);
+      }
+    }
+    return len;
+  }
+
+  // Sorted output; `arrival_order` reproduces ThresholdVec::into_vec when the
+  // list never filled (arrival order), otherwise the sorted list.
+  __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
+                                        uint32_t* __restrict__ out_i,
+                                        uint32_t* __restrict__ out_c, bool arrival_order,
+                                        int lane) const {
+    int slot = lane;
+    if (arrival_order && n < k) {
+      // rank of this entry by arrival among the n held entries
+      int rank = 0;
+      for (int j = 0; j < n; ++j) {
+        const uint32_t sj = shfl(lseq, j);
+        rank += (sj < lseq) ? 1 : 0;
+      }
+      slot = rank;
+    }
+    if (lane < k) {
+      const bool valid = lane < n;
+      const size_t o = size_t(qi) * k + (valid ? slot : lane);
+      out_d[o] = valid ? ld : inf_of<A>();
+      out_i[o] = valid ? li : 0xffffffffu;
+    }
+    if (lane == 0 && out_c) out_c[qi] = uint32_t(n);
+  }
+};
+
+// best_n_within: n smallest items among hits, ties by arrival
+// (kd_tree/query/best_n_within.rs:88-196, ctx :281-306; leaf filter
+// leaf_view_chunked/best_n_within/fallback.rs:40-104; heap replace-if-smaller
+// result_collection.rs:481-501; order by item best_query_result_item.rs:27-31).
+template <typename A, int K, typename M, bool kExclusive>
+struct BestNPolicy {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A ld;
+  uint32_t li;
+  int n;
+  int k;
+  A radius;
+  __device__ BestNPolicy(int k_, A r) : ld(inf_of<A>()), li(0xffffffffu), n(0), k(k_), radius(r) {}
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return false; }
+
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
+                                           int lane) {
+    const uint2 ex = __ldg(tv.extents + l);
+    const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+    const uint32_t len = ex.y;
+    const bool full_at_entry = n == k;
+    const uint32_t thr_item = shfl(li, k - 1);
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t p = b + lane;
+      A dd = inf_of<A>();
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < len) {
+        A c[K];
+        load_point<A, K>(base, len, p, c, it);
+        dd = point_dist<M, A, K>(c, q);
+        pass = kExclusive ? (dd < radius) : (dd <= radius);
+        if (full_at_entry && it >= thr_item) pass = false;
+      }
+      uint32_t mask = __ballot_sync(FULL, pass);
+      while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const A cd = shfl(dd, src);
+        const uint32_t ci = shfl(it, src);
+        if (n == k) {
+          const uint32_t last = shfl(li, k - 1);
+          if (!(ci < last)) continue;
+        }
+        const uint32_t le = __ballot_sync(FULL, lane < n && li <= ci);
+        const int pos = __popc(le);
+        const A up_d = shfl_up(ld, 1);
+        const uint32_t up_i = shfl_up(li, 1);
+        if (lane > pos) { ld = up_d; li = up_i; }
+        if (lane == pos) { ld = cd; li = ci; }
+        if (n < k) ++n;
+      }
+    }
+    return len;
+  }
+
+  __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
+                                        uint32_t* __restrict__ out_i,
+                                        uint32_t* __restrict__ out_c, int lane) const {
+    if (lane < k) {
+      const bool valid = lane < n;
+      const size_t o = size_t(qi) * k + lane;
+      out_d[o] = valid ? ld : inf_of<A>();
+      out_i[o] = valid ? li : 0xffffffffu;
+    }
+    if (lane == 0 && out_c) out_c[qi] = uint32_t(n);
+  }
+};
+
+// within / within().unsorted(): constant bound r (within.rs:18-41,
+// within_unsorted.rs:133-157); counting pass and filling pass.
+template <typename A, int K, typename M, bool kExclusive>
+struct WithinCountPolicy {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A radius;
+  uint64_t count;
+  __device__ WithinCountPolicy(A r) : radius(r), count(0) {}
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
+                                           int lane) {
+    const uint2 ex = __ldg(tv.extents + l);
+    const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+    const uint32_t len = ex.y;
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t p = b + lane;
+      bool pass = false;
+      if (p < len) {
+        A c[K];
+        uint32_t it;
+        load_point<A, K>(base, len, p, c, it);
+        const A dd = point_dist<M, A, K>(c, q);
+        pass = kExclusive ? (dd < radius) : (dd <= radius);
+      }
+      count += __popc(__ballot_sync(FULL, pass));
+    }
+    return len;
+  }
+};
+
+template <typename A, int K, typename M, bool kExclusive>
+struct WithinFillPolicy {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A radius;
+  uint64_t count;
+  uint64_t cap;  // the segment length the counting pass produced
+  A* __restrict__ out_d;
+  uint32_t* __restrict__ out_i;
+  __device__ WithinFillPolicy(A r, uint64_t c, A* d, uint32_t* i)
+      : radius(r), count(0), cap(c), out_d(d), out_i(i) {}
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
+                                           int lane) {
+    const uint2 ex = __ldg(tv.extents + l);
+    const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+    const uint32_t len = ex.y;
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t p = b + lane;
+      bool pass = false;
+      A dd = A(0);
+      uint32_t it = 0;
+      if (p < len) {
+        A c[K];
+        load_point<A, K>(base, len, p, c, it);
+        dd = point_dist<M, A, K>(c, q);
+        pass = kExclusive ? (dd < radius) : (dd <= radius);
+      }
+      const uint32_t m = __ballot_sync(FULL, pass);
+      if (pass) {
+        const uint64_t o = count + __popc(m & ((1u << lane) - 1u));
+        if (o < cap) {  // the same traversal as the counting pass: never false
+          out_d[o] = dd;
+          out_i[o] = it;
+        }
+      }
+      count += __popc(m);
+    }
+    return len;
+  }
+};
+
+}  // namespace kgpu

@@ -1,0 +1,38 @@
+// kgpu_internal.h — host-side internals shared by the library's translation units.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/kiddo_gpu.h"
+
+namespace kgpu {
+
+constexpr int kMaxDims = 4;
+constexpr int kMaxK = 32;          // largest max_qty served by the register top-k lists
+constexpr int kMaxStemLevel = 30;  // 31 levels: one continuation slot per lane, u32 stem index
+
+// Host copy of a tree layout as the reference stores it.
+struct Layout {
+  int dtype = 0;
+  int dims = 0;
+  uint64_t size = 0;
+  int32_t max_stem_level = -1;
+  uint64_t max_leaf_len = 0;
+  std::vector<uint8_t> stems_bytes;  // stem_count * sizeof(A)
+  std::vector<uint8_t> leaf_bytes;
+  std::vector<uint64_t> extents;     // (offset, len) pairs
+};
+
+// Records `msg` as the calling thread's last error and returns `status`.
+int set_error(int status, const std::string& msg);
+
+int build_layout_any(Layout& L, int dtype, int K, const void* pts, const uint32_t* items,
+                     uint64_t n, int nthreads);
+
+}  // namespace kgpu
+
+struct kgpu_layout {
+  kgpu::Layout L;
+};

@@ -1,0 +1,274 @@
+// kgpu_kernels.cuh — kernels of the query engine and their launchers.
+// Instantiated per coordinate type in kernels_f32.cu / kernels_f64.cu.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kgpu_device.cuh"
+#include "kgpu_launch.h"
+
+namespace kgpu {
+
+__device__ __forceinline__ void add_stats(unsigned long long* stats, const TravStats& st) {
+  atomicAdd(stats + 0, (unsigned long long)st.stems);
+  atomicAdd(stats + 1, (unsigned long long)st.leaves);
+  atomicAdd(stats + 2, (unsigned long long)st.points);
+}
+
+enum KernelFamily : int {
+  KF_NEAREST_ONE = 0,
+  KF_APPROX = 1,
+  KF_NEAREST_N = 2,
+  KF_BEST_N = 3,
+};
+
+// ---------------------------------------------------------------------------
+// Fixed-size families: one warp per query, warps stride over the batch.
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M, int FAM, bool EXCL>
+__global__ void __launch_bounds__(256) k_fixed(TreeView<A> tv, const A* __restrict__ Q,
+                                               const uint32_t* __restrict__ order, uint64_t nq,
+                                               int k, A radius, int arrival_order,
+                                               A* __restrict__ out_d, uint32_t* __restrict__ out_i,
+                                               uint32_t* __restrict__ out_c,
+                                               unsigned long long* __restrict__ stats) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t w = warp; w < nq; w += nwarps) {
+    const uint64_t qi = order ? order[w] : w;
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    TravStats st;
+    if constexpr (FAM == KF_NEAREST_ONE) {
+      NearestOnePolicy<A, K, M> pol;
+      warp_arith_query<A, K, M>(tv, q, pol, lane, st);
+      if (lane == 0) {
+        out_d[qi] = pol.best;
+        out_i[qi] = pol.item;
+        if (out_c) out_c[qi] = 1;
+      }
+    } else if constexpr (FAM == KF_APPROX) {
+      A best = inf_of<A>();
+      uint32_t item = 0;
+      if (tv.leaf_count > 0) {
+        st.points = scan_nearest_one<A, K, M>(tv, straight_leaf<A, K>(tv, q), q, lane, best, item);
+        st.stems = uint32_t(tv.max_stem_level + 1);
+        st.leaves = 1;
+      }
+      if (lane == 0) {
+        out_d[qi] = best;
+        out_i[qi] = item;
+        if (out_c) out_c[qi] = 1;
+      }
+    } else if constexpr (FAM == KF_NEAREST_N) {
+      NearestNPolicy<A, K, M, EXCL> pol(k, radius);
+      warp_arith_query<A, K, M>(tv, q, pol, lane, st);
+      pol.write(qi, out_d, out_i, out_c, arrival_order != 0, lane);
+    } else {
+      BestNPolicy<A, K, M, EXCL> pol(k, radius);
+      warp_arith_query<A, K, M>(tv, q, pol, lane, st);
+      pol.write(qi, out_d, out_i, out_c, lane);
+    }
+    if (stats && lane == 0) add_stats(stats, st);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Radius families: count pass, exclusive scan, fill pass, segmented sort.
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_within_count(TreeView<A> tv, const A* __restrict__ Q,
+                                                      const uint32_t* __restrict__ order,
+                                                      uint64_t nq, A radius,
+                                                      uint64_t* __restrict__ counts,
+                                                      unsigned long long* __restrict__ stats) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t w = warp; w < nq; w += nwarps) {
+    const uint64_t qi = order ? order[w] : w;
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    WithinCountPolicy<A, K, M, EXCL> pol(radius);
+    TravStats st;
+    warp_arith_query<A, K, M>(tv, q, pol, lane, st);
+    if (lane == 0) counts[qi] = pol.count;
+    if (stats && lane == 0) add_stats(stats, st);
+  }
+}
+
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_within_fill(TreeView<A> tv, const A* __restrict__ Q,
+                                                     const uint32_t* __restrict__ order,
+                                                     uint64_t nq, A radius,
+                                                     const uint64_t* __restrict__ offsets,
+                                                     A* __restrict__ out_d,
+                                                     uint32_t* __restrict__ out_i) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t w = warp; w < nq; w += nwarps) {
+    const uint64_t qi = order ? order[w] : w;
+    const uint64_t o = offsets[qi];
+    const uint64_t cap = offsets[qi + 1] - o;
+    if (cap == 0) continue;  // nothing to write
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    WithinFillPolicy<A, K, M, EXCL> pol(radius, cap, out_d + o, out_i + o);
+    TravStats st;
+    warp_arith_query<A, K, M>(tv, q, pol, lane, st);
+  }
+}
+
+// Segments of at most 32 hits: one warp, bitonic network on (distance, position)
+// so equal distances keep traversal order (a stable sort, as Vec::sort).
+template <typename A>
+__device__ __forceinline__ bool key_less(A da, uint32_t pa, A db, uint32_t pb) {
+  return da < db || (da == db && pa < pb);
+}
+
+template <typename A>
+__global__ void __launch_bounds__(256) k_seg_sort_warp(const uint64_t* __restrict__ offsets,
+                                                       uint64_t nq, A* __restrict__ d,
+                                                       uint32_t* __restrict__ it) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t s = warp; s < nq; s += nwarps) {
+    const uint64_t o = offsets[s];
+    const uint64_t n = offsets[s + 1] - o;
+    if (n <= 1 || n > 32) continue;
+    A kd = inf_of<A>();
+    uint32_t kp = 0xffffffffu, kv = 0;
+    if (lane < n) { kd = d[o + lane]; kv = it[o + lane]; kp = lane; }
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const A od = __shfl_xor_sync(FULL, kd, stride);
+        const uint32_t op = __shfl_xor_sync(FULL, kp, stride);
+        const uint32_t ov = __shfl_xor_sync(FULL, kv, stride);
+        const bool up = ((lane & size) == 0);
+        const bool lower = (lane & stride) == 0;
+        // lower lane keeps the min when ascending
+        const bool other_less = key_less(od, op, kd, kp);
+        const bool take = lower ? (up ? other_less : !other_less) : (up ? !other_less : other_less);
+        if (take && !(od == kd && op == kp)) { kd = od; kp = op; kv = ov; }
+      }
+    }
+    if (lane < n) { d[o + lane] = kd; it[o + lane] = kv; }
+  }
+}
+
+// Stable merge step (merge path): out[lo..hi) from runs a[0..na) and b[0..nb),
+// ties taken from `a` first.
+template <typename A>
+__device__ __forceinline__ void merge_range(const A* ad, const uint32_t* ai, uint32_t na,
+                                            const A* bd, const uint32_t* bi, uint32_t nb,
+                                            A* od, uint32_t* oi, uint32_t lo, uint32_t hi) {
+  if (lo >= hi) return;
+  uint32_t l = lo > nb ? lo - nb : 0, h = lo < na ? lo : na;
+  while (l < h) {
+    const uint32_t mid = (l + h) >> 1;
+    if (!(bd[lo - mid - 1] < ad[mid])) l = mid + 1;  // ad[mid] <= bd[...]: a first
+    else h = mid;
+  }
+  uint32_t x = l, y = lo - l;
+  for (uint32_t o = lo; o < hi; ++o) {
+    bool take_a = x < na && (y >= nb || !(bd[y] < ad[x]));
+    if (take_a) { od[o] = ad[x]; oi[o] = ai[x]; ++x; }
+    else { od[o] = bd[y]; oi[o] = bi[y]; ++y; }
+  }
+}
+
+// Bottom-up stable merge sort of one segment by the whole block, ping-ponging
+// between (d0, i0) and (d1, i1).  Returns true if the result ended in (d1, i1).
+template <typename A>
+__device__ bool block_merge_sort(A* d0, uint32_t* i0, A* d1, uint32_t* i1, uint32_t n) {
+  bool in1 = false;
+  for (uint32_t width = 1; width < n; width <<= 1) {
+    A* sd = in1 ? d1 : d0;
+    uint32_t* si = in1 ? i1 : i0;
+    A* td = in1 ? d0 : d1;
+    uint32_t* ti = in1 ? i0 : i1;
+    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t lo = threadIdx.x * per;
+    const uint32_t hi = min(n, lo + per);
+    // each thread's output range may span several run pairs
+    uint32_t o = lo;
+    while (o < hi) {
+      const uint32_t pair = o / (2 * width);
+      const uint32_t start = pair * 2 * width;
+      const uint32_t mid = min(n, start + width);
+      const uint32_t end = min(n, start + 2 * width);
+      const uint32_t stop = min(hi, end);
+      merge_range<A>(sd + start, si + start, mid - start, sd + mid, si + mid, end - mid,
+                     td + start, ti + start, o - start, stop - start);
+      o = stop;
+    }
+    __syncthreads();
+    in1 = !in1;
+  }
+  return in1;
+}
+
+// Segments longer than 32: one block per group of 256 segments; each long
+// segment is sorted by the whole block in shared memory when it fits, else in
+// global memory with `scratch` as the second buffer.
+template <typename A>
+__global__ void __launch_bounds__(256) k_seg_sort_block(const uint64_t* __restrict__ offsets,
+                                                        uint64_t nq, A* __restrict__ d,
+                                                        uint32_t* __restrict__ it,
+                                                        A* __restrict__ scratch_d,
+                                                        uint32_t* __restrict__ scratch_i,
+                                                        uint32_t smem_cap) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t list[256];
+  __shared__ uint32_t list_n;
+  const uint64_t first = uint64_t(blockIdx.x) * 256;
+  if (threadIdx.x == 0) list_n = 0;
+  __syncthreads();
+  {
+    const uint64_t s = first + threadIdx.x;
+    if (s < nq) {
+      const uint64_t n = offsets[s + 1] - offsets[s];
+      if (n > 32) list[atomicAdd(&list_n, 1u)] = uint32_t(threadIdx.x);
+    }
+  }
+  __syncthreads();
+  const uint32_t cnt = list_n;
+  A* sd0 = reinterpret_cast<A*>(smem_raw);
+  A* sd1 = sd0 + smem_cap;
+  uint32_t* si0 = reinterpret_cast<uint32_t*>(sd1 + smem_cap);
+  uint32_t* si1 = si0 + smem_cap;
+  for (uint32_t j = 0; j < cnt; ++j) {
+    const uint64_t s = first + list[j];
+    const uint64_t o = offsets[s];
+    const uint32_t n = uint32_t(offsets[s + 1] - o);
+    if (n <= smem_cap) {
+      for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) { sd0[x] = d[o + x]; si0[x] = it[o + x]; }
+      __syncthreads();
+      const bool in1 = block_merge_sort<A>(sd0, si0, sd1, si1, n);
+      const A* rd = in1 ? sd1 : sd0;
+      const uint32_t* ri = in1 ? si1 : si0;
+      for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) { d[o + x] = rd[x]; it[o + x] = ri[x]; }
+      __syncthreads();
+    } else {
+      const bool in1 = block_merge_sort<A>(d + o, it + o, scratch_d + o, scratch_i + o, n);
+      if (in1) {
+        for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) {
+          d[o + x] = scratch_d[o + x];
+          it[o + x] = scratch_i[o + x];
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace kgpu

@@ -1,0 +1,64 @@
+// kgpu_launch.h — host-side launch interface between the API and the kernels.
+#pragma once
+
+#include <atomic>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kgpu {
+
+struct DeviceTree {
+  int dtype = 0;
+  int dims = 0;
+  int device = 0;
+  void* stems = nullptr;       // A[stem_count]
+  uint8_t* arena = nullptr;    // leaf bytes
+  void* extents = nullptr;     // uint2 (offset/8, len) [leaf_count]
+  int max_stem_level = -1;
+  uint32_t leaf_count = 0;
+  uint64_t size = 0;
+  uint64_t stem_count = 0;
+  uint64_t leaf_bytes_len = 0;
+  uint64_t max_leaf_len = 0;
+  size_t device_bytes = 0;
+};
+
+struct QueryLaunch {
+  int family = 0;     // kgpu_family
+  int metric = 0;     // kgpu_metric
+  int k = 1;
+  double radius = 0;
+  bool exclusive = false;
+  bool sorted = true;
+  const void* queries = nullptr;  // device, nq * dims values of A
+  const uint32_t* order = nullptr;  // optional processing order (device)
+  uint64_t nq = 0;
+  void* out_d = nullptr;
+  uint32_t* out_i = nullptr;
+  uint32_t* out_c = nullptr;
+  unsigned long long* stats = nullptr;  // optional [stems, leaves, points] totals
+  cudaStream_t stream = nullptr;
+};
+
+// process-wide count of kernel launches made by this library
+extern std::atomic<uint64_t> g_launches;
+
+template <typename A> cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q);
+template <typename A> cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q,
+                                                       uint64_t* counts);
+template <typename A> cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
+                                                      const uint64_t* offsets);
+// Stable sort of every CSR segment by distance; scratch holds total entries.
+template <typename A> cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d,
+                                                  uint32_t* it, A* scratch_d,
+                                                  uint32_t* scratch_i, cudaStream_t s);
+
+// offsets[0..n] = exclusive prefix sum of counts[0..n) (offsets[n] = total).
+// `counts` and `offsets` may alias.  tmp needs scan_tmp_bytes(n) bytes.
+size_t scan_tmp_bytes(uint64_t n);
+cudaError_t launch_exclusive_scan(const uint64_t* counts, uint64_t* offsets, uint64_t n,
+                                  void* tmp, cudaStream_t s);
+
+int sm_count();
+
+}  // namespace kgpu

@@ -1,0 +1,171 @@
+// kgpu_launch_impl.cuh — dispatch from runtime options to kernel instantiations.
+#pragma once
+
+#include <type_traits>
+
+#include "../../include/kiddo_gpu.h"
+#include "kgpu_kernels.cuh"
+#include "kgpu_launch.h"
+
+namespace kgpu {
+
+template <typename A>
+inline TreeView<A> make_view(const DeviceTree& t) {
+  TreeView<A> v;
+  v.stems = static_cast<const A*>(t.stems);
+  v.arena = t.arena;
+  v.extents = static_cast<const uint2*>(t.extents);
+  v.max_stem_level = t.max_stem_level;
+  v.leaf_count = t.leaf_count;
+  v.size = t.size;
+  v.stem_count = t.stem_count;
+  return v;
+}
+
+// Persistent grid: as many 256-thread blocks as fit on all SMs at once.
+template <typename Kern>
+inline int grid_for(Kern kern, size_t smem, uint64_t work_warps) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const uint64_t full = uint64_t(per_sm) * sm_count();
+  const uint64_t need = (work_warps + 7) / 8;
+  return int(need < full ? (need > 0 ? need : 1) : full);
+}
+
+template <typename F>
+inline cudaError_t with_dims(int dims, F&& f) {
+  switch (dims) {
+    case 1: return f(std::integral_constant<int, 1>());
+    case 2: return f(std::integral_constant<int, 2>());
+    case 3: return f(std::integral_constant<int, 3>());
+    case 4: return f(std::integral_constant<int, 4>());
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename F>
+inline cudaError_t with_metric(int metric, F&& f) {
+  if (metric == KGPU_MANHATTAN) return f(Manhattan());
+  return f(SqEuclidean());
+}
+
+template <typename F>
+inline cudaError_t with_excl(bool e, F&& f) {
+  if (e) return f(std::true_type());
+  return f(std::false_type());
+}
+
+template <typename A>
+cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
+  const TreeView<A> tv = make_view<A>(t);
+  const A radius = A(q.radius);
+  return with_dims(t.dims, [&](auto kk) {
+    constexpr int K = decltype(kk)::value;
+    return with_metric(q.metric, [&](auto m) {
+      using M = decltype(m);
+      return with_excl(q.exclusive, [&](auto ex) {
+        constexpr bool EX = decltype(ex)::value;
+        auto run = [&](auto kern) {
+          const int grid = grid_for(kern, 0, q.nq);
+          kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                           q.k, radius, q.sorted ? 0 : 1,
+                                           static_cast<A*>(q.out_d), q.out_i, q.out_c, q.stats);
+          g_launches++;
+          return cudaGetLastError();
+        };
+        switch (q.family) {
+          case KGPU_NEAREST_ONE:
+            return run(k_fixed<A, K, M, KF_NEAREST_ONE, false>);
+          case KGPU_APPROX_NEAREST_ONE:
+            return run(k_fixed<A, K, M, KF_APPROX, false>);
+          case KGPU_NEAREST_N:
+          case KGPU_NEAREST_N_WITHIN:
+            return run(k_fixed<A, K, M, KF_NEAREST_N, EX>);
+          case KGPU_BEST_N_WITHIN:
+            return run(k_fixed<A, K, M, KF_BEST_N, EX>);
+        }
+        return cudaErrorInvalidValue;
+      });
+    });
+  });
+}
+
+template <typename A>
+cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts) {
+  const TreeView<A> tv = make_view<A>(t);
+  const A radius = A(q.radius);
+  return with_dims(t.dims, [&](auto kk) {
+    constexpr int K = decltype(kk)::value;
+    return with_metric(q.metric, [&](auto m) {
+      using M = decltype(m);
+      return with_excl(q.exclusive, [&](auto ex) {
+        constexpr bool EX = decltype(ex)::value;
+        auto kern = k_within_count<A, K, M, EX>;
+        const int grid = grid_for(kern, 0, q.nq);
+        kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                         radius, counts, q.stats);
+        g_launches++;
+        return cudaGetLastError();
+      });
+    });
+  });
+}
+
+template <typename A>
+cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
+                               const uint64_t* offsets) {
+  const TreeView<A> tv = make_view<A>(t);
+  const A radius = A(q.radius);
+  return with_dims(t.dims, [&](auto kk) {
+    constexpr int K = decltype(kk)::value;
+    return with_metric(q.metric, [&](auto m) {
+      using M = decltype(m);
+      return with_excl(q.exclusive, [&](auto ex) {
+        constexpr bool EX = decltype(ex)::value;
+        auto kern = k_within_fill<A, K, M, EX>;
+        const int grid = grid_for(kern, 0, q.nq);
+        kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                         radius, offsets, static_cast<A*>(q.out_d), q.out_i);
+        g_launches++;
+        return cudaGetLastError();
+      });
+    });
+  });
+}
+
+template <typename A>
+cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d, uint32_t* it,
+                            A* scratch_d, uint32_t* scratch_i, cudaStream_t s) {
+  if (nq == 0) return cudaSuccess;
+  {
+    auto kern = k_seg_sort_warp<A>;
+    const int grid = grid_for(kern, 0, nq);
+    kern<<<grid, 256, 0, s>>>(offsets, nq, d, it);
+    g_launches++;
+  }
+  {
+    // shared-memory ping-pong buffers for segments up to `cap` hits
+    const uint32_t cap = 4096;
+    const size_t smem = size_t(cap) * 2 * (sizeof(A) + sizeof(uint32_t));
+    auto kern = k_seg_sort_block<A>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const uint64_t blocks = (nq + 255) / 256;
+    kern<<<unsigned(blocks), 256, smem, s>>>(offsets, nq, d, it, scratch_d, scratch_i, cap);
+    g_launches++;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace kgpu
+
+#define KGPU_INSTANTIATE(A)                                                                      \
+  namespace kgpu {                                                                               \
+  template cudaError_t launch_fixed<A>(const DeviceTree&, const QueryLaunch&);                   \
+  template cudaError_t launch_within_count<A>(const DeviceTree&, const QueryLaunch&, uint64_t*); \
+  template cudaError_t launch_within_fill<A>(const DeviceTree&, const QueryLaunch&,              \
+                                             const uint64_t*);                                   \
+  template cudaError_t launch_seg_sort<A>(const uint64_t*, uint64_t, A*, uint32_t*, A*,          \
+                                          uint32_t*, cudaStream_t);                              \
+  }

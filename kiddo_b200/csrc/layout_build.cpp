@@ -1,0 +1,281 @@
+// layout_build.cpp — host construction of the ImmutableKdTree layout.
+//
+// Produces the exact bytes kiddo's soft-bucket bulk construction writes for
+// KdTree<A, u32, Eytzinger, VecOfArenas<A, u32, K, 32>, K, 32>:
+//   new_from_source_with        src/kd_tree/construction.rs:413-539
+//   populate_recursive_soft     src/kd_tree/construction.rs:868-968
+//   soft_left_leaf_budget/ideal src/kd_tree/construction.rs:673-691
+//   update_pivot                src/kd_tree/construction.rs:1089-1175
+//   VecOfArenas::append_leaf    src/leaf_strategy/vec_of_arenas.rs:292-323
+//
+// Design: the partition works on a u32 index permutation over per-axis
+// coordinate columns; subtrees below the top levels are built concurrently;
+// each leaf only records its index range during the recursion, and the arena
+// is written afterwards in one parallel pass once leaf offsets are known.  The
+// pivot rule is the reference's (the nudge-left / nudge-right of
+// update_pivot expressed as counts around the k-th order statistic), so stem
+// values and leaf membership match the reference exactly; points inside a
+// leaf are stored in ascending source index.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <stdexcept>
+#include <thread>
+#include <vector>
+
+#include "kgpu_internal.h"
+
+namespace kgpu {
+
+namespace {
+
+constexpr size_t kB = 32;
+
+inline size_t tile_width(size_t remaining) {
+  if (remaining >= 32) return 32;
+  if (remaining >= 8) return 8;
+  if (remaining >= 4) return 4;
+  if (remaining >= 2) return 2;
+  return 1;
+}
+
+template <typename A>
+size_t leaf_encoded_bytes(size_t len, int K) {
+  size_t total = 0;
+  while (len) {
+    size_t w = tile_width(len);
+    total += w * (K * sizeof(A) + sizeof(uint32_t));
+    len -= w;
+  }
+  return total;
+}
+
+template <typename A>
+struct SoftBuilder {
+  int K;
+  std::vector<std::vector<A>> cols;   // cols[d][i]
+  uint32_t* idx;
+  A* stems;
+  int max_stem_level;
+  uint32_t depth;
+  std::vector<uint64_t>* leaf_begin;  // per leaf: begin offset into idx
+  std::vector<uint32_t>* leaf_len;
+  int spawn_levels;
+
+  // Reference pivot rule (update_pivot) for chunk idx[b, e) on `dim`.
+  // Returns the pivot and the split value t (left = x < t) and the stem value.
+  size_t choose_pivot(uint32_t* b, size_t len, int dim, size_t ideal, std::vector<A>& buf,
+                      A* split_value) {
+    const A* col = cols[dim].data();
+    buf.resize(len);
+    for (size_t i = 0; i < len; ++i) buf[i] = col[b[i]];
+    std::nth_element(buf.begin(), buf.begin() + ideal, buf.end());
+    const A v = buf[ideal];
+    size_t lt = 0, le = 0;
+    A above = std::numeric_limits<A>::infinity();
+    for (size_t i = 0; i < len; ++i) {
+      const A x = buf[i];
+      lt += x < v;
+      le += x <= v;
+      if (x > v && x < above) above = x;
+    }
+    if (lt > 0) { *split_value = v; return lt; }
+    if (le >= len) { *split_value = v; return len; }
+    *split_value = above;  // left = {x <= v} = {x < above}
+    return le;
+  }
+
+  void build(uint32_t* b, size_t len, uint32_t stem_idx, int level, uint64_t budget,
+             uint64_t base) {
+    std::vector<A> buf;
+    build_rec(b, len, stem_idx, level, budget, base, buf);
+  }
+
+  void build_rec(uint32_t* b, size_t len, uint32_t stem_idx, int level, uint64_t budget,
+                 uint64_t base, std::vector<A>& buf) {
+    if (budget == 0) return;
+    if (level > max_stem_level) {
+      const uint32_t leaf = stem_idx - (uint32_t(1) << level);
+      (*leaf_begin)[leaf] = base;
+      (*leaf_len)[leaf] = uint32_t(len);
+      std::sort(b, b + len);
+      return;
+    }
+    const int dim = level % K;
+    uint64_t left_budget, right_budget;
+    size_t pivot;
+    A split = A(0);
+    if (budget == 1) {
+      left_budget = 1;
+      right_budget = 0;
+      pivot = len;
+    } else {
+      left_budget = uint64_t(1) << (63 - __builtin_clzll(budget - 1));
+      right_budget = budget - left_budget;
+      if (len == 0) {
+        pivot = 0;
+      } else {
+        unsigned __int128 num = (unsigned __int128)len * left_budget;
+        size_t p = size_t((num + budget - 1) / budget);
+        pivot = std::min(std::max<size_t>(p, 1), len);
+      }
+      if (pivot < len) pivot = choose_pivot(b, len, dim, pivot, buf, &split);
+    }
+    if (pivot < len) {
+      const A* col = cols[dim].data();
+      std::partition(b, b + len, [&](uint32_t i) { return col[i] < split; });
+      stems[stem_idx] = split;  // smallest coordinate of the right part
+    }
+    const size_t cut = std::min(pivot, len);
+    if (level < spawn_levels && len > 65536) {
+      std::thread th([&, b, cut, stem_idx, level, left_budget, base]() {
+        std::vector<A> buf2;
+        build_rec(b, cut, stem_idx * 2, level + 1, left_budget, base, buf2);
+      });
+      build_rec(b + cut, len - cut, stem_idx * 2 + 1, level + 1, right_budget, base + cut, buf);
+      th.join();
+    } else {
+      build_rec(b, cut, stem_idx * 2, level + 1, left_budget, base, buf);
+      build_rec(b + cut, len - cut, stem_idx * 2 + 1, level + 1, right_budget, base + cut, buf);
+    }
+  }
+};
+
+template <typename F>
+void parallel_range(size_t n, int nthreads, F&& f) {
+  if (nthreads <= 1 || n < 4096) {
+    f(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (n + nthreads - 1) / nthreads;
+  for (int t = 0; t < nthreads; ++t) {
+    size_t b = t * per, e = std::min(n, b + per);
+    if (b >= e) break;
+    th.emplace_back([&, b, e]() { f(b, e); });
+  }
+  for (auto& x : th) x.join();
+}
+
+template <typename A>
+void write_leaf(uint8_t* dst, const A* pts, const uint32_t* items, const uint32_t* idx,
+                size_t len, int K) {
+  size_t off = 0, base = 0;
+  while (len) {
+    const size_t w = tile_width(len);
+    for (int d = 0; d < K; ++d) {
+      A* col = reinterpret_cast<A*>(dst + off + d * w * sizeof(A));
+      for (size_t i = 0; i < w; ++i) col[i] = pts[size_t(idx[base + i]) * K + d];
+    }
+    uint32_t* it = reinterpret_cast<uint32_t*>(dst + off + K * w * sizeof(A));
+    for (size_t i = 0; i < w; ++i) it[i] = items ? items[idx[base + i]] : idx[base + i];
+    off += w * (K * sizeof(A) + sizeof(uint32_t));
+    base += w;
+    len -= w;
+  }
+}
+
+template <typename A>
+void build_layout(Layout& L, const A* pts, const uint32_t* items, uint64_t n, int K,
+                  int nthreads) {
+  L.dtype = sizeof(A) == 8 ? 1 : 0;
+  L.dims = K;
+  L.size = n;
+  L.max_stem_level = -1;
+  L.max_leaf_len = 0;
+  L.stems_bytes.clear();
+  L.leaf_bytes.clear();
+  L.extents.clear();
+  if (n == 0) return;
+  const uint64_t leaf_node_count = (n + kB - 1) / kB;
+  std::vector<uint32_t> idx(n);
+  for (uint64_t i = 0; i < n; ++i) idx[i] = uint32_t(i);
+
+  std::vector<uint64_t> leaf_begin;
+  std::vector<uint32_t> leaf_len;
+  if (leaf_node_count < 2) {
+    leaf_begin.assign(1, 0);
+    leaf_len.assign(1, uint32_t(n));
+  } else {
+    uint32_t depth = 0;
+    while ((uint64_t(1) << depth) < leaf_node_count) ++depth;
+    const uint64_t budget = uint64_t(1) << depth;
+    const size_t stem_count = (size_t(1) << (depth + 1));
+    const size_t padded = (stem_count + 7) / 8 * 8;
+    L.stems_bytes.resize(padded * sizeof(A));
+    A* stems = reinterpret_cast<A*>(L.stems_bytes.data());
+    for (size_t i = 0; i < padded; ++i) stems[i] = std::numeric_limits<A>::infinity();
+    leaf_begin.assign(budget, 0);
+    leaf_len.assign(budget, 0);
+
+    SoftBuilder<A> sb;
+    sb.K = K;
+    sb.cols.resize(K);
+    for (int d = 0; d < K; ++d) sb.cols[d].resize(n);
+    parallel_range(n, nthreads, [&](size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i)
+        for (int d = 0; d < K; ++d) sb.cols[d][i] = pts[i * K + d];
+    });
+    sb.idx = idx.data();
+    sb.stems = stems;
+    sb.max_stem_level = int(depth) - 1;
+    sb.depth = depth;
+    sb.leaf_begin = &leaf_begin;
+    sb.leaf_len = &leaf_len;
+    int spawn = 0;
+    while ((1 << spawn) < std::max(1, nthreads)) ++spawn;
+    sb.spawn_levels = spawn + 1;
+    sb.build(idx.data(), n, 1, 0, budget, 0);
+    L.max_stem_level = int(depth) - 1;
+  }
+  if (leaf_node_count < 2) std::sort(idx.begin(), idx.end());
+
+  // Arena offsets: each leaf starts on max(align A, align u32, 8) bytes.
+  const size_t nleaves = leaf_len.size();
+  L.extents.resize(2 * nleaves);
+  uint64_t cursor = 0;
+  for (size_t l = 0; l < nleaves; ++l) {
+    cursor = (cursor + 7) & ~uint64_t(7);
+    L.extents[2 * l] = cursor;
+    L.extents[2 * l + 1] = leaf_len[l];
+    cursor += leaf_encoded_bytes<A>(leaf_len[l], K);
+    L.max_leaf_len = std::max<uint64_t>(L.max_leaf_len, leaf_len[l]);
+  }
+  L.leaf_bytes.assign(cursor, 0);
+  parallel_range(nleaves, nthreads, [&](size_t b, size_t e) {
+    for (size_t l = b; l < e; ++l)
+      write_leaf<A>(L.leaf_bytes.data() + L.extents[2 * l], pts, items, idx.data() + leaf_begin[l],
+                    leaf_len[l], K);
+  });
+}
+
+}  // namespace
+
+int build_layout_any(Layout& L, int dtype, int K, const void* pts, const uint32_t* items,
+                     uint64_t n, int nthreads) {
+  if (K < 1 || K > kMaxDims) return set_error(KGPU_EUNSUPPORTED, "dims must be 1..4");
+  if (n > 0 && !pts) return set_error(KGPU_EINVAL, "points is NULL");
+  if (n > 0xFFFFFFFFull) return set_error(KGPU_EOVERFLOW, "more than 2^32 points");
+  if (nthreads <= 0) nthreads = int(std::max(1u, std::thread::hardware_concurrency()));
+  try {
+    if (dtype == KGPU_F32)
+      build_layout<float>(L, static_cast<const float*>(pts), items, n, K, nthreads);
+    else if (dtype == KGPU_F64)
+      build_layout<double>(L, static_cast<const double*>(pts), items, n, K, nthreads);
+    else
+      return set_error(KGPU_EINVAL, "dtype must be KGPU_F32 or KGPU_F64");
+  } catch (const std::bad_alloc&) {
+    return set_error(KGPU_ENOMEM, "host allocation failed while building the layout");
+  }
+  if (L.max_leaf_len > 1024)
+    return set_error(KGPU_EOVERFLOW,
+                     "a leaf holds more than 1024 points (leaf scratch capacity, "
+                     "leaf_view/mod.rs:18,58-65)");
+  return KGPU_OK;
+}
+
+}  // namespace kgpu

@@ -1,0 +1,215 @@
+"""CPU oracle for kiddo's ImmutableKdTree query path (test infrastructure).
+
+This package is the checker: a C++ restatement of the reference's construction
+and scalar query path (see kiddo_oracle.hpp for the file:line map), wrapped with
+ctypes.  Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline /
+reference legs may import it; the product package ``kiddo_b200`` never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libkiddo_oracle.so")
+_lib = None
+
+FAM_NEAREST_ONE = 0
+FAM_APPROX = 1
+FAM_NEAREST_N = 2
+FAM_BEST_N_WITHIN = 3
+FAM_PERIODIC_NEAREST_ONE = 4
+FAM_PERIODIC_NEAREST_N = 5
+FAM_WITHIN = 10
+FAM_PERIODIC_WITHIN = 11
+
+METRICS = {"sqeuclidean": 0, "manhattan": 1}
+
+
+def build_library(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++, -ffp-contract=off)."""
+    src = os.path.join(_HERE, "kiddo_oracle_capi.cpp")
+    hdr = os.path.join(_HERE, "kiddo_oracle.hpp")
+    stale = (not os.path.exists(_LIB_PATH)) or force or any(
+        os.path.getmtime(p) > os.path.getmtime(_LIB_PATH) for p in (src, hdr))
+    if stale:
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build_library()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+        L.kor_build.restype = vp
+        L.kor_build.argtypes = [i32, i32, vp, vp, u64]
+        L.kor_from_layout.restype = vp
+        L.kor_from_layout.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64, u64]
+        L.kor_free.argtypes = [vp]
+        L.kor_layout_info.argtypes = [vp, vp]
+        L.kor_copy_layout.argtypes = [vp, vp, vp, vp]
+        L.kor_query_fixed.restype = i32
+        L.kor_query_fixed.argtypes = [vp, i32, i32, vp, u64, ctypes.c_uint32, ctypes.c_double,
+                                      i32, i32, vp, vp, vp, vp, i32, vp]
+        L.kor_query_radius.restype = vp
+        L.kor_query_radius.argtypes = [vp, i32, i32, vp, u64, ctypes.c_double, i32, i32, vp, i32, vp]
+        L.kor_radius_total.restype = u64
+        L.kor_radius_total.argtypes = [vp]
+        L.kor_radius_copy.argtypes = [vp, vp, vp, vp]
+        L.kor_radius_free.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Layout:
+    """The reference's own ImmutableKdTree layout (stems, arena bytes, extents)."""
+
+    def __init__(self, dtype, k, stems, leaf_bytes, extents, max_stem_level, size, max_leaf_len):
+        self.dtype = np.dtype(dtype)
+        self.k = k
+        self.stems = stems
+        self.leaf_bytes = leaf_bytes
+        self.extents = extents  # uint64 [leaf_count, 2]
+        self.max_stem_level = int(max_stem_level)
+        self.size = int(size)
+        self.max_leaf_len = int(max_leaf_len)
+
+    @property
+    def leaf_count(self):
+        return int(self.extents.shape[0])
+
+
+class OracleTree:
+    """ImmutableKdTree<A, K> built and queried by the CPU restatement."""
+
+    def __init__(self, handle, dtype, k):
+        self._h = handle
+        self.dtype = np.dtype(dtype)
+        self.k = k
+
+    @classmethod
+    def build(cls, points, items=None):
+        points = np.ascontiguousarray(points)
+        assert points.dtype in (np.float32, np.float64) and points.ndim == 2
+        n, k = points.shape
+        it = None if items is None else np.ascontiguousarray(items, dtype=np.uint32)
+        h = lib().kor_build(0 if points.dtype == np.float32 else 1, k, _ptr(points), _ptr(it), n)
+        if not h:
+            raise ValueError("unsupported dtype/dimension for the oracle")
+        return cls(h, points.dtype, k)
+
+    @classmethod
+    def from_layout(cls, lay: Layout):
+        dt = 0 if lay.dtype == np.float32 else 1
+        stems = np.ascontiguousarray(lay.stems, dtype=lay.dtype)
+        lb = np.ascontiguousarray(lay.leaf_bytes, dtype=np.uint8)
+        ex = np.ascontiguousarray(lay.extents, dtype=np.uint64)
+        h = lib().kor_from_layout(dt, lay.k, _ptr(stems), stems.size, _ptr(lb), lb.size, _ptr(ex),
+                                  ex.shape[0], lay.max_stem_level, lay.size, lay.max_leaf_len)
+        return cls(h, lay.dtype, lay.k)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.kor_free(self._h)
+            self._h = None
+
+    def layout(self) -> Layout:
+        info = np.zeros(6, dtype=np.int64)
+        lib().kor_layout_info(self._h, _ptr(info))
+        stems = np.empty(int(info[0]), dtype=self.dtype)
+        lb = np.empty(int(info[1]), dtype=np.uint8)
+        ex = np.empty((int(info[2]), 2), dtype=np.uint64)
+        lib().kor_copy_layout(self._h, _ptr(stems), _ptr(lb), _ptr(ex))
+        return Layout(self.dtype, self.k, stems, lb, ex, info[3], info[4], info[5])
+
+    def _q(self, queries):
+        q = np.ascontiguousarray(queries, dtype=self.dtype)
+        assert q.ndim == 2 and q.shape[1] == self.k
+        return q
+
+    def _box(self, box):
+        if box is None:
+            return None
+        return np.ascontiguousarray(box, dtype=self.dtype).reshape(self.k)
+
+    def query_fixed(self, family, queries, k=1, radius=np.inf, metric="sqeuclidean",
+                    exclusive=False, sorted=True, box=None, threads=0, stats=False):
+        q = self._q(queries)
+        nq = q.shape[0]
+        kk = max(1, int(k))
+        d = np.empty(nq * kk, dtype=self.dtype)
+        it = np.empty(nq * kk, dtype=np.uint32)
+        c = np.empty(nq, dtype=np.uint32)
+        st = np.zeros(3, dtype=np.uint64) if stats else None
+        nth = threads if threads > 0 else (os.cpu_count() or 1)
+        bx = self._box(box)
+        lib().kor_query_fixed(self._h, family, METRICS[metric], _ptr(q), nq, kk, float(radius),
+                              int(exclusive), int(sorted), _ptr(bx), _ptr(d), _ptr(it), _ptr(c),
+                              nth, _ptr(st))
+        out = (d.reshape(nq, kk), it.reshape(nq, kk), c)
+        return out + (st,) if stats else out
+
+    def query_radius(self, family, queries, radius, metric="sqeuclidean", exclusive=False,
+                     sorted=True, box=None, threads=0, stats=False):
+        q = self._q(queries)
+        nq = q.shape[0]
+        st = np.zeros(3, dtype=np.uint64) if stats else None
+        nth = threads if threads > 0 else (os.cpu_count() or 1)
+        bx = self._box(box)
+        r = lib().kor_query_radius(self._h, family, METRICS[metric], _ptr(q), nq, float(radius),
+                                   int(exclusive), int(sorted), _ptr(bx), nth, _ptr(st))
+        total = lib().kor_radius_total(r)
+        off = np.empty(nq + 1, dtype=np.uint64)
+        d = np.empty(total, dtype=self.dtype)
+        it = np.empty(total, dtype=np.uint32)
+        lib().kor_radius_copy(r, _ptr(off), _ptr(d), _ptr(it))
+        lib().kor_radius_free(r)
+        out = (off, d, it)
+        return out + (st,) if stats else out
+
+    # Convenience wrappers mirroring the reference families -----------------
+    def nearest_one(self, queries, metric="sqeuclidean", **kw):
+        d, i, _ = self.query_fixed(FAM_NEAREST_ONE, queries, metric=metric, **kw)[:3]
+        return d[:, 0], i[:, 0]
+
+    def approx_nearest_one(self, queries, metric="sqeuclidean", **kw):
+        d, i, _ = self.query_fixed(FAM_APPROX, queries, metric=metric, **kw)[:3]
+        return d[:, 0], i[:, 0]
+
+    def nearest_n(self, queries, k, radius=np.inf, metric="sqeuclidean", exclusive=False,
+                  sorted=True, **kw):
+        return self.query_fixed(FAM_NEAREST_N, queries, k=k, radius=radius, metric=metric,
+                                exclusive=exclusive, sorted=sorted, **kw)
+
+    def best_n_within(self, queries, radius, n, metric="sqeuclidean", exclusive=False, **kw):
+        return self.query_fixed(FAM_BEST_N_WITHIN, queries, k=n, radius=radius, metric=metric,
+                                exclusive=exclusive, **kw)
+
+    def within(self, queries, radius, metric="sqeuclidean", exclusive=False, sorted=True, **kw):
+        return self.query_radius(FAM_WITHIN, queries, radius, metric=metric, exclusive=exclusive,
+                                 sorted=sorted, **kw)
+
+    def periodic_nearest_one(self, queries, box, metric="sqeuclidean", **kw):
+        d, i, _ = self.query_fixed(FAM_PERIODIC_NEAREST_ONE, queries, metric=metric, box=box,
+                                   **kw)[:3]
+        return d[:, 0], i[:, 0]
+
+    def periodic_nearest_n(self, queries, box, k, radius=np.inf, metric="sqeuclidean",
+                           exclusive=False, sorted=True, **kw):
+        return self.query_fixed(FAM_PERIODIC_NEAREST_N, queries, k=k, radius=radius,
+                                metric=metric, exclusive=exclusive, sorted=sorted, box=box, **kw)
+
+    def periodic_within(self, queries, box, radius, metric="sqeuclidean", exclusive=False,
+                        sorted=True, **kw):
+        return self.query_radius(FAM_PERIODIC_WITHIN, queries, radius, metric=metric,
+                                 exclusive=exclusive, sorted=sorted, box=box, **kw)

@@ -1,0 +1,345 @@
+// kiddo_oracle_capi.cpp — extern "C" surface of the CPU oracle for ctypes.
+//
+// TEST INFRASTRUCTURE ONLY (see kiddo_oracle.hpp).  Batch queries are spread
+// over std::thread workers so the same code also serves as the timed CPU
+// restatement of the reference path (a rayon par_iter over .execute() in
+// benches/query.rs:36-52).
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "kiddo_oracle.hpp"
+
+using namespace kiddo_oracle;
+
+namespace {
+
+enum Family : int {
+  FAM_NEAREST_ONE = 0,
+  FAM_APPROX = 1,
+  FAM_NEAREST_N = 2,       // nearest_n / nearest_n().within
+  FAM_BEST_N_WITHIN = 3,
+  FAM_PERIODIC_NEAREST_ONE = 4,
+  FAM_PERIODIC_NEAREST_N = 5,
+  FAM_WITHIN = 10,
+  FAM_PERIODIC_WITHIN = 11,
+};
+
+struct TreeBase {
+  int dtype;  // 0 f32, 1 f64
+  int k;
+  virtual ~TreeBase() = default;
+};
+
+template <typename A, int K>
+struct TreeHolder : TreeBase {
+  Tree<A, K> t;
+};
+
+struct RadiusResult {
+  std::vector<uint64_t> offsets;
+  std::vector<double> dists64;
+  std::vector<float> dists32;
+  std::vector<uint32_t> items;
+  int dtype;
+};
+
+template <typename F>
+void parallel_for(uint64_t n, int nthreads, F&& f) {
+  if (nthreads <= 1 || n < 64) {
+    for (uint64_t i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<uint64_t> next{0};
+  const uint64_t chunk = 256;
+  std::vector<std::thread> th;
+  for (int w = 0; w < nthreads; ++w)
+    th.emplace_back([&]() {
+      for (;;) {
+        uint64_t b = next.fetch_add(chunk);
+        if (b >= n) break;
+        uint64_t e = std::min(n, b + chunk);
+        for (uint64_t i = b; i < e; ++i) f(i);
+      }
+    });
+  for (auto& x : th) x.join();
+}
+
+struct StatsAcc {
+  std::atomic<uint64_t> stem{0}, leaf{0}, pts{0};
+  void add(const Stats& s) {
+    stem += s.stem_visits;
+    leaf += s.leaf_visits;
+    pts += s.points_scanned;
+  }
+};
+
+template <typename A, int K, typename M>
+int query_fixed_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq, uint32_t k,
+                  A radius, int exclusive, int sorted, const A* box, A* out_d,
+                  uint32_t* out_i, uint32_t* out_c, int nthreads, uint64_t* stats3) {
+  StatsAcc acc;
+  const bool want_stats = stats3 != nullptr;
+  parallel_for(nq, nthreads, [&](uint64_t qi) {
+    Stats s;
+    Stats* sp = want_stats ? &s : nullptr;
+    const A* q = queries + qi * K;
+    switch (family) {
+      case FAM_NEAREST_ONE: {
+        auto r = nearest_one<A, K, M>(t, q, sp);
+        out_d[qi] = r.first; out_i[qi] = r.second;
+        if (out_c) out_c[qi] = 1;
+        break;
+      }
+      case FAM_APPROX: {
+        auto r = approx_nearest_one<A, K, M>(t, q, sp);
+        out_d[qi] = r.first; out_i[qi] = r.second;
+        if (out_c) out_c[qi] = 1;
+        break;
+      }
+      case FAM_PERIODIC_NEAREST_ONE: {
+        auto r = periodic_nearest_one<A, K, M>(t, q, box, sp);
+        out_d[qi] = r.first; out_i[qi] = r.second;
+        if (out_c) out_c[qi] = 1;
+        break;
+      }
+      case FAM_NEAREST_N:
+      case FAM_BEST_N_WITHIN:
+      case FAM_PERIODIC_NEAREST_N: {
+        std::vector<Hit<A>> h;
+        if (family == FAM_NEAREST_N)
+          h = nearest_n_within<A, K, M>(t, q, radius, k, exclusive, sorted, sp);
+        else if (family == FAM_BEST_N_WITHIN)
+          h = best_n_within<A, K, M>(t, q, radius, k, exclusive, sp);
+        else
+          h = periodic_nearest<A, K, M>(t, q, box, radius, k, exclusive, sorted, sp);
+        for (uint32_t j = 0; j < k; ++j) {
+          if (j < h.size()) {
+            out_d[qi * k + j] = h[j].dist;
+            out_i[qi * k + j] = h[j].item;
+          } else {
+            out_d[qi * k + j] = inf_value<A>();
+            out_i[qi * k + j] = 0xFFFFFFFFu;
+          }
+        }
+        if (out_c) out_c[qi] = uint32_t(h.size());
+        break;
+      }
+      default:
+        break;
+    }
+    if (want_stats) acc.add(s);
+  });
+  if (want_stats) {
+    stats3[0] = acc.stem;
+    stats3[1] = acc.leaf;
+    stats3[2] = acc.pts;
+  }
+  return 0;
+}
+
+template <typename A, int K, typename M>
+RadiusResult* query_radius_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq,
+                             A radius, int exclusive, int sorted, const A* box, int nthreads,
+                             uint64_t* stats3) {
+  std::vector<std::vector<Hit<A>>> per(nq);
+  StatsAcc acc;
+  const bool want_stats = stats3 != nullptr;
+  parallel_for(nq, nthreads, [&](uint64_t qi) {
+    Stats s;
+    Stats* sp = want_stats ? &s : nullptr;
+    const A* q = queries + qi * K;
+    if (family == FAM_WITHIN)
+      per[qi] = within<A, K, M>(t, q, radius, exclusive, sorted, sp);
+    else
+      per[qi] = periodic_nearest<A, K, M>(t, q, box, radius, 0, exclusive, sorted, sp);
+    if (want_stats) acc.add(s);
+  });
+  auto* r = new RadiusResult();
+  r->dtype = sizeof(A) == 8 ? 1 : 0;
+  r->offsets.resize(nq + 1);
+  uint64_t total = 0;
+  for (uint64_t i = 0; i < nq; ++i) {
+    r->offsets[i] = total;
+    total += per[i].size();
+  }
+  r->offsets[nq] = total;
+  r->items.resize(total);
+  if (sizeof(A) == 8) r->dists64.resize(total); else r->dists32.resize(total);
+  for (uint64_t i = 0; i < nq; ++i) {
+    uint64_t o = r->offsets[i];
+    for (size_t j = 0; j < per[i].size(); ++j) {
+      r->items[o + j] = per[i][j].item;
+      if (sizeof(A) == 8) r->dists64[o + j] = double(per[i][j].dist);
+      else r->dists32[o + j] = float(per[i][j].dist);
+    }
+  }
+  if (want_stats) {
+    stats3[0] = acc.stem;
+    stats3[1] = acc.leaf;
+    stats3[2] = acc.pts;
+  }
+  return r;
+}
+
+template <typename F>
+auto dispatch(int dtype, int k, F&& f) -> decltype(f(float(), std::integral_constant<int, 3>())) {
+  using R = decltype(f(float(), std::integral_constant<int, 3>()));
+  if (dtype == 0) {
+    switch (k) {
+      case 1: return f(float(), std::integral_constant<int, 1>());
+      case 2: return f(float(), std::integral_constant<int, 2>());
+      case 3: return f(float(), std::integral_constant<int, 3>());
+      case 4: return f(float(), std::integral_constant<int, 4>());
+    }
+  } else if (dtype == 1) {
+    switch (k) {
+      case 1: return f(double(), std::integral_constant<int, 1>());
+      case 2: return f(double(), std::integral_constant<int, 2>());
+      case 3: return f(double(), std::integral_constant<int, 3>());
+      case 4: return f(double(), std::integral_constant<int, 4>());
+    }
+  }
+  return R();
+}
+
+}  // namespace
+
+extern "C" {
+
+// Build a tree with the restated soft construction.  `items` may be null, in
+// which case item = source index (new_from_slice).
+void* kor_build(int dtype, int k, const void* pts, const uint32_t* items, uint64_t n) {
+  return dispatch(dtype, k, [&](auto a, auto kk) -> void* {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    std::vector<uint32_t> gen;
+    if (!items) {
+      gen.resize(n);
+      for (uint64_t i = 0; i < n; ++i) gen[i] = uint32_t(i);
+      items = gen.data();
+    }
+    auto* h = new TreeHolder<A, K>();
+    h->dtype = dtype;
+    h->k = K;
+    h->t = build<A, K>(static_cast<const A*>(pts), items, n);
+    return static_cast<TreeBase*>(h);
+  });
+}
+
+// Wrap an externally produced layout (for example the one the product builder
+// made) so the oracle's queries can run on exactly those bytes.
+void* kor_from_layout(int dtype, int k, const void* stems, uint64_t stems_len,
+                      const uint8_t* bytes, uint64_t bytes_len, const uint64_t* extents,
+                      uint64_t leaf_count, int32_t max_stem_level, uint64_t size,
+                      uint64_t max_leaf_len) {
+  return dispatch(dtype, k, [&](auto a, auto kk) -> void* {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto* h = new TreeHolder<A, K>();
+    h->dtype = dtype;
+    h->k = K;
+    const A* s = static_cast<const A*>(stems);
+    h->t.stems.assign(s, s + stems_len);
+    h->t.leaf_bytes.assign(bytes, bytes + bytes_len);
+    h->t.extents.assign(extents, extents + 2 * leaf_count);
+    h->t.max_stem_level = max_stem_level;
+    h->t.size = size;
+    h->t.max_leaf_len = max_leaf_len;
+    return static_cast<TreeBase*>(h);
+  });
+}
+
+void kor_free(void* h) { delete static_cast<TreeBase*>(h); }
+
+// layout[0..5] = stems_len, leaf_bytes_len, leaf_count, max_stem_level, size, max_leaf_len
+void kor_layout_info(void* hp, int64_t* info) {
+  auto* b = static_cast<TreeBase*>(hp);
+  dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    info[0] = int64_t(t.stems.size());
+    info[1] = int64_t(t.leaf_bytes.size());
+    info[2] = int64_t(t.leaf_count());
+    info[3] = t.max_stem_level;
+    info[4] = int64_t(t.size);
+    info[5] = int64_t(t.max_leaf_len);
+    return 0;
+  });
+}
+
+void kor_copy_layout(void* hp, void* stems_out, uint8_t* bytes_out, uint64_t* extents_out) {
+  auto* b = static_cast<TreeBase*>(hp);
+  dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    if (stems_out) std::memcpy(stems_out, t.stems.data(), t.stems.size() * sizeof(A));
+    if (bytes_out) std::memcpy(bytes_out, t.leaf_bytes.data(), t.leaf_bytes.size());
+    if (extents_out) std::memcpy(extents_out, t.extents.data(), t.extents.size() * 8);
+    return 0;
+  });
+}
+
+// metric: 0 SquaredEuclidean, 1 Manhattan.  Outputs are dense [nq * k]
+// (k = 1 for the nearest-one families); unused slots hold +inf / 0xFFFFFFFF.
+int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint64_t nq,
+                    uint32_t k, double radius, int exclusive, int sorted, const void* box,
+                    void* out_d, uint32_t* out_i, uint32_t* out_c, int nthreads,
+                    uint64_t* stats3) {
+  auto* b = static_cast<TreeBase*>(hp);
+  return dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    const A r = A(radius);
+    if (metric == 0)
+      return query_fixed_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, k,
+                                              r, exclusive, sorted,
+                                              static_cast<const A*>(box), static_cast<A*>(out_d),
+                                              out_i, out_c, nthreads, stats3);
+    return query_fixed_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, k, r,
+                                          exclusive, sorted, static_cast<const A*>(box),
+                                          static_cast<A*>(out_d), out_i, out_c, nthreads,
+                                          stats3);
+  });
+}
+
+void* kor_query_radius(void* hp, int family, int metric, const void* queries, uint64_t nq,
+                       double radius, int exclusive, int sorted, const void* box, int nthreads,
+                       uint64_t* stats3) {
+  auto* b = static_cast<TreeBase*>(hp);
+  return dispatch(b->dtype, b->k, [&](auto a, auto kk) -> void* {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    const A r = A(radius);
+    if (metric == 0)
+      return query_radius_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, r,
+                                               exclusive, sorted, static_cast<const A*>(box),
+                                               nthreads, stats3);
+    return query_radius_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, r,
+                                           exclusive, sorted, static_cast<const A*>(box),
+                                           nthreads, stats3);
+  });
+}
+
+uint64_t kor_radius_total(void* r) {
+  auto* rr = static_cast<RadiusResult*>(r);
+  return rr->offsets.back();
+}
+
+void kor_radius_copy(void* r, uint64_t* offsets, void* dists, uint32_t* items) {
+  auto* rr = static_cast<RadiusResult*>(r);
+  std::memcpy(offsets, rr->offsets.data(), rr->offsets.size() * 8);
+  if (rr->dtype == 1) std::memcpy(dists, rr->dists64.data(), rr->dists64.size() * 8);
+  else std::memcpy(dists, rr->dists32.data(), rr->dists32.size() * 4);
+  std::memcpy(items, rr->items.data(), rr->items.size() * 4);
+}
+
+void kor_radius_free(void* r) { delete static_cast<RadiusResult*>(r); }
+
+}  // extern "C"

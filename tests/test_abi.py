@@ -1,0 +1,114 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol that
+include/kiddo_gpu.h declares, and rejects bad input with a status code (the
+reference panics instead: periodic.rs:710-717, builder.rs:1538-1543)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import kiddo_b200 as kb
+from kiddo_b200 import _capi as C
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "kiddo_gpu.h")).read()
+    return sorted(set(re.findall(r"\b(kgpu_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_exports_every_declared_symbol():
+    L = C.lib()
+    syms = header_symbols()
+    assert len(syms) >= 10
+    for s in syms:
+        assert hasattr(L, s), f"{s} declared in include/kiddo_gpu.h but not exported"
+    assert sorted(C.EXPORTED_SYMBOLS) == syms
+
+
+def test_version_and_status_strings():
+    L = C.lib()
+    assert L.kgpu_abi_version() == C.ABI_VERSION
+    assert L.kgpu_status_string(C.KGPU_EUNSUPPORTED) == b"unsupported layout or option"
+
+
+def _desc_of(tree):
+    d = C.TreeDesc()
+    ctypes.memmove(ctypes.byref(d), ctypes.byref(tree._desc), ctypes.sizeof(d))
+    return d
+
+
+def _create(d):
+    h = ctypes.c_void_p()
+    return C.lib().kgpu_tree_create(ctypes.byref(d), None, ctypes.byref(h))
+
+
+def test_tree_create_rejects_bad_layouts_before_touching_the_device():
+    t = kb.ImmutableKdTree.new_from_slice(np.random.default_rng(0).random((1000, 3)))
+    cases = [
+        ("abi_version", 99, C.KGPU_EINVAL),
+        ("dtype", 7, C.KGPU_EINVAL),
+        ("dims", 9, C.KGPU_EUNSUPPORTED),
+        ("item_size", 8, C.KGPU_EUNSUPPORTED),
+        ("bucket_size", 16, C.KGPU_EUNSUPPORTED),
+        ("stem_strategy", C.STEM_DONNELLY, C.KGPU_EUNSUPPORTED),
+        ("resolution", C.RES_MAPPED, C.KGPU_EUNSUPPORTED),
+        ("max_stem_level", 40, C.KGPU_EUNSUPPORTED),
+        ("leaf_count", 5, C.KGPU_EINVAL),
+        ("size", 999, C.KGPU_EINVAL),
+        ("leaf_bytes_len", 100, C.KGPU_EINVAL),
+    ]
+    for field, value, status in cases:
+        d = _desc_of(t)
+        setattr(d, field, value)
+        assert _create(d) == status, field
+        assert C.lib().kgpu_last_error()
+
+
+def test_layout_build_rejects_bad_arguments():
+    L = C.lib()
+    h = ctypes.c_void_p()
+    pts = np.zeros((10, 3), dtype=np.float32)
+    assert L.kgpu_layout_build(5, 3, pts.ctypes.data, None, 10, 1, ctypes.byref(h)) == C.KGPU_EINVAL
+    assert L.kgpu_layout_build(0, 9, pts.ctypes.data, None, 10, 1, ctypes.byref(h)) == \
+        C.KGPU_EUNSUPPORTED
+    assert L.kgpu_layout_build(0, 3, None, None, 10, 1, ctypes.byref(h)) == C.KGPU_EINVAL
+    # a chunk of more than 1024 identical points exceeds the leaf scratch capacity
+    # (leaf_view/mod.rs:18, 58-65), which the reference asserts at construction
+    same = np.zeros((2000, 3), dtype=np.float32)
+    assert L.kgpu_layout_build(0, 3, same.ctypes.data, None, 2000, 1, ctypes.byref(h)) == \
+        C.KGPU_EOVERFLOW
+
+
+def test_query_builder_typestate_errors():
+    # runtime mirror of the reference's compile-time typestate (builder.rs:1994-2077)
+    t = kb.ImmutableKdTree.new_from_slice(np.random.default_rng(0).random((100, 3)))
+    q = np.zeros((1, 3))
+
+    class Dummy:
+        pass
+
+    b = kb.QueryBuilder.__new__(kb.QueryBuilder)
+    kb.QueryBuilder.__init__(b, type("T", (), {"dtype": np.dtype(np.float64), "dims": 3})(), q)
+    with pytest.raises(TypeError):
+        b.approx()
+    b.nearest_n(kb.SquaredEuclidean, 3)
+    with pytest.raises(TypeError):
+        b.approx()
+    with pytest.raises(TypeError):
+        b.periodic_boundary_condition([1, 1, 1])
+    with pytest.raises(ValueError):
+        kb.QueryBuilder(b.tree, q).nearest_n(kb.SquaredEuclidean, 0)
+    with pytest.raises(ValueError):
+        kb.QueryBuilder(b.tree, q).periodic_boundary_condition([1.0, 0.0, 1.0])
+    with pytest.raises(TypeError):
+        kb.QueryBuilder(b.tree, q).periodic_boundary_condition([1, 1, 1]).best_n_within(
+            kb.SquaredEuclidean, 0.1, 3)
+    with pytest.raises(TypeError):
+        kb.QueryBuilder(b.tree, q).nearest_one(Dummy)
+    with pytest.raises(TypeError):
+        kb.QueryBuilder(b.tree, q).nearest_one(kb.SquaredEuclidean).exclusive_boundaries()
+    with pytest.raises(TypeError):
+        kb.QueryBuilder(b.tree, q).execute_gpu()
