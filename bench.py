@@ -54,8 +54,10 @@ def gaussian_mixture(n, rng, centres, dtype, sigma=0.005, background=0.2):
     return pts[rng.permutation(n)]
 
 
-def make_data(workload, rank):
-    dt, n, nq, fam, k = WORKLOADS[workload]
+def make_data(workload, rank, n=None, nq=None):
+    dt, n0, nq0, fam, k = WORKLOADS[workload]
+    n = n or n0
+    nq = nq or nq0
     dtype = np.float32 if dt == "f32" else np.float64
     if workload == "c1_nn1":
         P = np.random.default_rng(0).random((n, 3)).astype(dtype)
@@ -223,6 +225,8 @@ def main():
     ap.add_argument("--workload", default="c2_knn16", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spatial-order", action="store_true")
+    ap.add_argument("--points", type=int, default=0, help="override the tree size (profiling)")
+    ap.add_argument("--queries", type=int, default=0, help="override the batch size (profiling)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -241,7 +245,9 @@ def main():
         multi.init_process_group("nccl")
     dev = torch.device("cuda", local)
     dtype_name, n, nq, fam, k = WORKLOADS[args.workload]
-    P, Q = make_data(args.workload, rank)
+    n = args.points or n
+    nq = args.queries or nq
+    P, Q = make_data(args.workload, rank, n, nq)
     tree = kb.ImmutableKdTree.new_from_slice(P)
     gtree = tree.to_gpu()
     stream = torch.cuda.current_stream(dev)
