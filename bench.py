@@ -180,7 +180,7 @@ def cpu_baseline(tree, Q, workload, target_seconds=12.0, threads=0):
 
 
 def bytes_per_query(stats, nq, dtype_size, k):
-    """Algorithmic bytes of one query (SURVEY 8(d) model): the query, every
+    """Algorithmic bytes of one query: the query, every
     stem visited, every point scanned (K coords + u32 item), and the output."""
     stems, leaves, pts = (float(x) / nq for x in stats)
     out = k * (dtype_size + 4) + (4 if k > 1 else 0)

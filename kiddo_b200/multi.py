@@ -1,6 +1,6 @@
 """Multi-GPU plumbing: one process per GPU, each holding a replica of the tree.
 
-Queries are independent (SURVEY of the reference: rayon par_iter over
+Queries are independent (the reference parallelises them with a rayon par_iter over
 `.execute()`, benches/query.rs:36-52), so a batch shards by contiguous query
 ranges with no data-path collective.  The only collectives are the timing
 barrier and the max-over-ranks reduction of elapsed times, and optional result

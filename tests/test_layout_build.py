@@ -29,7 +29,7 @@ def test_uniform_layouts(dtype, dims, n):
 
 
 def test_config1_shape():
-    """C1: 100,000 f64 points -> stems_depth 12, 4,096 leaves, 8,192 stems."""
+    """100,000 f64 points -> stems_depth 12, 4,096 leaves, 8,192 stems (construction.rs:423-469)."""
     P = np.random.default_rng(0).random((100_000, 3))
     t, _ = same_layout(P)
     assert t.leaf_count() == 4096 and t.max_stem_level() == 11 and t.stems().size == 8192
