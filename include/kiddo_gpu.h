@@ -179,6 +179,26 @@ int32_t kgpu_query_radius_fill(kgpu_tree* tree, const kgpu_query_desc* desc,
                                const void* queries, uint64_t nq, const uint64_t* offsets,
                                void* out_dists, uint32_t* out_items, void* stream);
 
+/* ---- radius count without allocation -------------------------------------
+ * No counterpart in the reference: an addition of this engine for callers that
+ * cannot allocate device memory while they query (a process whose HBM is
+ * reserved up front by its own pool, a latency-critical loop that must not
+ * allocate, a host framework that owns every device buffer).
+ * Same result as kgpu_query_radius_count, with device pointers only
+ * (KGPU_FLAG_HOST_BUFFERS is rejected with KGPU_EINVAL).  It calls no
+ * cudaMalloc, cudaMallocAsync, cudaFree or allocating library routine: the
+ * prefix-sum scratch is a fixed 64 KiB array in device memory that every GPU
+ * loading the library holds until exit.  Limit: nq <= 16,777,216 queries
+ * (KGPU_EOVERFLOW beyond).  The tree's device must be current.  The first
+ * call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array, so calls that overlap on the GPU (on
+ * different streams or from different threads) race and must be serialised
+ * by the caller. */
+int32_t kgpu_query_radius_count_noalloc(kgpu_tree* tree, const kgpu_query_desc* desc,
+                                        const void* queries, uint64_t nq, uint64_t* offsets,
+                                        void* stream);
+
 /* ---- traversal statistics ----------------------------------------------
  * Runs the query's traversal (for the radius families: the counting pass)
  * with counters and writes the totals over the batch to stats[0..2]:

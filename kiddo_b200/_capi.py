@@ -30,7 +30,7 @@ EXPORTED_SYMBOLS = [
     "kgpu_last_error", "kgpu_status_string", "kgpu_abi_version", "kgpu_layout_build",
     "kgpu_layout_describe", "kgpu_layout_free", "kgpu_tree_create", "kgpu_tree_destroy",
     "kgpu_tree_info", "kgpu_query", "kgpu_query_radius_count", "kgpu_query_radius_fill",
-    "kgpu_launch_count", "kgpu_query_stats",
+    "kgpu_launch_count", "kgpu_query_stats", "kgpu_query_radius_count_noalloc",
 ]
 
 
@@ -98,6 +98,8 @@ def lib():
     L.kgpu_query_radius_fill.restype = i32
     L.kgpu_query_radius_fill.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, u64, vp, vp, vp, vp]
     L.kgpu_launch_count.restype = u64
+    L.kgpu_query_radius_count_noalloc.restype = i32
+    L.kgpu_query_radius_count_noalloc.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, u64, vp, vp]
     L.kgpu_query_stats.restype = i32
     L.kgpu_query_stats.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, u64, vp, vp]
     if L.kgpu_abi_version() != ABI_VERSION:

@@ -17,6 +17,7 @@
 #include "../../include/kiddo_gpu.h"
 #include "kgpu_internal.h"
 #include "kgpu_launch.h"
+#include "kgpu_tree_impl.h"
 
 namespace kgpu {
 
@@ -77,14 +78,8 @@ struct DevBuf {
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
-int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_family);
-
 }  // namespace
 }  // namespace kgpu
-
-struct kgpu_tree {
-  kgpu::DeviceTree dt;
-};
 
 using namespace kgpu;
 
@@ -275,7 +270,6 @@ int32_t kgpu_tree_info(const kgpu_tree* t, int64_t* info) {
 }  // extern "C"
 
 namespace kgpu {
-namespace {
 
 int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_family) {
   if (!t || !d) return set_error(KGPU_EINVAL, "NULL argument");
@@ -303,6 +297,8 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
   }
   return KGPU_OK;
 }
+
+namespace {
 
 template <typename A>
 cudaError_t run_fixed(const DeviceTree& dt, QueryLaunch& q) { return launch_fixed<A>(dt, q); }

@@ -1,0 +1,17 @@
+// kgpu_tree_impl.h — definition of the opaque kgpu_tree handle, shared by the
+// translation units that launch queries on it.
+#pragma once
+
+#include "../../include/kiddo_gpu.h"
+#include "kgpu_launch.h"
+
+struct kgpu_tree {
+  kgpu::DeviceTree dt;
+};
+
+namespace kgpu {
+// Validates a query description against a tree; `radius_family` selects the
+// within/within().unsorted() families.  Returns a kgpu_status and records the
+// message for kgpu_last_error().
+int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_family);
+}  // namespace kgpu
