@@ -110,7 +110,7 @@ typedef struct kgpu_query_desc {
   double radius;          /* metric units (squared distance for SquaredEuclidean); cast to A */
   int32_t exclusive;      /* .exclusive_boundaries(): strict `< radius` */
   int32_t sorted;         /* 1 = default sorted output, 0 = .unsorted() */
-  const void* periodic_box; /* host pointer to K values of A, or NULL (Cartesian) */
+  const void* periodic_box; /* host pointer to K values of A (each > 0), or NULL: Cartesian */
   uint32_t flags;         /* KGPU_FLAG_* */
   uint32_t reserved0;
 } kgpu_query_desc;

@@ -291,11 +291,26 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
     }
   }
   if (d->periodic_box) {
+    // builder.rs: periodic queries support nearest_one, nearest_n(.within) and
+    // within; best_n_within and approx are Cartesian-only.
     if (f == KGPU_BEST_N_WITHIN || f == KGPU_APPROX_NEAREST_ONE)
       return set_error(KGPU_EINVAL, "periodic boundaries apply to nearest_one, nearest_n and within");
-    return set_error(KGPU_EUNSUPPORTED, "periodic boundary conditions are not enabled in this build");
+    // PeriodicAxis::periodic_box_is_valid (builder.rs:29-35): every axis > 0
+    for (int a = 0; a < t->dt.dims; ++a) {
+      const double v = t->dt.dtype == KGPU_F64 ? static_cast<const double*>(d->periodic_box)[a]
+                                               : double(static_cast<const float*>(d->periodic_box)[a]);
+      if (!(v > 0.0)) return set_error(KGPU_EINVAL, "periodic box sizes must be strictly positive");
+    }
   }
   return KGPU_OK;
+}
+
+void apply_periodic(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch& q) {
+  q.periodic = d->periodic_box != nullptr;
+  if (!q.periodic) return;
+  for (int a = 0; a < dt.dims; ++a)
+    q.box[a] = dt.dtype == KGPU_F64 ? static_cast<const double*>(d->periodic_box)[a]
+                                    : double(static_cast<const float*>(d->periodic_box)[a]);
 }
 
 namespace {
@@ -332,6 +347,7 @@ int32_t kgpu_query(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, 
   q.exclusive = d->exclusive != 0;
   q.sorted = d->sorted != 0;
   q.nq = nq;
+  apply_periodic(dt, d, q);
   const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
   DevBuf bq, bd, bi, bc;
   cudaError_t e = cudaSuccess;
@@ -387,6 +403,7 @@ int32_t kgpu_query_radius_count(kgpu_tree* t, const kgpu_query_desc* d, const vo
   q.exclusive = d->exclusive != 0;
   q.sorted = d->family == KGPU_WITHIN && d->sorted != 0;
   q.nq = nq;
+  apply_periodic(dt, d, q);
   q.stream = s;
   uint64_t* doff = offsets;
   if (host) {
@@ -450,6 +467,7 @@ int32_t kgpu_query_radius_fill(kgpu_tree* t, const kgpu_query_desc* d, const voi
   q.exclusive = d->exclusive != 0;
   q.sorted = sorted;
   q.nq = nq;
+  apply_periodic(dt, d, q);
   q.stream = s;
   const uint64_t* doff = offsets;
   if (host) {
@@ -528,6 +546,7 @@ int32_t kgpu_query_stats(kgpu_tree* t, const kgpu_query_desc* d, const void* que
   q.exclusive = d->exclusive != 0;
   q.sorted = d->sorted != 0;
   q.nq = nq;
+  apply_periodic(dt, d, q);
   q.queries = dq;
   q.out_d = bd.p;
   q.out_i = bi.as<uint32_t>();

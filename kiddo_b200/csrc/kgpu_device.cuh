@@ -141,6 +141,33 @@ __device__ __forceinline__ A point_dist(const A (&c)[K], const A (&q)[K]) {
   return acc;
 }
 
+// Point-to-query distance of the Cartesian families.
+template <typename A, int K, typename M>
+struct CartesianDist {
+  __device__ __forceinline__ A operator()(const A (&c)[K], const A (&q)[K]) const {
+    return point_dist<M, A, K>(c, q);
+  }
+};
+
+// Minimum-image distance of the periodic leaf scan (periodic.rs:272-284,
+// 357-400): per axis delta = |q - c|, replaced by L - delta when smaller, then
+// acc += dist1(delta, 0).
+template <typename A, int K, typename M>
+struct PeriodicDist {
+  A box[K];
+  __device__ __forceinline__ A operator()(const A (&c)[K], const A (&q)[K]) const {
+    A acc = A(0);
+#pragma unroll
+    for (int d = 0; d < K; ++d) {
+      const A delta = abs_val(sub_rn(q[d], c[d]));
+      const A wrapped = sub_rn(box[d], delta);
+      const A m = wrapped < delta ? wrapped : delta;
+      acc = add_rn(acc, M::template dist1<A>(m, A(0)));
+    }
+    return acc;
+  }
+};
+
 template <typename A, int K>
 __device__ __forceinline__ A sel(const A (&v)[K], int d) {
   A r = v[0];
@@ -327,9 +354,10 @@ struct NearestOnePolicy {
 // fill sort.  Pruning bound = min(k-th distance once full, radius)
 // (nearest_n_within.rs:461-468); leaf filter `<=` or `<` against the bound at
 // leaf entry (leaf_view_chunked/nearest_n_within/fallback.rs:37-95).
-template <typename A, int K, typename M, bool kExclusive>
+template <typename A, int K, typename M, bool kExclusive, typename PD = CartesianDist<A, K, M>>
 struct NearestNPolicy {
   static constexpr bool kPruneOnEqual = kExclusive;
+  PD dist;
   A ld;           // lane j: j-th distance
   uint32_t li;    // lane j: j-th item
   uint32_t lseq;  // lane j: arrival number of the j-th entry
@@ -338,9 +366,9 @@ struct NearestNPolicy {
   A radius;
   A kth;          // ld of lane k-1 once full (uniform)
   uint32_t seq;   // arrivals so far (uniform)
-  __device__ NearestNPolicy(int k_, A r)
-      : ld(inf_of<A>()), li(0xffffffffu), lseq(0), n(0), k(k_), radius(r), kth(inf_of<A>()),
-        seq(0) {}
+  __device__ NearestNPolicy(int k_, A r, PD pd = PD())
+      : dist(pd), ld(inf_of<A>()), li(0xffffffffu), lseq(0), n(0), k(k_), radius(r),
+        kth(inf_of<A>()), seq(0) {}
   __device__ __forceinline__ A max_dist() const {
     return (n == k && kth < radius) ? kth : radius;
   }
@@ -373,7 +401,7 @@ struct NearestNPolicy {
       if (p < len) {
         A c[K];
         load_point<A, K>(base, len, p, c, it);
-        dd = point_dist<M, A, K>(c, q);
+        dd = dist(c, q);
         pass = kExclusive ? (dd < bound) : (dd <= bound);
       }
       uint32_t mask = __ballot_sync(FULL, pass);
@@ -488,12 +516,13 @@ struct BestNPolicy {
 
 // within / within().unsorted(): constant bound r (within.rs:18-41,
 // within_unsorted.rs:133-157); counting pass and filling pass.
-template <typename A, int K, typename M, bool kExclusive>
+template <typename A, int K, typename M, bool kExclusive, typename PD = CartesianDist<A, K, M>>
 struct WithinCountPolicy {
   static constexpr bool kPruneOnEqual = kExclusive;
+  PD dist;
   A radius;
   uint64_t count;
-  __device__ WithinCountPolicy(A r) : radius(r), count(0) {}
+  __device__ WithinCountPolicy(A r, PD pd = PD()) : dist(pd), radius(r), count(0) {}
   __device__ __forceinline__ A max_dist() const { return radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
@@ -508,7 +537,7 @@ struct WithinCountPolicy {
         A c[K];
         uint32_t it;
         load_point<A, K>(base, len, p, c, it);
-        const A dd = point_dist<M, A, K>(c, q);
+        const A dd = dist(c, q);
         pass = kExclusive ? (dd < radius) : (dd <= radius);
       }
       count += __popc(__ballot_sync(FULL, pass));
@@ -517,16 +546,17 @@ struct WithinCountPolicy {
   }
 };
 
-template <typename A, int K, typename M, bool kExclusive>
+template <typename A, int K, typename M, bool kExclusive, typename PD = CartesianDist<A, K, M>>
 struct WithinFillPolicy {
   static constexpr bool kPruneOnEqual = kExclusive;
+  PD dist;
   A radius;
   uint64_t count;
   uint64_t cap;  // the segment length the counting pass produced
   A* __restrict__ out_d;
   uint32_t* __restrict__ out_i;
-  __device__ WithinFillPolicy(A r, uint64_t c, A* d, uint32_t* i)
-      : radius(r), count(0), cap(c), out_d(d), out_i(i) {}
+  __device__ WithinFillPolicy(A r, uint64_t c, A* d, uint32_t* i, PD pd = PD())
+      : dist(pd), radius(r), count(0), cap(c), out_d(d), out_i(i) {}
   __device__ __forceinline__ A max_dist() const { return radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
@@ -542,7 +572,7 @@ struct WithinFillPolicy {
       if (p < len) {
         A c[K];
         load_point<A, K>(base, len, p, c, it);
-        dd = point_dist<M, A, K>(c, q);
+        dd = dist(c, q);
         pass = kExclusive ? (dd < radius) : (dd <= radius);
       }
       const uint32_t m = __ballot_sync(FULL, pass);
@@ -558,5 +588,226 @@ struct WithinFillPolicy {
     return len;
   }
 };
+
+
+// ---------------------------------------------------------------------------
+// Periodic boundary conditions (kd_tree/query/periodic.rs)
+// ---------------------------------------------------------------------------
+template <typename A>
+__device__ __forceinline__ A max_ref(A a, A b) { return b > a ? b : a; }
+
+// interval_distance_1d (stem_strategy/donnelly/simd_full/mod.rs:209-216)
+template <typename A>
+__device__ __forceinline__ A interval_distance(A q, A lo, A hi) {
+  return add_rn(max_ref(A(0), sub_rn(lo, q)), max_ref(A(0), sub_rn(q, hi)));
+}
+
+// periodic_interval_distance_1d (periodic.rs:286-308)
+template <typename A>
+__device__ __forceinline__ A periodic_interval_distance(A q, A lo, A hi, A L) {
+  A best = interval_distance(q, lo, hi);
+  const A minus = interval_distance(q, sub_rn(lo, L), sub_rn(hi, L));
+  if (minus < best) best = minus;
+  const A plus = interval_distance(q, add_rn(lo, L), add_rn(hi, L));
+  if (plus < best) best = plus;
+  return best;
+}
+
+// periodic_backtracking_query (periodic.rs:455-619), one warp per query.  The
+// frame stack holds at most one frame per level (frames are pushed at
+// increasing levels and popped LIFO), so the frame whose stem sits on level L
+// lives in lane L's registers and `has_frame` bit L marks it; popping takes
+// the deepest set bit.
+template <typename A, int K, typename M, typename P>
+__device__ __forceinline__ void warp_periodic_query(const TreeView<A>& tv, const A (&q)[K],
+                                                    const A (&box)[K], P& pol, int lane,
+                                                    TravStats& st) {
+  if (tv.size == 0) return;
+  const A INF = inf_of<A>();
+  const int msl = tv.max_stem_level;
+  uint32_t stem_idx = 1;
+  int level = 0, dim = 0;
+  A lower[K], upper[K], off[K];
+#pragma unroll
+  for (int d = 0; d < K; ++d) { lower[d] = A(0); upper[d] = box[d]; off[d] = A(0); }
+  A rd = A(0);
+  uint32_t has_frame = 0;
+  uint32_t f_stem = 0;
+  A f_lo[K], f_hi[K], f_off[K], f_rd = A(0);
+#pragma unroll
+  for (int d = 0; d < K; ++d) { f_lo[d] = A(0); f_hi[d] = A(0); f_off[d] = A(0); }
+
+  auto pop = [&]() -> bool {
+    if (!has_frame) return false;
+    const int L = 31 - __clz(has_frame);
+    has_frame &= ~(1u << L);
+    stem_idx = shfl(f_stem, L);
+    rd = shfl(f_rd, L);
+#pragma unroll
+    for (int d = 0; d < K; ++d) {
+      lower[d] = shfl(f_lo[d], L);
+      upper[d] = shfl(f_hi[d], L);
+      off[d] = shfl(f_off[d], L);
+    }
+    level = L;
+    dim = L % K;
+    return true;
+  };
+
+  for (;;) {
+    bool finished = false;
+    for (;;) {
+      if (level > msl) {
+        st.points += pol.leaf(tv, stem_idx & ~(1u << level), q, lane);
+        ++st.leaves;
+        break;
+      }
+      ++st.stems;
+      const A pivot = stem_idx < tv.stem_count ? __ldg(tv.stems + stem_idx) : INF;
+      if (pivot >= INF) {
+        stem_idx *= 2u;
+        ++level;
+        dim = dim + 1 == K ? 0 : dim + 1;
+        continue;
+      }
+      const A old_lo = sel(lower, dim), old_hi = sel(upper, dim);
+      const A qd = sel(q, dim), Ld = sel(box, dim);
+      const bool is_right = qd >= pivot;
+      const uint32_t near_idx = stem_idx * 2u + (is_right ? 1u : 0u);
+      const uint32_t far_idx = stem_idx * 2u + (is_right ? 0u : 1u);
+      const A minup = old_hi < pivot ? old_hi : pivot;
+      const A maxlo = max_ref(old_lo, pivot);
+      const A near_lo = is_right ? maxlo : old_lo;
+      const A near_hi = is_right ? old_hi : minup;
+      const A far_lo = is_right ? old_lo : maxlo;
+      const A far_hi = is_right ? minup : old_hi;
+      const A near_off = periodic_interval_distance(qd, near_lo, near_hi, Ld);
+      const A far_off = periodic_interval_distance(qd, far_lo, far_hi, Ld);
+      const A oo = sel(off, dim);
+      const A near_rd = M::template rect<A>(rd, oo, near_off);
+      const A far_rd = M::template rect<A>(rd, oo, far_off);
+      const A thr = pol.max_dist();
+      const bool near_pruned = near_rd > thr || (P::kPruneOnEqual && near_rd == thr);
+      const bool far_pruned = far_rd > thr || (P::kPruneOnEqual && far_rd == thr);
+      if (!far_pruned) {
+        const int FL = level + 1;
+        if (lane == FL) {
+          f_stem = far_idx;
+          f_rd = far_rd;
+#pragma unroll
+          for (int d = 0; d < K; ++d) {
+            f_lo[d] = d == dim ? far_lo : lower[d];
+            f_hi[d] = d == dim ? far_hi : upper[d];
+            f_off[d] = d == dim ? far_off : off[d];
+          }
+        }
+        has_frame |= 1u << FL;
+      }
+      if (near_pruned) {
+        if (pop()) continue;
+        finished = true;
+        break;
+      }
+      put(lower, dim, near_lo);
+      put(upper, dim, near_hi);
+      put(off, dim, near_off);
+      rd = near_rd;
+      stem_idx = near_idx;
+      ++level;
+      dim = dim + 1 == K ? 0 : dim + 1;
+    }
+    if (finished) return;
+    if (!pop()) return;
+  }
+}
+
+constexpr int pow3(int k) { return k == 0 ? 1 : 3 * pow3(k - 1); }
+
+// periodic_nearest_one_result (periodic.rs:156-214): the home query, then each
+// image whose lower bound beats the best so far, in (stable) lower-bound order.
+// Image j of the 3^K shifts has shift digit (j / 3^(K-1-a)) % 3 - 1 on axis a,
+// which is the generation order of periodic_image_candidates (periodic.rs:45-142).
+template <typename A, int K, typename M>
+__device__ __forceinline__ void warp_periodic_nearest_one(const TreeView<A>& tv, const A (&q)[K],
+                                                          const A (&box)[K], int lane, A& best,
+                                                          uint32_t& best_item, TravStats& st) {
+  {
+    NearestOnePolicy<A, K, M> home;
+    warp_arith_query<A, K, M>(tv, q, home, lane, st);
+    best = home.best;
+    best_item = home.item;
+  }
+  constexpr int NI = pow3(K);
+  constexpr int NC = (NI + 31) / 32;
+  A wq[NC][K];
+  A lb[NC];
+  bool valid[NC];
+  int rank[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int j = lane + 32 * c;
+    int rem = j;
+    bool nonzero = false;
+    A acc = A(0);
+#pragma unroll
+    for (int a = 0; a < K; ++a) {
+      int div = 1;
+      for (int b = a + 1; b < K; ++b) div *= 3;
+      const int digit = (rem / div) % 3;
+      const A L = box[a];
+      const A w = digit == 0 ? sub_rn(q[a], L) : (digit == 1 ? q[a] : add_rn(q[a], L));
+      nonzero |= digit != 1;
+      wq[c][a] = w;
+      // periodic_image_axis_offset (periodic.rs:29-37)
+      const A o = w < A(0) ? abs_val(sub_rn(w, A(0))) : (w > L ? abs_val(sub_rn(w, L)) : A(0));
+      acc = add_rn(acc, M::template dist1<A>(o, A(0)));
+    }
+    lb[c] = acc;
+    valid[c] = j < NI && nonzero && acc < best;
+  }
+  // stable rank by lower bound among the valid images
+  int nvalid = 0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    rank[c] = 0;
+    nvalid += __popc(__ballot_sync(FULL, valid[c]));
+  }
+#pragma unroll
+  for (int c2 = 0; c2 < NC; ++c2) {
+    for (int l2 = 0; l2 < 32; ++l2) {
+      const A olb = shfl(lb[c2], l2);
+      const bool ov = __shfl_sync(FULL, valid[c2] ? 1u : 0u, l2) != 0u;
+      const int oj = l2 + 32 * c2;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int j = lane + 32 * c;
+        if (ov && (olb < lb[c] || (olb == lb[c] && oj < j))) ++rank[c];
+      }
+    }
+  }
+  for (int r = 0; r < nvalid; ++r) {
+    A img[K];
+#pragma unroll
+    for (int a = 0; a < K; ++a) img[a] = q[a];
+    A ilb = inf_of<A>();
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const uint32_t m = __ballot_sync(FULL, valid[c] && rank[c] == r);
+      if (m) {
+        const int src = __ffs(m) - 1;
+#pragma unroll
+        for (int a = 0; a < K; ++a) img[a] = shfl(wq[c][a], src);
+        ilb = shfl(lb[c], src);
+      }
+    }
+    if (!(ilb < best)) continue;
+    NearestOnePolicy<A, K, M> pol;
+    warp_arith_query<A, K, M>(tv, img, pol, lane, st);
+    if (pol.best < best) {
+      best = pol.best;
+      best_item = pol.item;
+    }
+  }
+}
 
 }  // namespace kgpu

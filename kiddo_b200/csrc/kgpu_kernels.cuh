@@ -125,6 +125,102 @@ __global__ void __launch_bounds__(256) k_within_fill(TreeView<A> tv, const A* __
   }
 }
 
+// ---------------------------------------------------------------------------
+// Periodic families (kd_tree/query/periodic.rs)
+// ---------------------------------------------------------------------------
+template <typename A, int K>
+struct BoxArg {
+  A v[K];
+};
+
+template <typename A, int K, typename M, int FAM, bool EXCL>
+__global__ void __launch_bounds__(256) k_periodic_fixed(TreeView<A> tv, const A* __restrict__ Q,
+                                                        const uint32_t* __restrict__ order,
+                                                        uint64_t nq, BoxArg<A, K> box, int k,
+                                                        A radius, A* __restrict__ out_d,
+                                                        uint32_t* __restrict__ out_i,
+                                                        uint32_t* __restrict__ out_c,
+                                                        unsigned long long* __restrict__ stats) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t w = warp; w < nq; w += nwarps) {
+    const uint64_t qi = order ? order[w] : w;
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    TravStats st;
+    if constexpr (FAM == KF_NEAREST_ONE) {
+      A best;
+      uint32_t item;
+      warp_periodic_nearest_one<A, K, M>(tv, q, box.v, lane, best, item, st);
+      if (lane == 0) {
+        out_d[qi] = best;
+        out_i[qi] = item;
+        if (out_c) out_c[qi] = 1;
+      }
+    } else {
+      PeriodicDist<A, K, M> pd;
+#pragma unroll
+      for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
+      NearestNPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(k, radius, pd);
+      warp_periodic_query<A, K, M>(tv, q, box.v, pol, lane, st);
+      pol.write(qi, out_d, out_i, out_c, false, lane);
+    }
+    if (stats && lane == 0) add_stats(stats, st);
+  }
+}
+
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_periodic_within_count(
+    TreeView<A> tv, const A* __restrict__ Q, const uint32_t* __restrict__ order, uint64_t nq,
+    BoxArg<A, K> box, A radius, uint64_t* __restrict__ counts,
+    unsigned long long* __restrict__ stats) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  PeriodicDist<A, K, M> pd;
+#pragma unroll
+  for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
+  for (uint64_t w = warp; w < nq; w += nwarps) {
+    const uint64_t qi = order ? order[w] : w;
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    WithinCountPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(radius, pd);
+    TravStats st;
+    warp_periodic_query<A, K, M>(tv, q, box.v, pol, lane, st);
+    if (lane == 0) counts[qi] = pol.count;
+    if (stats && lane == 0) add_stats(stats, st);
+  }
+}
+
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_periodic_within_fill(
+    TreeView<A> tv, const A* __restrict__ Q, const uint32_t* __restrict__ order, uint64_t nq,
+    BoxArg<A, K> box, A radius, const uint64_t* __restrict__ offsets, A* __restrict__ out_d,
+    uint32_t* __restrict__ out_i) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  PeriodicDist<A, K, M> pd;
+#pragma unroll
+  for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
+  for (uint64_t w = warp; w < nq; w += nwarps) {
+    const uint64_t qi = order ? order[w] : w;
+    const uint64_t o = offsets[qi];
+    const uint64_t cap = offsets[qi + 1] - o;
+    if (cap == 0) continue;
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    WithinFillPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(radius, cap, out_d + o, out_i + o,
+                                                                pd);
+    TravStats st;
+    warp_periodic_query<A, K, M>(tv, q, box.v, pol, lane, st);
+  }
+}
+
 // Segments of at most 32 hits: one warp, bitonic network on (distance, position)
 // so equal distances keep traversal order (a stable sort, as Vec::sort).
 template <typename A>

@@ -37,6 +37,8 @@ struct QueryLaunch {
   uint32_t* out_i = nullptr;
   uint32_t* out_c = nullptr;
   unsigned long long* stats = nullptr;  // optional [stems, leaves, points] totals
+  bool periodic = false;          // periodic boundary conditions
+  double box[4] = {0, 0, 0, 0};   // periodic box (converted to A)
   cudaStream_t stream = nullptr;
 };
 

@@ -75,6 +75,22 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
           g_launches++;
           return cudaGetLastError();
         };
+        if (q.periodic) {
+          BoxArg<A, K> box;
+          for (int d = 0; d < K; ++d) box.v[d] = A(q.box[d]);
+          auto runp = [&](auto kern) {
+            const int grid = grid_for(kern, 0, q.nq);
+            kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                             box, q.k, radius, static_cast<A*>(q.out_d), q.out_i,
+                                             q.out_c, q.stats);
+            g_launches++;
+            return cudaGetLastError();
+          };
+          if (q.family == KGPU_NEAREST_ONE) return runp(k_periodic_fixed<A, K, M, KF_NEAREST_ONE, false>);
+          if (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN)
+            return runp(k_periodic_fixed<A, K, M, KF_NEAREST_N, EX>);
+          return cudaErrorInvalidValue;
+        }
         switch (q.family) {
           case KGPU_NEAREST_ONE:
             return run(k_fixed<A, K, M, KF_NEAREST_ONE, false>);
@@ -102,6 +118,16 @@ cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint6
       using M = decltype(m);
       return with_excl(q.exclusive, [&](auto ex) {
         constexpr bool EX = decltype(ex)::value;
+        if (q.periodic) {
+          BoxArg<A, K> box;
+          for (int d = 0; d < K; ++d) box.v[d] = A(q.box[d]);
+          auto kern = k_periodic_within_count<A, K, M, EX>;
+          const int grid = grid_for(kern, 0, q.nq);
+          kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                           box, radius, counts, q.stats);
+          g_launches++;
+          return cudaGetLastError();
+        }
         auto kern = k_within_count<A, K, M, EX>;
         const int grid = grid_for(kern, 0, q.nq);
         kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
@@ -124,6 +150,17 @@ cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
       using M = decltype(m);
       return with_excl(q.exclusive, [&](auto ex) {
         constexpr bool EX = decltype(ex)::value;
+        if (q.periodic) {
+          BoxArg<A, K> box;
+          for (int d = 0; d < K; ++d) box.v[d] = A(q.box[d]);
+          auto kern = k_periodic_within_fill<A, K, M, EX>;
+          const int grid = grid_for(kern, 0, q.nq);
+          kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                           box, radius, offsets, static_cast<A*>(q.out_d),
+                                           q.out_i);
+          g_launches++;
+          return cudaGetLastError();
+        }
         auto kern = k_within_fill<A, K, M, EX>;
         const int grid = grid_for(kern, 0, q.nq);
         kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,

@@ -96,6 +96,7 @@ extern "C" int32_t kgpu_query_radius_count_noalloc(kgpu_tree* t, const kgpu_quer
   q.exclusive = d->exclusive != 0;
   q.sorted = d->family == KGPU_WITHIN && d->sorted != 0;
   q.nq = nq;
+  apply_periodic(dt, d, q);
   q.queries = queries;
   q.stream = s;
   if (nq) {

@@ -1,0 +1,321 @@
+// kgpu_thread.cuh — thread-per-query variants of the exact query families.
+//
+// The warp-per-query kernels spend most issue slots on 32 lanes running the
+// same scalar traversal.  Here every thread runs one query's traversal,
+// exactly in the reference's order (kd_tree/orchestrator/mod.rs:388-603), so a
+// warp advances 32 queries per instruction.
+//
+// Continuation state per level L, in shared memory column `slot[L * stride]`:
+//  * while the far child of level L is pending: its rd_far;
+//  * once the far child has been entered: the off[dim] value to restore on the
+//    way back up (the reference's restore frame);
+// two bitmasks say which.  A level that never branched needs neither: along a
+// near path `off` does not change, so restoring it is a no-op.  far_off is
+// recomputed from the stem when the far child is entered (|q - pivot|, the
+// same operation the descent did).  Same visit order, same rd arithmetic, same
+// results as the per-level restore/far stacks of the reference.
+#pragma once
+
+#include "kgpu_device.cuh"
+
+namespace kgpu {
+
+// Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
+// leaf_view/mod.rs:431-446): f(coords, item) in tile order.
+template <typename A, int K, typename F>
+__device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint32_t leaf,
+                                                          F&& f) {
+  const uint2 ex = __ldg(tv.extents + leaf);
+  const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+  uint32_t rem = ex.y;
+  uint32_t boff = 0;
+  while (rem) {
+    const uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
+    const A* col = reinterpret_cast<const A*>(base + boff);
+    const uint32_t* its = reinterpret_cast<const uint32_t*>(base + boff + K * w * sizeof(A));
+    for (uint32_t i = 0; i < w; ++i) {
+      A c[K];
+#pragma unroll
+      for (int d = 0; d < K; ++d) c[d] = __ldg(col + d * w + i);
+      f(c, __ldg(its + i));
+    }
+    boff += w * (K * sizeof(A) + sizeof(uint32_t));
+    rem -= w;
+  }
+  return ex.y;
+}
+
+template <typename A, int K, typename M, typename P>
+__device__ __forceinline__ void thread_arith_query(const TreeView<A>& tv, const A (&q)[K], P& pol,
+                                                   A* __restrict__ slot, int stride,
+                                                   TravStats& st) {
+  if (tv.size == 0) return;
+  const A INF = inf_of<A>();
+  const int msl = tv.max_stem_level;
+  A off[K];
+#pragma unroll
+  for (int d = 0; d < K; ++d) off[d] = A(0);
+  uint32_t stem_idx = 1;
+  int level = 0, dim = 0;
+  A rd = A(0);
+  uint32_t pending = 0, taken = 0;
+
+  auto descend = [&](bool check_bound) -> uint32_t {
+    while (level <= msl) {
+      ++st.stems;
+      const A pivot = __ldg(tv.stems + stem_idx);
+      if (pivot < INF) {
+        const A qd = sel(q, dim);
+        const bool is_right = qd >= pivot;
+        const A new_off = abs_val(sub_rn(qd, pivot));
+        const A rd_far = M::template rect<A>(rd, sel(off, dim), new_off);
+        if (!check_bound || !(rd_far > pol.max_dist())) {
+          slot[level * stride] = rd_far;
+          pending |= 1u << level;
+        }
+        stem_idx = stem_idx * 2u + (is_right ? 1u : 0u);
+      } else {
+        stem_idx = stem_idx * 2u;
+      }
+      ++level;
+      dim = dim + 1 == K ? 0 : dim + 1;
+    }
+    return stem_idx & ~(1u << level);
+  };
+
+  st.points += pol.leaf(tv, descend(!pol.unbounded_start()), q);
+  ++st.leaves;
+  int cur = level;
+  for (;;) {
+    bool resumed = false;
+    while (cur > 0) {
+      const int L = cur - 1;
+      const int d = dim == 0 ? K - 1 : dim - 1;
+      dim = d;
+      const uint32_t bit = 1u << L;
+      if (taken & bit) {
+        put(off, d, slot[L * stride]);  // the restore frame of a far branch
+        taken &= ~bit;
+      } else if (pending & bit) {
+        pending &= ~bit;
+        const A frd = slot[L * stride];
+        const A md = pol.max_dist();
+        if (!(frd > md || (P::kPruneOnEqual && frd == md))) {
+          const A pivot = __ldg(tv.stems + (stem_idx >> 1));
+          const A old = sel(off, d);
+          slot[L * stride] = old;
+          taken |= bit;
+          put(off, d, abs_val(sub_rn(sel(q, d), pivot)));
+          rd = frd;
+          stem_idx ^= 1u;
+          level = cur;
+          dim = d + 1 == K ? 0 : d + 1;
+          st.points += pol.leaf(tv, descend(true), q);
+          ++st.leaves;
+          cur = level;
+          resumed = true;
+          break;
+        }
+      }
+      stem_idx >>= 1;
+      cur = L;
+    }
+    if (!resumed) break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Thread policies
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M>
+struct TNearestOne {
+  static constexpr bool kPruneOnEqual = true;
+  A best;
+  uint32_t item;
+  __device__ TNearestOne() : best(inf_of<A>()), item(0) {}
+  __device__ __forceinline__ A max_dist() const { return best; }
+  __device__ __forceinline__ bool unbounded_start() const { return true; }
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
+    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
+      const A d = point_dist<M, A, K>(c, q);
+      if (d < best) { best = d; item = it; }
+    });
+  }
+};
+
+// k smallest by (distance, arrival) in a register list of KC slots
+// (ThresholdVecResultCollection, results/result_collection.rs:136-215).
+template <typename A, int K, typename M, bool kExclusive, int KC, bool kTrack>
+struct TNearestN {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A ld[KC];
+  uint32_t li[KC];
+  uint32_t ls[kTrack ? KC : 1];
+  int n, k;
+  A radius, kth;
+  uint32_t seq;
+  __device__ TNearestN(int k_, A r) : n(0), k(k_), radius(r), kth(inf_of<A>()), seq(0) {
+#pragma unroll
+    for (int j = 0; j < KC; ++j) { ld[j] = inf_of<A>(); li[j] = 0xffffffffu; }
+#pragma unroll
+    for (int j = 0; j < (kTrack ? KC : 1); ++j) ls[j] = 0;
+  }
+  __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+
+  __device__ __forceinline__ void add(A d, uint32_t it) {
+    if (n == k && !(d < kth)) return;
+    const int m = n < k ? n + 1 : k;
+#pragma unroll
+    for (int j = KC - 1; j >= 0; --j) {
+      if (j < m) {
+        if (j > 0 && ld[j - 1] > d) {
+          ld[j] = ld[j - 1];
+          li[j] = li[j - 1];
+          if (kTrack) ls[j] = ls[j - 1];
+        } else if (j == n || ld[j] > d) {
+          ld[j] = d;
+          li[j] = it;
+          if (kTrack) ls[j] = seq;
+        }
+      }
+    }
+    ++seq;
+    n = m;
+    if (n == k) {
+      A t = ld[0];
+#pragma unroll
+      for (int j = 1; j < KC; ++j)
+        if (j == k - 1) t = ld[j];
+      kth = t;
+    }
+  }
+
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
+    const A bound = max_dist();
+    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
+      const A d = point_dist<M, A, K>(c, q);
+      if (kExclusive ? (d < bound) : (d <= bound)) add(d, it);
+    });
+  }
+
+  // ThresholdVec::into_vec keeps arrival order while the list never filled.
+  __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
+                                        uint32_t* __restrict__ out_i,
+                                        uint32_t* __restrict__ out_c, bool arrival_order) const {
+    A* od = out_d + size_t(qi) * k;
+    uint32_t* oi = out_i + size_t(qi) * k;
+    if (kTrack && arrival_order && n < k) {
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        if (j < n) {
+          int rank = 0;
+#pragma unroll
+          for (int t = 0; t < KC; ++t)
+            if (t < n && ls[t] < ls[j]) ++rank;
+          od[rank] = ld[j];
+          oi[rank] = li[j];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < KC; ++j)
+        if (j < n) { od[j] = ld[j]; oi[j] = li[j]; }
+    }
+#pragma unroll
+    for (int j = 0; j < KC; ++j)
+      if (j >= n && j < k) { od[j] = inf_of<A>(); oi[j] = 0xffffffffu; }
+    if (out_c) out_c[qi] = uint32_t(n);
+  }
+};
+
+// best_n_within: the n smallest items among hits, by (item, arrival)
+// (kd_tree/query/best_n_within.rs:88-196, leaf filter
+// leaf_view_chunked/best_n_within/fallback.rs:40-104).
+template <typename A, int K, typename M, bool kExclusive, int KC>
+struct TBestN {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A ld[KC];
+  uint32_t li[KC];
+  int n, k;
+  A radius;
+  __device__ TBestN(int k_, A r) : n(0), k(k_), radius(r) {
+#pragma unroll
+    for (int j = 0; j < KC; ++j) { ld[j] = inf_of<A>(); li[j] = 0xffffffffu; }
+  }
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return false; }
+  __device__ __forceinline__ uint32_t last_item() const {
+    uint32_t t = li[0];
+#pragma unroll
+    for (int j = 1; j < KC; ++j)
+      if (j == k - 1) t = li[j];
+    return t;
+  }
+  __device__ __forceinline__ void add(A d, uint32_t it) {
+    if (n == k && !(it < last_item())) return;
+    const int m = n < k ? n + 1 : k;
+#pragma unroll
+    for (int j = KC - 1; j >= 0; --j) {
+      if (j < m) {
+        if (j > 0 && li[j - 1] > it) {
+          ld[j] = ld[j - 1];
+          li[j] = li[j - 1];
+        } else if (j == n || li[j] > it) {
+          ld[j] = d;
+          li[j] = it;
+        }
+      }
+    }
+    n = m;
+  }
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
+    const bool full_at_entry = n == k;
+    const uint32_t thr_item = last_item();
+    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
+      const A d = point_dist<M, A, K>(c, q);
+      if (!(kExclusive ? (d < radius) : (d <= radius))) return;
+      if (full_at_entry && it >= thr_item) return;
+      add(d, it);
+    });
+  }
+  __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
+                                        uint32_t* __restrict__ out_i,
+                                        uint32_t* __restrict__ out_c) const {
+    A* od = out_d + size_t(qi) * k;
+    uint32_t* oi = out_i + size_t(qi) * k;
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      if (j < k) {
+        od[j] = j < n ? ld[j] : inf_of<A>();
+        oi[j] = j < n ? li[j] : 0xffffffffu;
+      }
+    }
+    if (out_c) out_c[qi] = uint32_t(n);
+  }
+};
+
+template <typename A, int K, typename M, bool kExclusive>
+struct TWithin {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A radius;
+  uint64_t count;
+  uint64_t cap;                 // fill pass: the segment length; count pass: unused
+  A* __restrict__ out_d;        // null in the counting pass
+  uint32_t* __restrict__ out_i;
+  __device__ TWithin(A r, uint64_t c, A* d, uint32_t* i)
+      : radius(r), count(0), cap(c), out_d(d), out_i(i) {}
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
+    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
+      const A d = point_dist<M, A, K>(c, q);
+      if (kExclusive ? (d < radius) : (d <= radius)) {
+        if (out_d && count < cap) { out_d[count] = d; out_i[count] = it; }
+        ++count;
+      }
+    });
+  }
+};
+
+}  // namespace kgpu
