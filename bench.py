@@ -225,6 +225,8 @@ def main():
     ap.add_argument("--workload", default="c2_knn16", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spatial-order", action="store_true")
+    ap.add_argument("--engine", default=None, choices=["warp", "thread"],
+                    help="force the kernel variant (default: the library chooses)")
     ap.add_argument("--points", type=int, default=0, help="override the tree size (profiling)")
     ap.add_argument("--queries", type=int, default=0, help="override the batch size (profiling)")
     args = ap.parse_args()
@@ -254,7 +256,7 @@ def main():
     dq = torch.from_numpy(Q).to(dev)
 
     def step():
-        b = builder_for(gtree, dq, args.workload)
+        b = builder_for(gtree, dq, args.workload).with_engine(args.engine)
         if args.spatial_order:
             b = b.with_spatial_order()
         return b.execute_gpu()
@@ -316,12 +318,13 @@ def main():
         "config": {"workload": args.workload, "points": n, "queries_per_gpu": nq, "family": fam,
                    "k": k, "metric": "SquaredEuclidean", "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (tree 256 MB, queries 192 MB), no flush",
-                   "spatial_order": bool(args.spatial_order)},
+                   "spatial_order": bool(args.spatial_order),
+                   "engine": args.engine or "auto"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "bytes_per_query": bpq,
                      "traffic": (traffic or {}).get("dram_bytes_per_launch"),
-                     "kernel": "k_fixed<nearest_n>"},
+                     "kernel": "k_tfixed<nearest_n>" if args.engine != "warp" else "k_fixed<nearest_n>"},
         "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),

@@ -260,6 +260,7 @@ class QueryBuilder:
         self.sorted = True
         self.box = None
         self.spatial_order = False
+        self.engine = None
         self.stream = None
 
     # ---- space --------------------------------------------------------------
@@ -335,6 +336,14 @@ class QueryBuilder:
         self.spatial_order = bool(on)
         return self
 
+    def with_engine(self, engine: Optional[str]) -> "QueryBuilder":
+        """Force the kernel variant: "warp" (one warp per query) or "thread"
+        (one thread per query); None lets the library choose.  Same results."""
+        if engine not in (None, "warp", "thread"):
+            raise ValueError("engine must be None, 'warp' or 'thread'")
+        self.engine = engine
+        return self
+
     def on_stream(self, stream) -> "QueryBuilder":
         self.stream = stream
         return self
@@ -357,7 +366,9 @@ class QueryBuilder:
         d.sorted = int(self.sorted)
         d.periodic_box = self.box.ctypes.data if self.box is not None else None
         d.flags = (C.FLAG_HOST_BUFFERS if host else 0) | (
-            C.FLAG_SPATIAL_ORDER if self.spatial_order else 0)
+            C.FLAG_SPATIAL_ORDER if self.spatial_order else 0) | (
+            C.FLAG_ENGINE_WARP if self.engine == "warp" else 0) | (
+            C.FLAG_ENGINE_THREAD if self.engine == "thread" else 0)
         return d
 
     def traversal_stats(self):

@@ -24,6 +24,8 @@ NEAREST_ONE, APPROX_NEAREST_ONE, NEAREST_N, NEAREST_N_WITHIN, WITHIN, WITHIN_UNS
     BEST_N_WITHIN = range(7)
 FLAG_HOST_BUFFERS = 0x1
 FLAG_SPATIAL_ORDER = 0x2
+FLAG_ENGINE_WARP = 0x4
+FLAG_ENGINE_THREAD = 0x8
 
 # Every symbol include/kiddo_gpu.h declares.
 EXPORTED_SYMBOLS = [

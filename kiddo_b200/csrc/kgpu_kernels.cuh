@@ -7,6 +7,7 @@
 
 #include "kgpu_device.cuh"
 #include "kgpu_launch.h"
+#include "kgpu_thread.cuh"
 
 namespace kgpu {
 
@@ -123,6 +124,99 @@ __global__ void __launch_bounds__(256) k_within_fill(TreeView<A> tv, const A* __
     TravStats st;
     warp_arith_query<A, K, M>(tv, q, pol, lane, st);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Thread-per-query kernels.  Dynamic shared memory: one continuation slot per
+// level per thread, (max_stem_level + 1) * blockDim values of A.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void flush_stats(unsigned long long* stats, const TravStats& st) {
+  const unsigned s0 = __reduce_add_sync(FULL, st.stems);
+  const unsigned s1 = __reduce_add_sync(FULL, st.leaves);
+  const unsigned s2 = __reduce_add_sync(FULL, st.points);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(stats + 0, (unsigned long long)s0);
+    atomicAdd(stats + 1, (unsigned long long)s1);
+    atomicAdd(stats + 2, (unsigned long long)s2);
+  }
+}
+
+template <typename A, int K, typename M, int FAM, bool EXCL, int KC>
+__global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv, const A* __restrict__ Q,
+                                                const uint32_t* __restrict__ order, uint64_t nq,
+                                                int k, A radius, A* __restrict__ out_d,
+                                                uint32_t* __restrict__ out_i,
+                                                uint32_t* __restrict__ out_c,
+                                                unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  const int stride = blockDim.x;
+  TravStats st;
+  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nq;
+       w += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t qi = order ? order[w] : w;
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    if constexpr (FAM == KF_NEAREST_ONE) {
+      TNearestOne<A, K, M> pol;
+      thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
+      out_d[qi] = pol.best;
+      out_i[qi] = pol.item;
+      if (out_c) out_c[qi] = 1;
+    } else if constexpr (FAM == KF_APPROX) {
+      TNearestOne<A, K, M> pol;
+      if (tv.leaf_count > 0) {
+        st.points += pol.leaf(tv, straight_leaf<A, K>(tv, q), q);
+        st.stems += uint32_t(tv.max_stem_level + 1);
+        st.leaves += 1;
+      }
+      out_d[qi] = pol.best;
+      out_i[qi] = pol.item;
+      if (out_c) out_c[qi] = 1;
+    } else if constexpr (FAM == KF_NEAREST_N) {
+      TNearestN<A, K, M, EXCL, KC, false> pol(k, radius);
+      thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
+      pol.write(qi, out_d, out_i, out_c, false);
+    } else {
+      TBestN<A, K, M, EXCL, KC> pol(k, radius);
+      thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
+      pol.write(qi, out_d, out_i, out_c);
+    }
+  }
+  if (stats) flush_stats(stats, st);
+}
+
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv, const A* __restrict__ Q,
+                                                 const uint32_t* __restrict__ order, uint64_t nq,
+                                                 A radius, uint64_t* __restrict__ counts,
+                                                 const uint64_t* __restrict__ offsets,
+                                                 A* __restrict__ out_d,
+                                                 uint32_t* __restrict__ out_i,
+                                                 unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  const int stride = blockDim.x;
+  TravStats st;
+  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nq;
+       w += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t qi = order ? order[w] : w;
+    uint64_t o = 0, cap = 0;
+    if (offsets) {
+      o = offsets[qi];
+      cap = offsets[qi + 1] - o;
+      if (cap == 0) continue;
+    }
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    TWithin<A, K, M, EXCL> pol(radius, cap, offsets ? out_d + o : nullptr,
+                               offsets ? out_i + o : nullptr);
+    thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
+    if (counts) counts[qi] = pol.count;
+  }
+  if (stats) flush_stats(stats, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -364,6 +458,42 @@ __global__ void __launch_bounds__(256) k_seg_sort_block(const uint64_t* __restri
       }
       __syncthreads();
     }
+  }
+}
+
+}  // namespace kgpu
+
+namespace kgpu {
+
+// ---------------------------------------------------------------------------
+// Leaf-bucketed processing order (KGPU_FLAG_SPATIAL_ORDER): each query's
+// straight-descent leaf (traits/stem_strategy.rs:182-200) is its bucket; a
+// counting sort over buckets gives an order in which neighbouring threads
+// walk the same stems and leaves.  Results do not depend on the order.
+// ---------------------------------------------------------------------------
+template <typename A, int K>
+__global__ void __launch_bounds__(256) k_leaf_histogram(TreeView<A> tv, const A* __restrict__ Q,
+                                                        uint64_t nq, uint32_t* __restrict__ leaf_of,
+                                                        unsigned long long* __restrict__ counts) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nq;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    A q[K];
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + i * K + d);
+    const uint32_t l = tv.leaf_count > 1 ? straight_leaf<A, K>(tv, q) : 0u;
+    leaf_of[i] = l;
+    atomicAdd(counts + l, 1ull);
+  }
+}
+
+static __global__ void __launch_bounds__(256) k_leaf_scatter(const uint32_t* __restrict__ leaf_of,
+                                                      uint64_t nq,
+                                                      unsigned long long* __restrict__ cursor,
+                                                      uint32_t* __restrict__ order) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nq;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    const unsigned long long pos = atomicAdd(cursor + leaf_of[i], 1ull);
+    order[pos] = uint32_t(i);
   }
 }
 

@@ -37,6 +37,7 @@ struct QueryLaunch {
   uint32_t* out_i = nullptr;
   uint32_t* out_c = nullptr;
   unsigned long long* stats = nullptr;  // optional [stems, leaves, points] totals
+  int engine = 0;                 // 0 auto, 1 warp per query, 2 thread per query
   bool periodic = false;          // periodic boundary conditions
   double box[4] = {0, 0, 0, 0};   // periodic box (converted to A)
   cudaStream_t stream = nullptr;
@@ -50,6 +51,13 @@ template <typename A> cudaError_t launch_within_count(const DeviceTree& t, const
                                                        uint64_t* counts);
 template <typename A> cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
                                                       const uint64_t* offsets);
+// Processing order grouped by straight-descent leaf.  `scratch` must hold
+// spatial_order_scratch_bytes(t, nq) bytes; order[nq] receives query indices.
+size_t spatial_order_scratch_bytes(const DeviceTree& t, uint64_t nq);
+template <typename A> cudaError_t launch_spatial_order(const DeviceTree& t, const void* queries,
+                                                       uint64_t nq, uint32_t* order,
+                                                       void* scratch, cudaStream_t s);
+
 // Stable sort of every CSR segment by distance; scratch holds total entries.
 template <typename A> cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d,
                                                   uint32_t* it, A* scratch_d,

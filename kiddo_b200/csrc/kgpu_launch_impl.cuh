@@ -57,6 +57,33 @@ inline cudaError_t with_excl(bool e, F&& f) {
   return f(std::false_type());
 }
 
+// Dynamic shared memory of the thread-per-query kernels.
+template <typename A>
+inline size_t thread_smem(const DeviceTree& t) {
+  return size_t(t.max_stem_level + 2) * 256 * sizeof(A);
+}
+
+template <typename F>
+inline cudaError_t with_kc(int k, F&& f) {
+  if (k <= 1) return f(std::integral_constant<int, 1>());
+  if (k <= 4) return f(std::integral_constant<int, 4>());
+  if (k <= 8) return f(std::integral_constant<int, 8>());
+  if (k <= 16) return f(std::integral_constant<int, 16>());
+  return f(std::integral_constant<int, 32>());
+}
+
+// Thread per query unless the warp engine is requested, or the family needs
+// the warp engine's arrival-order output (.unsorted() nearest_n with k <= 24,
+// ThresholdVec::into_vec).
+inline bool use_thread_engine(const QueryLaunch& q) {
+  if (q.engine == 1 || q.periodic) return false;
+  if (q.engine == 2) return !(q.family != KGPU_BEST_N_WITHIN && !q.sorted && q.k <= 24 &&
+                             (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN));
+  if ((q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN) && !q.sorted && q.k <= 24)
+    return false;
+  return true;
+}
+
 template <typename A>
 cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   const TreeView<A> tv = make_view<A>(t);
@@ -89,6 +116,34 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
           if (q.family == KGPU_NEAREST_ONE) return runp(k_periodic_fixed<A, K, M, KF_NEAREST_ONE, false>);
           if (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN)
             return runp(k_periodic_fixed<A, K, M, KF_NEAREST_N, EX>);
+          return cudaErrorInvalidValue;
+        }
+        if (use_thread_engine(q)) {
+          const size_t smem = thread_smem<A>(t);
+          auto runt = [&](auto kern) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+            kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order,
+                                                q.nq, q.k, radius, static_cast<A*>(q.out_d),
+                                                q.out_i, q.out_c, q.stats);
+            g_launches++;
+            return cudaGetLastError();
+          };
+          switch (q.family) {
+            case KGPU_NEAREST_ONE:
+              return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false, 1>);
+            case KGPU_APPROX_NEAREST_ONE:
+              return runt(k_tfixed<A, K, M, KF_APPROX, false, 1>);
+            case KGPU_NEAREST_N:
+            case KGPU_NEAREST_N_WITHIN:
+              return with_kc(q.k, [&](auto kc) {
+                return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX, decltype(kc)::value>);
+              });
+            case KGPU_BEST_N_WITHIN:
+              return with_kc(q.k, [&](auto kc) {
+                return runt(k_tfixed<A, K, M, KF_BEST_N, EX, decltype(kc)::value>);
+              });
+          }
           return cudaErrorInvalidValue;
         }
         switch (q.family) {
@@ -128,6 +183,16 @@ cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint6
           g_launches++;
           return cudaGetLastError();
         }
+        if (q.engine != 1) {
+          const size_t smem = thread_smem<A>(t);
+          auto kern = k_twithin<A, K, M, EX>;
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+          const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+          kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                              radius, counts, nullptr, nullptr, nullptr, q.stats);
+          g_launches++;
+          return cudaGetLastError();
+        }
         auto kern = k_within_count<A, K, M, EX>;
         const int grid = grid_for(kern, 0, q.nq);
         kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
@@ -158,6 +223,17 @@ cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
           kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
                                            box, radius, offsets, static_cast<A*>(q.out_d),
                                            q.out_i);
+          g_launches++;
+          return cudaGetLastError();
+        }
+        if (q.engine != 1) {
+          const size_t smem = thread_smem<A>(t);
+          auto kern = k_twithin<A, K, M, EX>;
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+          const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+          kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
+                                              radius, nullptr, offsets, static_cast<A*>(q.out_d),
+                                              q.out_i, nullptr);
           g_launches++;
           return cudaGetLastError();
         }
@@ -195,14 +271,55 @@ cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d, uint32_t
   return cudaGetLastError();
 }
 
+
+template <typename A>
+cudaError_t launch_spatial_order(const DeviceTree& t, const void* queries, uint64_t nq,
+                                 uint32_t* order, void* scratch, cudaStream_t s) {
+  const TreeView<A> tv = make_view<A>(t);
+  const uint64_t nl = t.leaf_count > 0 ? t.leaf_count : 1;
+  // scratch layout: leaf_of[nq] u32 | counts[nl + 1] u64 | scan tiles
+  uint8_t* p = static_cast<uint8_t*>(scratch);
+  uint32_t* leaf_of = reinterpret_cast<uint32_t*>(p);
+  p += ((nq * 4 + 255) / 256) * 256;
+  unsigned long long* counts = reinterpret_cast<unsigned long long*>(p);
+  p += (((nl + 1) * 8 + 255) / 256) * 256;
+  void* tiles = p;
+  cudaError_t e = cudaMemsetAsync(counts, 0, (nl + 1) * 8, s);
+  if (e != cudaSuccess) return e;
+  e = with_dims(t.dims, [&](auto kk) {
+    constexpr int K = decltype(kk)::value;
+    auto kern = k_leaf_histogram<A, K>;
+    const int grid = grid_for(kern, 0, (nq + 31) / 32);
+    kern<<<grid, 256, 0, s>>>(tv, static_cast<const A*>(queries), nq, leaf_of, counts);
+    g_launches++;
+    return cudaGetLastError();
+  });
+  if (e != cudaSuccess) return e;
+  e = launch_exclusive_scan(reinterpret_cast<uint64_t*>(counts), reinterpret_cast<uint64_t*>(counts),
+                            nl, tiles, s);
+  if (e != cudaSuccess) return e;
+  {
+    auto kern = k_leaf_scatter;
+    const int grid = grid_for(kern, 0, (nq + 31) / 32);
+    kern<<<grid, 256, 0, s>>>(leaf_of, nq, counts, order);
+    g_launches++;
+  }
+  return cudaGetLastError();
+}
 }  // namespace kgpu
 
-#define KGPU_INSTANTIATE(A)                                                                      \
+#define KGPU_INSTANTIATE_FIXED(A)                                                                \
   namespace kgpu {                                                                               \
   template cudaError_t launch_fixed<A>(const DeviceTree&, const QueryLaunch&);                   \
+  }
+
+#define KGPU_INSTANTIATE_RADIUS(A)                                                               \
+  namespace kgpu {                                                                               \
   template cudaError_t launch_within_count<A>(const DeviceTree&, const QueryLaunch&, uint64_t*); \
   template cudaError_t launch_within_fill<A>(const DeviceTree&, const QueryLaunch&,              \
                                              const uint64_t*);                                   \
   template cudaError_t launch_seg_sort<A>(const uint64_t*, uint64_t, A*, uint32_t*, A*,          \
                                           uint32_t*, cudaStream_t);                              \
+  template cudaError_t launch_spatial_order<A>(const DeviceTree&, const void*, uint64_t,         \
+                                               uint32_t*, void*, cudaStream_t);                  \
   }

@@ -35,11 +35,15 @@ DATASETS = {
 }
 
 
+ENGINES = [None, "warp", "thread"]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("dims", [2, 3])
 @pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
 @pytest.mark.parametrize("data", ["uniform", "quantized", "clustered"])
-def test_fixed_families(dtype, dims, metric, data):
+def test_fixed_families(dtype, dims, metric, data, engine):
     rng = np.random.default_rng(zlib.crc32(f"{dims}{metric}{data}".encode()))
     n = 20000
     P = DATASETS[data](rng, n, dims, dtype)
@@ -47,24 +51,24 @@ def test_fixed_families(dtype, dims, metric, data):
     t, o = _pair(P)
     M = _metric(metric)
     # nearest_one
-    g = t.query(Q).nearest_one(M).execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_one(M).execute_gpu()
     od, oi = o.nearest_one(Q, metric=metric)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "nearest_one")
     # approx
-    g = t.query(Q).nearest_one(M).approx().execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_one(M).approx().execute_gpu()
     od, oi = o.approx_nearest_one(Q, metric=metric)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "approx")
     # nearest_n, sorted and unsorted, and .within
     r = 0.001 if metric == "sqeuclidean" else 0.03
     for k in (1, 5, 16, 32):
-        g = t.query(Q).nearest_n(M, k).execute_gpu()
+        g = t.query(Q).with_engine(engine).nearest_n(M, k).execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, k, metric=metric),
                           f"nearest_n({k})")
-        g = t.query(Q).nearest_n(M, k).unsorted().execute_gpu()
+        g = t.query(Q).with_engine(engine).nearest_n(M, k).unsorted().execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts,
                           *o.nearest_n(Q, k, metric=metric, sorted=False), f"unsorted({k})")
         for excl in (False, True):
-            b = t.query(Q).nearest_n(M, k).within(r)
+            b = t.query(Q).with_engine(engine).nearest_n(M, k).within(r)
             if excl:
                 b = b.exclusive_boundaries()
             g = b.execute_gpu()
@@ -73,7 +77,7 @@ def test_fixed_families(dtype, dims, metric, data):
                               f"nearest_n({k}).within excl={excl}")
     # best_n_within
     for excl in (False, True):
-        b = t.query(Q).best_n_within(M, r, 5)
+        b = t.query(Q).with_engine(engine).best_n_within(M, r, 5)
         if excl:
             b = b.exclusive_boundaries()
         g = b.execute_gpu()
@@ -81,10 +85,11 @@ def test_fixed_families(dtype, dims, metric, data):
                           *o.best_n_within(Q, r, 5, metric=metric, exclusive=excl), "best_n")
 
 
+@pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
 @pytest.mark.parametrize("data", ["uniform", "quantized"])
-def test_within_families(dtype, metric, data):
+def test_within_families(dtype, metric, data, engine):
     rng = np.random.default_rng(11)
     P = DATASETS[data](rng, 30000, 3, dtype)
     Q = DATASETS[data](rng, 2000, 3, dtype)
@@ -98,7 +103,7 @@ def test_within_families(dtype, metric, data):
         Qr = Q[:nq]
         for excl in (False, True):
             for sorted_ in (True, False):
-                b = t.query(Qr).within(M, r)
+                b = t.query(Qr).with_engine(engine).within(M, r)
                 if not sorted_:
                     b = b.unsorted()
                 if excl:
@@ -109,25 +114,27 @@ def test_within_families(dtype, metric, data):
                                 f"within r={r} excl={excl} sorted={sorted_}")
 
 
+@pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("n", [0, 1, 2, 31, 32, 33, 47, 64, 65, 1000])
-def test_small_and_ragged_trees(n):
+def test_small_and_ragged_trees(n, engine):
     rng = np.random.default_rng(n)
     P = rng.random((n, 3))
     Q = rng.random((300, 3))
     t, o = _pair(P)
-    g = t.query(Q).nearest_one(kb.SquaredEuclidean).execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_one(kb.SquaredEuclidean).execute_gpu()
     od, oi = o.nearest_one(Q)
     assert_same_fixed(g.distances, g.items, np.ones(300), od, oi, np.ones(300), "nn1")
-    g = t.query(Q).nearest_n(kb.SquaredEuclidean, 7).execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_n(kb.SquaredEuclidean, 7).execute_gpu()
     assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, 7), "nn7")
-    g = t.query(Q).nearest_one(kb.SquaredEuclidean).approx().execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_one(kb.SquaredEuclidean).approx().execute_gpu()
     od, oi = o.approx_nearest_one(Q)
     assert_same_fixed(g.distances, g.items, np.ones(300), od, oi, np.ones(300), "approx")
-    g = t.query(Q).within(kb.SquaredEuclidean, 0.05).execute_gpu()
+    g = t.query(Q).with_engine(engine).within(kb.SquaredEuclidean, 0.05).execute_gpu()
     assert_same_csr((g.offsets, g.distances, g.items), o.within(Q, 0.05), "within")
 
 
-def test_duplicate_heavy_tree():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_duplicate_heavy_tree(engine):
     """Unsplittable chunks (construction.rs:1137-1150) give long and empty leaves."""
     rng = np.random.default_rng(3)
     P = np.concatenate([np.zeros((900, 3)), np.repeat(rng.random((20, 3)), 40, axis=0),
@@ -135,36 +142,38 @@ def test_duplicate_heavy_tree():
     Q = np.concatenate([rng.random((500, 3)), P[::50]])
     t, o = _pair(P)
     assert t.max_leaf_len() >= 900
-    g = t.query(Q).nearest_one(kb.SquaredEuclidean).execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_one(kb.SquaredEuclidean).execute_gpu()
     od, oi = o.nearest_one(Q)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "nn1")
     for k in (3, 32):
-        g = t.query(Q).nearest_n(kb.SquaredEuclidean, k).execute_gpu()
+        g = t.query(Q).with_engine(engine).nearest_n(kb.SquaredEuclidean, k).execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, k), f"nn{k}")
-    g = t.query(Q).within(kb.SquaredEuclidean, 0.01).execute_gpu()
+    g = t.query(Q).with_engine(engine).within(kb.SquaredEuclidean, 0.01).execute_gpu()
     assert_same_csr((g.offsets, g.distances, g.items), o.within(Q, 0.01), "within")
 
 
-def test_explicit_items_best_n():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_explicit_items_best_n(engine):
     rng = np.random.default_rng(5)
     P = rng.random((50000, 3)).astype(np.float32)
     items = rng.permutation(50000).astype(np.uint32)
     Q = rng.random((3000, 3)).astype(np.float32)
     t, o = _pair(P, items)
     for r in (1e-4, 1e-3):
-        g = t.query(Q).best_n_within(kb.SquaredEuclidean, r, 5).execute_gpu()
+        g = t.query(Q).with_engine(engine).best_n_within(kb.SquaredEuclidean, r, 5).execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts, *o.best_n_within(Q, r, 5), "best_n")
 
 
-def test_gaussian_mixture_knn16():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_gaussian_mixture_knn16(engine):
     """Medium case with the C2 shape (f32 mixture, dense clumps, in-leaf ties)."""
     rng = np.random.default_rng(2)
     P = gaussian_mixture(1_000_000, 1024, 0.005, 0.2, rng)
     Q = gaussian_mixture(50_000, 1024, 0.005, 0.2, rng)
     t, o = _pair(P)
-    g = t.query(Q).nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
     assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, 16), "gm knn16")
-    g = t.query(Q).nearest_one(kb.SquaredEuclidean).approx().execute_gpu()
+    g = t.query(Q).with_engine(engine).nearest_one(kb.SquaredEuclidean).approx().execute_gpu()
     od, oi = o.approx_nearest_one(Q)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "gm approx")
 
@@ -222,3 +231,47 @@ def test_known_answers_on_gpu():
                 assert items[0] == chk["expect_first_item"], kat["name"]
             if "expect_item_set" in chk:
                 assert sorted(items) == chk["expect_item_set"], kat["name"]
+
+
+def test_engines_report_identical_traversal_counters():
+    """Both kernels walk exactly the reference's traversal: equal stem, leaf and
+    point counts (exact_query_stats.rs:23-60) for every query family."""
+    rng = np.random.default_rng(21)
+    P = rng.random((40000, 3)).astype(np.float32)
+    Q = rng.random((5000, 3)).astype(np.float32)
+    t = kb.ImmutableKdTree.new_from_slice(P)
+    o = oracle.OracleTree.build(P)
+    for fam in ("nn1", "approx", "knn", "best", "within"):
+        stats = []
+        for engine in ("warp", "thread"):
+            b = t.query(Q).with_engine(engine)
+            if fam == "nn1":
+                b = b.nearest_one(kb.SquaredEuclidean)
+            elif fam == "approx":
+                b = b.nearest_one(kb.SquaredEuclidean).approx()
+            elif fam == "knn":
+                b = b.nearest_n(kb.SquaredEuclidean, 16)
+            elif fam == "best":
+                b = b.best_n_within(kb.SquaredEuclidean, 1e-3, 5)
+            else:
+                b = b.within(kb.SquaredEuclidean, 1e-3)
+            stats.append(b.traversal_stats())
+        assert np.array_equal(stats[0], stats[1]), fam
+        if fam == "knn":
+            _, _, _, ost = o.nearest_n(Q, 16, stats=True)
+            assert np.array_equal(stats[0], ost)
+
+
+@pytest.mark.parametrize("engine", ["warp", "thread"])
+def test_spatial_order_gives_identical_results(engine):
+    rng = np.random.default_rng(31)
+    P = gaussian_mixture(200_000, 64, 0.01, 0.2, rng)
+    Q = gaussian_mixture(30_000, 64, 0.01, 0.2, rng)
+    t, o = _pair(P)
+    g = t.query(Q).with_engine(engine).with_spatial_order().nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
+    assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, 16), "ordered knn16")
+    g = t.query(Q).with_engine(engine).with_spatial_order().nearest_one(kb.SquaredEuclidean).execute_gpu()
+    od, oi = o.nearest_one(Q)
+    assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "ordered nn1")
+    g = t.query(Q).with_engine(engine).with_spatial_order().within(kb.SquaredEuclidean, 1e-4).execute_gpu()
+    assert_same_csr((g.offsets, g.distances, g.items), o.within(Q, 1e-4), "ordered within")
