@@ -22,8 +22,20 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-f
               "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]
 
-CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kernels_f32_fixed.cu",
-              "kernels_f32_radius.cu", "kernels_f64_fixed.cu", "kernels_f64_radius.cu"]
+CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu",
+              "kernels_f32_warp.cu",
+              "kernels_f32_t1.cu",
+              "kernels_f32_t4.cu",
+              "kernels_f32_t8.cu",
+              "kernels_f32_t16.cu",
+              "kernels_f32_radius.cu",
+              "kernels_f64_warp.cu",
+              "kernels_f64_t1.cu",
+              "kernels_f64_t4.cu",
+              "kernels_f64_t8.cu",
+              "kernels_f64_t16.cu",
+              "kernels_f64_radius.cu",
+              ]
 CXX_SOURCES = ["layout_build.cpp"]
 HEADERS = ["kgpu_device.cuh", "kgpu_kernels.cuh", "kgpu_launch.h", "kgpu_launch_impl.cuh",
            "kgpu_internal.h", "kgpu_tree_impl.h", "kgpu_thread.cuh"]

@@ -1,0 +1,4 @@
+// kernels_f32_t4.cu — thread-per-query kernels with a 4-slot list for float coordinates.
+#include "kgpu_launch_impl.cuh"
+
+KGPU_INSTANTIATE_THREAD(float, 4)

@@ -1,0 +1,4 @@
+// kernels_f64_t4.cu — thread-per-query kernels with a 4-slot list for double coordinates.
+#include "kgpu_launch_impl.cuh"
+
+KGPU_INSTANTIATE_THREAD(double, 4)

@@ -313,7 +313,23 @@ void apply_periodic(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch&
                                     : double(static_cast<const float*>(d->periodic_box)[a]);
 }
 
+template <typename A>
+cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
+  const bool list_family = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
+                           q.family == KGPU_BEST_N_WITHIN;
+  const bool thread = q.engine != 1 && !q.periodic && (t.dims == 2 || t.dims == 3) &&
+                      (!list_family || q.k <= 16);
+  if (!thread) return launch_wfixed<A>(t, q);
+  if (!list_family || q.k <= 1) return launch_tfixed<A, 1>(t, q);
+  if (q.k <= 4) return launch_tfixed<A, 4>(t, q);
+  if (q.k <= 8) return launch_tfixed<A, 8>(t, q);
+  return launch_tfixed<A, 16>(t, q);
+}
+template cudaError_t launch_fixed<float>(const DeviceTree&, const QueryLaunch&);
+template cudaError_t launch_fixed<double>(const DeviceTree&, const QueryLaunch&);
+
 namespace {
+
 
 // With KGPU_FLAG_SPATIAL_ORDER, group the batch by straight-descent leaf and
 // hand the kernels that processing order (same results, better locality).

@@ -144,7 +144,8 @@ __device__ __forceinline__ void flush_stats(unsigned long long* stats, const Tra
 template <typename A, int K, typename M, int FAM, bool EXCL, int KC>
 __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv, const A* __restrict__ Q,
                                                 const uint32_t* __restrict__ order, uint64_t nq,
-                                                int k, A radius, A* __restrict__ out_d,
+                                                int k, A radius, int arrival_order,
+                                                A* __restrict__ out_d,
                                                 uint32_t* __restrict__ out_i,
                                                 uint32_t* __restrict__ out_c,
                                                 unsigned long long* __restrict__ stats) {
@@ -175,9 +176,9 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv, const A* __restr
       out_i[qi] = pol.item;
       if (out_c) out_c[qi] = 1;
     } else if constexpr (FAM == KF_NEAREST_N) {
-      TNearestN<A, K, M, EXCL, KC, false> pol(k, radius);
+      TNearestN<A, K, M, EXCL, KC> pol(k, radius);
       thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
-      pol.write(qi, out_d, out_i, out_c, false);
+      pol.write(qi, out_d, out_i, out_c, arrival_order != 0);
     } else {
       TBestN<A, K, M, EXCL, KC> pol(k, radius);
       thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);

@@ -46,7 +46,11 @@ struct QueryLaunch {
 // process-wide count of kernel launches made by this library
 extern std::atomic<uint64_t> g_launches;
 
+// Fixed-size families: dispatches to the thread engine (2-D/3-D trees, k <= 16)
+// or the warp engine (everything else, periodic included).
 template <typename A> cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q);
+template <typename A> cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q);
+template <typename A, int KC> cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q,
                                                        uint64_t* counts);
 template <typename A> cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,

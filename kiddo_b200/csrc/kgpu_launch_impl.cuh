@@ -72,20 +72,16 @@ inline cudaError_t with_kc(int k, F&& f) {
   return f(std::integral_constant<int, 32>());
 }
 
-// Thread per query unless the warp engine is requested, or the family needs
-// the warp engine's arrival-order output (.unsorted() nearest_n with k <= 24,
-// ThresholdVec::into_vec).
-inline bool use_thread_engine(const QueryLaunch& q) {
-  if (q.engine == 1 || q.periodic) return false;
-  if (q.engine == 2) return !(q.family != KGPU_BEST_N_WITHIN && !q.sorted && q.k <= 24 &&
-                             (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN));
-  if ((q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN) && !q.sorted && q.k <= 24)
-    return false;
-  return true;
+// Thread per query for 2-D and 3-D trees unless the warp engine is requested
+// or periodic boundaries (served by the warp kernels) are on; other
+// dimensionalities use the warp kernels (same results).
+constexpr bool thread_engine_dims(int K) { return K == 2 || K == 3; }
+inline bool use_thread_engine(const QueryLaunch& q, int dims) {
+  return q.engine != 1 && !q.periodic && thread_engine_dims(dims);
 }
 
 template <typename A>
-cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
+cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
   const TreeView<A> tv = make_view<A>(t);
   const A radius = A(q.radius);
   return with_dims(t.dims, [&](auto kk) {
@@ -118,34 +114,6 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
             return runp(k_periodic_fixed<A, K, M, KF_NEAREST_N, EX>);
           return cudaErrorInvalidValue;
         }
-        if (use_thread_engine(q)) {
-          const size_t smem = thread_smem<A>(t);
-          auto runt = [&](auto kern) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
-            kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order,
-                                                q.nq, q.k, radius, static_cast<A*>(q.out_d),
-                                                q.out_i, q.out_c, q.stats);
-            g_launches++;
-            return cudaGetLastError();
-          };
-          switch (q.family) {
-            case KGPU_NEAREST_ONE:
-              return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false, 1>);
-            case KGPU_APPROX_NEAREST_ONE:
-              return runt(k_tfixed<A, K, M, KF_APPROX, false, 1>);
-            case KGPU_NEAREST_N:
-            case KGPU_NEAREST_N_WITHIN:
-              return with_kc(q.k, [&](auto kc) {
-                return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX, decltype(kc)::value>);
-              });
-            case KGPU_BEST_N_WITHIN:
-              return with_kc(q.k, [&](auto kc) {
-                return runt(k_tfixed<A, K, M, KF_BEST_N, EX, decltype(kc)::value>);
-              });
-          }
-          return cudaErrorInvalidValue;
-        }
         switch (q.family) {
           case KGPU_NEAREST_ONE:
             return run(k_fixed<A, K, M, KF_NEAREST_ONE, false>);
@@ -160,6 +128,46 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
         return cudaErrorInvalidValue;
       });
     });
+  });
+}
+
+// Thread-per-query fixed-size families for one list size KC (nearest_one and
+// approx use KC == 1).  Only 2-D and 3-D trees; the caller checks.
+template <typename A, int KC>
+cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
+  const TreeView<A> tv = make_view<A>(t);
+  const A radius = A(q.radius);
+  const size_t smem = thread_smem<A>(t);
+  return with_dims(t.dims, [&](auto kk) -> cudaError_t {
+    constexpr int K = decltype(kk)::value;
+    if constexpr (!thread_engine_dims(K)) {
+      return cudaErrorInvalidValue;
+    } else {
+      return with_metric(q.metric, [&](auto m) {
+        using M = decltype(m);
+        return with_excl(q.exclusive, [&](auto ex) {
+          constexpr bool EX = decltype(ex)::value;
+          auto runt = [&](auto kern) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+            kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order,
+                                                q.nq, q.k, radius, q.sorted ? 0 : 1,
+                                                static_cast<A*>(q.out_d), q.out_i, q.out_c,
+                                                q.stats);
+            g_launches++;
+            return cudaGetLastError();
+          };
+          if constexpr (KC == 1) {
+            if (q.family == KGPU_NEAREST_ONE) return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false, 1>);
+            if (q.family == KGPU_APPROX_NEAREST_ONE) return runt(k_tfixed<A, K, M, KF_APPROX, false, 1>);
+          }
+          if (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN)
+            return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX, KC>);
+          if (q.family == KGPU_BEST_N_WITHIN) return runt(k_tfixed<A, K, M, KF_BEST_N, EX, KC>);
+          return cudaErrorInvalidValue;
+        });
+      });
+    }
   });
 }
 
@@ -183,7 +191,7 @@ cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint6
           g_launches++;
           return cudaGetLastError();
         }
-        if (q.engine != 1) {
+        if constexpr (thread_engine_dims(K)) if (q.engine != 1) {
           const size_t smem = thread_smem<A>(t);
           auto kern = k_twithin<A, K, M, EX>;
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -226,7 +234,7 @@ cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
           g_launches++;
           return cudaGetLastError();
         }
-        if (q.engine != 1) {
+        if constexpr (thread_engine_dims(K)) if (q.engine != 1) {
           const size_t smem = thread_smem<A>(t);
           auto kern = k_twithin<A, K, M, EX>;
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -308,9 +316,14 @@ cudaError_t launch_spatial_order(const DeviceTree& t, const void* queries, uint6
 }
 }  // namespace kgpu
 
-#define KGPU_INSTANTIATE_FIXED(A)                                                                \
+#define KGPU_INSTANTIATE_WARP(A)                                                                 \
   namespace kgpu {                                                                               \
-  template cudaError_t launch_fixed<A>(const DeviceTree&, const QueryLaunch&);                   \
+  template cudaError_t launch_wfixed<A>(const DeviceTree&, const QueryLaunch&);                  \
+  }
+
+#define KGPU_INSTANTIATE_THREAD(A, KC)                                                           \
+  namespace kgpu {                                                                               \
+  template cudaError_t launch_tfixed<A, KC>(const DeviceTree&, const QueryLaunch&);              \
   }
 
 #define KGPU_INSTANTIATE_RADIUS(A)                                                               \

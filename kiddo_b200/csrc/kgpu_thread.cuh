@@ -22,6 +22,15 @@ namespace kgpu {
 
 // Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
 // leaf_view/mod.rs:431-446): f(coords, item) in tile order.
+template <typename A> struct Pair;
+template <> struct Pair<float> { using T = float2; };
+template <> struct Pair<double> { using T = double2; };
+
+// Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
+// leaf_view/mod.rs:431-446): f(coords, item) in tile order.  Tiles of width
+// >= 2 are read two points per step (8-byte aligned pairs for f32: leaves
+// start on 8 bytes and every column of an even-width tile spans an even
+// number of floats).
 template <typename A, int K, typename F>
 __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint32_t leaf,
                                                           F&& f) {
@@ -33,11 +42,35 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
     const uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
     const A* col = reinterpret_cast<const A*>(base + boff);
     const uint32_t* its = reinterpret_cast<const uint32_t*>(base + boff + K * w * sizeof(A));
-    for (uint32_t i = 0; i < w; ++i) {
+    if (w >= 2) {
+      for (uint32_t i = 0; i < w; i += 2) {
+        A c0[K], c1[K];
+        if constexpr (sizeof(A) == 4) {
+#pragma unroll
+          for (int d = 0; d < K; ++d) {
+            const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
+            c0[d] = v.x;
+            c1[d] = v.y;
+          }
+          const uint2 it = __ldg(reinterpret_cast<const uint2*>(its + i));
+          f(c0, it.x);
+          f(c1, it.y);
+        } else {
+#pragma unroll
+          for (int d = 0; d < K; ++d) {
+            c0[d] = __ldg(col + d * w + i);
+            c1[d] = __ldg(col + d * w + i + 1);
+          }
+          const uint32_t i0 = __ldg(its + i), i1 = __ldg(its + i + 1);
+          f(c0, i0);
+          f(c1, i1);
+        }
+      }
+    } else {
       A c[K];
 #pragma unroll
-      for (int d = 0; d < K; ++d) c[d] = __ldg(col + d * w + i);
-      f(c, __ldg(its + i));
+      for (int d = 0; d < K; ++d) c[d] = __ldg(col + d);
+      f(c, __ldg(its));
     }
     boff += w * (K * sizeof(A) + sizeof(uint32_t));
     rem -= w;
@@ -143,52 +176,88 @@ struct TNearestOne {
   }
 };
 
-// k smallest by (distance, arrival) in a register list of KC slots
-// (ThresholdVecResultCollection, results/result_collection.rs:136-215).
-template <typename A, int K, typename M, bool kExclusive, int KC, bool kTrack>
+// k smallest by (distance, arrival) in a register list of KC slots: the
+// ThresholdVecResultCollection of results/result_collection.rs:136-215.
+// While filling, hits are appended in arrival order; when the k-th arrives the
+// list is sorted once by (distance, arrival) — a stable sort, as std's
+// small-slice sort is — and later hits are inserted after equal distances,
+// evicting the last.  A list that never fills stays in arrival order, which is
+// exactly ThresholdVec::into_vec; the sorted output sorts it at the end.
+template <typename A, int K, typename M, bool kExclusive, int KC>
 struct TNearestN {
   static constexpr bool kPruneOnEqual = kExclusive;
   A ld[KC];
   uint32_t li[KC];
-  uint32_t ls[kTrack ? KC : 1];
   int n, k;
   A radius, kth;
-  uint32_t seq;
-  __device__ TNearestN(int k_, A r) : n(0), k(k_), radius(r), kth(inf_of<A>()), seq(0) {
+  __device__ TNearestN(int k_, A r) : n(0), k(k_), radius(r), kth(inf_of<A>()) {
 #pragma unroll
     for (int j = 0; j < KC; ++j) { ld[j] = inf_of<A>(); li[j] = 0xffffffffu; }
-#pragma unroll
-    for (int j = 0; j < (kTrack ? KC : 1); ++j) ls[j] = 0;
   }
   __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
 
-  __device__ __forceinline__ void add(A d, uint32_t it) {
-    if (n == k && !(d < kth)) return;
-    const int m = n < k ? n + 1 : k;
+  // Stable sort of slots [0, m) by distance (slots >= m hold +inf and stay
+  // behind): bitonic network on (distance, slot) keys.
+  __device__ __forceinline__ void sort_prefix(int m) {
+    uint32_t pos[KC];
 #pragma unroll
-    for (int j = KC - 1; j >= 0; --j) {
-      if (j < m) {
-        if (j > 0 && ld[j - 1] > d) {
-          ld[j] = ld[j - 1];
-          li[j] = li[j - 1];
-          if (kTrack) ls[j] = ls[j - 1];
-        } else if (j == n || ld[j] > d) {
-          ld[j] = d;
-          li[j] = it;
-          if (kTrack) ls[j] = seq;
+    for (int j = 0; j < KC; ++j) pos[j] = j < m ? uint32_t(j) : 0xffffffffu;
+#pragma unroll
+    for (int size = 2; size <= KC; size <<= 1) {
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+        for (int i = 0; i < KC; ++i) {
+          const int j = i ^ stride;
+          if (j > i) {
+            const bool up = (i & size) == 0;
+            const bool gt = ld[i] > ld[j] || (ld[i] == ld[j] && pos[i] > pos[j]);
+            if (gt == up) {
+              const A td = ld[i]; ld[i] = ld[j]; ld[j] = td;
+              const uint32_t ti = li[i]; li[i] = li[j]; li[j] = ti;
+              const uint32_t tp = pos[i]; pos[i] = pos[j]; pos[j] = tp;
+            }
+          }
         }
       }
     }
-    ++seq;
-    n = m;
-    if (n == k) {
-      A t = ld[0];
+  }
+
+  __device__ __forceinline__ void refresh_kth() {
+    A t = ld[0];
 #pragma unroll
-      for (int j = 1; j < KC; ++j)
-        if (j == k - 1) t = ld[j];
-      kth = t;
+    for (int j = 1; j < KC; ++j)
+      if (j == k - 1) t = ld[j];
+    kth = t;
+  }
+
+  __device__ __forceinline__ void add(A d, uint32_t it) {
+    if (n < k) {
+#pragma unroll
+      for (int j = 0; j < KC; ++j)
+        if (j == n) { ld[j] = d; li[j] = it; }
+      ++n;
+      if (n == k) {
+        sort_prefix(k);
+        refresh_kth();
+      }
+      return;
     }
+    if (!(d < kth)) return;
+#pragma unroll
+    for (int j = KC - 1; j >= 0; --j) {
+      if (j < k) {
+        if (j > 0 && ld[j - 1] > d) {
+          ld[j] = ld[j - 1];
+          li[j] = li[j - 1];
+        } else if (ld[j] > d) {
+          ld[j] = d;
+          li[j] = it;
+        }
+      }
+    }
+    refresh_kth();
   }
 
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
@@ -199,32 +268,19 @@ struct TNearestN {
     });
   }
 
-  // ThresholdVec::into_vec keeps arrival order while the list never filled.
   __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
                                         uint32_t* __restrict__ out_i,
-                                        uint32_t* __restrict__ out_c, bool arrival_order) const {
+                                        uint32_t* __restrict__ out_c, bool arrival_order) {
+    if (n < k && !arrival_order) sort_prefix(n);
     A* od = out_d + size_t(qi) * k;
     uint32_t* oi = out_i + size_t(qi) * k;
-    if (kTrack && arrival_order && n < k) {
 #pragma unroll
-      for (int j = 0; j < KC; ++j) {
-        if (j < n) {
-          int rank = 0;
-#pragma unroll
-          for (int t = 0; t < KC; ++t)
-            if (t < n && ls[t] < ls[j]) ++rank;
-          od[rank] = ld[j];
-          oi[rank] = li[j];
-        }
+    for (int j = 0; j < KC; ++j) {
+      if (j < k) {
+        od[j] = j < n ? ld[j] : inf_of<A>();
+        oi[j] = j < n ? li[j] : 0xffffffffu;
       }
-    } else {
-#pragma unroll
-      for (int j = 0; j < KC; ++j)
-        if (j < n) { od[j] = ld[j]; oi[j] = li[j]; }
     }
-#pragma unroll
-    for (int j = 0; j < KC; ++j)
-      if (j >= n && j < k) { od[j] = inf_of<A>(); oi[j] = 0xffffffffu; }
     if (out_c) out_c[qi] = uint32_t(n);
   }
 };
