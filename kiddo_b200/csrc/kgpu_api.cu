@@ -338,10 +338,9 @@ cudaError_t maybe_spatial_order(const DeviceTree& dt, const kgpu_query_desc* d, 
   if (!(d->flags & KGPU_FLAG_SPATIAL_ORDER) || q.nq < 2) return cudaSuccess;
   cudaError_t e;
   if ((e = ob.alloc(q.nq * 4, s)) != cudaSuccess) return e;
-  if ((e = sb.alloc(spatial_order_scratch_bytes(dt, q.nq), s)) != cudaSuccess) return e;
-  e = dt.dtype == KGPU_F64
-          ? launch_spatial_order<double>(dt, q.queries, q.nq, ob.as<uint32_t>(), sb.p, s)
-          : launch_spatial_order<float>(dt, q.queries, q.nq, ob.as<uint32_t>(), sb.p, s);
+  if ((e = sb.alloc(spatial_order_scratch_bytes(dt, q), s)) != cudaSuccess) return e;
+  e = dt.dtype == KGPU_F64 ? launch_spatial_order<double>(dt, q, ob.as<uint32_t>(), sb.p)
+                           : launch_spatial_order<float>(dt, q, ob.as<uint32_t>(), sb.p);
   if (e == cudaSuccess) q.order = ob.as<uint32_t>();
   return e;
 }

@@ -1,5 +1,5 @@
-// kgpu_kernels.cuh — kernels of the query engine and their launchers.
-// Instantiated per coordinate type in kernels_f32.cu / kernels_f64.cu.
+// kgpu_kernels.cuh — kernels of the query engine.  Instantiated per
+// coordinate type and engine in the kernels_*.cu translation units.
 #pragma once
 
 #include <cstdint>
@@ -24,24 +24,86 @@ enum KernelFamily : int {
   KF_BEST_N = 3,
 };
 
+// The batch a kernel answers.  Single tree: `tv`; several trees: query qi
+// belongs to forest[tree_of[qi]].  radii (if set) gives each query its own
+// radius.  With `work` set, warps take queries from that device counter (a
+// work queue) instead of a fixed grid stride, which balances batches whose
+// queries cost very different amounts.
+template <typename A>
+struct Batch {
+  const A* __restrict__ Q;
+  const uint32_t* __restrict__ order;
+  uint64_t nq;
+  const TreeView<A>* __restrict__ forest;
+  const uint32_t* __restrict__ tree_of;
+  const A* __restrict__ radii;
+  unsigned long long* __restrict__ work;
+
+  __device__ __forceinline__ TreeView<A> tree(const TreeView<A>& tv, uint64_t qi) const {
+    return forest ? forest[tree_of[qi]] : tv;
+  }
+  __device__ __forceinline__ A radius(A r, uint64_t qi) const { return radii ? radii[qi] : r; }
+  template <int K>
+  __device__ __forceinline__ void query(uint64_t qi, A (&q)[K]) const {
+#pragma unroll
+    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+  }
+};
+
+// One query per warp: f(qi) with all 32 lanes.
+template <typename A, typename F>
+__device__ __forceinline__ void for_each_query_warp(const Batch<A>& b, F&& f) {
+  if (b.work) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+      unsigned long long w = 0;
+      if (lane == 0) w = atomicAdd(b.work, 1ull);
+      w = __shfl_sync(FULL, w, 0);
+      if (w >= b.nq) break;
+      f(b.order ? uint64_t(b.order[w]) : uint64_t(w));
+    }
+  } else {
+    const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t w = warp; w < b.nq; w += nwarps) f(b.order ? uint64_t(b.order[w]) : w);
+  }
+}
+
+// One query per thread; with a work counter a warp takes 32 consecutive slots.
+template <typename A, typename F>
+__device__ __forceinline__ void for_each_query_thread(const Batch<A>& b, F&& f) {
+  if (b.work) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(b.work, 32ull);
+      base = __shfl_sync(FULL, base, 0);
+      if (base >= b.nq) break;
+      const uint64_t w = base + lane;
+      if (w < b.nq) f(b.order ? uint64_t(b.order[w]) : w);
+    }
+  } else {
+    for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < b.nq;
+         w += uint64_t(gridDim.x) * blockDim.x)
+      f(b.order ? uint64_t(b.order[w]) : w);
+  }
+}
+
 // ---------------------------------------------------------------------------
-// Fixed-size families: one warp per query, warps stride over the batch.
+// Fixed-size families, one warp per query.
 // ---------------------------------------------------------------------------
 template <typename A, int K, typename M, int FAM, bool EXCL>
-__global__ void __launch_bounds__(256) k_fixed(TreeView<A> tv, const A* __restrict__ Q,
-                                               const uint32_t* __restrict__ order, uint64_t nq,
-                                               int k, A radius, int arrival_order,
-                                               A* __restrict__ out_d, uint32_t* __restrict__ out_i,
+__global__ void __launch_bounds__(256) k_fixed(TreeView<A> tv0, Batch<A> b, int k, A radius0,
+                                               int arrival_order, A* __restrict__ out_d,
+                                               uint32_t* __restrict__ out_i,
                                                uint32_t* __restrict__ out_c,
                                                unsigned long long* __restrict__ stats) {
   const int lane = threadIdx.x & 31;
-  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  for (uint64_t w = warp; w < nq; w += nwarps) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_warp(b, [&](uint64_t qi) {
+    const TreeView<A> tv = b.tree(tv0, qi);
+    const A radius = b.radius(radius0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    b.query(qi, q);
     TravStats st;
     if constexpr (FAM == KF_NEAREST_ONE) {
       NearestOnePolicy<A, K, M> pol;
@@ -74,61 +136,56 @@ __global__ void __launch_bounds__(256) k_fixed(TreeView<A> tv, const A* __restri
       pol.write(qi, out_d, out_i, out_c, lane);
     }
     if (stats && lane == 0) add_stats(stats, st);
-  }
+  });
 }
 
 // ---------------------------------------------------------------------------
 // Radius families: count pass, exclusive scan, fill pass, segmented sort.
+// The fill pass writes at most `cap` hits per query; a query whose count
+// differs from its segment (the caller passed offsets of another batch) sets
+// *status to KGPU_EOVERFLOW.
 // ---------------------------------------------------------------------------
 template <typename A, int K, typename M, bool EXCL>
-__global__ void __launch_bounds__(256) k_within_count(TreeView<A> tv, const A* __restrict__ Q,
-                                                      const uint32_t* __restrict__ order,
-                                                      uint64_t nq, A radius,
+__global__ void __launch_bounds__(256) k_within_count(TreeView<A> tv0, Batch<A> b, A radius0,
                                                       uint64_t* __restrict__ counts,
                                                       unsigned long long* __restrict__ stats) {
   const int lane = threadIdx.x & 31;
-  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  for (uint64_t w = warp; w < nq; w += nwarps) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_warp(b, [&](uint64_t qi) {
+    const TreeView<A> tv = b.tree(tv0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
-    WithinCountPolicy<A, K, M, EXCL> pol(radius);
+    b.query(qi, q);
+    WithinCountPolicy<A, K, M, EXCL> pol(b.radius(radius0, qi));
     TravStats st;
     warp_arith_query<A, K, M>(tv, q, pol, lane, st);
     if (lane == 0) counts[qi] = pol.count;
     if (stats && lane == 0) add_stats(stats, st);
-  }
+  });
 }
 
 template <typename A, int K, typename M, bool EXCL>
-__global__ void __launch_bounds__(256) k_within_fill(TreeView<A> tv, const A* __restrict__ Q,
-                                                     const uint32_t* __restrict__ order,
-                                                     uint64_t nq, A radius,
+__global__ void __launch_bounds__(256) k_within_fill(TreeView<A> tv0, Batch<A> b, A radius0,
                                                      const uint64_t* __restrict__ offsets,
-                                                     A* __restrict__ out_d,
-                                                     uint32_t* __restrict__ out_i) {
+                                                     uint64_t capacity, A* __restrict__ out_d,
+                                                     uint32_t* __restrict__ out_i,
+                                                     int* __restrict__ status) {
   const int lane = threadIdx.x & 31;
-  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  for (uint64_t w = warp; w < nq; w += nwarps) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_warp(b, [&](uint64_t qi) {
     const uint64_t o = offsets[qi];
-    const uint64_t cap = offsets[qi + 1] - o;
-    if (cap == 0) continue;  // nothing to write
+    const uint64_t end = offsets[qi + 1] < capacity ? offsets[qi + 1] : capacity;
+    if (end <= o) return;
+    const TreeView<A> tv = b.tree(tv0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
-    WithinFillPolicy<A, K, M, EXCL> pol(radius, cap, out_d + o, out_i + o);
+    b.query(qi, q);
+    WithinFillPolicy<A, K, M, EXCL> pol(b.radius(radius0, qi), end - o, out_d + o, out_i + o);
     TravStats st;
     warp_arith_query<A, K, M>(tv, q, pol, lane, st);
-  }
+    if (lane == 0 && status && pol.count != offsets[qi + 1] - o) atomicExch(status, 6);
+  });
 }
 
 // ---------------------------------------------------------------------------
 // Thread-per-query kernels.  Dynamic shared memory: one continuation slot per
-// level per thread, (max_stem_level + 1) * blockDim values of A.
+// level per thread, (max_stem_level + 2) * blockDim values of A.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void flush_stats(unsigned long long* stats, const TravStats& st) {
   const unsigned s0 = __reduce_add_sync(FULL, st.stems);
@@ -142,10 +199,8 @@ __device__ __forceinline__ void flush_stats(unsigned long long* stats, const Tra
 }
 
 template <typename A, int K, typename M, int FAM, bool EXCL, int KC>
-__global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv, const A* __restrict__ Q,
-                                                const uint32_t* __restrict__ order, uint64_t nq,
-                                                int k, A radius, int arrival_order,
-                                                A* __restrict__ out_d,
+__global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int k, A radius0,
+                                                int arrival_order, A* __restrict__ out_d,
                                                 uint32_t* __restrict__ out_i,
                                                 uint32_t* __restrict__ out_c,
                                                 unsigned long long* __restrict__ stats) {
@@ -153,12 +208,11 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv, const A* __restr
   A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
   const int stride = blockDim.x;
   TravStats st;
-  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nq;
-       w += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_thread(b, [&](uint64_t qi) {
+    const TreeView<A> tv = b.tree(tv0, qi);
+    const A radius = b.radius(radius0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    b.query(qi, q);
     if constexpr (FAM == KF_NEAREST_ONE) {
       TNearestOne<A, K, M> pol;
       thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
@@ -184,44 +238,45 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv, const A* __restr
       thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
       pol.write(qi, out_d, out_i, out_c);
     }
-  }
+  });
   if (stats) flush_stats(stats, st);
 }
 
+// Counting pass (offsets == nullptr) or filling pass of the radius families.
 template <typename A, int K, typename M, bool EXCL>
-__global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv, const A* __restrict__ Q,
-                                                 const uint32_t* __restrict__ order, uint64_t nq,
-                                                 A radius, uint64_t* __restrict__ counts,
+__global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv0, Batch<A> b, A radius0,
+                                                 uint64_t* __restrict__ counts,
                                                  const uint64_t* __restrict__ offsets,
-                                                 A* __restrict__ out_d,
+                                                 uint64_t capacity, A* __restrict__ out_d,
                                                  uint32_t* __restrict__ out_i,
+                                                 int* __restrict__ status,
                                                  unsigned long long* __restrict__ stats) {
   extern __shared__ __align__(16) unsigned char tsmem[];
   A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
   const int stride = blockDim.x;
   TravStats st;
-  for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nq;
-       w += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_thread(b, [&](uint64_t qi) {
     uint64_t o = 0, cap = 0;
     if (offsets) {
       o = offsets[qi];
-      cap = offsets[qi + 1] - o;
-      if (cap == 0) continue;
+      const uint64_t end = offsets[qi + 1] < capacity ? offsets[qi + 1] : capacity;
+      if (end <= o) return;
+      cap = end - o;
     }
+    const TreeView<A> tv = b.tree(tv0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
-    TWithin<A, K, M, EXCL> pol(radius, cap, offsets ? out_d + o : nullptr,
+    b.query(qi, q);
+    TWithin<A, K, M, EXCL> pol(b.radius(radius0, qi), cap, offsets ? out_d + o : nullptr,
                                offsets ? out_i + o : nullptr);
     thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
     if (counts) counts[qi] = pol.count;
-  }
+    if (offsets && status && pol.count != offsets[qi + 1] - o) atomicExch(status, 6);
+  });
   if (stats) flush_stats(stats, st);
 }
 
 // ---------------------------------------------------------------------------
-// Periodic families (kd_tree/query/periodic.rs)
+// Periodic families (kd_tree/query/periodic.rs), one warp per query.
 // ---------------------------------------------------------------------------
 template <typename A, int K>
 struct BoxArg {
@@ -229,21 +284,17 @@ struct BoxArg {
 };
 
 template <typename A, int K, typename M, int FAM, bool EXCL>
-__global__ void __launch_bounds__(256) k_periodic_fixed(TreeView<A> tv, const A* __restrict__ Q,
-                                                        const uint32_t* __restrict__ order,
-                                                        uint64_t nq, BoxArg<A, K> box, int k,
-                                                        A radius, A* __restrict__ out_d,
+__global__ void __launch_bounds__(256) k_periodic_fixed(TreeView<A> tv0, Batch<A> b,
+                                                        BoxArg<A, K> box, int k, A radius0,
+                                                        A* __restrict__ out_d,
                                                         uint32_t* __restrict__ out_i,
                                                         uint32_t* __restrict__ out_c,
                                                         unsigned long long* __restrict__ stats) {
   const int lane = threadIdx.x & 31;
-  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  for (uint64_t w = warp; w < nq; w += nwarps) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_warp(b, [&](uint64_t qi) {
+    const TreeView<A> tv = b.tree(tv0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
+    b.query(qi, q);
     TravStats st;
     if constexpr (FAM == KF_NEAREST_ONE) {
       A best;
@@ -258,62 +309,56 @@ __global__ void __launch_bounds__(256) k_periodic_fixed(TreeView<A> tv, const A*
       PeriodicDist<A, K, M> pd;
 #pragma unroll
       for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
-      NearestNPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(k, radius, pd);
+      NearestNPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(k, b.radius(radius0, qi), pd);
       warp_periodic_query<A, K, M>(tv, q, box.v, pol, lane, st);
       pol.write(qi, out_d, out_i, out_c, false, lane);
     }
     if (stats && lane == 0) add_stats(stats, st);
-  }
+  });
 }
 
 template <typename A, int K, typename M, bool EXCL>
 __global__ void __launch_bounds__(256) k_periodic_within_count(
-    TreeView<A> tv, const A* __restrict__ Q, const uint32_t* __restrict__ order, uint64_t nq,
-    BoxArg<A, K> box, A radius, uint64_t* __restrict__ counts,
+    TreeView<A> tv0, Batch<A> b, BoxArg<A, K> box, A radius0, uint64_t* __restrict__ counts,
     unsigned long long* __restrict__ stats) {
   const int lane = threadIdx.x & 31;
-  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
   PeriodicDist<A, K, M> pd;
 #pragma unroll
   for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
-  for (uint64_t w = warp; w < nq; w += nwarps) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_warp(b, [&](uint64_t qi) {
+    const TreeView<A> tv = b.tree(tv0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
-    WithinCountPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(radius, pd);
+    b.query(qi, q);
+    WithinCountPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(b.radius(radius0, qi), pd);
     TravStats st;
     warp_periodic_query<A, K, M>(tv, q, box.v, pol, lane, st);
     if (lane == 0) counts[qi] = pol.count;
     if (stats && lane == 0) add_stats(stats, st);
-  }
+  });
 }
 
 template <typename A, int K, typename M, bool EXCL>
 __global__ void __launch_bounds__(256) k_periodic_within_fill(
-    TreeView<A> tv, const A* __restrict__ Q, const uint32_t* __restrict__ order, uint64_t nq,
-    BoxArg<A, K> box, A radius, const uint64_t* __restrict__ offsets, A* __restrict__ out_d,
-    uint32_t* __restrict__ out_i) {
+    TreeView<A> tv0, Batch<A> b, BoxArg<A, K> box, A radius0, const uint64_t* __restrict__ offsets,
+    uint64_t capacity, A* __restrict__ out_d, uint32_t* __restrict__ out_i,
+    int* __restrict__ status) {
   const int lane = threadIdx.x & 31;
-  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
   PeriodicDist<A, K, M> pd;
 #pragma unroll
   for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
-  for (uint64_t w = warp; w < nq; w += nwarps) {
-    const uint64_t qi = order ? order[w] : w;
+  for_each_query_warp(b, [&](uint64_t qi) {
     const uint64_t o = offsets[qi];
-    const uint64_t cap = offsets[qi + 1] - o;
-    if (cap == 0) continue;
+    const uint64_t end = offsets[qi + 1] < capacity ? offsets[qi + 1] : capacity;
+    if (end <= o) return;
+    const TreeView<A> tv = b.tree(tv0, qi);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + qi * K + d);
-    WithinFillPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(radius, cap, out_d + o, out_i + o,
-                                                                pd);
+    b.query(qi, q);
+    WithinFillPolicy<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(b.radius(radius0, qi), end - o,
+                                                                out_d + o, out_i + o, pd);
     TravStats st;
     warp_periodic_query<A, K, M>(tv, q, box.v, pol, lane, st);
-  }
+    if (lane == 0 && status && pol.count != offsets[qi + 1] - o) atomicExch(status, 6);
+  });
 }
 
 // Segments of at most 32 hits: one warp, bitonic network on (distance, position)
@@ -473,16 +518,18 @@ namespace kgpu {
 // walk the same stems and leaves.  Results do not depend on the order.
 // ---------------------------------------------------------------------------
 template <typename A, int K>
-__global__ void __launch_bounds__(256) k_leaf_histogram(TreeView<A> tv, const A* __restrict__ Q,
-                                                        uint64_t nq, uint32_t* __restrict__ leaf_of,
+__global__ void __launch_bounds__(256) k_leaf_histogram(TreeView<A> tv0, Batch<A> b,
+                                                        const uint64_t* __restrict__ leaf_base,
+                                                        uint32_t* __restrict__ leaf_of,
                                                         unsigned long long* __restrict__ counts) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nq;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < b.nq;
        i += uint64_t(gridDim.x) * blockDim.x) {
+    const TreeView<A> tv = b.tree(tv0, i);
     A q[K];
-#pragma unroll
-    for (int d = 0; d < K; ++d) q[d] = __ldg(Q + i * K + d);
-    const uint32_t l = tv.leaf_count > 1 ? straight_leaf<A, K>(tv, q) : 0u;
-    leaf_of[i] = l;
+    b.query(i, q);
+    uint64_t l = tv.leaf_count > 1 ? straight_leaf<A, K>(tv, q) : 0u;
+    if (leaf_base) l += leaf_base[b.tree_of[i]];
+    leaf_of[i] = uint32_t(l);
     atomicAdd(counts + l, 1ull);
   }
 }

@@ -40,6 +40,15 @@ struct QueryLaunch {
   int engine = 0;                 // 0 auto, 1 warp per query, 2 thread per query
   bool periodic = false;          // periodic boundary conditions
   double box[4] = {0, 0, 0, 0};   // periodic box (converted to A)
+  // batches over many trees (see kgpu_forest_*): device arrays, or null
+  const void* forest = nullptr;          // TreeView<A>[n_trees]
+  const uint32_t* tree_of = nullptr;     // tree of each query
+  const uint64_t* leaf_base = nullptr;   // first global leaf number of each tree
+  uint64_t total_leaves = 0;             // leaves of all trees (spatial order)
+  const void* radii = nullptr;           // per-query radius (A), or null
+  unsigned long long* work = nullptr;    // work-queue counter (zeroed), or null
+  uint64_t capacity = ~uint64_t(0);      // fill pass: hits that fit the output
+  int* status = nullptr;                 // fill pass: set to KGPU_EOVERFLOW on mismatch
   cudaStream_t stream = nullptr;
 };
 
@@ -57,10 +66,9 @@ template <typename A> cudaError_t launch_within_fill(const DeviceTree& t, const 
                                                       const uint64_t* offsets);
 // Processing order grouped by straight-descent leaf.  `scratch` must hold
 // spatial_order_scratch_bytes(t, nq) bytes; order[nq] receives query indices.
-size_t spatial_order_scratch_bytes(const DeviceTree& t, uint64_t nq);
-template <typename A> cudaError_t launch_spatial_order(const DeviceTree& t, const void* queries,
-                                                       uint64_t nq, uint32_t* order,
-                                                       void* scratch, cudaStream_t s);
+size_t spatial_order_scratch_bytes(const DeviceTree& t, const QueryLaunch& q);
+template <typename A> cudaError_t launch_spatial_order(const DeviceTree& t, const QueryLaunch& q,
+                                                       uint32_t* order, void* scratch);
 
 // Stable sort of every CSR segment by distance; scratch holds total entries.
 template <typename A> cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d,

@@ -57,32 +57,40 @@ inline cudaError_t with_excl(bool e, F&& f) {
   return f(std::false_type());
 }
 
-// Dynamic shared memory of the thread-per-query kernels.
+template <typename A>
+inline Batch<A> make_batch(const QueryLaunch& q) {
+  Batch<A> b;
+  b.Q = static_cast<const A*>(q.queries);
+  b.order = q.order;
+  b.nq = q.nq;
+  b.forest = static_cast<const TreeView<A>*>(q.forest);
+  b.tree_of = q.tree_of;
+  b.radii = static_cast<const A*>(q.radii);
+  b.work = q.work;
+  return b;
+}
+
+template <typename A, int K>
+inline BoxArg<A, K> make_box(const QueryLaunch& q) {
+  BoxArg<A, K> box;
+  for (int d = 0; d < K; ++d) box.v[d] = A(q.box[d]);
+  return box;
+}
+
+// Dynamic shared memory of the thread-per-query kernels (one slot per level).
 template <typename A>
 inline size_t thread_smem(const DeviceTree& t) {
   return size_t(t.max_stem_level + 2) * 256 * sizeof(A);
 }
 
-template <typename F>
-inline cudaError_t with_kc(int k, F&& f) {
-  if (k <= 1) return f(std::integral_constant<int, 1>());
-  if (k <= 4) return f(std::integral_constant<int, 4>());
-  if (k <= 8) return f(std::integral_constant<int, 8>());
-  if (k <= 16) return f(std::integral_constant<int, 16>());
-  return f(std::integral_constant<int, 32>());
-}
-
-// Thread per query for 2-D and 3-D trees unless the warp engine is requested
-// or periodic boundaries (served by the warp kernels) are on; other
-// dimensionalities use the warp kernels (same results).
+// 2-D and 3-D trees have thread-per-query kernels; other dimensionalities use
+// the warp kernels (same results).
 constexpr bool thread_engine_dims(int K) { return K == 2 || K == 3; }
-inline bool use_thread_engine(const QueryLaunch& q, int dims) {
-  return q.engine != 1 && !q.periodic && thread_engine_dims(dims);
-}
 
 template <typename A>
 cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
   const TreeView<A> tv = make_view<A>(t);
+  const Batch<A> b = make_batch<A>(q);
   const A radius = A(q.radius);
   return with_dims(t.dims, [&](auto kk) {
     constexpr int K = decltype(kk)::value;
@@ -90,30 +98,28 @@ cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
       using M = decltype(m);
       return with_excl(q.exclusive, [&](auto ex) {
         constexpr bool EX = decltype(ex)::value;
-        auto run = [&](auto kern) {
-          const int grid = grid_for(kern, 0, q.nq);
-          kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                           q.k, radius, q.sorted ? 0 : 1,
-                                           static_cast<A*>(q.out_d), q.out_i, q.out_c, q.stats);
-          g_launches++;
-          return cudaGetLastError();
-        };
         if (q.periodic) {
-          BoxArg<A, K> box;
-          for (int d = 0; d < K; ++d) box.v[d] = A(q.box[d]);
+          const BoxArg<A, K> box = make_box<A, K>(q);
           auto runp = [&](auto kern) {
             const int grid = grid_for(kern, 0, q.nq);
-            kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                             box, q.k, radius, static_cast<A*>(q.out_d), q.out_i,
-                                             q.out_c, q.stats);
+            kern<<<grid, 256, 0, q.stream>>>(tv, b, box, q.k, radius, static_cast<A*>(q.out_d),
+                                             q.out_i, q.out_c, q.stats);
             g_launches++;
             return cudaGetLastError();
           };
-          if (q.family == KGPU_NEAREST_ONE) return runp(k_periodic_fixed<A, K, M, KF_NEAREST_ONE, false>);
+          if (q.family == KGPU_NEAREST_ONE)
+            return runp(k_periodic_fixed<A, K, M, KF_NEAREST_ONE, false>);
           if (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN)
             return runp(k_periodic_fixed<A, K, M, KF_NEAREST_N, EX>);
           return cudaErrorInvalidValue;
         }
+        auto run = [&](auto kern) {
+          const int grid = grid_for(kern, 0, q.nq);
+          kern<<<grid, 256, 0, q.stream>>>(tv, b, q.k, radius, q.sorted ? 0 : 1,
+                                           static_cast<A*>(q.out_d), q.out_i, q.out_c, q.stats);
+          g_launches++;
+          return cudaGetLastError();
+        };
         switch (q.family) {
           case KGPU_NEAREST_ONE:
             return run(k_fixed<A, K, M, KF_NEAREST_ONE, false>);
@@ -136,6 +142,7 @@ cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
 template <typename A, int KC>
 cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
   const TreeView<A> tv = make_view<A>(t);
+  const Batch<A> b = make_batch<A>(q);
   const A radius = A(q.radius);
   const size_t smem = thread_smem<A>(t);
   return with_dims(t.dims, [&](auto kk) -> cudaError_t {
@@ -150,16 +157,17 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
           auto runt = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
-            kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order,
-                                                q.nq, q.k, radius, q.sorted ? 0 : 1,
+            kern<<<grid, 256, smem, q.stream>>>(tv, b, q.k, radius, q.sorted ? 0 : 1,
                                                 static_cast<A*>(q.out_d), q.out_i, q.out_c,
                                                 q.stats);
             g_launches++;
             return cudaGetLastError();
           };
           if constexpr (KC == 1) {
-            if (q.family == KGPU_NEAREST_ONE) return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false, 1>);
-            if (q.family == KGPU_APPROX_NEAREST_ONE) return runt(k_tfixed<A, K, M, KF_APPROX, false, 1>);
+            if (q.family == KGPU_NEAREST_ONE)
+              return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false, 1>);
+            if (q.family == KGPU_APPROX_NEAREST_ONE)
+              return runt(k_tfixed<A, K, M, KF_APPROX, false, 1>);
           }
           if (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN)
             return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX, KC>);
@@ -171,40 +179,56 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
   });
 }
 
+// Counting (offsets == nullptr, counts set) or filling pass of the radius
+// families.
 template <typename A>
-cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts) {
+cudaError_t launch_within_pass(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts,
+                               const uint64_t* offsets) {
   const TreeView<A> tv = make_view<A>(t);
+  const Batch<A> b = make_batch<A>(q);
   const A radius = A(q.radius);
   return with_dims(t.dims, [&](auto kk) {
     constexpr int K = decltype(kk)::value;
     return with_metric(q.metric, [&](auto m) {
       using M = decltype(m);
-      return with_excl(q.exclusive, [&](auto ex) {
+      return with_excl(q.exclusive, [&](auto ex) -> cudaError_t {
         constexpr bool EX = decltype(ex)::value;
         if (q.periodic) {
-          BoxArg<A, K> box;
-          for (int d = 0; d < K; ++d) box.v[d] = A(q.box[d]);
-          auto kern = k_periodic_within_count<A, K, M, EX>;
-          const int grid = grid_for(kern, 0, q.nq);
-          kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                           box, radius, counts, q.stats);
+          const BoxArg<A, K> box = make_box<A, K>(q);
+          if (!offsets) {
+            auto kern = k_periodic_within_count<A, K, M, EX>;
+            kern<<<grid_for(kern, 0, q.nq), 256, 0, q.stream>>>(tv, b, box, radius, counts,
+                                                                 q.stats);
+          } else {
+            auto kern = k_periodic_within_fill<A, K, M, EX>;
+            kern<<<grid_for(kern, 0, q.nq), 256, 0, q.stream>>>(
+                tv, b, box, radius, offsets, q.capacity, static_cast<A*>(q.out_d), q.out_i,
+                q.status);
+          }
           g_launches++;
           return cudaGetLastError();
         }
-        if constexpr (thread_engine_dims(K)) if (q.engine != 1) {
-          const size_t smem = thread_smem<A>(t);
-          auto kern = k_twithin<A, K, M, EX>;
-          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-          const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
-          kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                              radius, counts, nullptr, nullptr, nullptr, q.stats);
-          g_launches++;
-          return cudaGetLastError();
+        if constexpr (thread_engine_dims(K)) {
+          if (q.engine != 1) {
+            const size_t smem = thread_smem<A>(t);
+            auto kern = k_twithin<A, K, M, EX>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+            kern<<<grid, 256, smem, q.stream>>>(tv, b, radius, counts, offsets, q.capacity,
+                                                static_cast<A*>(q.out_d), q.out_i, q.status,
+                                                q.stats);
+            g_launches++;
+            return cudaGetLastError();
+          }
         }
-        auto kern = k_within_count<A, K, M, EX>;
-        const int grid = grid_for(kern, 0, q.nq);
-        kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                         radius, counts, q.stats);
+        if (!offsets) {
+          auto kern = k_within_count<A, K, M, EX>;
+          kern<<<grid_for(kern, 0, q.nq), 256, 0, q.stream>>>(tv, b, radius, counts, q.stats);
+        } else {
+          auto kern = k_within_fill<A, K, M, EX>;
+          kern<<<grid_for(kern, 0, q.nq), 256, 0, q.stream>>>(
+              tv, b, radius, offsets, q.capacity, static_cast<A*>(q.out_d), q.out_i, q.status);
+        }
         g_launches++;
         return cudaGetLastError();
       });
@@ -213,47 +237,14 @@ cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint6
 }
 
 template <typename A>
+cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts) {
+  return launch_within_pass<A>(t, q, counts, nullptr);
+}
+
+template <typename A>
 cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
                                const uint64_t* offsets) {
-  const TreeView<A> tv = make_view<A>(t);
-  const A radius = A(q.radius);
-  return with_dims(t.dims, [&](auto kk) {
-    constexpr int K = decltype(kk)::value;
-    return with_metric(q.metric, [&](auto m) {
-      using M = decltype(m);
-      return with_excl(q.exclusive, [&](auto ex) {
-        constexpr bool EX = decltype(ex)::value;
-        if (q.periodic) {
-          BoxArg<A, K> box;
-          for (int d = 0; d < K; ++d) box.v[d] = A(q.box[d]);
-          auto kern = k_periodic_within_fill<A, K, M, EX>;
-          const int grid = grid_for(kern, 0, q.nq);
-          kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                           box, radius, offsets, static_cast<A*>(q.out_d),
-                                           q.out_i);
-          g_launches++;
-          return cudaGetLastError();
-        }
-        if constexpr (thread_engine_dims(K)) if (q.engine != 1) {
-          const size_t smem = thread_smem<A>(t);
-          auto kern = k_twithin<A, K, M, EX>;
-          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-          const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
-          kern<<<grid, 256, smem, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                              radius, nullptr, offsets, static_cast<A*>(q.out_d),
-                                              q.out_i, nullptr);
-          g_launches++;
-          return cudaGetLastError();
-        }
-        auto kern = k_within_fill<A, K, M, EX>;
-        const int grid = grid_for(kern, 0, q.nq);
-        kern<<<grid, 256, 0, q.stream>>>(tv, static_cast<const A*>(q.queries), q.order, q.nq,
-                                         radius, offsets, static_cast<A*>(q.out_d), q.out_i);
-        g_launches++;
-        return cudaGetLastError();
-      });
-    });
-  });
+  return launch_within_pass<A>(t, q, nullptr, offsets);
 }
 
 template <typename A>
@@ -279,12 +270,13 @@ cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d, uint32_t
   return cudaGetLastError();
 }
 
-
 template <typename A>
-cudaError_t launch_spatial_order(const DeviceTree& t, const void* queries, uint64_t nq,
-                                 uint32_t* order, void* scratch, cudaStream_t s) {
+cudaError_t launch_spatial_order(const DeviceTree& t, const QueryLaunch& q, uint32_t* order,
+                                 void* scratch) {
   const TreeView<A> tv = make_view<A>(t);
-  const uint64_t nl = t.leaf_count > 0 ? t.leaf_count : 1;
+  const Batch<A> b = make_batch<A>(q);
+  const uint64_t nq = q.nq;
+  const uint64_t nl = q.forest ? q.total_leaves : (t.leaf_count > 0 ? t.leaf_count : 1);
   // scratch layout: leaf_of[nq] u32 | counts[nl + 1] u64 | scan tiles
   uint8_t* p = static_cast<uint8_t*>(scratch);
   uint32_t* leaf_of = reinterpret_cast<uint32_t*>(p);
@@ -292,28 +284,29 @@ cudaError_t launch_spatial_order(const DeviceTree& t, const void* queries, uint6
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(p);
   p += (((nl + 1) * 8 + 255) / 256) * 256;
   void* tiles = p;
-  cudaError_t e = cudaMemsetAsync(counts, 0, (nl + 1) * 8, s);
+  cudaError_t e = cudaMemsetAsync(counts, 0, (nl + 1) * 8, q.stream);
   if (e != cudaSuccess) return e;
   e = with_dims(t.dims, [&](auto kk) {
     constexpr int K = decltype(kk)::value;
     auto kern = k_leaf_histogram<A, K>;
     const int grid = grid_for(kern, 0, (nq + 31) / 32);
-    kern<<<grid, 256, 0, s>>>(tv, static_cast<const A*>(queries), nq, leaf_of, counts);
+    kern<<<grid, 256, 0, q.stream>>>(tv, b, q.forest ? q.leaf_base : nullptr, leaf_of, counts);
     g_launches++;
     return cudaGetLastError();
   });
   if (e != cudaSuccess) return e;
-  e = launch_exclusive_scan(reinterpret_cast<uint64_t*>(counts), reinterpret_cast<uint64_t*>(counts),
-                            nl, tiles, s);
+  e = launch_exclusive_scan(reinterpret_cast<uint64_t*>(counts),
+                            reinterpret_cast<uint64_t*>(counts), nl, tiles, q.stream);
   if (e != cudaSuccess) return e;
   {
     auto kern = k_leaf_scatter;
     const int grid = grid_for(kern, 0, (nq + 31) / 32);
-    kern<<<grid, 256, 0, s>>>(leaf_of, nq, counts, order);
+    kern<<<grid, 256, 0, q.stream>>>(leaf_of, nq, counts, order);
     g_launches++;
   }
   return cudaGetLastError();
 }
+
 }  // namespace kgpu
 
 #define KGPU_INSTANTIATE_WARP(A)                                                                 \
@@ -333,6 +326,6 @@ cudaError_t launch_spatial_order(const DeviceTree& t, const void* queries, uint6
                                              const uint64_t*);                                   \
   template cudaError_t launch_seg_sort<A>(const uint64_t*, uint64_t, A*, uint32_t*, A*,          \
                                           uint32_t*, cudaStream_t);                              \
-  template cudaError_t launch_spatial_order<A>(const DeviceTree&, const void*, uint64_t,         \
-                                               uint32_t*, void*, cudaStream_t);                  \
+  template cudaError_t launch_spatial_order<A>(const DeviceTree&, const QueryLaunch&, uint32_t*, \
+                                               void*);                                           \
   }

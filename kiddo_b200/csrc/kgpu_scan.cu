@@ -102,9 +102,10 @@ __global__ void __launch_bounds__(kThreads) k_tile_apply(const uint64_t* counts,
 
 size_t scan_tmp_bytes(uint64_t n) { return size_t((n + kTile - 1) / kTile + 1) * sizeof(uint64_t); }
 
-size_t spatial_order_scratch_bytes(const DeviceTree& t, uint64_t nq) {
-  const uint64_t nl = t.leaf_count > 0 ? t.leaf_count : 1;
-  return ((nq * 4 + 255) / 256) * 256 + (((nl + 1) * 8 + 255) / 256) * 256 + scan_tmp_bytes(nl) + 256;
+size_t spatial_order_scratch_bytes(const DeviceTree& t, const QueryLaunch& q) {
+  const uint64_t nl = q.forest ? q.total_leaves : (t.leaf_count > 0 ? t.leaf_count : 1);
+  return ((q.nq * 4 + 255) / 256) * 256 + (((nl + 1) * 8 + 255) / 256) * 256 +
+         scan_tmp_bytes(nl) + 256;
 }
 
 cudaError_t launch_exclusive_scan(const uint64_t* counts, uint64_t* offsets, uint64_t n, void* tmp,

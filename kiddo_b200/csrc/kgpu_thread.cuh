@@ -22,18 +22,15 @@ namespace kgpu {
 
 // Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
 // leaf_view/mod.rs:431-446): f(coords, item) in tile order.
-template <typename A> struct Pair;
-template <> struct Pair<float> { using T = float2; };
-template <> struct Pair<double> { using T = double2; };
-
 // Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
-// leaf_view/mod.rs:431-446): f(coords, item) in tile order.  Tiles of width
-// >= 2 are read two points per step (8-byte aligned pairs for f32: leaves
-// start on 8 bytes and every column of an even-width tile spans an even
-// number of floats).
-template <typename A, int K, typename F>
+// leaf_view/mod.rs:431-446) calling f(distance, item) in tile order, with
+// distance = dist(coords).  Tiles of width >= 2 are read two points per step
+// (8-byte aligned pairs for f32: leaves start on 8 bytes and every column of
+// an even-width tile spans an even number of floats); both points then go
+// through one call site of f, so the policy's insertion code is emitted once.
+template <typename A, int K, typename D, typename F>
 __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint32_t leaf,
-                                                          F&& f) {
+                                                          const D& dist, F&& f) {
   const uint2 ex = __ldg(tv.extents + leaf);
   const uint8_t* base = tv.arena + size_t(ex.x) * 8;
   uint32_t rem = ex.y;
@@ -42,35 +39,36 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
     const uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
     const A* col = reinterpret_cast<const A*>(base + boff);
     const uint32_t* its = reinterpret_cast<const uint32_t*>(base + boff + K * w * sizeof(A));
-    if (w >= 2) {
-      for (uint32_t i = 0; i < w; i += 2) {
-        A c0[K], c1[K];
-        if constexpr (sizeof(A) == 4) {
+    for (uint32_t i = 0; i < w; i += 2) {
+      A c0[K], c1[K];
+      uint32_t i0, i1;
+      if (w == 1) {
 #pragma unroll
-          for (int d = 0; d < K; ++d) {
-            const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
-            c0[d] = v.x;
-            c1[d] = v.y;
-          }
-          const uint2 it = __ldg(reinterpret_cast<const uint2*>(its + i));
-          f(c0, it.x);
-          f(c1, it.y);
-        } else {
+        for (int d = 0; d < K; ++d) c0[d] = c1[d] = __ldg(col + d);
+        i0 = i1 = __ldg(its);
+      } else if constexpr (sizeof(A) == 4) {
 #pragma unroll
-          for (int d = 0; d < K; ++d) {
-            c0[d] = __ldg(col + d * w + i);
-            c1[d] = __ldg(col + d * w + i + 1);
-          }
-          const uint32_t i0 = __ldg(its + i), i1 = __ldg(its + i + 1);
-          f(c0, i0);
-          f(c1, i1);
+        for (int d = 0; d < K; ++d) {
+          const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
+          c0[d] = v.x;
+          c1[d] = v.y;
         }
-      }
-    } else {
-      A c[K];
+        const uint2 it = __ldg(reinterpret_cast<const uint2*>(its + i));
+        i0 = it.x;
+        i1 = it.y;
+      } else {
 #pragma unroll
-      for (int d = 0; d < K; ++d) c[d] = __ldg(col + d);
-      f(c, __ldg(its));
+        for (int d = 0; d < K; ++d) {
+          c0[d] = __ldg(col + d * w + i);
+          c1[d] = __ldg(col + d * w + i + 1);
+        }
+        i0 = __ldg(its + i);
+        i1 = __ldg(its + i + 1);
+      }
+      const A d0 = dist(c0), d1 = dist(c1);
+      const int nu = w == 1 ? 1 : 2;
+#pragma unroll 1
+      for (int u = 0; u < nu; ++u) f(u ? d1 : d0, u ? i1 : i0);
     }
     boff += w * (K * sizeof(A) + sizeof(uint32_t));
     rem -= w;
@@ -160,6 +158,14 @@ __device__ __forceinline__ void thread_arith_query(const TreeView<A>& tv, const 
 // ---------------------------------------------------------------------------
 // Thread policies
 // ---------------------------------------------------------------------------
+// Distance of a leaf point to the query (binds the query for the leaf walk).
+template <typename A, int K, typename M>
+struct CartesianQ {
+  const A (&q)[K];
+  __device__ __forceinline__ A operator()(const A (&c)[K]) const {
+    return point_dist<M, A, K>(c, q);
+  }
+};
 template <typename A, int K, typename M>
 struct TNearestOne {
   static constexpr bool kPruneOnEqual = true;
@@ -169,8 +175,8 @@ struct TNearestOne {
   __device__ __forceinline__ A max_dist() const { return best; }
   __device__ __forceinline__ bool unbounded_start() const { return true; }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
-    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
-      const A d = point_dist<M, A, K>(c, q);
+    const CartesianQ<A, K, M> dist{q};
+    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
       if (d < best) { best = d; item = it; }
     });
   }
@@ -197,28 +203,17 @@ struct TNearestN {
   __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
 
-  // Stable sort of slots [0, m) by distance (slots >= m hold +inf and stay
-  // behind): bitonic network on (distance, slot) keys.
-  __device__ __forceinline__ void sort_prefix(int m) {
-    uint32_t pos[KC];
+  // Stable sort of the list by distance: odd-even transposition network that
+  // swaps only on a strict `>`, so equal distances keep arrival order (slots
+  // past the held entries hold +inf and stay behind).
+  __device__ __forceinline__ void sort_list() {
 #pragma unroll
-    for (int j = 0; j < KC; ++j) pos[j] = j < m ? uint32_t(j) : 0xffffffffu;
+    for (int round = 0; round < KC; ++round) {
 #pragma unroll
-    for (int size = 2; size <= KC; size <<= 1) {
-#pragma unroll
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-#pragma unroll
-        for (int i = 0; i < KC; ++i) {
-          const int j = i ^ stride;
-          if (j > i) {
-            const bool up = (i & size) == 0;
-            const bool gt = ld[i] > ld[j] || (ld[i] == ld[j] && pos[i] > pos[j]);
-            if (gt == up) {
-              const A td = ld[i]; ld[i] = ld[j]; ld[j] = td;
-              const uint32_t ti = li[i]; li[i] = li[j]; li[j] = ti;
-              const uint32_t tp = pos[i]; pos[i] = pos[j]; pos[j] = tp;
-            }
-          }
+      for (int j = round & 1; j + 1 < KC; j += 2) {
+        if (ld[j] > ld[j + 1]) {
+          const A td = ld[j]; ld[j] = ld[j + 1]; ld[j + 1] = td;
+          const uint32_t ti = li[j]; li[j] = li[j + 1]; li[j + 1] = ti;
         }
       }
     }
@@ -239,7 +234,7 @@ struct TNearestN {
         if (j == n) { ld[j] = d; li[j] = it; }
       ++n;
       if (n == k) {
-        sort_prefix(k);
+        sort_list();
         refresh_kth();
       }
       return;
@@ -262,8 +257,8 @@ struct TNearestN {
 
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
     const A bound = max_dist();
-    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
-      const A d = point_dist<M, A, K>(c, q);
+    const CartesianQ<A, K, M> dist{q};
+    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
       if (kExclusive ? (d < bound) : (d <= bound)) add(d, it);
     });
   }
@@ -271,7 +266,7 @@ struct TNearestN {
   __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
                                         uint32_t* __restrict__ out_i,
                                         uint32_t* __restrict__ out_c, bool arrival_order) {
-    if (n < k && !arrival_order) sort_prefix(n);
+    if (n < k && !arrival_order) sort_list();
     A* od = out_d + size_t(qi) * k;
     uint32_t* oi = out_i + size_t(qi) * k;
 #pragma unroll
@@ -328,8 +323,8 @@ struct TBestN {
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
     const bool full_at_entry = n == k;
     const uint32_t thr_item = last_item();
-    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
-      const A d = point_dist<M, A, K>(c, q);
+    const CartesianQ<A, K, M> dist{q};
+    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
       if (!(kExclusive ? (d < radius) : (d <= radius))) return;
       if (full_at_entry && it >= thr_item) return;
       add(d, it);
@@ -364,8 +359,8 @@ struct TWithin {
   __device__ __forceinline__ A max_dist() const { return radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
-    return thread_for_each_point<A, K>(tv, l, [&](const A (&c)[K], uint32_t it) {
-      const A d = point_dist<M, A, K>(c, q);
+    const CartesianQ<A, K, M> dist{q};
+    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
       if (kExclusive ? (d < radius) : (d <= radius)) {
         if (out_d && count < cap) { out_d[count] = d; out_i[count] = it; }
         ++count;
