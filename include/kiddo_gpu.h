@@ -210,6 +210,49 @@ int32_t kgpu_query_radius_count_noalloc(kgpu_tree* tree, const kgpu_query_desc* 
 int32_t kgpu_query_stats(kgpu_tree* tree, const kgpu_query_desc* desc, const void* queries,
                          uint64_t nq, uint64_t* stats, void* stream);
 
+/* ---- batches over many trees --------------------------------------------
+ * A forest groups uploaded trees of one dtype and dimensionality (the trees
+ * must outlive it).  Forest queries take device pointers only: queries
+ * [nq, dims], tree_of[nq] (index into the forest; a query naming no tree gets
+ * empty results) and optionally radii[nq] (one radius per query, type A;
+ * NULL = desc->radius).  One persistent launch answers the whole batch, its
+ * warps pulling queries from a device work counter.  Output layouts are those
+ * of the single-tree calls.  Replaces running the reference's per-tree
+ * `.execute()` (or one GPU launch per tree) over a catalogue of trees. */
+typedef struct kgpu_forest kgpu_forest;
+int32_t kgpu_forest_create(kgpu_tree* const* trees, uint32_t n_trees, void* stream,
+                           kgpu_forest** out);
+int32_t kgpu_forest_destroy(kgpu_forest* forest);
+int32_t kgpu_forest_query(kgpu_forest* forest, const kgpu_query_desc* desc, const void* queries,
+                          const uint32_t* tree_of, const void* radii, uint64_t nq,
+                          void* out_dists, uint32_t* out_items, uint32_t* out_counts,
+                          void* stream);
+int32_t kgpu_forest_query_radius_count(kgpu_forest* forest, const kgpu_query_desc* desc,
+                                       const void* queries, const uint32_t* tree_of,
+                                       const void* radii, uint64_t nq, uint64_t* offsets,
+                                       void* stream);
+/* Fills at most `capacity` hits (the caller sizes the output, for example from
+ * a previous batch) and never reads the total back to the host, so the call
+ * can be captured in a CUDA graph.  If a query's hits do not fit, *status
+ * (device int32, zeroed by the caller; may be NULL) becomes KGPU_EOVERFLOW
+ * and the caller retries with offsets[nq] as the capacity. */
+int32_t kgpu_forest_query_radius_fill(kgpu_forest* forest, const kgpu_query_desc* desc,
+                                      const void* queries, const uint32_t* tree_of,
+                                      const void* radii, uint64_t nq, const uint64_t* offsets,
+                                      uint64_t capacity, void* out_dists, uint32_t* out_items,
+                                      int32_t* status, void* stream);
+
+/* ---- CUDA graphs --------------------------------------------------------
+ * Capture a sequence of device-pointer calls on `stream` (not the legacy
+ * default stream) and replay it.  Capturable: kgpu_query, kgpu_query_radius_count,
+ * the forest calls; not capturable: calls with KGPU_FLAG_HOST_BUFFERS and
+ * kgpu_query_radius_fill (both read back to the host). */
+typedef struct kgpu_graph kgpu_graph;
+int32_t kgpu_graph_begin(void* stream);
+int32_t kgpu_graph_end(void* stream, kgpu_graph** out);
+int32_t kgpu_graph_launch(kgpu_graph* graph, void* stream);
+int32_t kgpu_graph_destroy(kgpu_graph* graph);
+
 /* ---- accounting --------------------------------------------------------
  * Number of CUDA kernels this library has launched in the process so far
  * (all threads).  Lets a caller count the launches inside a timed region. */

@@ -28,8 +28,9 @@ import numpy as np
 from . import _capi as C
 from ._capi import KiddoGpuError, launch_count
 
-__all__ = ["ImmutableKdTree", "GpuTree", "SquaredEuclidean", "Manhattan", "KiddoGpuError",
-           "NearestOneResult", "NearestNResult", "WithinResult", "launch_count"]
+__all__ = ["ImmutableKdTree", "GpuTree", "Forest", "CapturedGraph", "SquaredEuclidean",
+           "Manhattan", "KiddoGpuError", "NearestOneResult", "NearestNResult", "WithinResult",
+           "launch_count"]
 
 
 class SquaredEuclidean:
@@ -457,3 +458,123 @@ class QueryBuilder:
         if self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE):
             return NearestOneResult(dist[:, 0], items[:, 0])
         return NearestNResult(dist, items, counts)
+
+
+class Forest:
+    """Many uploaded trees of one dtype/dimensionality answered in one launch.
+
+    ``forest.query(queries, tree_of, radii=None)`` takes CUDA tensors: queries
+    [nq, dims], tree_of [nq] (int32 index into ``trees``) and optionally one
+    radius per query.  The builder is the same as a single tree's.
+    """
+
+    def __init__(self, trees, stream=None):
+        gts = [t.to_gpu() if isinstance(t, ImmutableKdTree) else t for t in trees]
+        if not gts:
+            raise ValueError("a forest needs at least one tree")
+        self.trees = gts
+        self.dtype = gts[0].dtype
+        self.dims = gts[0].dims
+        arr = (ctypes.c_void_p * len(gts))(*[g._h.value for g in gts])
+        h = ctypes.c_void_p()
+        C.check(C.lib().kgpu_forest_create(arr, len(gts), _stream_ptr(stream), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and C._lib is not None:
+            C._lib.kgpu_forest_destroy(self._h)
+            self._h = None
+
+    def query(self, queries, tree_of, radii=None) -> "ForestQueryBuilder":
+        return ForestQueryBuilder(self, queries, tree_of, radii)
+
+
+class ForestQueryBuilder(QueryBuilder):
+    def __init__(self, forest: Forest, queries, tree_of, radii):
+        super().__init__(forest, queries)
+        self.tree_of = tree_of
+        self.radii = radii
+
+    def execute_gpu(self):
+        import torch
+        if self.family is None:
+            raise TypeError("choose a query type before execute_gpu()")
+        L = C.lib()
+        f = self.tree
+        tdt = torch.float32 if f.dtype == np.float32 else torch.float64
+        q = self.queries
+        if not (_is_torch_cuda(q) and _is_torch_cuda(self.tree_of)):
+            raise TypeError("forest queries take CUDA tensors")
+        q = q.contiguous()
+        tof = self.tree_of.to(torch.int32).contiguous()
+        rad = None if self.radii is None else self.radii.to(tdt).contiguous()
+        nq = q.shape[0]
+        d = self._desc(False)
+        stream = self.stream if self.stream is not None else torch.cuda.current_stream(q.device)
+        st = _stream_ptr(stream)
+        vp = ctypes.c_void_p
+        rp = vp(rad.data_ptr()) if rad is not None else None
+        dev = q.device
+        if self.family in (C.WITHIN, C.WITHIN_UNSORTED):
+            off = torch.empty(nq + 1, dtype=torch.int64, device=dev)
+            C.check(L.kgpu_forest_query_radius_count(f._h, ctypes.byref(d), vp(q.data_ptr()),
+                                                     vp(tof.data_ptr()), rp, nq,
+                                                     vp(off.data_ptr()), st))
+            total = int(off[-1].item())
+            dist = torch.empty(max(total, 1), dtype=tdt, device=dev)
+            items = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
+            C.check(L.kgpu_forest_query_radius_fill(f._h, ctypes.byref(d), vp(q.data_ptr()),
+                                                    vp(tof.data_ptr()), rp, nq,
+                                                    vp(off.data_ptr()), total,
+                                                    vp(dist.data_ptr()), vp(items.data_ptr()),
+                                                    vp(status.data_ptr()), st))
+            if int(status.item()) != 0:
+                raise KiddoGpuError(int(status.item()), "forest fill overflowed its capacity")
+            return WithinResult(off, dist[:total], items[:total])
+        w = 1 if self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE) else self.max_qty
+        dist = torch.empty((nq, w), dtype=tdt, device=dev)
+        items = torch.empty((nq, w), dtype=torch.int32, device=dev)
+        counts = torch.empty(nq, dtype=torch.int32, device=dev)
+        C.check(L.kgpu_forest_query(f._h, ctypes.byref(d), vp(q.data_ptr()), vp(tof.data_ptr()),
+                                    rp, nq, vp(dist.data_ptr()), vp(items.data_ptr()),
+                                    vp(counts.data_ptr()), st))
+        if self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE):
+            return NearestOneResult(dist[:, 0], items[:, 0])
+        return NearestNResult(dist, items, counts)
+
+
+class CapturedGraph:
+    """CUDA-graph capture of device-pointer engine calls on a stream.
+
+        g = CapturedGraph(stream)
+        with g:                      # cudaStreamBeginCapture ... EndCapture
+            forest.query(...).best_n_within(...).on_stream(stream).execute_gpu()
+        g.replay()
+    Only calls that never read back to the host can be captured (see
+    include/kiddo_gpu.h).
+    """
+
+    def __init__(self, stream):
+        self.stream = stream
+        self._g = None
+
+    def __enter__(self):
+        C.check(C.lib().kgpu_graph_begin(_stream_ptr(self.stream)))
+        return self
+
+    def __exit__(self, exc_type, exc, tb):
+        h = ctypes.c_void_p()
+        st = C.lib().kgpu_graph_end(_stream_ptr(self.stream), ctypes.byref(h))
+        if exc_type is None:
+            C.check(st)
+            self._g = h
+        return False
+
+    def replay(self):
+        C.check(C.lib().kgpu_graph_launch(self._g, _stream_ptr(self.stream)))
+
+    def __del__(self):
+        if getattr(self, "_g", None) and C._lib is not None:
+            C._lib.kgpu_graph_destroy(self._g)
+            self._g = None

@@ -33,6 +33,9 @@ EXPORTED_SYMBOLS = [
     "kgpu_layout_describe", "kgpu_layout_free", "kgpu_tree_create", "kgpu_tree_destroy",
     "kgpu_tree_info", "kgpu_query", "kgpu_query_radius_count", "kgpu_query_radius_fill",
     "kgpu_launch_count", "kgpu_query_stats", "kgpu_query_radius_count_noalloc",
+    "kgpu_forest_create", "kgpu_forest_destroy", "kgpu_forest_query",
+    "kgpu_forest_query_radius_count", "kgpu_forest_query_radius_fill", "kgpu_graph_begin",
+    "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy",
 ]
 
 
@@ -104,6 +107,26 @@ def lib():
     L.kgpu_query_radius_count_noalloc.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, u64, vp, vp]
     L.kgpu_query_stats.restype = i32
     L.kgpu_query_stats.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, u64, vp, vp]
+    L.kgpu_forest_create.restype = i32
+    L.kgpu_forest_create.argtypes = [vp, u32, vp, ctypes.POINTER(vp)]
+    L.kgpu_forest_destroy.restype = i32
+    L.kgpu_forest_destroy.argtypes = [vp]
+    L.kgpu_forest_query.restype = i32
+    L.kgpu_forest_query.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, vp, vp, u64, vp, vp, vp, vp]
+    L.kgpu_forest_query_radius_count.restype = i32
+    L.kgpu_forest_query_radius_count.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, vp, vp, u64,
+                                                 vp, vp]
+    L.kgpu_forest_query_radius_fill.restype = i32
+    L.kgpu_forest_query_radius_fill.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, vp, vp, u64,
+                                                vp, u64, vp, vp, vp, vp]
+    L.kgpu_graph_begin.restype = i32
+    L.kgpu_graph_begin.argtypes = [vp]
+    L.kgpu_graph_end.restype = i32
+    L.kgpu_graph_end.argtypes = [vp, ctypes.POINTER(vp)]
+    L.kgpu_graph_launch.restype = i32
+    L.kgpu_graph_launch.argtypes = [vp, vp]
+    L.kgpu_graph_destroy.restype = i32
+    L.kgpu_graph_destroy.argtypes = [vp]
     if L.kgpu_abi_version() != ABI_VERSION:
         raise ImportError("libkiddo_gpu.so ABI version mismatch")
     _lib = L

@@ -22,18 +22,12 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-f
               "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]
 
-CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu",
+CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kgpu_forest.cu",
               "kernels_f32_warp.cu",
-              "kernels_f32_t1.cu",
-              "kernels_f32_t4.cu",
-              "kernels_f32_t8.cu",
-              "kernels_f32_t16.cu",
+              "kernels_f32_thread.cu",
               "kernels_f32_radius.cu",
               "kernels_f64_warp.cu",
-              "kernels_f64_t1.cu",
-              "kernels_f64_t4.cu",
-              "kernels_f64_t8.cu",
-              "kernels_f64_t16.cu",
+              "kernels_f64_thread.cu",
               "kernels_f64_radius.cu",
               ]
 CXX_SOURCES = ["layout_build.cpp"]

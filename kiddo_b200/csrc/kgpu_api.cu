@@ -315,15 +315,8 @@ void apply_periodic(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch&
 
 template <typename A>
 cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
-  const bool list_family = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
-                           q.family == KGPU_BEST_N_WITHIN;
-  const bool thread = q.engine != 1 && !q.periodic && (t.dims == 2 || t.dims == 3) &&
-                      (!list_family || q.k <= 16);
-  if (!thread) return launch_wfixed<A>(t, q);
-  if (!list_family || q.k <= 1) return launch_tfixed<A, 1>(t, q);
-  if (q.k <= 4) return launch_tfixed<A, 4>(t, q);
-  if (q.k <= 8) return launch_tfixed<A, 8>(t, q);
-  return launch_tfixed<A, 16>(t, q);
+  const bool thread = q.engine != 1 && !q.periodic && (t.dims == 2 || t.dims == 3);
+  return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);
 }
 template cudaError_t launch_fixed<float>(const DeviceTree&, const QueryLaunch&);
 template cudaError_t launch_fixed<double>(const DeviceTree&, const QueryLaunch&);
@@ -536,9 +529,9 @@ int32_t kgpu_query_radius_fill(kgpu_tree* t, const kgpu_query_desc* d, const voi
     if ((e = sd.alloc(total * sa, s)) != cudaSuccess || (e = si.alloc(total * 4, s)) != cudaSuccess)
       return set_error(KGPU_ENOMEM, "device allocation failed");
     e = dt.dtype == KGPU_F64
-            ? launch_seg_sort<double>(doff, nq, static_cast<double*>(q.out_d), q.out_i,
+            ? launch_seg_sort<double>(doff, nq, total, static_cast<double*>(q.out_d), q.out_i,
                                       sd.as<double>(), si.as<uint32_t>(), s)
-            : launch_seg_sort<float>(doff, nq, static_cast<float*>(q.out_d), q.out_i,
+            : launch_seg_sort<float>(doff, nq, total, static_cast<float*>(q.out_d), q.out_i,
                                      sd.as<float>(), si.as<uint32_t>(), s);
     if (e != cudaSuccess) return cuda_fail(e, "launching the segmented sort");
   }

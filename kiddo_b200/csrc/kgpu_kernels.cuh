@@ -36,11 +36,19 @@ struct Batch {
   uint64_t nq;
   const TreeView<A>* __restrict__ forest;
   const uint32_t* __restrict__ tree_of;
+  uint32_t n_trees;
   const A* __restrict__ radii;
   unsigned long long* __restrict__ work;
 
+  // A query naming no tree of the forest sees an empty tree (no results).
   __device__ __forceinline__ TreeView<A> tree(const TreeView<A>& tv, uint64_t qi) const {
-    return forest ? forest[tree_of[qi]] : tv;
+    if (!forest) return tv;
+    const uint32_t t = tree_of[qi];
+    if (t < n_trees) return forest[t];
+    TreeView<A> empty = tv;
+    empty.size = 0;
+    empty.leaf_count = 0;
+    return empty;
   }
   __device__ __forceinline__ A radius(A r, uint64_t qi) const { return radii ? radii[qi] : r; }
   template <int K>
@@ -198,15 +206,21 @@ __device__ __forceinline__ void flush_stats(unsigned long long* stats, const Tra
   }
 }
 
-template <typename A, int K, typename M, int FAM, bool EXCL, int KC>
-__global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int k, A radius0,
-                                                int arrival_order, A* __restrict__ out_d,
+// Shared memory: the continuation slots ((max_stem_level + 2) * blockDim
+// values of A), then for the list families k distances and k items per thread.
+template <typename A, int K, typename M, int FAM, bool EXCL>
+__global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k,
+                                                A radius0, int arrival_order,
+                                                A* __restrict__ out_d,
                                                 uint32_t* __restrict__ out_i,
                                                 uint32_t* __restrict__ out_c,
                                                 unsigned long long* __restrict__ stats) {
   extern __shared__ __align__(16) unsigned char tsmem[];
-  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
   const int stride = blockDim.x;
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  A* list_d = reinterpret_cast<A*>(tsmem) + size_t(levels) * stride + threadIdx.x;
+  uint32_t* list_i = reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(tsmem) +
+                                                 size_t(levels + k) * stride) + threadIdx.x;
   TravStats st;
   for_each_query_thread(b, [&](uint64_t qi) {
     const TreeView<A> tv = b.tree(tv0, qi);
@@ -230,11 +244,11 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int
       out_i[qi] = pol.item;
       if (out_c) out_c[qi] = 1;
     } else if constexpr (FAM == KF_NEAREST_N) {
-      TNearestN<A, K, M, EXCL, KC> pol(k, radius);
+      TNearestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius);
       thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
       pol.write(qi, out_d, out_i, out_c, arrival_order != 0);
     } else {
-      TBestN<A, K, M, EXCL, KC> pol(k, radius);
+      TBestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius);
       thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
       pol.write(qi, out_d, out_i, out_c);
     }
@@ -370,14 +384,15 @@ __device__ __forceinline__ bool key_less(A da, uint32_t pa, A db, uint32_t pb) {
 
 template <typename A>
 __global__ void __launch_bounds__(256) k_seg_sort_warp(const uint64_t* __restrict__ offsets,
-                                                       uint64_t nq, A* __restrict__ d,
+                                                       uint64_t nq, uint64_t capacity,
+                                                       A* __restrict__ d,
                                                        uint32_t* __restrict__ it) {
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
   for (uint64_t s = warp; s < nq; s += nwarps) {
-    const uint64_t o = offsets[s];
-    const uint64_t n = offsets[s + 1] - o;
+    const uint64_t o = min(offsets[s], capacity);
+    const uint64_t n = min(offsets[s + 1], capacity) - o;
     if (n <= 1 || n > 32) continue;
     A kd = inf_of<A>();
     uint32_t kp = 0xffffffffu, kv = 0;
@@ -458,7 +473,8 @@ __device__ bool block_merge_sort(A* d0, uint32_t* i0, A* d1, uint32_t* i1, uint3
 // global memory with `scratch` as the second buffer.
 template <typename A>
 __global__ void __launch_bounds__(256) k_seg_sort_block(const uint64_t* __restrict__ offsets,
-                                                        uint64_t nq, A* __restrict__ d,
+                                                        uint64_t nq, uint64_t capacity,
+                                                        A* __restrict__ d,
                                                         uint32_t* __restrict__ it,
                                                         A* __restrict__ scratch_d,
                                                         uint32_t* __restrict__ scratch_i,
@@ -472,7 +488,7 @@ __global__ void __launch_bounds__(256) k_seg_sort_block(const uint64_t* __restri
   {
     const uint64_t s = first + threadIdx.x;
     if (s < nq) {
-      const uint64_t n = offsets[s + 1] - offsets[s];
+      const uint64_t n = min(offsets[s + 1], capacity) - min(offsets[s], capacity);
       if (n > 32) list[atomicAdd(&list_n, 1u)] = uint32_t(threadIdx.x);
     }
   }
@@ -484,8 +500,8 @@ __global__ void __launch_bounds__(256) k_seg_sort_block(const uint64_t* __restri
   uint32_t* si1 = si0 + smem_cap;
   for (uint32_t j = 0; j < cnt; ++j) {
     const uint64_t s = first + list[j];
-    const uint64_t o = offsets[s];
-    const uint32_t n = uint32_t(offsets[s + 1] - o);
+    const uint64_t o = min(offsets[s], capacity);
+    const uint32_t n = uint32_t(min(offsets[s + 1], capacity) - o);
     if (n <= smem_cap) {
       for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) { sd0[x] = d[o + x]; si0[x] = it[o + x]; }
       __syncthreads();
@@ -528,7 +544,7 @@ __global__ void __launch_bounds__(256) k_leaf_histogram(TreeView<A> tv0, Batch<A
     A q[K];
     b.query(i, q);
     uint64_t l = tv.leaf_count > 1 ? straight_leaf<A, K>(tv, q) : 0u;
-    if (leaf_base) l += leaf_base[b.tree_of[i]];
+    if (leaf_base) l += b.tree_of[i] < b.n_trees ? leaf_base[b.tree_of[i]] : 0u;
     leaf_of[i] = uint32_t(l);
     atomicAdd(counts + l, 1ull);
   }

@@ -43,6 +43,7 @@ struct QueryLaunch {
   // batches over many trees (see kgpu_forest_*): device arrays, or null
   const void* forest = nullptr;          // TreeView<A>[n_trees]
   const uint32_t* tree_of = nullptr;     // tree of each query
+  uint32_t n_trees = 0;
   const uint64_t* leaf_base = nullptr;   // first global leaf number of each tree
   uint64_t total_leaves = 0;             // leaves of all trees (spatial order)
   const void* radii = nullptr;           // per-query radius (A), or null
@@ -55,11 +56,11 @@ struct QueryLaunch {
 // process-wide count of kernel launches made by this library
 extern std::atomic<uint64_t> g_launches;
 
-// Fixed-size families: dispatches to the thread engine (2-D/3-D trees, k <= 16)
-// or the warp engine (everything else, periodic included).
+// Fixed-size families: dispatches to the thread engine (2-D/3-D trees) or the
+// warp engine (everything else, periodic included).
 template <typename A> cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q);
-template <typename A, int KC> cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q);
+template <typename A> cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q,
                                                        uint64_t* counts);
 template <typename A> cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
@@ -71,9 +72,11 @@ template <typename A> cudaError_t launch_spatial_order(const DeviceTree& t, cons
                                                        uint32_t* order, void* scratch);
 
 // Stable sort of every CSR segment by distance; scratch holds total entries.
-template <typename A> cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d,
-                                                  uint32_t* it, A* scratch_d,
-                                                  uint32_t* scratch_i, cudaStream_t s);
+// Segments are clamped to the first `capacity` entries.
+template <typename A> cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq,
+                                                  uint64_t capacity, A* d, uint32_t* it,
+                                                  A* scratch_d, uint32_t* scratch_i,
+                                                  cudaStream_t s);
 
 // offsets[0..n] = exclusive prefix sum of counts[0..n) (offsets[n] = total).
 // `counts` and `offsets` may alias.  tmp needs scan_tmp_bytes(n) bytes.

@@ -65,6 +65,7 @@ inline Batch<A> make_batch(const QueryLaunch& q) {
   b.nq = q.nq;
   b.forest = static_cast<const TreeView<A>*>(q.forest);
   b.tree_of = q.tree_of;
+  b.n_trees = q.n_trees;
   b.radii = static_cast<const A*>(q.radii);
   b.work = q.work;
   return b;
@@ -137,14 +138,19 @@ cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
   });
 }
 
-// Thread-per-query fixed-size families for one list size KC (nearest_one and
-// approx use KC == 1).  Only 2-D and 3-D trees; the caller checks.
-template <typename A, int KC>
+// Thread-per-query fixed-size families.  Only 2-D and 3-D trees; the caller
+// checks.  Shared memory per block: continuation slots plus, for the list
+// families, k (distance, item) pairs per thread.
+template <typename A>
 cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
   const TreeView<A> tv = make_view<A>(t);
   const Batch<A> b = make_batch<A>(q);
   const A radius = A(q.radius);
-  const size_t smem = thread_smem<A>(t);
+  const int levels = t.max_stem_level + 2;
+  const bool list = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
+                    q.family == KGPU_BEST_N_WITHIN;
+  const size_t smem = size_t(levels) * 256 * sizeof(A) +
+                      (list ? size_t(q.k) * 256 * (sizeof(A) + sizeof(uint32_t)) : 0);
   return with_dims(t.dims, [&](auto kk) -> cudaError_t {
     constexpr int K = decltype(kk)::value;
     if constexpr (!thread_engine_dims(K)) {
@@ -157,21 +163,23 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
           auto runt = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
-            kern<<<grid, 256, smem, q.stream>>>(tv, b, q.k, radius, q.sorted ? 0 : 1,
+            kern<<<grid, 256, smem, q.stream>>>(tv, b, levels, q.k, radius, q.sorted ? 0 : 1,
                                                 static_cast<A*>(q.out_d), q.out_i, q.out_c,
                                                 q.stats);
             g_launches++;
             return cudaGetLastError();
           };
-          if constexpr (KC == 1) {
-            if (q.family == KGPU_NEAREST_ONE)
-              return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false, 1>);
-            if (q.family == KGPU_APPROX_NEAREST_ONE)
-              return runt(k_tfixed<A, K, M, KF_APPROX, false, 1>);
+          switch (q.family) {
+            case KGPU_NEAREST_ONE:
+              return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false>);
+            case KGPU_APPROX_NEAREST_ONE:
+              return runt(k_tfixed<A, K, M, KF_APPROX, false>);
+            case KGPU_NEAREST_N:
+            case KGPU_NEAREST_N_WITHIN:
+              return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX>);
+            case KGPU_BEST_N_WITHIN:
+              return runt(k_tfixed<A, K, M, KF_BEST_N, EX>);
           }
-          if (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN)
-            return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX, KC>);
-          if (q.family == KGPU_BEST_N_WITHIN) return runt(k_tfixed<A, K, M, KF_BEST_N, EX, KC>);
           return cudaErrorInvalidValue;
         });
       });
@@ -248,13 +256,13 @@ cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
 }
 
 template <typename A>
-cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d, uint32_t* it,
-                            A* scratch_d, uint32_t* scratch_i, cudaStream_t s) {
+cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, uint64_t capacity, A* d,
+                            uint32_t* it, A* scratch_d, uint32_t* scratch_i, cudaStream_t s) {
   if (nq == 0) return cudaSuccess;
   {
     auto kern = k_seg_sort_warp<A>;
     const int grid = grid_for(kern, 0, nq);
-    kern<<<grid, 256, 0, s>>>(offsets, nq, d, it);
+    kern<<<grid, 256, 0, s>>>(offsets, nq, capacity, d, it);
     g_launches++;
   }
   {
@@ -264,7 +272,8 @@ cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, A* d, uint32_t
     auto kern = k_seg_sort_block<A>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     const uint64_t blocks = (nq + 255) / 256;
-    kern<<<unsigned(blocks), 256, smem, s>>>(offsets, nq, d, it, scratch_d, scratch_i, cap);
+    kern<<<unsigned(blocks), 256, smem, s>>>(offsets, nq, capacity, d, it, scratch_d, scratch_i,
+                                             cap);
     g_launches++;
   }
   return cudaGetLastError();
@@ -314,9 +323,9 @@ cudaError_t launch_spatial_order(const DeviceTree& t, const QueryLaunch& q, uint
   template cudaError_t launch_wfixed<A>(const DeviceTree&, const QueryLaunch&);                  \
   }
 
-#define KGPU_INSTANTIATE_THREAD(A, KC)                                                           \
+#define KGPU_INSTANTIATE_THREAD(A)                                                               \
   namespace kgpu {                                                                               \
-  template cudaError_t launch_tfixed<A, KC>(const DeviceTree&, const QueryLaunch&);              \
+  template cudaError_t launch_tfixed<A>(const DeviceTree&, const QueryLaunch&);                  \
   }
 
 #define KGPU_INSTANTIATE_RADIUS(A)                                                               \
@@ -324,8 +333,8 @@ cudaError_t launch_spatial_order(const DeviceTree& t, const QueryLaunch& q, uint
   template cudaError_t launch_within_count<A>(const DeviceTree&, const QueryLaunch&, uint64_t*); \
   template cudaError_t launch_within_fill<A>(const DeviceTree&, const QueryLaunch&,              \
                                              const uint64_t*);                                   \
-  template cudaError_t launch_seg_sort<A>(const uint64_t*, uint64_t, A*, uint32_t*, A*,          \
-                                          uint32_t*, cudaStream_t);                              \
+  template cudaError_t launch_seg_sort<A>(const uint64_t*, uint64_t, uint64_t, A*, uint32_t*,    \
+                                          A*, uint32_t*, cudaStream_t);                          \
   template cudaError_t launch_spatial_order<A>(const DeviceTree&, const QueryLaunch&, uint32_t*, \
                                                void*);                                           \
   }

@@ -182,77 +182,64 @@ struct TNearestOne {
   }
 };
 
-// k smallest by (distance, arrival) in a register list of KC slots: the
-// ThresholdVecResultCollection of results/result_collection.rs:136-215.
-// While filling, hits are appended in arrival order; when the k-th arrives the
-// list is sorted once by (distance, arrival) — a stable sort, as std's
-// small-slice sort is — and later hits are inserted after equal distances,
-// evicting the last.  A list that never fills stays in arrival order, which is
-// exactly ThresholdVec::into_vec; the sorted output sorts it at the end.
-template <typename A, int K, typename M, bool kExclusive, int KC>
+// k smallest by (distance, arrival): the ThresholdVecResultCollection of
+// results/result_collection.rs:136-215.  The list lives in shared memory, one
+// column per thread (slot j of thread t at j * stride + t, so a warp touches
+// 32 distinct banks whatever slot each thread is on).  While filling, hits are
+// appended in arrival order; when the k-th arrives the list is sorted once,
+// stably, by distance (std's small-slice sort is an insertion sort); after
+// that a hit is inserted after equal distances, evicting the last.  A list
+// that never fills stays in arrival order, which is ThresholdVec::into_vec;
+// the sorted output sorts it at the end.
+template <typename A, int K, typename M, bool kExclusive>
 struct TNearestN {
   static constexpr bool kPruneOnEqual = kExclusive;
-  A ld[KC];
-  uint32_t li[KC];
+  A* __restrict__ ld;
+  uint32_t* __restrict__ li;
+  int stride;
   int n, k;
   A radius, kth;
-  __device__ TNearestN(int k_, A r) : n(0), k(k_), radius(r), kth(inf_of<A>()) {
-#pragma unroll
-    for (int j = 0; j < KC; ++j) { ld[j] = inf_of<A>(); li[j] = 0xffffffffu; }
-  }
+  __device__ TNearestN(A* d, uint32_t* i, int s, int k_, A r)
+      : ld(d), li(i), stride(s), n(0), k(k_), radius(r), kth(inf_of<A>()) {}
   __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
 
-  // Stable sort of the list by distance: odd-even transposition network that
-  // swaps only on a strict `>`, so equal distances keep arrival order (slots
-  // past the held entries hold +inf and stay behind).
-  __device__ __forceinline__ void sort_list() {
-#pragma unroll
-    for (int round = 0; round < KC; ++round) {
-#pragma unroll
-      for (int j = round & 1; j + 1 < KC; j += 2) {
-        if (ld[j] > ld[j + 1]) {
-          const A td = ld[j]; ld[j] = ld[j + 1]; ld[j + 1] = td;
-          const uint32_t ti = li[j]; li[j] = li[j + 1]; li[j + 1] = ti;
-        }
+  // stable insertion sort of the m held entries
+  __device__ __forceinline__ void sort_held(int m) {
+    for (int a = 1; a < m; ++a) {
+      const A d = ld[a * stride];
+      const uint32_t it = li[a * stride];
+      int j = a;
+      while (j > 0 && ld[(j - 1) * stride] > d) {
+        ld[j * stride] = ld[(j - 1) * stride];
+        li[j * stride] = li[(j - 1) * stride];
+        --j;
       }
+      ld[j * stride] = d;
+      li[j * stride] = it;
     }
-  }
-
-  __device__ __forceinline__ void refresh_kth() {
-    A t = ld[0];
-#pragma unroll
-    for (int j = 1; j < KC; ++j)
-      if (j == k - 1) t = ld[j];
-    kth = t;
   }
 
   __device__ __forceinline__ void add(A d, uint32_t it) {
     if (n < k) {
-#pragma unroll
-      for (int j = 0; j < KC; ++j)
-        if (j == n) { ld[j] = d; li[j] = it; }
-      ++n;
-      if (n == k) {
-        sort_list();
-        refresh_kth();
+      ld[n * stride] = d;
+      li[n * stride] = it;
+      if (++n == k) {
+        sort_held(k);
+        kth = ld[(k - 1) * stride];
       }
       return;
     }
     if (!(d < kth)) return;
-#pragma unroll
-    for (int j = KC - 1; j >= 0; --j) {
-      if (j < k) {
-        if (j > 0 && ld[j - 1] > d) {
-          ld[j] = ld[j - 1];
-          li[j] = li[j - 1];
-        } else if (ld[j] > d) {
-          ld[j] = d;
-          li[j] = it;
-        }
-      }
+    int j = k - 1;
+    while (j > 0 && ld[(j - 1) * stride] > d) {
+      ld[j * stride] = ld[(j - 1) * stride];
+      li[j * stride] = li[(j - 1) * stride];
+      --j;
     }
-    refresh_kth();
+    ld[j * stride] = d;
+    li[j * stride] = it;
+    kth = ld[(k - 1) * stride];
   }
 
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
@@ -266,15 +253,12 @@ struct TNearestN {
   __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
                                         uint32_t* __restrict__ out_i,
                                         uint32_t* __restrict__ out_c, bool arrival_order) {
-    if (n < k && !arrival_order) sort_list();
+    if (n < k && !arrival_order) sort_held(n);
     A* od = out_d + size_t(qi) * k;
     uint32_t* oi = out_i + size_t(qi) * k;
-#pragma unroll
-    for (int j = 0; j < KC; ++j) {
-      if (j < k) {
-        od[j] = j < n ? ld[j] : inf_of<A>();
-        oi[j] = j < n ? li[j] : 0xffffffffu;
-      }
+    for (int j = 0; j < k; ++j) {
+      od[j] = j < n ? ld[j * stride] : inf_of<A>();
+      oi[j] = j < n ? li[j * stride] : 0xffffffffu;
     }
     if (out_c) out_c[qi] = uint32_t(n);
   }
@@ -282,47 +266,39 @@ struct TNearestN {
 
 // best_n_within: the n smallest items among hits, by (item, arrival)
 // (kd_tree/query/best_n_within.rs:88-196, leaf filter
-// leaf_view_chunked/best_n_within/fallback.rs:40-104).
-template <typename A, int K, typename M, bool kExclusive, int KC>
+// leaf_view_chunked/best_n_within/fallback.rs:40-104); list in shared memory
+// kept sorted by item.
+template <typename A, int K, typename M, bool kExclusive>
 struct TBestN {
   static constexpr bool kPruneOnEqual = kExclusive;
-  A ld[KC];
-  uint32_t li[KC];
+  A* __restrict__ ld;
+  uint32_t* __restrict__ li;
+  int stride;
   int n, k;
   A radius;
-  __device__ TBestN(int k_, A r) : n(0), k(k_), radius(r) {
-#pragma unroll
-    for (int j = 0; j < KC; ++j) { ld[j] = inf_of<A>(); li[j] = 0xffffffffu; }
-  }
+  __device__ TBestN(A* d, uint32_t* i, int s, int k_, A r)
+      : ld(d), li(i), stride(s), n(0), k(k_), radius(r) {}
   __device__ __forceinline__ A max_dist() const { return radius; }
   __device__ __forceinline__ bool unbounded_start() const { return false; }
-  __device__ __forceinline__ uint32_t last_item() const {
-    uint32_t t = li[0];
-#pragma unroll
-    for (int j = 1; j < KC; ++j)
-      if (j == k - 1) t = li[j];
-    return t;
-  }
   __device__ __forceinline__ void add(A d, uint32_t it) {
-    if (n == k && !(it < last_item())) return;
-    const int m = n < k ? n + 1 : k;
-#pragma unroll
-    for (int j = KC - 1; j >= 0; --j) {
-      if (j < m) {
-        if (j > 0 && li[j - 1] > it) {
-          ld[j] = ld[j - 1];
-          li[j] = li[j - 1];
-        } else if (j == n || li[j] > it) {
-          ld[j] = d;
-          li[j] = it;
-        }
-      }
+    int j;
+    if (n < k) {
+      j = n++;
+    } else {
+      if (!(it < li[(k - 1) * stride])) return;
+      j = k - 1;
     }
-    n = m;
+    while (j > 0 && li[(j - 1) * stride] > it) {
+      ld[j * stride] = ld[(j - 1) * stride];
+      li[j * stride] = li[(j - 1) * stride];
+      --j;
+    }
+    ld[j * stride] = d;
+    li[j * stride] = it;
   }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
     const bool full_at_entry = n == k;
-    const uint32_t thr_item = last_item();
+    const uint32_t thr_item = full_at_entry ? li[(k - 1) * stride] : 0u;
     const CartesianQ<A, K, M> dist{q};
     return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
       if (!(kExclusive ? (d < radius) : (d <= radius))) return;
@@ -335,12 +311,9 @@ struct TBestN {
                                         uint32_t* __restrict__ out_c) const {
     A* od = out_d + size_t(qi) * k;
     uint32_t* oi = out_i + size_t(qi) * k;
-#pragma unroll
-    for (int j = 0; j < KC; ++j) {
-      if (j < k) {
-        od[j] = j < n ? ld[j] : inf_of<A>();
-        oi[j] = j < n ? li[j] : 0xffffffffu;
-      }
+    for (int j = 0; j < k; ++j) {
+      od[j] = j < n ? ld[j * stride] : inf_of<A>();
+      oi[j] = j < n ? li[j * stride] : 0xffffffffu;
     }
     if (out_c) out_c[qi] = uint32_t(n);
   }
