@@ -284,7 +284,7 @@ int32_t kgpu_forest_query_radius_fill(kgpu_forest* f, const kgpu_query_desc* d,
 int32_t kgpu_graph_begin(void* stream) {
   if (!stream) return set_error(KGPU_EINVAL, "capture needs a stream other than the legacy default");
   cudaError_t e = cudaStreamBeginCapture(static_cast<cudaStream_t>(stream),
-                                         cudaStreamCaptureModeThreadLocal);
+                                         cudaStreamCaptureModeRelaxed);
   return e == cudaSuccess ? KGPU_OK : cuda_err(e, "cudaStreamBeginCapture");
 }
 
