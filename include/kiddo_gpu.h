@@ -242,6 +242,26 @@ int32_t kgpu_forest_query_radius_fill(kgpu_forest* forest, const kgpu_query_desc
                                       uint64_t capacity, void* out_dists, uint32_t* out_items,
                                       int32_t* status, void* stream);
 
+/* ---- Chamfer / ICP neighbour loss and its adjoint ------------------------
+ * No counterpart in the reference (an addition built on the nearest_n path).
+ * f32, 3-D, device pointers.  With the neighbours of each source point from a
+ * nearest_n query (SquaredEuclidean) on the target tree:
+ *   L = sum_i sum_{j < counts[i]} phi(d_ij),  phi(d) = d * exp(-d / (2 sigma^2)).
+ * kgpu_chamfer_loss reduces phi over dists[n_src * k] in a fixed order into
+ * *loss (device float); per_src (optional) receives each source's term.
+ * kgpu_chamfer_backward writes grad_scale * dL/dsrc [n_src, 3] and
+ * grad_scale * dL/dtgt [n_tgt, 3] (either may be NULL).  items[n_src * k] are
+ * the neighbours' items = row numbers into tgt (new_from_slice); for batches
+ * of cloud pairs, tree_of[i] names the pair of source i and tgt_base[pair]
+ * the first row of that pair's targets in tgt.  Deterministic: fixed-order
+ * sums and an integer counting sort, no floating-point atomics. */
+int32_t kgpu_chamfer_loss(const float* dists, const uint32_t* counts, uint64_t n_src, uint32_t k,
+                          double sigma, float* per_src, float* loss, void* stream);
+int32_t kgpu_chamfer_backward(const float* src, uint64_t n_src, const float* tgt, uint64_t n_tgt,
+                              const uint32_t* items, const uint32_t* counts, uint32_t k,
+                              const uint32_t* tree_of, const uint64_t* tgt_base, double sigma,
+                              float grad_scale, float* grad_src, float* grad_tgt, void* stream);
+
 /* ---- CUDA graphs --------------------------------------------------------
  * Capture a sequence of device-pointer calls on `stream` (not the legacy
  * default stream) and replay it.  Capturable: kgpu_query, kgpu_query_radius_count,

@@ -35,7 +35,8 @@ EXPORTED_SYMBOLS = [
     "kgpu_launch_count", "kgpu_query_stats", "kgpu_query_radius_count_noalloc",
     "kgpu_forest_create", "kgpu_forest_destroy", "kgpu_forest_query",
     "kgpu_forest_query_radius_count", "kgpu_forest_query_radius_fill", "kgpu_graph_begin",
-    "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy",
+    "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy", "kgpu_chamfer_loss",
+    "kgpu_chamfer_backward",
 ]
 
 
@@ -127,6 +128,11 @@ def lib():
     L.kgpu_graph_launch.argtypes = [vp, vp]
     L.kgpu_graph_destroy.restype = i32
     L.kgpu_graph_destroy.argtypes = [vp]
+    L.kgpu_chamfer_loss.restype = i32
+    L.kgpu_chamfer_loss.argtypes = [vp, vp, u64, u32, ctypes.c_double, vp, vp, vp]
+    L.kgpu_chamfer_backward.restype = i32
+    L.kgpu_chamfer_backward.argtypes = [vp, u64, vp, u64, vp, vp, u32, vp, vp, ctypes.c_double,
+                                        ctypes.c_float, vp, vp, vp]
     if L.kgpu_abi_version() != ABI_VERSION:
         raise ImportError("libkiddo_gpu.so ABI version mismatch")
     _lib = L
