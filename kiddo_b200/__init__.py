@@ -345,6 +345,20 @@ class QueryBuilder:
         self.engine = engine
         return self
 
+    def autotuned(self, tune_if_missing: bool = True) -> "QueryBuilder":
+        """Apply the cached autotuner choice of engine and processing order for
+        this kind of query (kiddo_b200.autotune); tune on a sample of this batch
+        if there is none yet.  Device batches only; results are unchanged."""
+        from . import autotune
+        if self.family is None:
+            raise TypeError("choose a query type before autotuned()")
+        choice = autotune.lookup(self)
+        if choice is None and tune_if_missing and _is_torch_cuda(self.queries):
+            choice = autotune.tune(self)
+        if choice is not None:
+            self.engine, self.spatial_order = choice
+        return self
+
     def on_stream(self, stream) -> "QueryBuilder":
         self.stream = stream
         return self

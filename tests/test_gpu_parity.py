@@ -275,3 +275,20 @@ def test_spatial_order_gives_identical_results(engine):
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "ordered nn1")
     g = t.query(Q).with_engine(engine).with_spatial_order().within(kb.SquaredEuclidean, 1e-4).execute_gpu()
     assert_same_csr((g.offsets, g.distances, g.items), o.within(Q, 1e-4), "ordered within")
+
+
+def test_autotuner_caches_a_choice_and_keeps_results(tmp_path, monkeypatch):
+    import torch
+    monkeypatch.setenv("KIDDO_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    rng = np.random.default_rng(41)
+    P = rng.random((300_000, 3)).astype(np.float32)
+    Q = torch.from_numpy(rng.random((100_000, 3)).astype(np.float32)).cuda()
+    t = kb.ImmutableKdTree.new_from_slice(P)
+    plain = t.query(Q).nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
+    b = t.query(Q).nearest_n(kb.SquaredEuclidean, 16).autotuned()
+    assert b.engine in ("warp", "thread")
+    tuned = b.execute_gpu()
+    assert torch.equal(plain.distances, tuned.distances) and torch.equal(plain.items, tuned.items)
+    import json
+    db = json.loads((tmp_path / "tune.json").read_text())
+    assert len(db) == 1 and len(next(iter(db.values()))["ms"]) == 4
