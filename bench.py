@@ -482,6 +482,7 @@ def chamfer_workload(scale, seed=4):
     for p in range(64):
         n = int(np.exp(rng.uniform(np.log(1e4), np.log(1e6))) * scale) + 16
         kind = "plane" if p % 2 == 0 else "sphere"
+        rot, _ = np.linalg.qr(rng.normal(size=(3, 3)))  # one orientation per pair
 
         def cloud(m):
             if kind == "plane":
@@ -489,8 +490,7 @@ def chamfer_workload(scale, seed=4):
             else:
                 v = rng.normal(size=(m, 3))
                 c = 0.5 * v / np.linalg.norm(v, axis=1, keepdims=True)
-            q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
-            return (c @ q + rng.normal(0, 0.001, (m, 3))).astype(np.float32)
+            return (c @ rot + rng.normal(0, 0.001, (m, 3))).astype(np.float32)
         pairs.append((cloud(n), cloud(4 * n)))
     return pairs
 

@@ -40,8 +40,10 @@ def _vp(t):
 def _knn(target, src, k, tree_of):
     from . import Forest, SquaredEuclidean
     if isinstance(target, Forest):
-        return target.query(src, tree_of).nearest_n(SquaredEuclidean, k).execute_gpu()
-    return target.query(src).nearest_n(SquaredEuclidean, k).execute_gpu()
+        b = target.query(src, tree_of)
+    else:
+        b = target.query(src)
+    return b.with_spatial_order().nearest_n(SquaredEuclidean, k).execute_gpu()
 
 
 def chamfer_forward(target, src, tgt_points, k, sigma, tree_of=None, tgt_base=None):

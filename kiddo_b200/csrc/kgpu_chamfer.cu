@@ -133,40 +133,37 @@ __global__ void k_pair_histogram(const uint32_t* __restrict__ items,
   }
 }
 
+// Bucket the pairs by target; inside a bucket the order is arbitrary here and
+// is fixed afterwards by sorting each bucket on the pair id (`key`, exact in
+// a double up to 2^53).
 __global__ void k_pair_scatter(const uint32_t* __restrict__ items,
                                const uint32_t* __restrict__ counts,
                                const uint32_t* __restrict__ tree_of,
                                const uint64_t* __restrict__ tgt_base, uint64_t n_src, int k,
                                const uint64_t* __restrict__ start,
-                               unsigned long long* __restrict__ cursor, uint32_t* __restrict__ pairs) {
+                               unsigned long long* __restrict__ cursor, double* __restrict__ key,
+                               uint32_t* __restrict__ pairs) {
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_src;
        i += uint64_t(gridDim.x) * blockDim.x) {
     const int c = int(counts[i]);
     for (int j = 0; j < c; ++j) {
       const uint64_t m = target_of(items, tree_of, tgt_base, i, k, j);
       const unsigned long long pos = start[m] + atomicAdd(cursor + m, 1ull);
-      pairs[pos] = uint32_t(i * k + j);
+      const uint32_t id = uint32_t(i * k + j);
+      pairs[pos] = id;
+      key[pos] = double(id);
     }
   }
 }
 
-// One target per thread: order its pairs by pair id, then sum in that order.
+// One target per thread: sum its pairs in pair-id order.
 __global__ void k_grad_tgt(const float* __restrict__ src, const float* __restrict__ tgt,
-                           const uint64_t* __restrict__ start, uint32_t* __restrict__ pairs,
+                           const uint64_t* __restrict__ start, const uint32_t* __restrict__ pairs,
                            uint64_t n_tgt, int k, float inv2s2, float scale,
                            float* __restrict__ grad_tgt) {
   for (uint64_t m = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; m < n_tgt;
        m += uint64_t(gridDim.x) * blockDim.x) {
     const uint64_t lo = start[m], hi = start[m + 1];
-    for (uint64_t a = lo + 1; a < hi; ++a) {  // insertion sort of the bucket
-      const uint32_t v = pairs[a];
-      uint64_t b = a;
-      while (b > lo && pairs[b - 1] > v) {
-        pairs[b] = pairs[b - 1];
-        --b;
-      }
-      pairs[b] = v;
-    }
     float t[3];
     load3(tgt, m, t);
     float g[3] = {0.f, 0.f, 0.f};
@@ -246,10 +243,12 @@ int32_t kgpu_chamfer_backward(const float* src, uint64_t n_src, const float* tgt
     g_launches++;
   }
   if (grad_tgt && n_tgt) {
-    DevBuf bucket, cursor, pairs, tmp;
+    DevBuf bucket, cursor, pairs, keys, skeys, spairs, tmp;
+    const uint64_t np = n_src * k;
     if ((e = bucket.alloc((n_tgt + 1) * 8, s)) != cudaSuccess ||
         (e = cursor.alloc(n_tgt * 8, s)) != cudaSuccess ||
-        (e = pairs.alloc(n_src * k * 4, s)) != cudaSuccess ||
+        (e = pairs.alloc(np * 4, s)) != cudaSuccess || (e = keys.alloc(np * 8, s)) != cudaSuccess ||
+        (e = spairs.alloc(np * 4, s)) != cudaSuccess || (e = skeys.alloc(np * 8, s)) != cudaSuccess ||
         (e = tmp.alloc(scan_tmp_bytes(n_tgt), s)) != cudaSuccess)
       return set_error(KGPU_ENOMEM, "device allocation failed");
     if ((e = cudaMemsetAsync(bucket.p, 0, (n_tgt + 1) * 8, s)) != cudaSuccess ||
@@ -267,8 +266,12 @@ int32_t kgpu_chamfer_backward(const float* src, uint64_t n_src, const float* tgt
       k_pair_scatter<<<grid_of(n_src), 256, 0, s>>>(items, counts, tree_of, tgt_base, n_src,
                                                     int(k), bucket.as<uint64_t>(),
                                                     cursor.as<unsigned long long>(),
-                                                    pairs.as<uint32_t>());
+                                                    keys.as<double>(), pairs.as<uint32_t>());
       g_launches++;
+      e = launch_seg_sort<double>(bucket.as<uint64_t>(), n_tgt, np, keys.as<double>(),
+                                  pairs.as<uint32_t>(), skeys.as<double>(), spairs.as<uint32_t>(),
+                                  s);
+      if (e != cudaSuccess) return cuda_err(e, "ordering the pairs");
     }
     k_grad_tgt<<<grid_of(n_tgt), 256, 0, s>>>(src, tgt, bucket.as<uint64_t>(), pairs.as<uint32_t>(),
                                               n_tgt, int(k), inv2s2, grad_scale, grad_tgt);

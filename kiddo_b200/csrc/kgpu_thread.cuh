@@ -24,13 +24,13 @@ namespace kgpu {
 // leaf_view/mod.rs:431-446): f(coords, item) in tile order.
 // Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
 // leaf_view/mod.rs:431-446) calling f(distance, item) in tile order, with
-// distance = dist(coords).  Tiles of width >= 2 are read two points per step
+// distance = dist(coords); pairs where pass() rejects both points skip f.  Tiles of width >= 2 are read two points per step
 // (8-byte aligned pairs for f32: leaves start on 8 bytes and every column of
 // an even-width tile spans an even number of floats); both points then go
 // through one call site of f, so the policy's insertion code is emitted once.
-template <typename A, int K, typename D, typename F>
+template <typename A, int K, typename D, typename P, typename F>
 __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint32_t leaf,
-                                                          const D& dist, F&& f) {
+                                                          const D& dist, P&& pass, F&& f) {
   const uint2 ex = __ldg(tv.extents + leaf);
   const uint8_t* base = tv.arena + size_t(ex.x) * 8;
   uint32_t rem = ex.y;
@@ -66,6 +66,9 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
         i1 = __ldg(its + i + 1);
       }
       const A d0 = dist(c0), d1 = dist(c1);
+      // `pass` is a cheap necessary condition for f to act: most points fail
+      // it once a list has filled, and then f is not entered at all.
+      if (!pass(d0) && !(w > 1 && pass(d1))) continue;
       const int nu = w == 1 ? 1 : 2;
 #pragma unroll 1
       for (int u = 0; u < nu; ++u) f(u ? d1 : d0, u ? i1 : i0);
@@ -176,9 +179,11 @@ struct TNearestOne {
   __device__ __forceinline__ bool unbounded_start() const { return true; }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
     const CartesianQ<A, K, M> dist{q};
-    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
-      if (d < best) { best = d; item = it; }
-    });
+    return thread_for_each_point<A, K>(
+        tv, l, dist, [&](A d) { return d < best; },
+        [&](A d, uint32_t it) {
+          if (d < best) { best = d; item = it; }
+        });
   }
 };
 
@@ -245,9 +250,12 @@ struct TNearestN {
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
     const A bound = max_dist();
     const CartesianQ<A, K, M> dist{q};
-    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
-      if (kExclusive ? (d < bound) : (d <= bound)) add(d, it);
-    });
+    return thread_for_each_point<A, K>(
+        tv, l, dist,
+        [&](A d) { return (kExclusive ? (d < bound) : (d <= bound)) && (n < k || d < kth); },
+        [&](A d, uint32_t it) {
+          if (kExclusive ? (d < bound) : (d <= bound)) add(d, it);
+        });
   }
 
   __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
@@ -300,11 +308,13 @@ struct TBestN {
     const bool full_at_entry = n == k;
     const uint32_t thr_item = full_at_entry ? li[(k - 1) * stride] : 0u;
     const CartesianQ<A, K, M> dist{q};
-    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
-      if (!(kExclusive ? (d < radius) : (d <= radius))) return;
-      if (full_at_entry && it >= thr_item) return;
-      add(d, it);
-    });
+    return thread_for_each_point<A, K>(
+        tv, l, dist, [&](A d) { return kExclusive ? (d < radius) : (d <= radius); },
+        [&](A d, uint32_t it) {
+          if (!(kExclusive ? (d < radius) : (d <= radius))) return;
+          if (full_at_entry && it >= thr_item) return;
+          add(d, it);
+        });
   }
   __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
                                         uint32_t* __restrict__ out_i,
@@ -333,7 +343,9 @@ struct TWithin {
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
     const CartesianQ<A, K, M> dist{q};
-    return thread_for_each_point<A, K>(tv, l, dist, [&](A d, uint32_t it) {
+    return thread_for_each_point<A, K>(
+        tv, l, dist, [&](A d) { return kExclusive ? (d < radius) : (d <= radius); },
+        [&](A d, uint32_t it) {
       if (kExclusive ? (d < radius) : (d <= radius)) {
         if (out_d && count < cap) { out_d[count] = d; out_i[count] = it; }
         ++count;
