@@ -55,6 +55,22 @@ def _vp(a: np.ndarray):
     return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else None
 
 
+def _host_array(shape, dtype):
+    """Result buffer in pinned host memory when torch can provide it (the
+    library then copies results back at full bus speed), else pageable."""
+    n = int(np.prod(shape))
+    if n * np.dtype(dtype).itemsize >= (1 << 20):
+        try:
+            import torch
+            if torch.cuda.is_available():
+                tdt = {np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
+                       np.dtype(np.uint32): torch.int32}[np.dtype(dtype)]
+                return torch.empty(n, dtype=tdt, pin_memory=True).numpy().view(dtype).reshape(shape)
+        except Exception:
+            pass
+    return np.empty(shape, dtype=dtype)
+
+
 def _is_torch_cuda(x) -> bool:
     try:
         import torch
@@ -426,9 +442,9 @@ class QueryBuilder:
                                              _vp(dist), _vp(items), st))
             return WithinResult(off, dist, items)
         w = 1 if self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE) else self.max_qty
-        dist = np.empty((nq, w), dtype=self.tree.dtype)
-        items = np.empty((nq, w), dtype=np.uint32)
-        counts = np.empty(nq, dtype=np.uint32)
+        dist = _host_array((nq, w), self.tree.dtype)
+        items = _host_array((nq, w), np.uint32)
+        counts = _host_array((nq,), np.uint32)
         C.check(L.kgpu_query(self.tree._h, ctypes.byref(d), _vp(q), nq, _vp(dist), _vp(items),
                              _vp(counts), st))
         if w == 1 and self.family in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE):

@@ -347,6 +347,87 @@ int out_width(const kgpu_query_desc* d) {
              : int(d->max_qty);
 }
 
+// Host buffers: the batch goes through in chunks on two internal streams, so
+// the copy of one chunk's queries in, another chunk's kernel and a third
+// chunk's results out run at the same time (full overlap needs pinned host
+// memory).  Work already queued on the caller's stream runs first; the call
+// returns when every result is on the host.
+int query_host_pipelined(const DeviceTree& dt, const kgpu_query_desc* d, const QueryLaunch& base,
+                         const void* queries, uint64_t nq, int w, void* out_dists,
+                         uint32_t* out_items, uint32_t* out_counts, cudaStream_t s) {
+  const size_t sa = dt.dtype == KGPU_F64 ? 8 : 4;
+  const uint64_t chunk = std::min<uint64_t>(nq, uint64_t(1) << 21);
+  const int nslots = nq > chunk ? 2 : 1;
+  cudaStream_t st[2] = {nullptr, nullptr};
+  cudaEvent_t ready = nullptr;
+  cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(ready, s);
+  for (int i = 0; i < nslots && e == cudaSuccess; ++i) {
+    e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st[i], ready, 0);
+  }
+  int status = KGPU_OK;
+  if (e != cudaSuccess) status = cuda_fail(e, "creating the copy streams");
+  {
+    DevBuf bq[2], bd[2], bi[2], bc[2], bord[2], bos[2];
+    for (int i = 0; i < nslots && status == KGPU_OK; ++i) {
+      if ((e = bq[i].alloc(chunk * dt.dims * sa, st[i])) != cudaSuccess ||
+          (e = bd[i].alloc(chunk * w * sa, st[i])) != cudaSuccess ||
+          (e = bi[i].alloc(chunk * w * 4, st[i])) != cudaSuccess ||
+          (out_counts && (e = bc[i].alloc(chunk * 4, st[i])) != cudaSuccess))
+        status = e == cudaErrorMemoryAllocation ? set_error(KGPU_ENOMEM, "device allocation failed")
+                                                : cuda_fail(e, "cudaMallocAsync");
+    }
+    for (uint64_t c0 = 0, ci = 0; c0 < nq && status == KGPU_OK; c0 += chunk, ++ci) {
+      const int slot = int(ci % nslots);
+      cudaStream_t ss = st[slot];
+      const uint64_t nc = std::min(chunk, nq - c0);
+      QueryLaunch q = base;
+      q.nq = nc;
+      q.queries = bq[slot].p;
+      q.out_d = bd[slot].p;
+      q.out_i = bi[slot].as<uint32_t>();
+      q.out_c = out_counts ? bc[slot].as<uint32_t>() : nullptr;
+      q.stream = ss;
+      const char* what = nullptr;
+      if ((e = cudaMemcpyAsync(bq[slot].p, static_cast<const uint8_t*>(queries) + c0 * dt.dims * sa,
+                               nc * dt.dims * sa, cudaMemcpyHostToDevice, ss)) != cudaSuccess) {
+        what = "copying queries to the device";
+      } else {
+        // the order buffers of the previous chunk on this slot are freed on
+        // this stream, after that chunk's kernel
+        bord[slot].~DevBuf();
+        new (&bord[slot]) DevBuf();
+        bos[slot].~DevBuf();
+        new (&bos[slot]) DevBuf();
+        if ((e = maybe_spatial_order(dt, d, q, bord[slot], bos[slot], ss)) != cudaSuccess)
+          what = "ordering the batch";
+        else if ((e = dt.dtype == KGPU_F64 ? run_fixed<double>(dt, q) : run_fixed<float>(dt, q)) !=
+                 cudaSuccess)
+          what = "launching the query kernel";
+        else if ((e = cudaMemcpyAsync(static_cast<uint8_t*>(out_dists) + c0 * w * sa, bd[slot].p,
+                                      nc * w * sa, cudaMemcpyDeviceToHost, ss)) != cudaSuccess ||
+                 (e = cudaMemcpyAsync(out_items + c0 * w, bi[slot].p, nc * w * 4,
+                                      cudaMemcpyDeviceToHost, ss)) != cudaSuccess ||
+                 (out_counts && (e = cudaMemcpyAsync(out_counts + c0, bc[slot].p, nc * 4,
+                                                     cudaMemcpyDeviceToHost, ss)) != cudaSuccess))
+          what = "copying results to the host";
+      }
+      if (what) status = cuda_fail(e, what);
+    }
+    for (int i = 0; i < nslots; ++i)
+      if (st[i] && (e = cudaStreamSynchronize(st[i])) != cudaSuccess && status == KGPU_OK)
+        status = cuda_fail(e, "query execution");
+  }  // device buffers are released on their streams here
+  for (int i = 0; i < nslots; ++i)
+    if (st[i]) {
+      cudaStreamSynchronize(st[i]);
+      cudaStreamDestroy(st[i]);
+    }
+  if (ready) cudaEventDestroy(ready);
+  return status;
+}
+
 }  // namespace
 }  // namespace kgpu
 
@@ -373,41 +454,18 @@ int32_t kgpu_query(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, 
   apply_periodic(dt, d, q);
   q.engine = (d->flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (d->flags & KGPU_FLAG_ENGINE_THREAD) ? 2 : 0;
   const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
-  DevBuf bq, bd, bi, bc;
   cudaError_t e = cudaSuccess;
-  if (host) {
-    const size_t qbytes = nq * dt.dims * sa;
-    if ((e = bq.alloc(qbytes, s)) != cudaSuccess || (e = bd.alloc(nq * w * sa, s)) != cudaSuccess ||
-        (e = bi.alloc(nq * w * 4, s)) != cudaSuccess ||
-        (out_counts && (e = bc.alloc(nq * 4, s)) != cudaSuccess))
-      return e == cudaErrorMemoryAllocation ? set_error(KGPU_ENOMEM, "device allocation failed")
-                                            : cuda_fail(e, "cudaMallocAsync");
-    if ((e = cudaMemcpyAsync(bq.p, queries, qbytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_fail(e, "copying queries to the device");
-    q.queries = bq.p;
-    q.out_d = bd.p;
-    q.out_i = bi.as<uint32_t>();
-    q.out_c = out_counts ? bc.as<uint32_t>() : nullptr;
-  } else {
-    q.queries = queries;
-    q.out_d = out_dists;
-    q.out_i = out_items;
-    q.out_c = out_counts;
-  }
+  if (host) return query_host_pipelined(dt, d, q, queries, nq, w, out_dists, out_items, out_counts, s);
+  q.queries = queries;
+  q.out_d = out_dists;
+  q.out_i = out_items;
+  q.out_c = out_counts;
   q.stream = s;
   DevBuf bord, bos;
   if ((e = maybe_spatial_order(dt, d, q, bord, bos, s)) != cudaSuccess)
     return cuda_fail(e, "ordering the batch");
   e = dt.dtype == KGPU_F64 ? run_fixed<double>(dt, q) : run_fixed<float>(dt, q);
   if (e != cudaSuccess) return cuda_fail(e, "launching the query kernel");
-  if (host) {
-    if ((e = cudaMemcpyAsync(out_dists, bd.p, nq * w * sa, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(out_items, bi.p, nq * w * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-        (out_counts &&
-         (e = cudaMemcpyAsync(out_counts, bc.p, nq * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess))
-      return cuda_fail(e, "copying results to the host");
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "query execution");
-  }
   return KGPU_OK;
 }
 
