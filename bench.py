@@ -229,7 +229,9 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="scale the c3/c4 workloads (tests and profiling only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--spatial-order", action="store_true")
+    ap.add_argument("--spatial-order", default=None, action="store_true",
+                    help="force leaf-grouped processing (default: the library decides)")
+    ap.add_argument("--no-spatial-order", dest="spatial_order", action="store_false")
     ap.add_argument("--engine", default=None, choices=["warp", "thread"],
                     help="force the kernel variant (default: the library chooses)")
     ap.add_argument("--points", type=int, default=0, help="override the tree size (profiling)")
@@ -266,9 +268,7 @@ def main():
 
     def step():
         b = builder_for(gtree, dq, args.workload).with_engine(args.engine)
-        if args.spatial_order:
-            b = b.with_spatial_order()
-        return b.execute_gpu()
+        return b.with_spatial_order(args.spatial_order).execute_gpu()
 
     # algorithmic bytes per query from the engine's own traversal counters
     sub = Q[: min(nq, 2_000_000)]
@@ -327,7 +327,7 @@ def main():
         "config": {"workload": args.workload, "points": n, "queries_per_gpu": nq, "family": fam,
                    "k": k, "metric": "SquaredEuclidean", "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (tree 256 MB, queries 192 MB), no flush",
-                   "spatial_order": bool(args.spatial_order),
+                   "spatial_order": "auto" if args.spatial_order is None else args.spatial_order,
                    "engine": args.engine or "auto"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,

@@ -77,7 +77,9 @@ typedef enum kgpu_family {
 
 /* Query flags */
 #define KGPU_FLAG_HOST_BUFFERS 0x1u  /* queries/outputs are host pointers */
-#define KGPU_FLAG_SPATIAL_ORDER 0x2u /* process queries in leaf order (same results) */
+#define KGPU_FLAG_SPATIAL_ORDER 0x2u /* process queries grouped by leaf (same results); */
+                                     /* default for >= 65,536 queries on >= 4,096 leaves */
+#define KGPU_FLAG_NO_SPATIAL_ORDER 0x10u /* process queries in the order given */
 #define KGPU_FLAG_ENGINE_WARP 0x4u   /* force one warp per query (same results) */
 #define KGPU_FLAG_ENGINE_THREAD 0x8u /* force one thread per query (same results) */
 

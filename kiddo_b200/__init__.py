@@ -276,7 +276,7 @@ class QueryBuilder:
         self.exclusive = False
         self.sorted = True
         self.box = None
-        self.spatial_order = False
+        self.spatial_order = None  # None: the library decides
         self.engine = None
         self.stream = None
 
@@ -348,9 +348,10 @@ class QueryBuilder:
         self.exclusive = True
         return self
 
-    def with_spatial_order(self, on: bool = True) -> "QueryBuilder":
-        """Process the batch in a cache-friendly order (identical results)."""
-        self.spatial_order = bool(on)
+    def with_spatial_order(self, on: Optional[bool] = True) -> "QueryBuilder":
+        """Process the batch grouped by leaf (True), in the given order (False),
+        or let the library decide (None, the default).  Results are identical."""
+        self.spatial_order = None if on is None else bool(on)
         return self
 
     def with_engine(self, engine: Optional[str]) -> "QueryBuilder":
@@ -398,6 +399,7 @@ class QueryBuilder:
         d.periodic_box = self.box.ctypes.data if self.box is not None else None
         d.flags = (C.FLAG_HOST_BUFFERS if host else 0) | (
             C.FLAG_SPATIAL_ORDER if self.spatial_order else 0) | (
+            C.FLAG_NO_SPATIAL_ORDER if self.spatial_order is False else 0) | (
             C.FLAG_ENGINE_WARP if self.engine == "warp" else 0) | (
             C.FLAG_ENGINE_THREAD if self.engine == "thread" else 0)
         return d

@@ -305,6 +305,14 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
   return KGPU_OK;
 }
 
+// Leaf-grouped processing order: forced on or off by the flags, otherwise on
+// for batches large enough to share leaves (it never changes results).
+bool want_spatial_order(uint32_t flags, uint64_t nq, uint64_t leaves) {
+  if (nq < 2 || (flags & KGPU_FLAG_NO_SPATIAL_ORDER)) return false;
+  if (flags & KGPU_FLAG_SPATIAL_ORDER) return true;
+  return nq >= 65536 && leaves >= 4096;
+}
+
 void apply_periodic(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch& q) {
   q.periodic = d->periodic_box != nullptr;
   if (!q.periodic) return;
@@ -328,7 +336,8 @@ namespace {
 // hand the kernels that processing order (same results, better locality).
 cudaError_t maybe_spatial_order(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch& q,
                                 DevBuf& ob, DevBuf& sb, cudaStream_t s) {
-  if (!(d->flags & KGPU_FLAG_SPATIAL_ORDER) || q.nq < 2) return cudaSuccess;
+  if (!want_spatial_order(d->flags, q.nq, q.forest ? q.total_leaves : dt.leaf_count))
+    return cudaSuccess;
   cudaError_t e;
   if ((e = ob.alloc(q.nq * 4, s)) != cudaSuccess) return e;
   if ((e = sb.alloc(spatial_order_scratch_bytes(dt, q), s)) != cudaSuccess) return e;

@@ -113,7 +113,7 @@ cudaError_t prepare(kgpu_forest* f, const kgpu_query_desc* d, QueryLaunch& q, De
   if (e != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(work.p, 0, sizeof(unsigned long long), s)) != cudaSuccess) return e;
   q.work = static_cast<unsigned long long*>(work.p);
-  if ((d->flags & KGPU_FLAG_SPATIAL_ORDER) && q.nq > 1) {
+  if (want_spatial_order(d->flags, q.nq, f->total_leaves)) {
     if ((e = ord.alloc(q.nq * 4, s)) != cudaSuccess) return e;
     if ((e = scratch.alloc(spatial_order_scratch_bytes(f->meta, q), s)) != cudaSuccess) return e;
     e = f->meta.dtype == KGPU_F64

@@ -14,6 +14,8 @@ namespace kgpu {
 // within/within().unsorted() families.  Returns a kgpu_status and records the
 // message for kgpu_last_error().
 int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_family);
+// Whether a batch is processed grouped by leaf (KGPU_FLAG_[NO_]SPATIAL_ORDER).
+bool want_spatial_order(uint32_t flags, uint64_t nq, uint64_t leaves);
 // Copies the periodic box of `d` (if any) into the launch description.
 void apply_periodic(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch& q);
 }  // namespace kgpu
