@@ -206,8 +206,98 @@ __device__ __forceinline__ void flush_stats(unsigned long long* stats, const Tra
   }
 }
 
+// Queries handed out to the lanes of one warp in 64-query chunks: from the
+// batch's work counter when it has one, else chunks gw, gw + W, gw + 2W, ...
+// (gw = this warp, W = warps in the grid).  Interleaving spreads the costly
+// regions of a leaf-ordered batch evenly over the warps.
+struct LaneFeeder {
+  static constexpr uint32_t kChunk = 64;
+  uint64_t next, end, chunk, step;
+  bool done;
+
+  __device__ __forceinline__ void start() {
+    step = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    chunk = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    next = end = 0;
+    done = false;
+  }
+
+  // Warp-uniform: moves to the next chunk; false once the batch is used up.
+  template <typename A>
+  __device__ __forceinline__ bool advance(const Batch<A>& b) {
+    if (done) return false;
+    uint64_t base;
+    if (b.work) {
+      unsigned long long v = 0;
+      if ((threadIdx.x & 31) == 0) v = atomicAdd(b.work, (unsigned long long)kChunk);
+      base = __shfl_sync(FULL, v, 0);
+    } else {
+      base = chunk * kChunk;
+      chunk += step;
+    }
+    if (base >= b.nq) {
+      done = true;
+      return false;
+    }
+    next = base;
+    end = base + kChunk < b.nq ? base + kChunk : b.nq;
+    return true;
+  }
+};
+
+// Warp-uniform: once at least KGPU_REFILL_MIN_IDLE lanes of the warp (or all
+// of them) have no query, gives each of them the next query of the batch
+// (lowest lanes first, so new queries start side by side); returns whether
+// any lane of the warp still has a query.
+#ifndef KGPU_REFILL_MIN_IDLE
+#define KGPU_REFILL_MIN_IDLE 24
+#endif
+template <typename A>
+__device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, bool& active,
+                                             bool& fresh, uint64_t& qi) {
+  const unsigned lane = threadIdx.x & 31;
+  unsigned need = __ballot_sync(FULL, !active);
+  if (need != FULL && __popc(need) < KGPU_REFILL_MIN_IDLE) return true;
+  while (need) {
+    if (fd.next >= fd.end && !fd.advance(b)) break;
+    const uint64_t avail = fd.end - fd.next;
+    const int cnt = __popc(need);
+    const int take = avail < uint64_t(cnt) ? int(avail) : cnt;
+    if (!active) {
+      const int rank = __popc(need & ((1u << lane) - 1u));
+      if (rank < take) {
+        const uint64_t w = fd.next + uint64_t(rank);
+        qi = b.order ? uint64_t(b.order[w]) : w;
+        active = fresh = true;
+      }
+    }
+    fd.next += uint64_t(take);
+    need = __ballot_sync(FULL, !active);
+  }
+  return __any_sync(FULL, active);
+}
+
+template <typename A, int K, typename M, int FAM, bool EXCL>
+struct TPolicyOf {
+  using type = TBestN<A, K, M, EXCL>;
+};
+template <typename A, int K, typename M, bool EXCL>
+struct TPolicyOf<A, K, M, KF_NEAREST_ONE, EXCL> {
+  using type = TNearestOne<A, K, M>;
+};
+template <typename A, int K, typename M, bool EXCL>
+struct TPolicyOf<A, K, M, KF_NEAREST_N, EXCL> {
+  using type = TNearestN<A, K, M, EXCL>;
+};
+
 // Shared memory: the continuation slots ((max_stem_level + 2) * blockDim
 // values of A), then for the list families k distances and k items per thread.
+//
+// The exact families run one query per thread with lane refill: a thread whose
+// query has finished takes the next one at a leaf boundary, so the lanes of a
+// warp stay busy until the batch runs dry instead of waiting for the warp's
+// slowest query (the queries of one leaf-ordered warp differ by 2-3x in the
+// leaves they visit).  Each query's own traversal is unchanged.
 template <typename A, int K, typename M, int FAM, bool EXCL>
 __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k,
                                                 A radius0, int arrival_order,
@@ -222,18 +312,11 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int
   uint32_t* list_i = reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(tsmem) +
                                                  size_t(levels + k) * stride) + threadIdx.x;
   TravStats st;
-  for_each_query_thread(b, [&](uint64_t qi) {
-    const TreeView<A> tv = b.tree(tv0, qi);
-    const A radius = b.radius(radius0, qi);
-    A q[K];
-    b.query(qi, q);
-    if constexpr (FAM == KF_NEAREST_ONE) {
-      TNearestOne<A, K, M> pol;
-      thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
-      out_d[qi] = pol.best;
-      out_i[qi] = pol.item;
-      if (out_c) out_c[qi] = 1;
-    } else if constexpr (FAM == KF_APPROX) {
+  if constexpr (FAM == KF_APPROX) {
+    for_each_query_thread(b, [&](uint64_t qi) {
+      const TreeView<A> tv = b.tree(tv0, qi);
+      A q[K];
+      b.query(qi, q);
       TNearestOne<A, K, M> pol;
       if (tv.leaf_count > 0) {
         st.points += pol.leaf(tv, straight_leaf<A, K>(tv, q), q);
@@ -243,16 +326,56 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int
       out_d[qi] = pol.best;
       out_i[qi] = pol.item;
       if (out_c) out_c[qi] = 1;
-    } else if constexpr (FAM == KF_NEAREST_N) {
-      TNearestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius);
-      thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
-      pol.write(qi, out_d, out_i, out_c, arrival_order != 0);
-    } else {
-      TBestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius);
-      thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
-      pol.write(qi, out_d, out_i, out_c);
+    });
+  } else {
+    using Pol = typename TPolicyOf<A, K, M, FAM, EXCL>::type;
+    Pol pol = [&] {
+      if constexpr (FAM == KF_NEAREST_ONE) return Pol();
+      else return Pol(list_d, list_i, stride, k, radius0);
+    }();
+    auto finish = [&](uint64_t qi) {
+      if constexpr (FAM == KF_NEAREST_ONE) {
+        out_d[qi] = pol.best;
+        out_i[qi] = pol.item;
+        if (out_c) out_c[qi] = 1;
+      } else if constexpr (FAM == KF_NEAREST_N) {
+        pol.write(qi, out_d, out_i, out_c, arrival_order != 0);
+      } else {
+        pol.write(qi, out_d, out_i, out_c);
+      }
+    };
+    ThreadWalk<A, K, M> wk;
+    LaneFeeder fd;
+    fd.start();
+    TreeView<A> tv = tv0;
+    A q[K];
+    bool active = false, fresh = false;
+    uint64_t qi = 0;
+    for (;;) {
+      if (active && !wk.backtrack(tv, q, pol, slot, stride)) {
+        finish(qi);
+        active = false;
+      }
+      if (!refill_lanes(b, fd, active, fresh, qi)) break;
+      bool bounded = true;
+      if (fresh) {
+        fresh = false;
+        tv = b.tree(tv0, qi);
+        b.query(qi, q);
+        pol.reset(b.radius(radius0, qi));
+        wk.init();
+        bounded = !pol.unbounded_start();
+        if (tv.size == 0) {
+          finish(qi);
+          active = false;
+        }
+      }
+      if (active) {
+        st.points += pol.leaf(tv, wk.descend(tv, q, pol, bounded, slot, stride, st), q);
+        ++st.leaves;
+      }
     }
-  });
+  }
   if (stats) flush_stats(stats, st);
 }
 
@@ -269,23 +392,53 @@ __global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv0, Batch<A> b, A 
   A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
   const int stride = blockDim.x;
   TravStats st;
-  for_each_query_thread(b, [&](uint64_t qi) {
-    uint64_t o = 0, cap = 0;
-    if (offsets) {
-      o = offsets[qi];
-      const uint64_t end = offsets[qi + 1] < capacity ? offsets[qi + 1] : capacity;
-      if (end <= o) return;
-      cap = end - o;
-    }
-    const TreeView<A> tv = b.tree(tv0, qi);
-    A q[K];
-    b.query(qi, q);
-    TWithin<A, K, M, EXCL> pol(b.radius(radius0, qi), cap, offsets ? out_d + o : nullptr,
-                               offsets ? out_i + o : nullptr);
-    thread_arith_query<A, K, M>(tv, q, pol, slot, stride, st);
+  // One query per thread with lane refill (as k_tfixed).
+  TWithin<A, K, M, EXCL> pol(radius0, 0, nullptr, nullptr);
+  auto finish = [&](uint64_t qi, uint64_t o) {
     if (counts) counts[qi] = pol.count;
     if (offsets && status && pol.count != offsets[qi + 1] - o) atomicExch(status, 6);
-  });
+  };
+  ThreadWalk<A, K, M> wk;
+  LaneFeeder fd;
+  fd.start();
+  TreeView<A> tv = tv0;
+  A q[K];
+  bool active = false, fresh = false;
+  uint64_t qi = 0, o = 0;
+  for (;;) {
+    if (active && !wk.backtrack(tv, q, pol, slot, stride)) {
+      finish(qi, o);
+      active = false;
+    }
+    if (!refill_lanes(b, fd, active, fresh, qi)) break;
+    bool bounded = true;
+    if (fresh) {
+      fresh = false;
+      uint64_t cap = 0;
+      o = 0;
+      if (offsets) {
+        o = offsets[qi];
+        const uint64_t end = offsets[qi + 1] < capacity ? offsets[qi + 1] : capacity;
+        cap = end > o ? end - o : 0;
+      }
+      tv = b.tree(tv0, qi);
+      b.query(qi, q);
+      pol = TWithin<A, K, M, EXCL>(b.radius(radius0, qi), cap, offsets ? out_d + o : nullptr,
+                                   offsets ? out_i + o : nullptr);
+      wk.init();
+      bounded = !pol.unbounded_start();
+      if (offsets && cap == 0) {
+        active = false;  // no hits to place (empty segment, or past the capacity)
+      } else if (tv.size == 0) {
+        finish(qi, o);
+        active = false;
+      }
+    }
+    if (active) {
+      st.points += pol.leaf(tv, wk.descend(tv, q, pol, bounded, slot, stride, st), q);
+      ++st.leaves;
+    }
+  }
   if (stats) flush_stats(stats, st);
 }
 

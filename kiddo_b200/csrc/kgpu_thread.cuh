@@ -79,22 +79,33 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
   return ex.y;
 }
 
-template <typename A, int K, typename M, typename P>
-__device__ __forceinline__ void thread_arith_query(const TreeView<A>& tv, const A (&q)[K], P& pol,
-                                                   A* __restrict__ slot, int stride,
-                                                   TravStats& st) {
-  if (tv.size == 0) return;
-  const A INF = inf_of<A>();
-  const int msl = tv.max_stem_level;
+// Resumable traversal state of one query: the reference's DFS
+// (kd_tree/orchestrator/mod.rs:388-603) cut at its leaves, so a thread can
+// stop after any leaf and carry on later.  descend() runs from the current
+// position to the next leaf; backtrack() climbs until a pending far child
+// survives the prune test (and enters it) or the root is passed.
+template <typename A, int K, typename M>
+struct ThreadWalk {
   A off[K];
-#pragma unroll
-  for (int d = 0; d < K; ++d) off[d] = A(0);
-  uint32_t stem_idx = 1;
-  int level = 0, dim = 0;
-  A rd = A(0);
-  uint32_t pending = 0, taken = 0;
+  A rd;
+  uint32_t stem_idx, pending, taken;
+  int level, dim, cur;
 
-  auto descend = [&](bool check_bound) -> uint32_t {
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int d = 0; d < K; ++d) off[d] = A(0);
+    rd = A(0);
+    stem_idx = 1;
+    pending = taken = 0;
+    level = dim = cur = 0;
+  }
+
+  template <typename P>
+  __device__ __forceinline__ uint32_t descend(const TreeView<A>& tv, const A (&q)[K], const P& pol,
+                                              bool check_bound, A* __restrict__ slot, int stride,
+                                              TravStats& st) {
+    const A INF = inf_of<A>();
+    const int msl = tv.max_stem_level;
     while (level <= msl) {
       ++st.stems;
       const A pivot = __ldg(tv.stems + stem_idx);
@@ -114,14 +125,13 @@ __device__ __forceinline__ void thread_arith_query(const TreeView<A>& tv, const 
       ++level;
       dim = dim + 1 == K ? 0 : dim + 1;
     }
+    cur = level;
     return stem_idx & ~(1u << level);
-  };
+  }
 
-  st.points += pol.leaf(tv, descend(!pol.unbounded_start()), q);
-  ++st.leaves;
-  int cur = level;
-  for (;;) {
-    bool resumed = false;
+  template <typename P>
+  __device__ __forceinline__ bool backtrack(const TreeView<A>& tv, const A (&q)[K], const P& pol,
+                                            A* __restrict__ slot, int stride) {
     while (cur > 0) {
       const int L = cur - 1;
       const int d = dim == 0 ? K - 1 : dim - 1;
@@ -144,17 +154,28 @@ __device__ __forceinline__ void thread_arith_query(const TreeView<A>& tv, const 
           stem_idx ^= 1u;
           level = cur;
           dim = d + 1 == K ? 0 : d + 1;
-          st.points += pol.leaf(tv, descend(true), q);
-          ++st.leaves;
-          cur = level;
-          resumed = true;
-          break;
+          return true;
         }
       }
       stem_idx >>= 1;
       cur = L;
     }
-    if (!resumed) break;
+    return false;
+  }
+};
+
+template <typename A, int K, typename M, typename P>
+__device__ __forceinline__ void thread_arith_query(const TreeView<A>& tv, const A (&q)[K], P& pol,
+                                                   A* __restrict__ slot, int stride,
+                                                   TravStats& st) {
+  if (tv.size == 0) return;
+  ThreadWalk<A, K, M> w;
+  w.init();
+  st.points += pol.leaf(tv, w.descend(tv, q, pol, !pol.unbounded_start(), slot, stride, st), q);
+  ++st.leaves;
+  while (w.backtrack(tv, q, pol, slot, stride)) {
+    st.points += pol.leaf(tv, w.descend(tv, q, pol, true, slot, stride, st), q);
+    ++st.leaves;
   }
 }
 
@@ -175,6 +196,7 @@ struct TNearestOne {
   A best;
   uint32_t item;
   __device__ TNearestOne() : best(inf_of<A>()), item(0) {}
+  __device__ __forceinline__ void reset(A) { best = inf_of<A>(); item = 0; }
   __device__ __forceinline__ A max_dist() const { return best; }
   __device__ __forceinline__ bool unbounded_start() const { return true; }
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
@@ -206,6 +228,7 @@ struct TNearestN {
   A radius, kth;
   __device__ TNearestN(A* d, uint32_t* i, int s, int k_, A r)
       : ld(d), li(i), stride(s), n(0), k(k_), radius(r), kth(inf_of<A>()) {}
+  __device__ __forceinline__ void reset(A r) { n = 0; radius = r; kth = inf_of<A>(); }
   __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
 
@@ -286,6 +309,7 @@ struct TBestN {
   A radius;
   __device__ TBestN(A* d, uint32_t* i, int s, int k_, A r)
       : ld(d), li(i), stride(s), n(0), k(k_), radius(r) {}
+  __device__ __forceinline__ void reset(A r) { n = 0; radius = r; }
   __device__ __forceinline__ A max_dist() const { return radius; }
   __device__ __forceinline__ bool unbounded_start() const { return false; }
   __device__ __forceinline__ void add(A d, uint32_t it) {
