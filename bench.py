@@ -140,6 +140,13 @@ class ClockSampler:
         self._t.start()
         return self
 
+    def wait_first(self, timeout=15.0):
+        """Block until the first sample is in, so that starting nvidia-smi does
+        not land inside the timed region."""
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < timeout and self._t.is_alive():
+            time.sleep(0.05)
+
     def __exit__(self, *a):
         self._stop.set()
         if self._t:
@@ -325,11 +332,12 @@ def main():
     stats = builder_for(gtree, sub, args.workload).traversal_stats()
     bpq = bytes_per_query(stats, len(sub), Q.itemsize, k)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    multi.barrier()
     with ClockSampler(local) as clk:
+        clk.wait_first()
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        multi.barrier()
         l0 = kb.launch_count()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         torch.cuda.synchronize()

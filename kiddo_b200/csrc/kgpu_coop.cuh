@@ -1,0 +1,200 @@
+// kgpu_coop.cuh — warp-cooperative leaf scans for the thread-per-query engine.
+//
+// Each thread walks its own query's tree (ThreadWalk, the reference's DFS).
+// When the lanes of a warp have reached their next leaves, the warp scans
+// those leaves one after another, all 32 lanes on one leaf: lane p takes
+// point p, so the coordinate columns of a 32-point tile load as one coalesced
+// 128-byte row per axis.  A ballot picks the points that pass the leaf-start
+// filter, and the candidates are then applied in arrival order (lane order)
+// to the owner's result list, which sits one entry per lane for the scan:
+// an insertion is one ballot (its position) and one shuffle up (the shift).
+//
+// Each family keeps the sequential semantics of its reference collector:
+// best_n_within the n smallest by (item, arrival) (kd_tree/query/
+// best_n_within.rs:88-196), within appends hits in arrival order
+// (kd_tree/query/within.rs:18-41).  (For nearest_n the per-candidate
+// insertions cost more warp instructions than a per-thread scan saves, so
+// nearest_one and nearest_n scan per thread.)
+#pragma once
+
+#include "kgpu_device.cuh"
+#include "kgpu_thread.cuh"
+
+namespace kgpu {
+
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
+  return __shfl_sync(FULL, static_cast<unsigned long long>(v), src);
+}
+
+__device__ __forceinline__ unsigned lanes_below() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// The leaf one lane reached, as the whole warp sees it while scanning it.
+template <typename A, int K>
+struct CoopLeaf {
+  const uint8_t* base;
+  uint32_t len;
+  A q[K];
+};
+
+template <typename A, int K>
+__device__ __forceinline__ CoopLeaf<A, K> coop_leaf(int o, const uint8_t* base, uint32_t len,
+                                                    const A (&q)[K]) {
+  CoopLeaf<A, K> L;
+  L.base = reinterpret_cast<const uint8_t*>(shfl64(reinterpret_cast<uint64_t>(base), o));
+  L.len = shfl(len, o);
+#pragma unroll
+  for (int d = 0; d < K; ++d) L.q[d] = shfl(q[d], o);
+  return L;
+}
+
+// Distance from the owner's query to point p (< len) of the leaf.
+template <typename A, int K, typename M>
+__device__ __forceinline__ A coop_point(const CoopLeaf<A, K>& L, uint32_t p, uint32_t& item) {
+  A c[K];
+  load_point<A, K>(L.base, L.len, p, c, item);
+  return point_dist<M, A, K>(c, L.q);
+}
+
+// ---------------------------------------------------------------------------
+// best_n_within: the n smallest items among the hits, by (item, arrival);
+// the leaf filter drops items >= the list's last item when the leaf starts
+// with a full list (leaf_view_chunked/best_n_within/fallback.rs:40-104).
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M, bool kExclusive>
+struct CBestN {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A* __restrict__ wd;
+  uint32_t* __restrict__ wi;
+  int k;
+  int n;
+  A radius;
+  uint32_t last;  // the list's last item once full
+  __device__ CBestN(A* d, uint32_t* i, uint32_t*, int k_, A r)
+      : wd(d), wi(i), k(k_), n(0), radius(r), last(0) {}
+  __device__ __forceinline__ void reset(A r) { n = 0; radius = r; last = 0; }
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return false; }
+
+  __device__ __forceinline__ void leaf(int o, const CoopLeaf<A, K>& L, int lane) {
+    int nn = __shfl_sync(FULL, n, o);
+    uint32_t lk = shfl(last, o);
+    const A orad = shfl(radius, o);
+    const bool full_at_entry = nn == k;
+    const uint32_t thr_item = lk;
+    A* ld = wd + o * k;
+    uint32_t* li = wi + o * k;
+    A Ld = A(0);
+    uint32_t Li = 0xffffffffu;
+    bool loaded = false;
+    for (uint32_t c0 = 0; c0 < L.len; c0 += 32) {
+      const uint32_t p = c0 + lane;
+      A d = A(0);
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < L.len) {
+        d = coop_point<A, K, M>(L, p, it);
+        pass = (kExclusive ? (d < orad) : (d <= orad)) && !(full_at_entry && it >= thr_item) &&
+               (nn < k || it < lk);
+      }
+      unsigned m = __ballot_sync(FULL, pass);
+      if (m && !loaded) {
+        if (lane < nn) {
+          Ld = ld[lane];
+          Li = li[lane];
+        }
+        loaded = true;
+      }
+      while (m) {
+        const int c = __ffs(m) - 1;
+        m &= m - 1;
+        const A dc = shfl(d, c);
+        const uint32_t ic = shfl(it, c);
+        if (nn == k && !(ic < lk)) continue;
+        const int pos = __popc(__ballot_sync(FULL, lane < nn && Li <= ic));
+        const A ud = __shfl_up_sync(FULL, Ld, 1);
+        const uint32_t ui = __shfl_up_sync(FULL, Li, 1);
+        if (lane > pos) {
+          Ld = ud;
+          Li = ui;
+        } else if (lane == pos) {
+          Ld = dc;
+          Li = ic;
+        }
+        if (nn < k) ++nn;
+        if (nn == k) lk = shfl(Li, k - 1);
+      }
+    }
+    if (loaded && lane < nn) {
+      ld[lane] = Ld;
+      li[lane] = Li;
+    }
+    if (lane == o) {
+      n = nn;
+      last = lk;
+    }
+  }
+
+  __device__ __forceinline__ void finish(int o, uint64_t qi, int lane, A* __restrict__ out_d,
+                                         uint32_t* __restrict__ out_i,
+                                         uint32_t* __restrict__ out_c) const {
+    const int on = __shfl_sync(FULL, n, o);
+    if (lane < k) {
+      const bool h = lane < on;
+      out_d[qi * k + lane] = h ? wd[o * k + lane] : inf_of<A>();
+      out_i[qi * k + lane] = h ? wi[o * k + lane] : 0xffffffffu;
+    }
+    if (lane == 0 && out_c) out_c[qi] = uint32_t(on);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// within: counting pass (no output) or filling pass (hits written in arrival
+// order into the query's CSR segment, `cap` long); a leaf's hits are one
+// coalesced store.
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M, bool kExclusive>
+struct CWithin {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A radius;
+  uint64_t count;
+  uint64_t cap;
+  A* out_d;
+  uint32_t* out_i;
+  __device__ CWithin() : radius(A(0)), count(0), cap(0), out_d(nullptr), out_i(nullptr) {}
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+
+  __device__ __forceinline__ void leaf(int o, const CoopLeaf<A, K>& L, int lane) {
+    uint64_t cnt = shfl64(count, o);
+    const uint64_t ocap = shfl64(cap, o);
+    A* od = reinterpret_cast<A*>(shfl64(reinterpret_cast<uint64_t>(out_d), o));
+    uint32_t* oi = reinterpret_cast<uint32_t*>(shfl64(reinterpret_cast<uint64_t>(out_i), o));
+    const A orad = shfl(radius, o);
+    for (uint32_t c0 = 0; c0 < L.len; c0 += 32) {
+      const uint32_t p = c0 + lane;
+      A d = A(0);
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < L.len) {
+        d = coop_point<A, K, M>(L, p, it);
+        pass = kExclusive ? (d < orad) : (d <= orad);
+      }
+      const unsigned m = __ballot_sync(FULL, pass);
+      if (od && pass) {
+        const uint64_t w = cnt + uint64_t(__popc(m & lanes_below()));
+        if (w < ocap) {
+          od[w] = d;
+          oi[w] = it;
+        }
+      }
+      cnt += uint64_t(__popc(m));
+    }
+    if (lane == o) count = cnt;
+  }
+};
+
+}  // namespace kgpu

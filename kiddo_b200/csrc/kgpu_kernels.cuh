@@ -8,6 +8,7 @@
 #include "kgpu_device.cuh"
 #include "kgpu_launch.h"
 #include "kgpu_thread.cuh"
+#include "kgpu_coop.cuh"
 
 namespace kgpu {
 
@@ -277,27 +278,127 @@ __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, 
   return __any_sync(FULL, active);
 }
 
-template <typename A, int K, typename M, int FAM, bool EXCL>
-struct TPolicyOf {
-  using type = TBestN<A, K, M, EXCL>;
-};
-template <typename A, int K, typename M, bool EXCL>
-struct TPolicyOf<A, K, M, KF_NEAREST_ONE, EXCL> {
-  using type = TNearestOne<A, K, M>;
-};
-template <typename A, int K, typename M, bool EXCL>
-struct TPolicyOf<A, K, M, KF_NEAREST_N, EXCL> {
-  using type = TNearestN<A, K, M, EXCL>;
-};
+// ---------------------------------------------------------------------------
+// The driver: lane-refilled per-thread walks, cooperative leaf scans.
+//   start(qi, tv) sets the policy up for a fresh query in this lane and says
+//   whether the query needs a walk at all; finish(o, qi) runs on the whole
+//   warp for lane o's finished query.
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M, typename Pol, typename Start, typename Finish>
+__device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Pol& pol,
+                                           A* __restrict__ slot, int stride, TravStats& st,
+                                           Start&& start, Finish&& finish) {
+  const int lane = threadIdx.x & 31;
+  ThreadWalk<A, K, M> wk;
+  LaneFeeder fd;
+  fd.start();
+  TreeView<A> tv = tv0;
+  A q[K];
+#pragma unroll
+  for (int d = 0; d < K; ++d) q[d] = A(0);
+  bool active = false, fresh = false;
+  uint64_t qi = 0;
+  for (;;) {
+    bool done = false;
+    if (active && !wk.backtrack(tv, q, pol, slot, stride)) {
+      done = true;
+      active = false;
+    }
+    for (unsigned fm = __ballot_sync(FULL, done); fm; fm &= fm - 1) {
+      const int o = __ffs(fm) - 1;
+      finish(o, shfl64(qi, o));
+    }
+    if (!refill_lanes(b, fd, active, fresh, qi)) break;
+    bool bounded = true, empty = false;
+    if (fresh) {
+      fresh = false;
+      tv = b.tree(tv0, qi);
+      b.query(qi, q);
+      wk.init();
+      if (!start(qi, tv)) {
+        active = false;
+      } else if (tv.size == 0) {
+        empty = true;
+        active = false;
+      }
+      bounded = !pol.unbounded_start();
+    }
+    for (unsigned fm = __ballot_sync(FULL, empty); fm; fm &= fm - 1) {
+      const int o = __ffs(fm) - 1;
+      finish(o, shfl64(qi, o));
+    }
+    const uint8_t* lb = nullptr;
+    uint32_t len = 0;
+    if (active) {
+      const uint32_t leaf = wk.descend(tv, q, pol, bounded, slot, stride, st);
+      const uint2 ex = __ldg(tv.extents + leaf);
+      lb = tv.arena + size_t(ex.x) * 8;
+      len = ex.y;
+      st.points += len;
+      ++st.leaves;
+    }
+    for (unsigned lm = __ballot_sync(FULL, active); lm; lm &= lm - 1) {
+      const int o = __ffs(lm) - 1;
+      pol.leaf(o, coop_leaf<A, K>(o, lb, len, q), lane);
+    }
+  }
+}
+
+// The per-thread driver: lane-refilled walks, each thread scanning its own
+// leaves (the list families keep their lists in shared-memory columns).
+//   finish(qi) writes a finished query's results from its own lane.
+template <typename A, int K, typename M, typename Pol, typename Finish>
+__device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch<A>& b, A radius0,
+                                             Pol& pol, A* __restrict__ slot, int stride,
+                                             TravStats& st, Finish&& finish) {
+  ThreadWalk<A, K, M> wk;
+  LaneFeeder fd;
+  fd.start();
+  TreeView<A> tv = tv0;
+  A q[K];
+#pragma unroll
+  for (int d = 0; d < K; ++d) q[d] = A(0);
+  bool active = false, fresh = false;
+  uint64_t qi = 0;
+  for (;;) {
+    if (active && !wk.backtrack(tv, q, pol, slot, stride)) {
+      finish(qi);
+      active = false;
+    }
+    if (!refill_lanes(b, fd, active, fresh, qi)) break;
+    bool bounded = true;
+    if (fresh) {
+      fresh = false;
+      tv = b.tree(tv0, qi);
+      b.query(qi, q);
+      pol.reset(b.radius(radius0, qi));
+      wk.init();
+      bounded = !pol.unbounded_start();
+      if (tv.size == 0) {
+        finish(qi);
+        active = false;
+      }
+    }
+    if (active) {
+      st.points += pol.leaf(tv, wk.descend(tv, q, pol, bounded, slot, stride, st), q);
+      ++st.leaves;
+    }
+  }
+}
+
+#ifndef KGPU_BESTN_COOP
+#define KGPU_BESTN_COOP 1
+#endif
 
 // Shared memory: the continuation slots ((max_stem_level + 2) * blockDim
-// values of A), then for the list families k distances and k items per thread.
+// values of A, slot of level L for thread t at L * blockDim + t), then for the
+// list families k distances and k items per thread.
 //
-// The exact families run one query per thread with lane refill: a thread whose
-// query has finished takes the next one at a leaf boundary, so the lanes of a
-// warp stay busy until the batch runs dry instead of waiting for the warp's
-// slowest query (the queries of one leaf-ordered warp differ by 2-3x in the
-// leaves they visit).  Each query's own traversal is unchanged.
+// The exact families walk one query per thread with lane refill: a lane whose
+// query has finished takes the next one once enough lanes of its warp are
+// idle, so lanes do not wait for the warp's slowest query.  nearest_one and
+// nearest_n scan their leaves per thread; best_n_within scans them
+// warp-cooperatively (kgpu_coop.cuh).  Each query's own traversal is unchanged.
 template <typename A, int K, typename M, int FAM, bool EXCL>
 __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k,
                                                 A radius0, int arrival_order,
@@ -308,9 +409,6 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int
   extern __shared__ __align__(16) unsigned char tsmem[];
   const int stride = blockDim.x;
   A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
-  A* list_d = reinterpret_cast<A*>(tsmem) + size_t(levels) * stride + threadIdx.x;
-  uint32_t* list_i = reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(tsmem) +
-                                                 size_t(levels + k) * stride) + threadIdx.x;
   TravStats st;
   if constexpr (FAM == KF_APPROX) {
     for_each_query_thread(b, [&](uint64_t qi) {
@@ -327,54 +425,42 @@ __global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int
       out_i[qi] = pol.item;
       if (out_c) out_c[qi] = 1;
     });
-  } else {
-    using Pol = typename TPolicyOf<A, K, M, FAM, EXCL>::type;
-    Pol pol = [&] {
-      if constexpr (FAM == KF_NEAREST_ONE) return Pol();
-      else return Pol(list_d, list_i, stride, k, radius0);
-    }();
-    auto finish = [&](uint64_t qi) {
-      if constexpr (FAM == KF_NEAREST_ONE) {
-        out_d[qi] = pol.best;
-        out_i[qi] = pol.item;
-        if (out_c) out_c[qi] = 1;
-      } else if constexpr (FAM == KF_NEAREST_N) {
+  } else if constexpr (FAM == KF_NEAREST_ONE) {
+    TNearestOne<A, K, M> pol;
+    thread_drive<A, K, M>(tv0, b, radius0, pol, slot, stride, st, [&](uint64_t qi) {
+      out_d[qi] = pol.best;
+      out_i[qi] = pol.item;
+      if (out_c) out_c[qi] = 1;
+    });
+  } else if constexpr (FAM == KF_NEAREST_N || !KGPU_BESTN_COOP) {
+    // lists in shared-memory columns: entry j of thread t at j * blockDim + t
+    A* list_d = reinterpret_cast<A*>(tsmem) + size_t(levels) * stride + threadIdx.x;
+    uint32_t* list_i = reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(tsmem) +
+                                                   size_t(levels + k) * stride) + threadIdx.x;
+    if constexpr (FAM == KF_NEAREST_N) {
+      TNearestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius0);
+      thread_drive<A, K, M>(tv0, b, radius0, pol, slot, stride, st, [&](uint64_t qi) {
         pol.write(qi, out_d, out_i, out_c, arrival_order != 0);
-      } else {
-        pol.write(qi, out_d, out_i, out_c);
-      }
-    };
-    ThreadWalk<A, K, M> wk;
-    LaneFeeder fd;
-    fd.start();
-    TreeView<A> tv = tv0;
-    A q[K];
-    bool active = false, fresh = false;
-    uint64_t qi = 0;
-    for (;;) {
-      if (active && !wk.backtrack(tv, q, pol, slot, stride)) {
-        finish(qi);
-        active = false;
-      }
-      if (!refill_lanes(b, fd, active, fresh, qi)) break;
-      bool bounded = true;
-      if (fresh) {
-        fresh = false;
-        tv = b.tree(tv0, qi);
-        b.query(qi, q);
-        pol.reset(b.radius(radius0, qi));
-        wk.init();
-        bounded = !pol.unbounded_start();
-        if (tv.size == 0) {
-          finish(qi);
-          active = false;
-        }
-      }
-      if (active) {
-        st.points += pol.leaf(tv, wk.descend(tv, q, pol, bounded, slot, stride, st), q);
-        ++st.leaves;
-      }
+      });
+    } else {
+      TBestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius0);
+      thread_drive<A, K, M>(tv0, b, radius0, pol, slot, stride, st,
+                            [&](uint64_t qi) { pol.write(qi, out_d, out_i, out_c); });
     }
+  } else {
+    // best_n_within with warp-cooperative leaf scans: thread t's k entries
+    // consecutive at t * k
+    const size_t warp0 = threadIdx.x & ~31u;
+    A* lists_d = reinterpret_cast<A*>(tsmem) + size_t(levels) * stride;
+    uint32_t* lists_i = reinterpret_cast<uint32_t*>(lists_d + size_t(k) * stride);
+    CBestN<A, K, M, EXCL> pol(lists_d + warp0 * k, lists_i + warp0 * k, nullptr, k, radius0);
+    coop_drive<A, K, M>(
+        tv0, b, pol, slot, stride, st,
+        [&](uint64_t qi, const TreeView<A>&) {
+          pol.reset(b.radius(radius0, qi));
+          return true;
+        },
+        [&](int o, uint64_t qo) { pol.finish(o, qo, threadIdx.x & 31, out_d, out_i, out_c); });
   }
   if (stats) flush_stats(stats, st);
 }
@@ -391,54 +477,35 @@ __global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv0, Batch<A> b, A 
   extern __shared__ __align__(16) unsigned char tsmem[];
   A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
   const int stride = blockDim.x;
+  const int lane = threadIdx.x & 31;
   TravStats st;
-  // One query per thread with lane refill (as k_tfixed).
-  TWithin<A, K, M, EXCL> pol(radius0, 0, nullptr, nullptr);
-  auto finish = [&](uint64_t qi, uint64_t o) {
-    if (counts) counts[qi] = pol.count;
-    if (offsets && status && pol.count != offsets[qi + 1] - o) atomicExch(status, 6);
-  };
-  ThreadWalk<A, K, M> wk;
-  LaneFeeder fd;
-  fd.start();
-  TreeView<A> tv = tv0;
-  A q[K];
-  bool active = false, fresh = false;
-  uint64_t qi = 0, o = 0;
-  for (;;) {
-    if (active && !wk.backtrack(tv, q, pol, slot, stride)) {
-      finish(qi, o);
-      active = false;
-    }
-    if (!refill_lanes(b, fd, active, fresh, qi)) break;
-    bool bounded = true;
-    if (fresh) {
-      fresh = false;
-      uint64_t cap = 0;
-      o = 0;
-      if (offsets) {
+  CWithin<A, K, M, EXCL> pol;
+  uint64_t o = 0;  // this lane's segment start (filling pass)
+  coop_drive<A, K, M>(
+      tv0, b, pol, slot, stride, st,
+      [&](uint64_t qi, const TreeView<A>&) {
+        pol.radius = b.radius(radius0, qi);
+        pol.count = 0;
+        pol.cap = 0;
+        pol.out_d = nullptr;
+        pol.out_i = nullptr;
+        if (!offsets) return true;
         o = offsets[qi];
         const uint64_t end = offsets[qi + 1] < capacity ? offsets[qi + 1] : capacity;
-        cap = end > o ? end - o : 0;
-      }
-      tv = b.tree(tv0, qi);
-      b.query(qi, q);
-      pol = TWithin<A, K, M, EXCL>(b.radius(radius0, qi), cap, offsets ? out_d + o : nullptr,
-                                   offsets ? out_i + o : nullptr);
-      wk.init();
-      bounded = !pol.unbounded_start();
-      if (offsets && cap == 0) {
-        active = false;  // no hits to place (empty segment, or past the capacity)
-      } else if (tv.size == 0) {
-        finish(qi, o);
-        active = false;
-      }
-    }
-    if (active) {
-      st.points += pol.leaf(tv, wk.descend(tv, q, pol, bounded, slot, stride, st), q);
-      ++st.leaves;
-    }
-  }
+        if (end <= o) return false;  // no hits to place (empty segment, or past the capacity)
+        pol.cap = end - o;
+        pol.out_d = out_d + o;
+        pol.out_i = out_i + o;
+        return true;
+      },
+      [&](int w, uint64_t qo) {
+        const uint64_t cnt = shfl64(pol.count, w);
+        const uint64_t ow = shfl64(o, w);
+        if (lane == 0) {
+          if (counts) counts[qo] = cnt;
+          if (offsets && status && cnt != offsets[qo + 1] - ow) atomicExch(status, 6);
+        }
+      });
   if (stats) flush_stats(stats, st);
 }
 

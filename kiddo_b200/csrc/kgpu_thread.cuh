@@ -1,9 +1,10 @@
-// kgpu_thread.cuh — thread-per-query variants of the exact query families.
+// kgpu_thread.cuh — per-thread traversal of the thread-per-query engine.
 //
 // The warp-per-query kernels spend most issue slots on 32 lanes running the
-// same scalar traversal.  Here every thread runs one query's traversal,
-// exactly in the reference's order (kd_tree/orchestrator/mod.rs:388-603), so a
-// warp advances 32 queries per instruction.
+// same scalar traversal.  Here every thread walks one query's tree, exactly
+// in the reference's order (kd_tree/orchestrator/mod.rs:388-603), so a warp
+// advances 32 walks per instruction; the leaves they reach are scanned by the
+// whole warp (kgpu_coop.cuh).
 //
 // Continuation state per level L, in shared memory column `slot[L * stride]`:
 //  * while the far child of level L is pending: its rd_far;
@@ -21,10 +22,9 @@
 namespace kgpu {
 
 // Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
-// leaf_view/mod.rs:431-446): f(coords, item) in tile order.
-// Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
 // leaf_view/mod.rs:431-446) calling f(distance, item) in tile order, with
-// distance = dist(coords); pairs where pass() rejects both points skip f.  Tiles of width >= 2 are read two points per step
+// distance = dist(coords); pairs where pass() rejects both points skip f.
+// Used by the one-leaf approx query.  Tiles of width >= 2 are read two points per step
 // (8-byte aligned pairs for f32: leaves start on 8 bytes and every column of
 // an even-width tile spans an even number of floats); both points then go
 // through one call site of f, so the policy's insertion code is emitted once.
@@ -163,21 +163,6 @@ struct ThreadWalk {
     return false;
   }
 };
-
-template <typename A, int K, typename M, typename P>
-__device__ __forceinline__ void thread_arith_query(const TreeView<A>& tv, const A (&q)[K], P& pol,
-                                                   A* __restrict__ slot, int stride,
-                                                   TravStats& st) {
-  if (tv.size == 0) return;
-  ThreadWalk<A, K, M> w;
-  w.init();
-  st.points += pol.leaf(tv, w.descend(tv, q, pol, !pol.unbounded_start(), slot, stride, st), q);
-  ++st.leaves;
-  while (w.backtrack(tv, q, pol, slot, stride)) {
-    st.points += pol.leaf(tv, w.descend(tv, q, pol, true, slot, stride, st), q);
-    ++st.leaves;
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Thread policies
@@ -350,31 +335,6 @@ struct TBestN {
       oi[j] = j < n ? li[j * stride] : 0xffffffffu;
     }
     if (out_c) out_c[qi] = uint32_t(n);
-  }
-};
-
-template <typename A, int K, typename M, bool kExclusive>
-struct TWithin {
-  static constexpr bool kPruneOnEqual = kExclusive;
-  A radius;
-  uint64_t count;
-  uint64_t cap;                 // fill pass: the segment length; count pass: unused
-  A* __restrict__ out_d;        // null in the counting pass
-  uint32_t* __restrict__ out_i;
-  __device__ TWithin(A r, uint64_t c, A* d, uint32_t* i)
-      : radius(r), count(0), cap(c), out_d(d), out_i(i) {}
-  __device__ __forceinline__ A max_dist() const { return radius; }
-  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
-  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
-    const CartesianQ<A, K, M> dist{q};
-    return thread_for_each_point<A, K>(
-        tv, l, dist, [&](A d) { return kExclusive ? (d < radius) : (d <= radius); },
-        [&](A d, uint32_t it) {
-      if (kExclusive ? (d < radius) : (d <= radius)) {
-        if (out_d && count < cap) { out_d[count] = d; out_i[count] = it; }
-        ++count;
-      }
-    });
   }
 };
 
