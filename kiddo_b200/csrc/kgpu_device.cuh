@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace kgpu {
@@ -132,12 +133,14 @@ __device__ __forceinline__ void load_point(const uint8_t* __restrict__ leaf, uin
   item = __ldg(reinterpret_cast<const uint32_t*>(leaf + off + K * w * sizeof(A)) + i);
 }
 
-// acc = ((0 + dist1(c0, q0)) + dist1(c1, q1)) + ...   (combine_component order)
+// acc = ((0 + dist1(c0, q0)) + dist1(c1, q1)) + ...   (combine_component order).
+// Every dist1 is +0 or more (a square, or fabs), so the leading 0 + dist1 is
+// exact and is left out.
 template <typename M, typename A, int K>
 __device__ __forceinline__ A point_dist(const A (&c)[K], const A (&q)[K]) {
-  A acc = A(0);
+  A acc = M::template dist1<A>(c[0], q[0]);
 #pragma unroll
-  for (int d = 0; d < K; ++d) acc = add_rn(acc, M::template dist1<A>(c[d], q[d]));
+  for (int d = 1; d < K; ++d) acc = add_rn(acc, M::template dist1<A>(c[d], q[d]));
   return acc;
 }
 

@@ -399,13 +399,14 @@ __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch
 // idle, so lanes do not wait for the warp's slowest query.  nearest_one and
 // nearest_n scan their leaves per thread; best_n_within scans them
 // warp-cooperatively (kgpu_coop.cuh).  Each query's own traversal is unchanged.
+#ifndef KGPU_TFIXED_MIN_BLOCKS
+#define KGPU_TFIXED_MIN_BLOCKS 4
+#endif
 template <typename A, int K, typename M, int FAM, bool EXCL>
-__global__ void __launch_bounds__(256) k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k,
-                                                A radius0, int arrival_order,
-                                                A* __restrict__ out_d,
-                                                uint32_t* __restrict__ out_i,
-                                                uint32_t* __restrict__ out_c,
-                                                unsigned long long* __restrict__ stats) {
+__global__ void __launch_bounds__(256, KGPU_TFIXED_MIN_BLOCKS)
+    k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k, A radius0, int arrival_order,
+             A* __restrict__ out_d, uint32_t* __restrict__ out_i, uint32_t* __restrict__ out_c,
+             unsigned long long* __restrict__ stats) {
   extern __shared__ __align__(16) unsigned char tsmem[];
   const int stride = blockDim.x;
   A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;

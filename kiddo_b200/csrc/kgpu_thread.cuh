@@ -24,10 +24,11 @@ namespace kgpu {
 // Sequential tile walk of one leaf (LeafArena::for_each_tiled_chunk,
 // leaf_view/mod.rs:431-446) calling f(distance, item) in tile order, with
 // distance = dist(coords); pairs where pass() rejects both points skip f.
-// Used by the one-leaf approx query.  Tiles of width >= 2 are read two points per step
-// (8-byte aligned pairs for f32: leaves start on 8 bytes and every column of
-// an even-width tile spans an even number of floats); both points then go
-// through one call site of f, so the policy's insertion code is emitted once.
+// Tiles of width >= 2 are read two points per step (8-byte aligned pairs for
+// f32: leaves start on 8 bytes and every column of an even-width tile spans
+// an even number of floats).  Items are read only for points that reach f, and
+// both points of a pair go through one call site of f, so the policy's
+// insertion code is emitted once.
 template <typename A, int K, typename D, typename P, typename F>
 __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint32_t leaf,
                                                           const D& dist, P&& pass, F&& f) {
@@ -40,38 +41,38 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
     const A* col = reinterpret_cast<const A*>(base + boff);
     const uint32_t* its = reinterpret_cast<const uint32_t*>(base + boff + K * w * sizeof(A));
     for (uint32_t i = 0; i < w; i += 2) {
-      A c0[K], c1[K];
-      uint32_t i0, i1;
+      A d0, d1;
       if (w == 1) {
+        A c0[K];
 #pragma unroll
-        for (int d = 0; d < K; ++d) c0[d] = c1[d] = __ldg(col + d);
-        i0 = i1 = __ldg(its);
+        for (int d = 0; d < K; ++d) c0[d] = __ldg(col + d);
+        d0 = d1 = dist(c0);
       } else if constexpr (sizeof(A) == 4) {
+        A c0[K], c1[K];
 #pragma unroll
         for (int d = 0; d < K; ++d) {
           const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
           c0[d] = v.x;
           c1[d] = v.y;
         }
-        const uint2 it = __ldg(reinterpret_cast<const uint2*>(its + i));
-        i0 = it.x;
-        i1 = it.y;
+        d0 = dist(c0);
+        d1 = dist(c1);
       } else {
+        A c0[K], c1[K];
 #pragma unroll
         for (int d = 0; d < K; ++d) {
           c0[d] = __ldg(col + d * w + i);
           c1[d] = __ldg(col + d * w + i + 1);
         }
-        i0 = __ldg(its + i);
-        i1 = __ldg(its + i + 1);
+        d0 = dist(c0);
+        d1 = dist(c1);
       }
-      const A d0 = dist(c0), d1 = dist(c1);
       // `pass` is a cheap necessary condition for f to act: most points fail
       // it once a list has filled, and then f is not entered at all.
       if (!pass(d0) && !(w > 1 && pass(d1))) continue;
       const int nu = w == 1 ? 1 : 2;
 #pragma unroll 1
-      for (int u = 0; u < nu; ++u) f(u ? d1 : d0, u ? i1 : i0);
+      for (int u = 0; u < nu; ++u) f(u ? d1 : d0, __ldg(its + i + u));
     }
     boff += w * (K * sizeof(A) + sizeof(uint32_t));
     rem -= w;
