@@ -323,7 +323,10 @@ void apply_periodic(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch&
 
 template <typename A>
 cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
-  const bool thread = q.engine != 1 && !q.periodic && (t.dims == 2 || t.dims == 3);
+  // thread engine for 2-D/3-D trees; periodic nearest_one stays on the warp
+  // engine (home query plus images)
+  const bool thread = q.engine != 1 && (t.dims == 2 || t.dims == 3) &&
+                      (!q.periodic || q.family != KGPU_NEAREST_ONE);
   return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);
 }
 template cudaError_t launch_fixed<float>(const DeviceTree&, const QueryLaunch&);

@@ -51,12 +51,14 @@ __device__ __forceinline__ CoopLeaf<A, K> coop_leaf(int o, const uint8_t* base, 
   return L;
 }
 
-// Distance from the owner's query to point p (< len) of the leaf.
-template <typename A, int K, typename M>
-__device__ __forceinline__ A coop_point(const CoopLeaf<A, K>& L, uint32_t p, uint32_t& item) {
+// Distance (Cartesian or periodic functor) from the owner's query to point
+// p (< len) of the leaf.
+template <typename A, int K, typename Dist>
+__device__ __forceinline__ A coop_point(const CoopLeaf<A, K>& L, uint32_t p, uint32_t& item,
+                                        const Dist& dist) {
   A c[K];
   load_point<A, K>(L.base, L.len, p, c, item);
-  return point_dist<M, A, K>(c, L.q);
+  return dist(c, L.q);
 }
 
 // ---------------------------------------------------------------------------
@@ -96,7 +98,7 @@ struct CBestN {
       uint32_t it = 0;
       bool pass = false;
       if (p < L.len) {
-        d = coop_point<A, K, M>(L, p, it);
+        d = coop_point<A, K>(L, p, it, CartesianDist<A, K, M>());
         pass = (kExclusive ? (d < orad) : (d <= orad)) && !(full_at_entry && it >= thr_item) &&
                (nn < k || it < lk);
       }
@@ -152,11 +154,104 @@ struct CBestN {
 };
 
 // ---------------------------------------------------------------------------
+// nearest_n / nearest_n().within, sorted output: the k smallest by (distance,
+// arrival) (ThresholdVecResultCollection, results/result_collection.rs:
+// 136-215), kept sorted in the query's own output row, which a leaf scan
+// reads and writes one entry per lane.  A candidate goes after every held
+// entry of distance <= its own (those arrived first); once the list is full
+// it must beat the last entry, which it evicts.
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M, bool kExclusive, typename Dist>
+struct CNearestNRow {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A* __restrict__ out_d;
+  uint32_t* __restrict__ out_i;
+  int k;
+  int n;
+  A radius, kth;
+  Dist dist;
+  __device__ CNearestNRow(A* d, uint32_t* i, int k_, Dist ds)
+      : out_d(d), out_i(i), k(k_), n(0), radius(A(0)), kth(inf_of<A>()), dist(ds) {}
+  __device__ __forceinline__ void reset(A r) { n = 0; radius = r; kth = inf_of<A>(); }
+  __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+
+  __device__ __forceinline__ void leaf(int o, uint64_t qo, const CoopLeaf<A, K>& L, int lane) {
+    int nn = __shfl_sync(FULL, n, o);
+    A kk = shfl(kth, o);
+    const A orad = shfl(radius, o);
+    const A bound = (nn == k && kk < orad) ? kk : orad;  // max_dist() at leaf start
+    A* ld = out_d + qo * uint64_t(k);
+    uint32_t* li = out_i + qo * uint64_t(k);
+    A Ld = inf_of<A>();
+    uint32_t Li = 0;
+    bool loaded = false;
+    for (uint32_t c0 = 0; c0 < L.len; c0 += 32) {
+      const uint32_t p = c0 + lane;
+      A d = inf_of<A>();
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < L.len) {
+        d = coop_point<A, K>(L, p, it, dist);
+        pass = (kExclusive ? (d < bound) : (d <= bound)) && (nn < k || d < kk);
+      }
+      unsigned m = __ballot_sync(FULL, pass);
+      if (m && !loaded) {
+        if (lane < nn) {
+          Ld = ld[lane];
+          Li = li[lane];
+        }
+        loaded = true;
+      }
+      while (m) {
+        const int c = __ffs(m) - 1;
+        m &= m - 1;
+        const A dc = shfl(d, c);
+        const uint32_t ic = shfl(it, c);
+        if (nn == k && !(dc < kk)) continue;
+        const int pos = __popc(__ballot_sync(FULL, lane < nn && Ld <= dc));
+        const A ud = __shfl_up_sync(FULL, Ld, 1);
+        const uint32_t ui = __shfl_up_sync(FULL, Li, 1);
+        if (lane > pos) {
+          Ld = ud;
+          Li = ui;
+        } else if (lane == pos) {
+          Ld = dc;
+          Li = ic;
+        }
+        if (nn < k) ++nn;
+        if (nn == k) kk = shfl(Ld, k - 1);
+      }
+    }
+    if (loaded && lane < nn) {
+      ld[lane] = Ld;
+      li[lane] = Li;
+    }
+    if (lane == o) {
+      n = nn;
+      kth = kk;
+    }
+  }
+
+  // The held entries are already in place; the rest of the row is
+  // (+inf, u32::MAX).
+  __device__ __forceinline__ void finish(int o, uint64_t qo, int lane,
+                                         uint32_t* __restrict__ out_c) const {
+    const int on = __shfl_sync(FULL, n, o);
+    if (lane >= on && lane < k) {
+      out_d[qo * uint64_t(k) + lane] = inf_of<A>();
+      out_i[qo * uint64_t(k) + lane] = 0xffffffffu;
+    }
+    if (lane == 0 && out_c) out_c[qo] = uint32_t(on);
+  }
+};
+
+// ---------------------------------------------------------------------------
 // within: counting pass (no output) or filling pass (hits written in arrival
 // order into the query's CSR segment, `cap` long); a leaf's hits are one
 // coalesced store.
 // ---------------------------------------------------------------------------
-template <typename A, int K, typename M, bool kExclusive>
+template <typename A, int K, typename M, bool kExclusive, typename Dist = CartesianDist<A, K, M>>
 struct CWithin {
   static constexpr bool kPruneOnEqual = kExclusive;
   A radius;
@@ -164,10 +259,15 @@ struct CWithin {
   uint64_t cap;
   A* out_d;
   uint32_t* out_i;
-  __device__ CWithin() : radius(A(0)), count(0), cap(0), out_d(nullptr), out_i(nullptr) {}
+  Dist dist;
+  __device__ explicit CWithin(Dist ds = Dist())
+      : radius(A(0)), count(0), cap(0), out_d(nullptr), out_i(nullptr), dist(ds) {}
   __device__ __forceinline__ A max_dist() const { return radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
 
+  __device__ __forceinline__ void leaf(int o, uint64_t, const CoopLeaf<A, K>& L, int lane) {
+    leaf(o, L, lane);
+  }
   __device__ __forceinline__ void leaf(int o, const CoopLeaf<A, K>& L, int lane) {
     uint64_t cnt = shfl64(count, o);
     const uint64_t ocap = shfl64(cap, o);
@@ -180,7 +280,7 @@ struct CWithin {
       uint32_t it = 0;
       bool pass = false;
       if (p < L.len) {
-        d = coop_point<A, K, M>(L, p, it);
+        d = coop_point<A, K>(L, p, it, dist);
         pass = kExclusive ? (d < orad) : (d <= orad);
       }
       const unsigned m = __ballot_sync(FULL, pass);

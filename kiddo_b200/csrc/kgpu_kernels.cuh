@@ -518,6 +518,137 @@ struct BoxArg {
   A v[K];
 };
 
+// Periodic families, one query per thread: PeriodicWalk with lane refill,
+// leaves scanned warp-cooperatively.  Each iteration: finish the lanes whose
+// walks ended, refill, take every active walk to its next leaf, scan those.
+template <typename A, int K, typename M, typename Pol, typename Start, typename Finish>
+__device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Batch<A>& b,
+                                               const A (&box)[K], Pol& pol, A* __restrict__ slot,
+                                               int stride, TravStats& st, Start&& start,
+                                               Finish&& finish) {
+  const int lane = threadIdx.x & 31;
+  PeriodicWalk<A, K, M> wk;
+  wk.init(box);
+  LaneFeeder fd;
+  fd.start();
+  TreeView<A> tv = tv0;
+  A q[K];
+#pragma unroll
+  for (int d = 0; d < K; ++d) q[d] = A(0);
+  bool active = false, fresh = false, done = false;
+  uint64_t qi = 0;
+  for (;;) {
+    for (unsigned fm = __ballot_sync(FULL, done); fm; fm &= fm - 1) {
+      const int o = __ffs(fm) - 1;
+      finish(o, shfl64(qi, o));
+    }
+    done = false;
+    if (!refill_lanes(b, fd, active, fresh, qi)) break;
+    if (fresh) {
+      fresh = false;
+      tv = b.tree(tv0, qi);
+      b.query(qi, q);
+      wk.init(box);
+      if (!start(qi)) {
+        active = false;
+      } else if (tv.size == 0) {
+        done = true;
+        active = false;
+      }
+    }
+    const uint8_t* lb = nullptr;
+    uint32_t len = 0;
+    if (active) {
+      const uint32_t leaf = wk.next(tv, q, box, pol, slot, stride, st);
+      if (leaf == PeriodicWalk<A, K, M>::kDone) {
+        done = true;
+        active = false;
+      } else {
+        const uint2 ex = __ldg(tv.extents + leaf);
+        lb = tv.arena + size_t(ex.x) * 8;
+        len = ex.y;
+        st.points += len;
+        ++st.leaves;
+      }
+    }
+    for (unsigned lm = __ballot_sync(FULL, active); lm; lm &= lm - 1) {
+      const int o = __ffs(lm) - 1;
+      pol.leaf(o, shfl64(qi, o), coop_leaf<A, K>(o, lb, len, q), lane);
+    }
+  }
+}
+
+// Periodic nearest_n / nearest_n().within (always sorted, periodic.rs
+// into_sorted): shared memory holds one rd slot per level per thread.
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_tperiodic_nn(TreeView<A> tv0, Batch<A> b,
+                                                      BoxArg<A, K> box, int k, A radius0,
+                                                      A* __restrict__ out_d,
+                                                      uint32_t* __restrict__ out_i,
+                                                      uint32_t* __restrict__ out_c,
+                                                      unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  TravStats st;
+  PeriodicDist<A, K, M> pd;
+#pragma unroll
+  for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
+  CNearestNRow<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(out_d, out_i, k, pd);
+  periodic_drive<A, K, M>(
+      tv0, b, box.v, pol, slot, blockDim.x, st,
+      [&](uint64_t qi) {
+        pol.reset(b.radius(radius0, qi));
+        return true;
+      },
+      [&](int o, uint64_t qo) { pol.finish(o, qo, lane, out_c); });
+  if (stats) flush_stats(stats, st);
+}
+
+// Periodic within: counting pass (offsets == nullptr) or filling pass.
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_tperiodic_within(
+    TreeView<A> tv0, Batch<A> b, BoxArg<A, K> box, A radius0, uint64_t* __restrict__ counts,
+    const uint64_t* __restrict__ offsets, uint64_t capacity, A* __restrict__ out_d,
+    uint32_t* __restrict__ out_i, int* __restrict__ status,
+    unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  TravStats st;
+  PeriodicDist<A, K, M> pd;
+#pragma unroll
+  for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
+  CWithin<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(pd);
+  uint64_t o = 0;  // this lane's segment start (filling pass)
+  periodic_drive<A, K, M>(
+      tv0, b, box.v, pol, slot, blockDim.x, st,
+      [&](uint64_t qi) {
+        pol.radius = b.radius(radius0, qi);
+        pol.count = 0;
+        pol.cap = 0;
+        pol.out_d = nullptr;
+        pol.out_i = nullptr;
+        if (!offsets) return true;
+        o = offsets[qi];
+        const uint64_t end = offsets[qi + 1] < capacity ? offsets[qi + 1] : capacity;
+        if (end <= o) return false;  // no hits to place (empty segment, or past the capacity)
+        pol.cap = end - o;
+        pol.out_d = out_d + o;
+        pol.out_i = out_i + o;
+        return true;
+      },
+      [&](int w, uint64_t qo) {
+        const uint64_t cnt = shfl64(pol.count, w);
+        const uint64_t ow = shfl64(o, w);
+        if (lane == 0) {
+          if (counts) counts[qo] = cnt;
+          if (offsets && status && cnt != offsets[qo + 1] - ow) atomicExch(status, 6);
+        }
+      });
+  if (stats) flush_stats(stats, st);
+}
+
 template <typename A, int K, typename M, int FAM, bool EXCL>
 __global__ void __launch_bounds__(256) k_periodic_fixed(TreeView<A> tv0, Batch<A> b,
                                                         BoxArg<A, K> box, int k, A radius0,

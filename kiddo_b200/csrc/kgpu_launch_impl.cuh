@@ -160,6 +160,20 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
         using M = decltype(m);
         return with_excl(q.exclusive, [&](auto ex) {
           constexpr bool EX = decltype(ex)::value;
+          if (q.periodic) {
+            // periodic nearest_n: per-thread walk, cooperative leaf scans,
+            // lists in the output rows
+            const auto box = make_box<A, K>(q);
+            const size_t psmem = thread_smem<A>(t);
+            auto kern = k_tperiodic_nn<A, K, M, EX>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(psmem));
+            const int grid = grid_for(kern, psmem, (q.nq + 31) / 32);
+            kern<<<grid, 256, psmem, q.stream>>>(tv, b, box, q.k, radius,
+                                                  static_cast<A*>(q.out_d), q.out_i, q.out_c,
+                                                  q.stats);
+            g_launches++;
+            return cudaGetLastError();
+          }
           auto runt = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
@@ -201,6 +215,20 @@ cudaError_t launch_within_pass(const DeviceTree& t, const QueryLaunch& q, uint64
       using M = decltype(m);
       return with_excl(q.exclusive, [&](auto ex) -> cudaError_t {
         constexpr bool EX = decltype(ex)::value;
+        if constexpr (thread_engine_dims(K)) {
+          if (q.periodic && q.engine != 1) {
+            const auto box = make_box<A, K>(q);
+            const size_t smem = thread_smem<A>(t);
+            auto kern = k_tperiodic_within<A, K, M, EX>;
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+            kern<<<grid, 256, smem, q.stream>>>(tv, b, box, radius, counts, offsets, q.capacity,
+                                                static_cast<A*>(q.out_d), q.out_i, q.status,
+                                                q.stats);
+            g_launches++;
+            return cudaGetLastError();
+          }
+        }
         if (q.periodic) {
           const BoxArg<A, K> box = make_box<A, K>(q);
           if (!offsets) {

@@ -165,6 +165,155 @@ struct ThreadWalk {
   }
 };
 
+// Per-thread periodic_backtracking_query (periodic.rs:455-619).  The
+// reference's frames carry the far child's whole (lower, upper, off) state;
+// here a frame is only its rd (slot[FL * stride], FL = the far child's level)
+// and a bit in `frames`.  The rest is rebuilt when the frame is popped:
+//  * the bound of axis d is the pivot of the deepest ancestor step that set
+//    it (bit L of lo_set / hi_set: the step out of level L made lower /
+//    upper of axis L % K equal to that stem's pivot), else 0 / the box size;
+//  * off of axis d is periodic_interval_distance of those bounds once some
+//    ancestor step split axis d (bit L of `split`), else 0.
+// Both are exactly what the reference's step computed from the same inputs,
+// so the rebuilt state equals the frame it replaces.
+template <typename A, int K, typename M>
+struct PeriodicWalk {
+  static constexpr uint32_t kDone = 0xffffffffu;
+  A lo[K], hi[K], off[K];
+  A rd;
+  uint32_t stem_idx;
+  int level;
+  uint32_t frames, split, lo_set, hi_set;
+  bool at_leaf;
+
+  __device__ __forceinline__ static uint32_t axis_levels(int d) {
+    uint32_t m = 0;
+    for (int l = d; l < 32; l += K) m |= 1u << l;
+    return m;
+  }
+
+  __device__ __forceinline__ void init(const A (&box)[K]) {
+#pragma unroll
+    for (int d = 0; d < K; ++d) {
+      lo[d] = A(0);
+      hi[d] = box[d];
+      off[d] = A(0);
+    }
+    rd = A(0);
+    stem_idx = 1;
+    level = 0;
+    frames = split = lo_set = hi_set = 0;
+    at_leaf = false;
+  }
+
+  // Pops the deepest pending frame (the reference's stack.pop()); false when
+  // there is none.
+  __device__ __forceinline__ bool pop(const TreeView<A>& tv, const A (&q)[K], const A (&box)[K],
+                                      const A* __restrict__ slot, int stride) {
+    if (!frames) return false;
+    const int FL = 31 - __clz(frames);
+    frames &= ~(1u << FL);
+    const int P = FL - 1;
+    const uint32_t parent = stem_idx >> (level - P);
+    const uint32_t below = (1u << P) - 1u;
+#pragma unroll
+    for (int d = 0; d < K; ++d) {
+      const uint32_t am = axis_levels(d) & below;
+      const uint32_t ml = lo_set & am, mh = hi_set & am;
+      lo[d] = ml ? __ldg(tv.stems + (parent >> (P - (31 - __clz(ml))))) : A(0);
+      hi[d] = mh ? __ldg(tv.stems + (parent >> (P - (31 - __clz(mh))))) : box[d];
+      off[d] = (split & am) ? periodic_interval_distance(q[d], lo[d], hi[d], box[d]) : A(0);
+    }
+    const int dP = P % K;
+    const A pivot = __ldg(tv.stems + parent);
+    const A qd = sel(q, dP);
+    const bool is_right = qd >= pivot;
+    const A old_lo = sel(lo, dP), old_hi = sel(hi, dP);
+    const A minup = old_hi < pivot ? old_hi : pivot;
+    const A maxlo = max_ref(old_lo, pivot);
+    const A far_lo = is_right ? old_lo : maxlo;
+    const A far_hi = is_right ? minup : old_hi;
+    put(lo, dP, far_lo);
+    put(hi, dP, far_hi);
+    put(off, dP, periodic_interval_distance(qd, far_lo, far_hi, sel(box, dP)));
+    rd = slot[FL * stride];
+    split &= below;
+    lo_set &= below;
+    hi_set &= below;
+    split |= 1u << P;
+    if (!is_right && pivot > old_lo) lo_set |= 1u << P;   // far = right child: lower = maxlo
+    if (is_right && !(old_hi < pivot)) hi_set |= 1u << P;  // far = left child: upper = minup
+    stem_idx = parent * 2u + (is_right ? 0u : 1u);
+    level = FL;
+    return true;
+  }
+
+  // The next leaf of the walk, or kDone.
+  template <typename P>
+  __device__ __forceinline__ uint32_t next(const TreeView<A>& tv, const A (&q)[K],
+                                           const A (&box)[K], const P& pol, A* __restrict__ slot,
+                                           int stride, TravStats& st) {
+    if (at_leaf) {
+      at_leaf = false;
+      if (!pop(tv, q, box, slot, stride)) return kDone;
+    }
+    const A INF = inf_of<A>();
+    const int msl = tv.max_stem_level;
+    int dim = level % K;
+    for (;;) {
+      if (level > msl) {
+        at_leaf = true;
+        return stem_idx & ~(1u << level);
+      }
+      ++st.stems;
+      const A pivot = stem_idx < tv.stem_count ? __ldg(tv.stems + stem_idx) : INF;
+      if (!(pivot < INF)) {
+        stem_idx *= 2u;
+        ++level;
+        dim = dim + 1 == K ? 0 : dim + 1;
+        continue;
+      }
+      const A old_lo = sel(lo, dim), old_hi = sel(hi, dim);
+      const A qd = sel(q, dim), Ld = sel(box, dim);
+      const bool is_right = qd >= pivot;
+      const A minup = old_hi < pivot ? old_hi : pivot;
+      const A maxlo = max_ref(old_lo, pivot);
+      const A near_lo = is_right ? maxlo : old_lo;
+      const A near_hi = is_right ? old_hi : minup;
+      const A far_lo = is_right ? old_lo : maxlo;
+      const A far_hi = is_right ? minup : old_hi;
+      const A near_off = periodic_interval_distance(qd, near_lo, near_hi, Ld);
+      const A far_off = periodic_interval_distance(qd, far_lo, far_hi, Ld);
+      const A oo = sel(off, dim);
+      const A near_rd = M::template rect<A>(rd, oo, near_off);
+      const A far_rd = M::template rect<A>(rd, oo, far_off);
+      const A thr = pol.max_dist();
+      const bool near_pruned = near_rd > thr || (P::kPruneOnEqual && near_rd == thr);
+      const bool far_pruned = far_rd > thr || (P::kPruneOnEqual && far_rd == thr);
+      if (!far_pruned) {
+        slot[(level + 1) * stride] = far_rd;
+        frames |= 1u << (level + 1);
+      }
+      if (near_pruned) {
+        if (!pop(tv, q, box, slot, stride)) return kDone;
+        dim = level % K;
+        continue;
+      }
+      const uint32_t bit = 1u << level;
+      split |= bit;
+      if (is_right && pivot > old_lo) lo_set |= bit;
+      if (!is_right && !(old_hi < pivot)) hi_set |= bit;
+      put(lo, dim, near_lo);
+      put(hi, dim, near_hi);
+      put(off, dim, near_off);
+      rd = near_rd;
+      stem_idx = stem_idx * 2u + (is_right ? 1u : 0u);
+      ++level;
+      dim = dim + 1 == K ? 0 : dim + 1;
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Thread policies
 // ---------------------------------------------------------------------------
