@@ -403,7 +403,7 @@ __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch
 #define KGPU_TFIXED_MIN_BLOCKS 4
 #endif
 template <typename A, int K, typename M, int FAM, bool EXCL>
-__global__ void __launch_bounds__(256, KGPU_TFIXED_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, FAM == KF_BEST_N ? 3 : KGPU_TFIXED_MIN_BLOCKS)
     k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k, A radius0, int arrival_order,
              A* __restrict__ out_d, uint32_t* __restrict__ out_i, uint32_t* __restrict__ out_c,
              unsigned long long* __restrict__ stats) {

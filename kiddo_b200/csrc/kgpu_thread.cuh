@@ -80,6 +80,64 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
   return ex.y;
 }
 
+// Bit j of the result: point c0 + j of the leaf passes pass(distance).  A
+// chunk is one 32-point tile (c0 below len & ~31) or the leaf's remainder
+// tiles (widths 8, 4, 2, 1); pairs are read as in thread_for_each_point and
+// nothing but the mask depends on the outcome, so the loop stays convergent.
+template <typename A, int K, typename D, typename P>
+__device__ __forceinline__ uint32_t leaf_chunk_mask(const uint8_t* __restrict__ base, uint32_t len,
+                                                    uint32_t c0, const D& dist, P&& pass) {
+  constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
+  const uint32_t full = len & ~31u;
+  uint32_t boff, rem;
+  if (c0 < full) {
+    boff = (c0 >> 5) * (32 * per);
+    rem = 32;
+  } else {
+    boff = full * per;
+    rem = len - full;
+  }
+  uint32_t mask = 0, bit = 0;
+  while (rem) {
+    const uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
+    const A* col = reinterpret_cast<const A*>(base + boff);
+    for (uint32_t i = 0; i < w; i += 2) {
+      A d0, d1;
+      if (w == 1) {
+        A c[K];
+#pragma unroll
+        for (int d = 0; d < K; ++d) c[d] = __ldg(col + d);
+        d0 = d1 = dist(c);
+      } else if constexpr (sizeof(A) == 4) {
+        A c0v[K], c1v[K];
+#pragma unroll
+        for (int d = 0; d < K; ++d) {
+          const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
+          c0v[d] = v.x;
+          c1v[d] = v.y;
+        }
+        d0 = dist(c0v);
+        d1 = dist(c1v);
+      } else {
+        A c0v[K], c1v[K];
+#pragma unroll
+        for (int d = 0; d < K; ++d) {
+          c0v[d] = __ldg(col + d * w + i);
+          c1v[d] = __ldg(col + d * w + i + 1);
+        }
+        d0 = dist(c0v);
+        d1 = dist(c1v);
+      }
+      mask |= (pass(d0) ? 1u : 0u) << (bit + i);
+      if (w > 1) mask |= (pass(d1) ? 1u : 0u) << (bit + i + 1);
+    }
+    boff += w * per;
+    bit += w;
+    rem -= w;
+  }
+  return mask;
+}
+
 // Resumable traversal state of one query: the reference's DFS
 // (kd_tree/orchestrator/mod.rs:388-603) cut at its leaves, so a thread can
 // stop after any leaf and carry on later.  descend() runs from the current
@@ -405,15 +463,36 @@ struct TNearestN {
     kth = ld[(k - 1) * stride];
   }
 
+  // The leaf filter of leaf_view_chunked/nearest_n_within/fallback.rs:37-95
+  // (distance against max_dist() at leaf start, then the collector's own
+  // test), in two passes per 32-point chunk: a convergent scan marks the
+  // points that can enter the list (bound and, when the list starts full,
+  // kth at leaf start), then the lanes insert their marked points in leaf
+  // order together, each re-read from L1 and re-tested against the current
+  // kth.  The add() calls are the sequential ones minus those add() would
+  // reject, so the list is the same.
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
     const A bound = max_dist();
+    const bool full0 = n == k;
+    const A kth0 = kth;
     const CartesianQ<A, K, M> dist{q};
-    return thread_for_each_point<A, K>(
-        tv, l, dist,
-        [&](A d) { return (kExclusive ? (d < bound) : (d <= bound)) && (n < k || d < kth); },
-        [&](A d, uint32_t it) {
-          if (kExclusive ? (d < bound) : (d <= bound)) add(d, it);
-        });
+    const uint2 ex = __ldg(tv.extents + l);
+    const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+    const uint32_t len = ex.y;
+    for (uint32_t c0 = 0; c0 < len; c0 += 32) {
+      uint32_t mask = leaf_chunk_mask<A, K>(base, len, c0, dist, [&](A d) {
+        return (kExclusive ? (d < bound) : (d <= bound)) && (!full0 || d < kth0);
+      });
+      while (mask) {
+        const uint32_t p = c0 + uint32_t(__ffs(mask) - 1);
+        mask &= mask - 1;
+        A c[K];
+        uint32_t it;
+        load_point<A, K>(base, len, p, c, it);
+        add(dist(c), it);
+      }
+    }
+    return len;
   }
 
   __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
