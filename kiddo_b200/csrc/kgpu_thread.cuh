@@ -32,58 +32,67 @@ namespace kgpu {
 template <typename A, int K, typename D, typename P, typename F>
 __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint32_t leaf,
                                                           const D& dist, P&& pass, F&& f) {
+  constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
   const uint2 ex = __ldg(tv.extents + leaf);
   const uint8_t* base = tv.arena + size_t(ex.x) * 8;
   uint32_t rem = ex.y;
-  uint32_t boff = 0;
+  uint32_t boff = 0, i = 0;
+  uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
+  // one flat loop step per pair; the next tile is taken in a short tail
   while (rem) {
-    const uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
     const A* col = reinterpret_cast<const A*>(base + boff);
-    const uint32_t* its = reinterpret_cast<const uint32_t*>(base + boff + K * w * sizeof(A));
-    for (uint32_t i = 0; i < w; i += 2) {
-      A d0, d1;
-      if (w == 1) {
-        A c0[K];
+    A d0, d1;
+    if (w == 1) {
+      A c0[K];
 #pragma unroll
-        for (int d = 0; d < K; ++d) c0[d] = __ldg(col + d);
-        d0 = d1 = dist(c0);
-      } else if constexpr (sizeof(A) == 4) {
-        A c0[K], c1[K];
+      for (int d = 0; d < K; ++d) c0[d] = __ldg(col + d);
+      d0 = d1 = dist(c0);
+    } else if constexpr (sizeof(A) == 4) {
+      A c0[K], c1[K];
 #pragma unroll
-        for (int d = 0; d < K; ++d) {
-          const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
-          c0[d] = v.x;
-          c1[d] = v.y;
-        }
-        d0 = dist(c0);
-        d1 = dist(c1);
-      } else {
-        A c0[K], c1[K];
-#pragma unroll
-        for (int d = 0; d < K; ++d) {
-          c0[d] = __ldg(col + d * w + i);
-          c1[d] = __ldg(col + d * w + i + 1);
-        }
-        d0 = dist(c0);
-        d1 = dist(c1);
+      for (int d = 0; d < K; ++d) {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
+        c0[d] = v.x;
+        c1[d] = v.y;
       }
-      // `pass` is a cheap necessary condition for f to act: most points fail
-      // it once a list has filled, and then f is not entered at all.
-      if (!pass(d0) && !(w > 1 && pass(d1))) continue;
+      d0 = dist(c0);
+      d1 = dist(c1);
+    } else {
+      A c0[K], c1[K];
+#pragma unroll
+      for (int d = 0; d < K; ++d) {
+        c0[d] = __ldg(col + d * w + i);
+        c1[d] = __ldg(col + d * w + i + 1);
+      }
+      d0 = dist(c0);
+      d1 = dist(c1);
+    }
+    // `pass` is a cheap necessary condition for f to act: most points fail
+    // it once a list has filled, and then f is not entered at all.
+    if (pass(d0) || (w > 1 && pass(d1))) {
+      const uint32_t* its = reinterpret_cast<const uint32_t*>(base + boff + K * w * sizeof(A));
       const int nu = w == 1 ? 1 : 2;
 #pragma unroll 1
       for (int u = 0; u < nu; ++u) f(u ? d1 : d0, __ldg(its + i + u));
     }
-    boff += w * (K * sizeof(A) + sizeof(uint32_t));
-    rem -= w;
+    i += 2;
+    if (i >= w) {
+      boff += w * per;
+      rem -= w;
+      w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
+      i = 0;
+    }
   }
   return ex.y;
 }
 
 // Bit j of the result: point c0 + j of the leaf passes pass(distance).  A
 // chunk is one 32-point tile (c0 below len & ~31) or the leaf's remainder
-// tiles (widths 8, 4, 2, 1); pairs are read as in thread_for_each_point and
-// nothing but the mask depends on the outcome, so the loop stays convergent.
+// tiles (widths 8, 4, 2, 1).  One flat loop step per pair of points (tiles of
+// width >= 2 are read in 8-byte aligned pairs, as in thread_for_each_point),
+// moving to the next tile in a short tail, so lanes whose leaves have
+// different tile shapes still run the same loop body; nothing but the mask
+// depends on the distances.
 template <typename A, int K, typename D, typename P>
 __device__ __forceinline__ uint32_t leaf_chunk_mask(const uint8_t* __restrict__ base, uint32_t len,
                                                     uint32_t c0, const D& dist, P&& pass) {
@@ -97,43 +106,45 @@ __device__ __forceinline__ uint32_t leaf_chunk_mask(const uint8_t* __restrict__ 
     boff = full * per;
     rem = len - full;
   }
-  uint32_t mask = 0, bit = 0;
+  uint32_t mask = 0, bit = 0, i = 0;
+  uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
   while (rem) {
-    const uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
     const A* col = reinterpret_cast<const A*>(base + boff);
-    for (uint32_t i = 0; i < w; i += 2) {
-      A d0, d1;
-      if (w == 1) {
-        A c[K];
+    A d0, d1;
+    if (w == 1) {
+      A c[K];
 #pragma unroll
-        for (int d = 0; d < K; ++d) c[d] = __ldg(col + d);
-        d0 = d1 = dist(c);
-      } else if constexpr (sizeof(A) == 4) {
-        A c0v[K], c1v[K];
+      for (int d = 0; d < K; ++d) c[d] = __ldg(col + d);
+      d0 = d1 = dist(c);
+    } else if constexpr (sizeof(A) == 4) {
+      A c0v[K], c1v[K];
 #pragma unroll
-        for (int d = 0; d < K; ++d) {
-          const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
-          c0v[d] = v.x;
-          c1v[d] = v.y;
-        }
-        d0 = dist(c0v);
-        d1 = dist(c1v);
-      } else {
-        A c0v[K], c1v[K];
-#pragma unroll
-        for (int d = 0; d < K; ++d) {
-          c0v[d] = __ldg(col + d * w + i);
-          c1v[d] = __ldg(col + d * w + i + 1);
-        }
-        d0 = dist(c0v);
-        d1 = dist(c1v);
+      for (int d = 0; d < K; ++d) {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
+        c0v[d] = v.x;
+        c1v[d] = v.y;
       }
-      mask |= (pass(d0) ? 1u : 0u) << (bit + i);
-      if (w > 1) mask |= (pass(d1) ? 1u : 0u) << (bit + i + 1);
+      d0 = dist(c0v);
+      d1 = dist(c1v);
+    } else {
+      A c0v[K], c1v[K];
+#pragma unroll
+      for (int d = 0; d < K; ++d) {
+        c0v[d] = __ldg(col + d * w + i);
+        c1v[d] = __ldg(col + d * w + i + 1);
+      }
+      d0 = dist(c0v);
+      d1 = dist(c1v);
     }
-    boff += w * per;
-    bit += w;
-    rem -= w;
+    mask |= ((pass(d0) ? 1u : 0u) | ((w > 1 && pass(d1)) ? 2u : 0u)) << (bit + i);
+    i += 2;
+    if (i >= w) {
+      boff += w * per;
+      bit += w;
+      rem -= w;
+      w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
+      i = 0;
+    }
   }
   return mask;
 }
