@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/kiddo_gpu.h"
+#include "kgpu_devbuf.h"
 #include "kgpu_internal.h"
 #include "kgpu_launch.h"
 #include "kgpu_tree_impl.h"
@@ -64,21 +65,29 @@ size_t leaf_encoded_bytes(uint64_t len, int K, size_t sa) {
 }
 
 // RAII device buffer allocated on a stream (stream-ordered allocator).
-struct DevBuf {
-  void* p = nullptr;
-  cudaStream_t s = nullptr;
-  cudaError_t alloc(size_t bytes, cudaStream_t st) {
-    s = st;
-    if (bytes == 0) bytes = 16;
-    return cudaMallocAsync(&p, bytes, st);
-  }
-  ~DevBuf() {
-    if (p) cudaFreeAsync(p, s);
-  }
-  template <typename T> T* as() const { return static_cast<T*>(p); }
-};
 
 }  // namespace
+}  // namespace kgpu
+
+namespace kgpu {
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
+  static std::atomic<uint64_t> cached_devices{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
+  if (bit && !(cached_devices.load(std::memory_order_relaxed) & bit)) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = ~uint64_t(0);
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cached_devices.fetch_or(bit, std::memory_order_relaxed);
+  }
+  return cudaMallocAsync(p, bytes, s);
+}
+
 }  // namespace kgpu
 
 using namespace kgpu;

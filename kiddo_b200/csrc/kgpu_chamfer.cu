@@ -21,6 +21,7 @@
 
 #include "../../include/kiddo_gpu.h"
 #include "kgpu_device.cuh"
+#include "kgpu_devbuf.h"
 #include "kgpu_internal.h"
 #include "kgpu_launch.h"
 #include "kgpu_tree_impl.h"
@@ -28,18 +29,6 @@
 namespace kgpu {
 namespace {
 
-struct DevBuf {
-  void* p = nullptr;
-  cudaStream_t s = nullptr;
-  cudaError_t alloc(size_t bytes, cudaStream_t st) {
-    s = st;
-    return cudaMallocAsync(&p, bytes ? bytes : 16, st);
-  }
-  ~DevBuf() {
-    if (p) cudaFreeAsync(p, s);
-  }
-  template <typename T> T* as() const { return static_cast<T*>(p); }
-};
 
 __device__ __forceinline__ float sq_dist3(const float* a, const float* b) {
   float acc = 0.f;

@@ -20,6 +20,7 @@
 
 #include "../../include/kiddo_gpu.h"
 #include "kgpu_device.cuh"
+#include "kgpu_devbuf.h"
 #include "kgpu_internal.h"
 #include "kgpu_launch.h"
 #include "kgpu_tree_impl.h"
@@ -44,17 +45,6 @@ int cuda_err(cudaError_t e, const char* what) {
   return set_error(KGPU_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-struct DevBuf {
-  void* p = nullptr;
-  cudaStream_t s = nullptr;
-  cudaError_t alloc(size_t bytes, cudaStream_t st) {
-    s = st;
-    return cudaMallocAsync(&p, bytes ? bytes : 16, st);
-  }
-  ~DevBuf() {
-    if (p) cudaFreeAsync(p, s);
-  }
-};
 
 template <typename A>
 void fill_views(const std::vector<kgpu_tree*>& trees, std::vector<uint8_t>& out) {
