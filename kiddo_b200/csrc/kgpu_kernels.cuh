@@ -580,8 +580,11 @@ __device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Bat
 
 // Periodic nearest_n / nearest_n().within (always sorted, periodic.rs
 // into_sorted): shared memory holds one rd slot per level per thread.
+#ifndef KGPU_TPERIODIC_MIN_BLOCKS
+#define KGPU_TPERIODIC_MIN_BLOCKS 3
+#endif
 template <typename A, int K, typename M, bool EXCL>
-__global__ void __launch_bounds__(256) k_tperiodic_nn(TreeView<A> tv0, Batch<A> b,
+__global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_nn(TreeView<A> tv0, Batch<A> b,
                                                       BoxArg<A, K> box, int k, A radius0,
                                                       A* __restrict__ out_d,
                                                       uint32_t* __restrict__ out_i,
@@ -607,7 +610,7 @@ __global__ void __launch_bounds__(256) k_tperiodic_nn(TreeView<A> tv0, Batch<A> 
 
 // Periodic within: counting pass (offsets == nullptr) or filling pass.
 template <typename A, int K, typename M, bool EXCL>
-__global__ void __launch_bounds__(256) k_tperiodic_within(
+__global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_within(
     TreeView<A> tv0, Batch<A> b, BoxArg<A, K> box, A radius0, uint64_t* __restrict__ counts,
     const uint64_t* __restrict__ offsets, uint64_t capacity, A* __restrict__ out_d,
     uint32_t* __restrict__ out_i, int* __restrict__ status,
@@ -734,37 +737,92 @@ __device__ __forceinline__ bool key_less(A da, uint32_t pa, A db, uint32_t pb) {
   return da < db || (da == db && pa < pb);
 }
 
+// Stable sort of one segment of n <= N hits by its own thread: the segment is
+// loaded into registers (padding +inf after it), insertion-sorted by a fully
+// unrolled network of adjacent compare-swaps that swap only strictly greater
+// keys (so equal keys keep their order and padding stays behind), and written
+// back.
+template <typename A, int N>
+__device__ __forceinline__ void small_segment_sort(A* __restrict__ d, uint32_t* __restrict__ it,
+                                                   uint32_t n) {
+  A kd[N];
+  uint32_t kv[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    kd[j] = uint32_t(j) < n ? d[j] : inf_of<A>();
+    kv[j] = uint32_t(j) < n ? it[j] : 0u;
+  }
+#pragma unroll
+  for (int a = 1; a < N; ++a) {
+#pragma unroll
+    for (int j = a; j > 0; --j) {
+      const bool sw = kd[j - 1] > kd[j];
+      const A td = kd[j - 1];
+      const uint32_t tv = kv[j - 1];
+      kd[j - 1] = sw ? kd[j] : td;
+      kv[j - 1] = sw ? kv[j] : tv;
+      kd[j] = sw ? td : kd[j];
+      kv[j] = sw ? tv : kv[j];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+    if (uint32_t(j) < n) {
+      d[j] = kd[j];
+      it[j] = kv[j];
+    }
+}
+
+// Segments of up to 32 hits.  A warp takes 32 segments at a time (lane l
+// reads segment base + l's bounds, coalesced): segments of 2..kThreadSort
+// hits are sorted in registers by their own lane (small_segment_sort), and
+// the warp then bitonic-sorts its segments of
+// kThreadSort+1..32 hits one after another on (key, position).
 template <typename A>
 __global__ void __launch_bounds__(256) k_seg_sort_warp(const uint64_t* __restrict__ offsets,
                                                        uint64_t nq, uint64_t capacity,
                                                        A* __restrict__ d,
                                                        uint32_t* __restrict__ it) {
+  constexpr uint64_t kThreadSort = 8;
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-  for (uint64_t s = warp; s < nq; s += nwarps) {
-    const uint64_t o = min(offsets[s], capacity);
-    const uint64_t n = min(offsets[s + 1], capacity) - o;
-    if (n <= 1 || n > 32) continue;
-    A kd = inf_of<A>();
-    uint32_t kp = 0xffffffffu, kv = 0;
-    if (lane < n) { kd = d[o + lane]; kv = it[o + lane]; kp = lane; }
-#pragma unroll
-    for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        const A od = __shfl_xor_sync(FULL, kd, stride);
-        const uint32_t op = __shfl_xor_sync(FULL, kp, stride);
-        const uint32_t ov = __shfl_xor_sync(FULL, kv, stride);
-        const bool up = ((lane & size) == 0);
-        const bool lower = (lane & stride) == 0;
-        // lower lane keeps the min when ascending
-        const bool other_less = key_less(od, op, kd, kp);
-        const bool take = lower ? (up ? other_less : !other_less) : (up ? !other_less : other_less);
-        if (take && !(od == kd && op == kp)) { kd = od; kp = op; kv = ov; }
-      }
+  for (uint64_t base = warp * 32; base < nq; base += nwarps * 32) {
+    const uint64_t s = base + lane;
+    uint64_t o = 0, n = 0;
+    if (s < nq) {
+      o = min(offsets[s], capacity);
+      n = min(offsets[s + 1], capacity) - o;
     }
-    if (lane < n) { d[o + lane] = kd; it[o + lane] = kv; }
+    if (n >= 2 && n <= 4) {
+      small_segment_sort<A, 4>(d + o, it + o, uint32_t(n));
+    } else if (n > 4 && n <= kThreadSort) {
+      small_segment_sort<A, kThreadSort>(d + o, it + o, uint32_t(n));
+    }
+    for (unsigned big = __ballot_sync(FULL, n > kThreadSort && n <= 32); big; big &= big - 1) {
+      const int src = __ffs(big) - 1;
+      const uint64_t so = __shfl_sync(FULL, (unsigned long long)o, src);
+      const uint32_t sn = uint32_t(__shfl_sync(FULL, (unsigned long long)n, src));
+      A kd = inf_of<A>();
+      uint32_t kp = 0xffffffffu, kv = 0;
+      if (uint32_t(lane) < sn) { kd = d[so + lane]; kv = it[so + lane]; kp = lane; }
+#pragma unroll
+      for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          const A od = __shfl_xor_sync(FULL, kd, stride);
+          const uint32_t op = __shfl_xor_sync(FULL, kp, stride);
+          const uint32_t ov = __shfl_xor_sync(FULL, kv, stride);
+          const bool up = ((lane & size) == 0);
+          const bool lower = (lane & stride) == 0;
+          // lower lane keeps the min when ascending
+          const bool other_less = key_less(od, op, kd, kp);
+          const bool take = lower ? (up ? other_less : !other_less) : (up ? !other_less : other_less);
+          if (take && !(od == kd && op == kp)) { kd = od; kp = op; kv = ov; }
+        }
+      }
+      if (uint32_t(lane) < sn) { d[so + lane] = kd; it[so + lane] = kv; }
+    }
   }
 }
 

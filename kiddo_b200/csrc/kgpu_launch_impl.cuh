@@ -289,7 +289,7 @@ cudaError_t launch_seg_sort(const uint64_t* offsets, uint64_t nq, uint64_t capac
   if (nq == 0) return cudaSuccess;
   {
     auto kern = k_seg_sort_warp<A>;
-    const int grid = grid_for(kern, 0, nq);
+    const int grid = grid_for(kern, 0, (nq + 31) / 32);
     kern<<<grid, 256, 0, s>>>(offsets, nq, capacity, d, it);
     g_launches++;
   }
