@@ -72,8 +72,9 @@ def periodic_particles(n, rng, dtype, clumps=4096, sigma=0.002, clumped=0.7):
     return pts[rng.permutation(n)].astype(dtype)
 
 
-# radius of the periodic neighbour lists: 0.01 Euclidean = 1e-4 SquaredEuclidean
-C5_RADIUS = 1e-4
+# radius argument of the periodic neighbour lists, in the metric's own units
+# (SquaredEuclidean: 0.01 = a Euclidean radius of 0.1), as within(0.01) takes it
+C5_RADIUS = 0.01
 
 
 def make_data(workload, rank, n=None, nq=None):
@@ -377,6 +378,11 @@ def main():
     achieved = bpq * nq / (kern_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = profile_traffic(args.workload)
+    # compulsory bytes: the whole tree once, the queries once, the results once
+    tree_bytes = sum(a.nbytes for a in (tree.stems(), tree.leaf_bytes(), tree.leaf_extents()))
+    out_bytes = nq * w * (Q.itemsize + 4) + (nq * 4 if w > 1 else 0)
+    compulsory = tree_bytes + nq * 3 * Q.itemsize + out_bytes
+    comp_gbs = compulsory / (kern_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
@@ -391,6 +397,8 @@ def main():
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "bytes_per_query": bpq,
                      "traffic": (traffic or {}).get("dram_bytes_per_launch"),
+                     "compulsory": {"bytes": int(compulsory), "achieved": comp_gbs,
+                                    "frac": comp_gbs / peak},
                      "kernel": kernel_name(fam, args.engine)},
         "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},

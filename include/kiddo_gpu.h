@@ -51,7 +51,7 @@ typedef enum kgpu_dtype { KGPU_F32 = 0, KGPU_F64 = 1 } kgpu_dtype;
 
 typedef enum kgpu_stem_strategy {
   KGPU_STEM_EYTZINGER = 0, /* src/stem_strategy/eytzinger/mod.rs */
-  KGPU_STEM_DONNELLY = 1   /* src/stem_strategy/donnelly/core.rs (not accepted yet) */
+  KGPU_STEM_DONNELLY = 1   /* src/stem_strategy/donnelly/core.rs, Donnelly<3> and Donnelly<4> */
 } kgpu_stem_strategy;
 
 typedef enum kgpu_resolution {
@@ -138,6 +138,14 @@ uint32_t kgpu_abi_version(void);
 int32_t kgpu_layout_build(int32_t dtype, uint32_t dims, const void* points,
                           const uint32_t* items, uint64_t n, int32_t nthreads,
                           kgpu_layout** out);
+/* The same construction over another stem order (replaces KdTree<A, u32, SS, ...>
+ * ::new_from_slice / new_from_entries for SS = Eytzinger or Donnelly<BH>,
+ * src/lib.rs:235, construction.rs:431-469): stem_strategy KGPU_STEM_EYTZINGER
+ * (block_height ignored) or KGPU_STEM_DONNELLY with block_height 3 or 4, the
+ * heights the reference uses (Donnelly<3> for f64, Donnelly<4> for f32 trees). */
+int32_t kgpu_layout_build_stems(int32_t dtype, uint32_t dims, const void* points,
+                                const uint32_t* items, uint64_t n, int32_t stem_strategy,
+                                uint32_t block_height, int32_t nthreads, kgpu_layout** out);
 /* Fills `desc` with pointers into the layout's own storage (valid until free). */
 int32_t kgpu_layout_describe(const kgpu_layout* layout, kgpu_tree_desc* desc);
 int32_t kgpu_layout_free(kgpu_layout* layout);

@@ -84,6 +84,10 @@ class ImmutableKdTree:
 
     Built with the reference's soft construction by ``kgpu_layout_build``, or
     wrapped around a layout the reference itself produced (``from_layout``).
+    ``block_height`` 3 or 4 builds the same tree over Donnelly<block_height>
+    stems (``KdTree<A, u32, Donnelly<BH>, VecOfArenas<..>, K, 32>``,
+    src/lib.rs:235) instead of the Eytzinger order; those trees are queried by
+    the reference's scalar backtracking, and the same results come back.
     """
 
     def __init__(self, desc: C.TreeDesc, keepalive, dtype, dims):
@@ -95,15 +99,17 @@ class ImmutableKdTree:
 
     # ---- construction (construction.rs:278-303, 403-409) -------------------
     @classmethod
-    def new_from_slice(cls, points, threads: int = 0) -> "ImmutableKdTree":
-        return cls._build(points, None, threads)
+    def new_from_slice(cls, points, threads: int = 0, block_height: int = 0) -> "ImmutableKdTree":
+        return cls._build(points, None, threads, block_height)
 
     @classmethod
-    def new_from_entries(cls, items, points, threads: int = 0) -> "ImmutableKdTree":
-        return cls._build(points, np.ascontiguousarray(items, dtype=np.uint32), threads)
+    def new_from_entries(cls, items, points, threads: int = 0,
+                         block_height: int = 0) -> "ImmutableKdTree":
+        return cls._build(points, np.ascontiguousarray(items, dtype=np.uint32), threads,
+                          block_height)
 
     @classmethod
-    def _build(cls, points, items, threads):
+    def _build(cls, points, items, threads, block_height=0):
         pts = np.ascontiguousarray(points)
         if pts.dtype not in (np.float32, np.float64) or pts.ndim != 2:
             raise TypeError("points must be a 2-D float32 or float64 array")
@@ -112,8 +118,10 @@ class ImmutableKdTree:
             raise ValueError("items and points differ in length")
         L = C.lib()
         h = ctypes.c_void_p()
-        C.check(L.kgpu_layout_build(C.F32 if pts.dtype == np.float32 else C.F64, k, _vp(pts),
-                                    _vp(items), n, threads, ctypes.byref(h)))
+        C.check(L.kgpu_layout_build_stems(C.F32 if pts.dtype == np.float32 else C.F64, k,
+                                          _vp(pts), _vp(items), n,
+                                          C.STEM_DONNELLY if block_height else C.STEM_EYTZINGER,
+                                          int(block_height), threads, ctypes.byref(h)))
         holder = _LayoutHandle(h)
         desc = C.TreeDesc()
         C.check(L.kgpu_layout_describe(h, ctypes.byref(desc)))
@@ -121,8 +129,9 @@ class ImmutableKdTree:
 
     @classmethod
     def from_layout(cls, dtype, dims, stems, leaf_bytes, extents, max_stem_level, size,
-                    max_leaf_len) -> "ImmutableKdTree":
-        """Wrap the reference's own layout arrays (KdTreeAccessor, traits/kd_tree.rs:15-46)."""
+                    max_leaf_len, block_height: int = 0) -> "ImmutableKdTree":
+        """Wrap the reference's own layout arrays (KdTreeAccessor, traits/kd_tree.rs:15-46);
+        block_height > 0 for Donnelly<block_height> stems."""
         dt = np.dtype(dtype)
         stems = np.ascontiguousarray(stems, dtype=dt)
         lb = np.ascontiguousarray(leaf_bytes, dtype=np.uint8)
@@ -133,7 +142,8 @@ class ImmutableKdTree:
         d.dims = dims
         d.item_size = 4
         d.bucket_size = 32
-        d.stem_strategy = C.STEM_EYTZINGER
+        d.stem_strategy = C.STEM_DONNELLY if block_height else C.STEM_EYTZINGER
+        d.block_height = int(block_height)
         d.resolution = C.RES_ARITHMETIC
         d.stems = stems.ctypes.data if stems.size else None
         d.stem_count = stems.size
@@ -158,6 +168,10 @@ class ImmutableKdTree:
 
     def max_leaf_len(self) -> int:
         return int(self._desc.max_leaf_len)
+
+    def block_height(self) -> int:
+        """0 for Eytzinger stems, else the Donnelly block height."""
+        return int(self._desc.block_height)
 
     def stems(self) -> np.ndarray:
         n = int(self._desc.stem_count)

@@ -26,6 +26,8 @@ CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kgpu_forest.cu"
               "kgpu_chamfer.cu",
               "kernels_f32_warp.cu",
               "kernels_f32_thread.cu",
+              "kernels_f32_donnelly.cu",
+              "kernels_f64_donnelly.cu",
               "kernels_f32_radius.cu",
               "kernels_f64_warp.cu",
               "kernels_f64_thread.cu",

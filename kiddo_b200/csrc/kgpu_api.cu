@@ -117,11 +117,25 @@ uint64_t kgpu_launch_count(void) { return g_launches.load(); }
 // ---- host construction ----------------------------------------------------
 int32_t kgpu_layout_build(int32_t dtype, uint32_t dims, const void* points, const uint32_t* items,
                           uint64_t n, int32_t nthreads, kgpu_layout** out) {
+  return kgpu_layout_build_stems(dtype, dims, points, items, n, KGPU_STEM_EYTZINGER, 0, nthreads,
+                                 out);
+}
+
+int32_t kgpu_layout_build_stems(int32_t dtype, uint32_t dims, const void* points,
+                                const uint32_t* items, uint64_t n, int32_t stem_strategy,
+                                uint32_t block_height, int32_t nthreads, kgpu_layout** out) {
   if (!out) return set_error(KGPU_EINVAL, "out is NULL");
   *out = nullptr;
+  if (stem_strategy == KGPU_STEM_EYTZINGER) {
+    block_height = 0;
+  } else if (stem_strategy != KGPU_STEM_DONNELLY) {
+    return set_error(KGPU_EINVAL, "unknown stem strategy");
+  } else if (block_height != 3 && block_height != 4) {
+    return set_error(KGPU_EUNSUPPORTED, "Donnelly block height must be 3 or 4");
+  }
   auto* lay = new (std::nothrow) kgpu_layout();
   if (!lay) return set_error(KGPU_ENOMEM, "host allocation failed");
-  int st = build_layout_any(lay->L, dtype, int(dims), points, items, n, nthreads);
+  int st = build_layout_any(lay->L, dtype, int(dims), points, items, n, nthreads, block_height);
   if (st != KGPU_OK) {
     delete lay;
     return st;
@@ -139,8 +153,8 @@ int32_t kgpu_layout_describe(const kgpu_layout* lay, kgpu_tree_desc* d) {
   d->dims = uint32_t(L.dims);
   d->item_size = 4;
   d->bucket_size = 32;
-  d->stem_strategy = KGPU_STEM_EYTZINGER;
-  d->block_height = 0;
+  d->stem_strategy = L.block_height ? KGPU_STEM_DONNELLY : KGPU_STEM_EYTZINGER;
+  d->block_height = L.block_height;
   d->resolution = KGPU_RES_ARITHMETIC;
   const size_t sa = L.dtype == KGPU_F64 ? 8 : 4;
   d->stems = L.stems_bytes.empty() ? nullptr : L.stems_bytes.data();
@@ -171,8 +185,11 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
     return set_error(KGPU_EUNSUPPORTED, "dims must be 1..4");
   if (d->item_size != 4) return set_error(KGPU_EUNSUPPORTED, "only u32 items (ImmutableKdTree)");
   if (d->bucket_size != 32) return set_error(KGPU_EUNSUPPORTED, "only bucket size 32");
-  if (d->stem_strategy != KGPU_STEM_EYTZINGER)
-    return set_error(KGPU_EUNSUPPORTED, "only the Eytzinger stem strategy is accepted");
+  const bool donnelly = d->stem_strategy == KGPU_STEM_DONNELLY;
+  if (d->stem_strategy != KGPU_STEM_EYTZINGER && !donnelly)
+    return set_error(KGPU_EINVAL, "unknown stem strategy");
+  if (donnelly && d->block_height != 3 && d->block_height != 4)
+    return set_error(KGPU_EUNSUPPORTED, "Donnelly block height must be 3 or 4");
   if (d->resolution != KGPU_RES_ARITHMETIC)
     return set_error(KGPU_EUNSUPPORTED,
                      "only arithmetic stem/leaf resolution (soft immutable trees) is accepted");
@@ -180,12 +197,49 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
     return set_error(KGPU_EUNSUPPORTED, "max_stem_level must be -1..30");
   const size_t sa = d->dtype == KGPU_F64 ? 8 : 4;
   const int K = int(d->dims);
-  const uint64_t expect_leaves =
-      d->max_stem_level >= 0 ? (uint64_t(1) << (d->max_stem_level + 1)) : (d->size ? 1 : 0);
-  if (d->leaf_count != expect_leaves)
-    return set_error(KGPU_EINVAL, "leaf_count does not match max_stem_level (arithmetic layout)");
-  if (d->max_stem_level >= 0 && d->stem_count < (uint64_t(1) << (d->max_stem_level + 1)))
-    return set_error(KGPU_EINVAL, "stem array shorter than 2^(max_stem_level+1)");
+  if (!donnelly) {
+    const uint64_t expect_leaves =
+        d->max_stem_level >= 0 ? (uint64_t(1) << (d->max_stem_level + 1)) : (d->size ? 1 : 0);
+    if (d->leaf_count != expect_leaves)
+      return set_error(KGPU_EINVAL,
+                       "leaf_count does not match max_stem_level (arithmetic layout)");
+    if (d->max_stem_level >= 0 && d->stem_count < (uint64_t(1) << (d->max_stem_level + 1)))
+      return set_error(KGPU_EINVAL, "stem array shorter than 2^(max_stem_level+1)");
+  } else if (d->max_stem_level >= 0) {
+    // Donnelly: stems_depth = max_stem_level + 1 is a multiple of bh, the
+    // first (padding) levels carry no split, and the 2^o leaves hang below
+    // the o levels that do (construction.rs:431-446); stem loads are
+    // bounds-checked against stem_count on the device.
+    const uint32_t depth = uint32_t(d->max_stem_level + 1);
+    if (depth % d->block_height)
+      return set_error(KGPU_EINVAL, "Donnelly stem depth is not a multiple of the block height");
+    uint32_t o = 0;
+    while (o < 63 && (uint64_t(1) << o) < d->leaf_count) ++o;
+    if (d->leaf_count == 0 || (uint64_t(1) << o) != d->leaf_count || o > depth ||
+        depth - o >= d->block_height)
+      return set_error(KGPU_EINVAL, "leaf_count does not match a Donnelly arithmetic layout");
+    if (d->stem_count > 0xFFFFFFFFull)
+      return set_error(KGPU_EOVERFLOW, "Donnelly stem indices beyond 32 bits");
+    // The padding levels (the first depth - o, walked to the left) must carry
+    // no split, so that the path bits of every leaf stay below leaf_count.
+    const uint32_t bh = d->block_height;
+    uint32_t stem = 0, minor = 0;
+    for (uint32_t lvl = 0; lvl < depth - o; ++lvl) {
+      if (stem < d->stem_count) {
+        double v;
+        if (d->dtype == KGPU_F64) v = static_cast<const double*>(d->stems)[stem];
+        else v = double(static_cast<const float*>(d->stems)[stem]);
+        if (v < __builtin_inf())
+          return set_error(KGPU_EINVAL, "a Donnelly padding level holds a split");
+      }
+      const uint32_t mask = (1u << bh) - 1u, min_idx = stem & mask, base = (stem & ~mask) + 1u;
+      stem = minor + 1u == bh ? (base + ((min_idx - minor - 1u) << 1)) << bh
+                              : base + (min_idx << 1);
+      minor = minor + 1u == bh ? 0u : minor + 1u;
+    }
+  } else if (d->leaf_count != (d->size ? 1u : 0u)) {
+    return set_error(KGPU_EINVAL, "leaf_count does not match a tree without stems");
+  }
   if (d->leaf_count && (!d->leaf_extents || !d->leaf_bytes))
     return set_error(KGPU_EINVAL, "leaf arrays are NULL");
   if (d->max_stem_level >= 0 && !d->stems) return set_error(KGPU_EINVAL, "stems is NULL");
@@ -223,6 +277,7 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
   dt.stem_count = d->stem_count;
   dt.leaf_bytes_len = d->leaf_bytes_len;
   dt.max_leaf_len = d->max_leaf_len;
+  dt.bh = donnelly ? d->block_height : 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t stem_bytes = std::max<size_t>(16, d->stem_count * sa);
   const size_t arena_bytes = std::max<size_t>(16, d->leaf_bytes_len + 16);
@@ -299,6 +354,16 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
         return set_error(KGPU_EUNSUPPORTED, "max_qty above 32 is not supported");
     }
   }
+  if (t->dt.bh) {
+    // Donnelly stems run on the thread engine (2-D and 3-D trees), Cartesian
+    // families only.
+    if (t->dt.dims != 2 && t->dt.dims != 3)
+      return set_error(KGPU_EUNSUPPORTED, "Donnelly trees are served for 2-D and 3-D points");
+    if (d->flags & KGPU_FLAG_ENGINE_WARP)
+      return set_error(KGPU_EUNSUPPORTED, "Donnelly trees run on the thread engine");
+    if (d->periodic_box)
+      return set_error(KGPU_EUNSUPPORTED, "periodic queries need an Eytzinger tree");
+  }
   if (d->periodic_box) {
     // builder.rs: periodic queries support nearest_one, nearest_n(.within) and
     // within; best_n_within and approx are Cartesian-only.
@@ -334,7 +399,7 @@ template <typename A>
 cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   // thread engine for 2-D/3-D trees; periodic nearest_one stays on the warp
   // engine (home query plus images)
-  const bool thread = q.engine != 1 && (t.dims == 2 || t.dims == 3) &&
+  const bool thread = (t.bh || q.engine != 1) && (t.dims == 2 || t.dims == 3) &&
                       (!q.periodic || q.family != KGPU_NEAREST_ONE);
   return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);
 }

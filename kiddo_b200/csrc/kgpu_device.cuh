@@ -87,7 +87,26 @@ struct TreeView {
   uint32_t leaf_count;
   uint64_t size;
   uint64_t stem_count;
+  uint32_t bh;  // 0: Eytzinger stem order; 3 or 4: Donnelly<bh>
 };
+
+// Children of a Donnelly<bh> stem (stem_strategy/donnelly/core.rs:400-428):
+// inside a minor triangle of bh levels the children of heap slot m of the
+// line are slots 2m + 1 and 2m + 2; from the bottom row (minor == bh - 1) they
+// are the roots of lines (base + 1 + 2(m - minor - 1) + side) << bh.
+__device__ __forceinline__ void donnelly_children(uint32_t stem, uint32_t minor, uint32_t bh,
+                                                  uint32_t& left, uint32_t& right) {
+  const uint32_t mask = (1u << bh) - 1u;
+  const uint32_t min_idx = stem & mask;
+  const uint32_t base = (stem & ~mask) + 1u;
+  if (minor + 1u == bh) {
+    left = (base + ((min_idx - minor - 1u) << 1)) << bh;
+    right = left + (1u << bh);
+  } else {
+    left = base + (min_idx << 1);
+    right = left + 1u;
+  }
+}
 
 // Byte offset inside the leaf, tile width and index in tile of point p of a
 // leaf of `len` points laid out as tiles of 32, then 8, then 4, 2, 1.
@@ -286,6 +305,23 @@ __device__ __forceinline__ void warp_arith_query(const TreeView<A>& tv, const A 
 // Straight descent for approx (traits/stem_strategy.rs:182-200).
 template <typename A, int K>
 __device__ __forceinline__ uint32_t straight_leaf(const TreeView<A>& tv, const A (&q)[K]) {
+  if (tv.bh) {
+    // StemStrategy::get_leaf_idx over Donnelly stems (traits/stem_strategy.rs:
+    // 182-200): the leaf index accumulates the path bits.
+    uint32_t stem = 0, minor = 0, leaf = 0;
+    int dim = 0;
+    for (int level = 0; level <= tv.max_stem_level; ++level) {
+      const A pivot = stem < tv.stem_count ? __ldg(tv.stems + stem) : inf_of<A>();
+      const bool r = sel(q, dim) >= pivot;
+      uint32_t l, rr;
+      donnelly_children(stem, minor, tv.bh, l, rr);
+      stem = r ? rr : l;
+      minor = minor + 1u == tv.bh ? 0u : minor + 1u;
+      leaf = (leaf << 1) | (r ? 1u : 0u);
+      dim = dim + 1 == K ? 0 : dim + 1;
+    }
+    return leaf;
+  }
   uint32_t stem_idx = 1;
   int level = 0, dim = 0;
   while (level <= tv.max_stem_level) {

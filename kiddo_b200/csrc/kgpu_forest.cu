@@ -59,6 +59,7 @@ void fill_views(const std::vector<kgpu_tree*>& trees, std::vector<uint8_t>& out)
     v.leaf_count = t.leaf_count;
     v.size = t.size;
     v.stem_count = t.stem_count;
+    v.bh = 0;
     std::memcpy(out.data() + i * sizeof(TreeView<A>), &v, sizeof(v));
   }
 }
@@ -134,6 +135,8 @@ int32_t kgpu_forest_create(kgpu_tree* const* trees, uint32_t n_trees, void* stre
     if (!t) return set_error(KGPU_EINVAL, "NULL tree in the forest");
     if (t->dt.dtype != ts[0]->dt.dtype || t->dt.dims != ts[0]->dt.dims)
       return set_error(KGPU_EINVAL, "forest trees must share dtype and dims");
+    if (t->dt.bh)
+      return set_error(KGPU_EUNSUPPORTED, "forests hold Eytzinger trees (ImmutableKdTree)");
     if (t->dt.device != cur) return set_error(KGPU_EINVAL, "forest trees must be on the current device");
   }
   auto* f = new (std::nothrow) kgpu_forest();

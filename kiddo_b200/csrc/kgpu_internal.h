@@ -20,6 +20,7 @@ struct Layout {
   uint64_t size = 0;
   int32_t max_stem_level = -1;
   uint64_t max_leaf_len = 0;
+  uint32_t block_height = 0;         // 0: Eytzinger stems; 3 or 4: Donnelly<block_height>
   std::vector<uint8_t> stems_bytes;  // stem_count * sizeof(A)
   std::vector<uint8_t> leaf_bytes;
   std::vector<uint64_t> extents;     // (offset, len) pairs
@@ -29,7 +30,7 @@ struct Layout {
 int set_error(int status, const std::string& msg);
 
 int build_layout_any(Layout& L, int dtype, int K, const void* pts, const uint32_t* items,
-                     uint64_t n, int nthreads);
+                     uint64_t n, int nthreads, uint32_t block_height = 0);
 
 }  // namespace kgpu
 

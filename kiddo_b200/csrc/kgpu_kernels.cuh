@@ -284,12 +284,12 @@ __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, 
 //   whether the query needs a walk at all; finish(o, qi) runs on the whole
 //   warp for lane o's finished query.
 // ---------------------------------------------------------------------------
-template <typename A, int K, typename M, typename Pol, typename Start, typename Finish>
-__device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Pol& pol,
-                                           A* __restrict__ slot, int stride, TravStats& st,
-                                           Start&& start, Finish&& finish) {
+template <typename A, int K, typename M, typename Walk, typename Pol, typename Start,
+          typename Finish>
+__device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Walk& wk,
+                                           Pol& pol, A* __restrict__ slot, int stride,
+                                           TravStats& st, Start&& start, Finish&& finish) {
   const int lane = threadIdx.x & 31;
-  ThreadWalk<A, K, M> wk;
   LaneFeeder fd;
   fd.start();
   TreeView<A> tv = tv0;
@@ -347,11 +347,10 @@ __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A
 // The per-thread driver: lane-refilled walks, each thread scanning its own
 // leaves (the list families keep their lists in shared-memory columns).
 //   finish(qi) writes a finished query's results from its own lane.
-template <typename A, int K, typename M, typename Pol, typename Finish>
+template <typename A, int K, typename M, typename Walk, typename Pol, typename Finish>
 __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch<A>& b, A radius0,
-                                             Pol& pol, A* __restrict__ slot, int stride,
+                                             Walk& wk, Pol& pol, A* __restrict__ slot, int stride,
                                              TravStats& st, Finish&& finish) {
-  ThreadWalk<A, K, M> wk;
   LaneFeeder fd;
   fd.start();
   TreeView<A> tv = tv0;
@@ -386,6 +385,32 @@ __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch
   }
 }
 
+// The per-thread walk of a stem order: Eytzinger arithmetic DFS (STEMS == 0)
+// or Donnelly scalar backtracking (STEMS == 1).  Shared memory begins with the
+// walk's per-level columns: rd slots for both, then for Donnelly the off
+// values and the far stem indices.
+template <typename A, int K, typename M, int STEMS>
+struct WalkOf {
+  using type = ThreadWalk<A, K, M>;
+  __device__ static type make(unsigned char*, int, int) { return type(); }
+  __host__ __device__ static size_t bytes(int levels, int stride) {
+    return size_t(levels) * stride * sizeof(A);
+  }
+};
+template <typename A, int K, typename M>
+struct WalkOf<A, K, M, 1> {
+  using type = DonnellyWalk<A, K, M>;
+  __device__ static type make(unsigned char* smem, int levels, int stride) {
+    A* offs = reinterpret_cast<A*>(smem) + size_t(levels) * stride + threadIdx.x;
+    uint32_t* stems = reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(smem) +
+                                                  2 * size_t(levels) * stride) + threadIdx.x;
+    return type(offs, stems);
+  }
+  __host__ __device__ static size_t bytes(int levels, int stride) {
+    return size_t(levels) * stride * (2 * sizeof(A) + sizeof(uint32_t));
+  }
+};
+
 #ifndef KGPU_BESTN_COOP
 #define KGPU_BESTN_COOP 1
 #endif
@@ -402,7 +427,7 @@ __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch
 #ifndef KGPU_TFIXED_MIN_BLOCKS
 #define KGPU_TFIXED_MIN_BLOCKS 4
 #endif
-template <typename A, int K, typename M, int FAM, bool EXCL>
+template <typename A, int K, typename M, int FAM, bool EXCL, int STEMS = 0>
 __global__ void __launch_bounds__(256, FAM == KF_BEST_N ? 3 : KGPU_TFIXED_MIN_BLOCKS)
     k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k, A radius0, int arrival_order,
              A* __restrict__ out_d, uint32_t* __restrict__ out_i, uint32_t* __restrict__ out_c,
@@ -410,6 +435,10 @@ __global__ void __launch_bounds__(256, FAM == KF_BEST_N ? 3 : KGPU_TFIXED_MIN_BL
   extern __shared__ __align__(16) unsigned char tsmem[];
   const int stride = blockDim.x;
   A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  using W = WalkOf<A, K, M, STEMS>;
+  auto wk = W::make(tsmem, levels, stride);
+  // the list families' shared memory follows the walk's columns
+  unsigned char* lists = tsmem + W::bytes(levels, stride);
   TravStats st;
   if constexpr (FAM == KF_APPROX) {
     for_each_query_thread(b, [&](uint64_t qi) {
@@ -428,35 +457,36 @@ __global__ void __launch_bounds__(256, FAM == KF_BEST_N ? 3 : KGPU_TFIXED_MIN_BL
     });
   } else if constexpr (FAM == KF_NEAREST_ONE) {
     TNearestOne<A, K, M> pol;
-    thread_drive<A, K, M>(tv0, b, radius0, pol, slot, stride, st, [&](uint64_t qi) {
+    thread_drive<A, K, M>(tv0, b, radius0, wk, pol, slot, stride, st, [&](uint64_t qi) {
       out_d[qi] = pol.best;
       out_i[qi] = pol.item;
       if (out_c) out_c[qi] = 1;
     });
   } else if constexpr (FAM == KF_NEAREST_N || !KGPU_BESTN_COOP) {
     // lists in shared-memory columns: entry j of thread t at j * blockDim + t
-    A* list_d = reinterpret_cast<A*>(tsmem) + size_t(levels) * stride + threadIdx.x;
-    uint32_t* list_i = reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(tsmem) +
-                                                   size_t(levels + k) * stride) + threadIdx.x;
+    A* list_d = reinterpret_cast<A*>(lists) + threadIdx.x;
+    uint32_t* list_i =
+        reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(lists) + size_t(k) * stride) +
+        threadIdx.x;
     if constexpr (FAM == KF_NEAREST_N) {
       TNearestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius0);
-      thread_drive<A, K, M>(tv0, b, radius0, pol, slot, stride, st, [&](uint64_t qi) {
+      thread_drive<A, K, M>(tv0, b, radius0, wk, pol, slot, stride, st, [&](uint64_t qi) {
         pol.write(qi, out_d, out_i, out_c, arrival_order != 0);
       });
     } else {
       TBestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius0);
-      thread_drive<A, K, M>(tv0, b, radius0, pol, slot, stride, st,
+      thread_drive<A, K, M>(tv0, b, radius0, wk, pol, slot, stride, st,
                             [&](uint64_t qi) { pol.write(qi, out_d, out_i, out_c); });
     }
   } else {
     // best_n_within with warp-cooperative leaf scans: thread t's k entries
     // consecutive at t * k
     const size_t warp0 = threadIdx.x & ~31u;
-    A* lists_d = reinterpret_cast<A*>(tsmem) + size_t(levels) * stride;
+    A* lists_d = reinterpret_cast<A*>(lists);
     uint32_t* lists_i = reinterpret_cast<uint32_t*>(lists_d + size_t(k) * stride);
     CBestN<A, K, M, EXCL> pol(lists_d + warp0 * k, lists_i + warp0 * k, nullptr, k, radius0);
     coop_drive<A, K, M>(
-        tv0, b, pol, slot, stride, st,
+        tv0, b, wk, pol, slot, stride, st,
         [&](uint64_t qi, const TreeView<A>&) {
           pol.reset(b.radius(radius0, qi));
           return true;
@@ -467,7 +497,7 @@ __global__ void __launch_bounds__(256, FAM == KF_BEST_N ? 3 : KGPU_TFIXED_MIN_BL
 }
 
 // Counting pass (offsets == nullptr) or filling pass of the radius families.
-template <typename A, int K, typename M, bool EXCL>
+template <typename A, int K, typename M, bool EXCL, int STEMS = 0>
 __global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv0, Batch<A> b, A radius0,
                                                  uint64_t* __restrict__ counts,
                                                  const uint64_t* __restrict__ offsets,
@@ -481,9 +511,11 @@ __global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv0, Batch<A> b, A 
   const int lane = threadIdx.x & 31;
   TravStats st;
   CWithin<A, K, M, EXCL> pol;
+  // the launch sizes shared memory for max_stem_level + 2 levels
+  auto wk = WalkOf<A, K, M, STEMS>::make(tsmem, tv0.max_stem_level + 2, stride);
   uint64_t o = 0;  // this lane's segment start (filling pass)
   coop_drive<A, K, M>(
-      tv0, b, pol, slot, stride, st,
+      tv0, b, wk, pol, slot, stride, st,
       [&](uint64_t qi, const TreeView<A>&) {
         pol.radius = b.radius(radius0, qi);
         pol.count = 0;

@@ -21,6 +21,7 @@ struct DeviceTree {
   uint64_t leaf_bytes_len = 0;
   uint64_t max_leaf_len = 0;
   size_t device_bytes = 0;
+  uint32_t bh = 0;             // 0: Eytzinger stems; 3 or 4: Donnelly<bh>
 };
 
 struct QueryLaunch {
@@ -61,6 +62,15 @@ extern std::atomic<uint64_t> g_launches;
 template <typename A> cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q);
+// Donnelly-stem kernels, defined in their own translation units
+// (kernels_f32_donnelly.cu, kernels_f64_donnelly.cu); the last argument only
+// selects the coordinate type.
+cudaError_t launch_tfixed_donnelly(const DeviceTree& t, const QueryLaunch& q, float);
+cudaError_t launch_tfixed_donnelly(const DeviceTree& t, const QueryLaunch& q, double);
+cudaError_t launch_within_donnelly(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts,
+                                   const uint64_t* offsets, float);
+cudaError_t launch_within_donnelly(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts,
+                                   const uint64_t* offsets, double);
 template <typename A> cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q,
                                                        uint64_t* counts);
 template <typename A> cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,

@@ -19,6 +19,7 @@ inline TreeView<A> make_view(const DeviceTree& t) {
   v.leaf_count = t.leaf_count;
   v.size = t.size;
   v.stem_count = t.stem_count;
+  v.bh = t.bh;
   return v;
 }
 
@@ -141,16 +142,19 @@ cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
 // Thread-per-query fixed-size families.  Only 2-D and 3-D trees; the caller
 // checks.  Shared memory per block: continuation slots plus, for the list
 // families, k (distance, item) pairs per thread.
-template <typename A>
-cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
+// STEMS: 0 for Eytzinger stems (arithmetic DFS), 1 for Donnelly stems
+// (scalar backtracking); the Donnelly instantiation lives in its own
+// translation units (kernels_*_donnelly.cu).
+template <typename A, int STEMS>
+cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
   const TreeView<A> tv = make_view<A>(t);
   const Batch<A> b = make_batch<A>(q);
   const A radius = A(q.radius);
   const int levels = t.max_stem_level + 2;
   const bool list = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
                     q.family == KGPU_BEST_N_WITHIN;
-  const size_t smem = size_t(levels) * 256 * sizeof(A) +
-                      (list ? size_t(q.k) * 256 * (sizeof(A) + sizeof(uint32_t)) : 0);
+  const size_t walk = size_t(levels) * 256 * (STEMS ? 2 * sizeof(A) + 4 : sizeof(A));
+  const size_t smem = walk + (list ? size_t(q.k) * 256 * (sizeof(A) + sizeof(uint32_t)) : 0);
   return with_dims(t.dims, [&](auto kk) -> cudaError_t {
     constexpr int K = decltype(kk)::value;
     if constexpr (!thread_engine_dims(K)) {
@@ -160,7 +164,7 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
         using M = decltype(m);
         return with_excl(q.exclusive, [&](auto ex) {
           constexpr bool EX = decltype(ex)::value;
-          if (q.periodic) {
+          if (STEMS == 0 && q.periodic) {
             // periodic nearest_n: per-thread walk, cooperative leaf scans,
             // lists in the output rows
             const auto box = make_box<A, K>(q);
@@ -185,14 +189,14 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
           };
           switch (q.family) {
             case KGPU_NEAREST_ONE:
-              return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false>);
-            case KGPU_APPROX_NEAREST_ONE:
-              return runt(k_tfixed<A, K, M, KF_APPROX, false>);
+              return runt(k_tfixed<A, K, M, KF_NEAREST_ONE, false, STEMS>);
+            case KGPU_APPROX_NEAREST_ONE:  // one straight descent, either stem order
+              return runt(k_tfixed<A, K, M, KF_APPROX, false, 0>);
             case KGPU_NEAREST_N:
             case KGPU_NEAREST_N_WITHIN:
-              return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX>);
+              return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX, STEMS>);
             case KGPU_BEST_N_WITHIN:
-              return runt(k_tfixed<A, K, M, KF_BEST_N, EX>);
+              return runt(k_tfixed<A, K, M, KF_BEST_N, EX, STEMS>);
           }
           return cudaErrorInvalidValue;
         });
@@ -201,11 +205,17 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
   });
 }
 
+template <typename A>
+cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
+  if (t.bh) return launch_tfixed_donnelly(t, q, A());
+  return launch_tfixed_stems<A, 0>(t, q);
+}
+
 // Counting (offsets == nullptr, counts set) or filling pass of the radius
 // families.
-template <typename A>
-cudaError_t launch_within_pass(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts,
-                               const uint64_t* offsets) {
+template <typename A, int STEMS>
+cudaError_t launch_within_pass_stems(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts,
+                                     const uint64_t* offsets) {
   const TreeView<A> tv = make_view<A>(t);
   const Batch<A> b = make_batch<A>(q);
   const A radius = A(q.radius);
@@ -245,9 +255,10 @@ cudaError_t launch_within_pass(const DeviceTree& t, const QueryLaunch& q, uint64
           return cudaGetLastError();
         }
         if constexpr (thread_engine_dims(K)) {
-          if (q.engine != 1) {
-            const size_t smem = thread_smem<A>(t);
-            auto kern = k_twithin<A, K, M, EX>;
+          if (q.engine != 1 || STEMS) {
+            const size_t smem = size_t(t.max_stem_level + 2) * 256 *
+                                (STEMS ? 2 * sizeof(A) + 4 : sizeof(A));
+            auto kern = k_twithin<A, K, M, EX, STEMS>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
             kern<<<grid, 256, smem, q.stream>>>(tv, b, radius, counts, offsets, q.capacity,
@@ -274,13 +285,15 @@ cudaError_t launch_within_pass(const DeviceTree& t, const QueryLaunch& q, uint64
 
 template <typename A>
 cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts) {
-  return launch_within_pass<A>(t, q, counts, nullptr);
+  if (t.bh) return launch_within_donnelly(t, q, counts, nullptr, A());
+  return launch_within_pass_stems<A, 0>(t, q, counts, nullptr);
 }
 
 template <typename A>
 cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
                                const uint64_t* offsets) {
-  return launch_within_pass<A>(t, q, nullptr, offsets);
+  if (t.bh) return launch_within_donnelly(t, q, nullptr, offsets, A());
+  return launch_within_pass_stems<A, 0>(t, q, nullptr, offsets);
 }
 
 template <typename A>
@@ -354,6 +367,17 @@ cudaError_t launch_spatial_order(const DeviceTree& t, const QueryLaunch& q, uint
 #define KGPU_INSTANTIATE_THREAD(A)                                                               \
   namespace kgpu {                                                                               \
   template cudaError_t launch_tfixed<A>(const DeviceTree&, const QueryLaunch&);                  \
+  }
+
+#define KGPU_INSTANTIATE_DONNELLY(A)                                                             \
+  namespace kgpu {                                                                               \
+  cudaError_t launch_tfixed_donnelly(const DeviceTree& t, const QueryLaunch& q, A) {             \
+    return launch_tfixed_stems<A, 1>(t, q);                                                      \
+  }                                                                                              \
+  cudaError_t launch_within_donnelly(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts, \
+                                     const uint64_t* offsets, A) {                               \
+    return launch_within_pass_stems<A, 1>(t, q, counts, offsets);                                \
+  }                                                                                              \
   }
 
 #define KGPU_INSTANTIATE_RADIUS(A)                                                               \

@@ -234,6 +234,96 @@ struct ThreadWalk {
   }
 };
 
+// Per-thread scalar backtracking over Donnelly<bh> stems, the reference's
+// path for strategies with BLOCK_SIZE != 1 (kd_tree/orchestrator/mod.rs:
+// 265-345, 607-669; traits/stem_strategy.rs:209-325).  The reference's stack
+// holds frames at strictly increasing levels, so the frame of the far child at
+// level FL lives in slot FL of three shared-memory columns (its rd, the off
+// value to put on its parent's axis, its stem index) with a bit in `pending`;
+// its dimension is (FL - 1) % K, its minor level FL % bh and its leaf-index
+// prefix the current path's at FL with the last bit flipped.  As in the
+// reference, a descent keeps the popped frame's rd, pushes a far child when
+// rd_far is not greater than max_dist() read when the descent began, and a pop
+// resets only its own axis of `off`.
+template <typename A, int K, typename M>
+struct DonnellyWalk {
+  A off[K];
+  A rd;
+  uint32_t stem, leaf, pending;
+  int level;
+  A* __restrict__ off_slot;         // column base: slot L at L * stride
+  uint32_t* __restrict__ stem_slot;
+
+  __device__ DonnellyWalk(A* offs, uint32_t* stems) : off_slot(offs), stem_slot(stems) {}
+
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int d = 0; d < K; ++d) off[d] = A(0);
+    rd = A(0);
+    stem = leaf = pending = 0;
+    level = 0;
+  }
+
+  template <typename P>
+  __device__ __forceinline__ uint32_t descend(const TreeView<A>& tv, const A (&q)[K], const P& pol,
+                                              bool, A* __restrict__ slot, int stride,
+                                              TravStats& st) {
+    const A INF = inf_of<A>();
+    const A best = pol.max_dist();
+    const int msl = tv.max_stem_level;
+    const uint32_t bh = tv.bh;
+    int dim = level % K;
+    uint32_t minor = uint32_t(level) % bh;
+    while (level <= msl) {
+      ++st.stems;
+      const A pivot = stem < tv.stem_count ? __ldg(tv.stems + stem) : INF;
+      uint32_t l, r;
+      donnelly_children(stem, minor, bh, l, r);
+      if (pivot < INF) {
+        const A qd = sel(q, dim);
+        const bool is_right = qd >= pivot;
+        const A new_off = abs_val(sub_rn(qd, pivot));
+        const A rd_far = M::template rect<A>(rd, sel(off, dim), new_off);
+        if (!(rd_far > best)) {
+          const int fl = level + 1;
+          slot[fl * stride] = rd_far;
+          off_slot[fl * stride] = new_off;
+          stem_slot[fl * stride] = is_right ? l : r;
+          pending |= 1u << fl;
+        }
+        stem = is_right ? r : l;
+        leaf = (leaf << 1) | (is_right ? 1u : 0u);
+      } else {
+        stem = l;
+        leaf <<= 1;
+      }
+      ++level;
+      dim = dim + 1 == K ? 0 : dim + 1;
+      minor = minor + 1u == bh ? 0u : minor + 1u;
+    }
+    return leaf;
+  }
+
+  template <typename P>
+  __device__ __forceinline__ bool backtrack(const TreeView<A>&, const A (&)[K], const P& pol,
+                                            A* __restrict__ slot, int stride) {
+    while (pending) {
+      const int fl = 31 - __clz(pending);
+      pending &= ~(1u << fl);
+      const A frd = slot[fl * stride];
+      const A md = pol.max_dist();
+      if (frd > md || (P::kPruneOnEqual && frd == md)) continue;
+      put(off, (fl - 1) % K, off_slot[fl * stride]);
+      stem = stem_slot[fl * stride];
+      leaf = (leaf >> (level - fl)) ^ 1u;
+      level = fl;
+      rd = frd;
+      return true;
+    }
+    return false;
+  }
+};
+
 // Per-thread periodic_backtracking_query (periodic.rs:455-619).  The
 // reference's frames carry the far child's whole (lower, upper, off) state;
 // here a frame is only its rd (slot[FL * stride], FL = the far child's level)

@@ -54,9 +54,53 @@ size_t leaf_encoded_bytes(size_t len, int K) {
   return total;
 }
 
+// Position of a node in the stem tree: its stem index, level, split
+// dimension, arithmetic leaf prefix (the path bits), and for Donnelly stems its
+// level inside the current minor triangle.
+struct NodePos {
+  uint32_t stem = 1;
+  int level = 0;
+  uint32_t minor = 0;
+  uint64_t leaf = 0;
+  int dim = 0;
+};
+
+// Children of a node.  bh == 0: Eytzinger (children 2i and 2i + 1,
+// stem_strategy/eytzinger/mod.rs:131-168).  bh > 0: Donnelly<bh>
+// (stem_strategy/donnelly/core.rs:400-428): inside a minor triangle the
+// children are 2m + 1 and 2m + 2 of the line's heap; from the triangle's
+// bottom row they are the roots of lines (base + 1 + 2(m - minor - 1) + side)
+// << bh.  The dimension advances once per level in both.
+inline void node_children(const NodePos& n, int K, uint32_t bh, NodePos& l, NodePos& r) {
+  l = n;
+  l.level = n.level + 1;
+  l.leaf = n.leaf << 1;
+  l.dim = n.dim + 1 == K ? 0 : n.dim + 1;
+  r = l;
+  r.leaf = l.leaf | 1u;
+  if (!bh) {
+    l.stem = n.stem * 2u;
+    r.stem = l.stem + 1u;
+    return;
+  }
+  const uint32_t mask = (1u << bh) - 1u;
+  const uint32_t min_idx = n.stem & mask;
+  const uint32_t base = (n.stem & ~mask) + 1u;
+  if (n.minor + 1u == bh) {
+    l.stem = (base + ((min_idx - n.minor - 1u) << 1)) << bh;
+    r.stem = l.stem + (1u << bh);
+    l.minor = r.minor = 0;
+  } else {
+    l.stem = base + (min_idx << 1);
+    r.stem = l.stem + 1u;
+    l.minor = r.minor = n.minor + 1u;
+  }
+}
+
 template <typename A>
 struct SoftBuilder {
   int K;
+  uint32_t bh = 0;  // 0: Eytzinger stems; 3 or 4: Donnelly<bh>
   std::vector<std::vector<A>> cols;   // cols[d][i]
   uint32_t* idx;
   A* stems;
@@ -65,6 +109,7 @@ struct SoftBuilder {
   std::vector<uint64_t>* leaf_begin;  // per leaf: begin offset into idx
   std::vector<uint32_t>* leaf_len;
   int spawn_levels;
+  int root_level = 0;
 
   // Reference pivot rule (update_pivot) for chunk idx[b, e) on `dim`.
   // Returns the pivot and the split value t (left = x < t) and the stem value.
@@ -89,23 +134,24 @@ struct SoftBuilder {
     return le;
   }
 
-  void build(uint32_t* b, size_t len, uint32_t stem_idx, int level, uint64_t budget,
-             uint64_t base) {
+  void build(uint32_t* b, size_t len, NodePos root, uint64_t budget, uint64_t base) {
     std::vector<A> buf;
-    build_rec(b, len, stem_idx, level, budget, base, buf);
+    build_rec(b, len, root, budget, base, buf);
   }
 
-  void build_rec(uint32_t* b, size_t len, uint32_t stem_idx, int level, uint64_t budget,
-                 uint64_t base, std::vector<A>& buf) {
+  void build_rec(uint32_t* b, size_t len, NodePos node, uint64_t budget, uint64_t base,
+                 std::vector<A>& buf) {
     if (budget == 0) return;
+    const int level = node.level;
+    const uint32_t stem_idx = node.stem;
     if (level > max_stem_level) {
-      const uint32_t leaf = stem_idx - (uint32_t(1) << level);
+      const uint64_t leaf = node.leaf;
       (*leaf_begin)[leaf] = base;
       (*leaf_len)[leaf] = uint32_t(len);
       std::sort(b, b + len);
       return;
     }
-    const int dim = level % K;
+    const int dim = node.dim;
     uint64_t left_budget, right_budget;
     size_t pivot;
     A split = A(0);
@@ -131,16 +177,18 @@ struct SoftBuilder {
       stems[stem_idx] = split;  // smallest coordinate of the right part
     }
     const size_t cut = std::min(pivot, len);
-    if (level < spawn_levels && len > 65536) {
-      std::thread th([&, b, cut, stem_idx, level, left_budget, base]() {
+    NodePos left, right;
+    node_children(node, K, bh, left, right);
+    if (level - root_level < spawn_levels && len > 65536) {
+      std::thread th([&, b, cut, left, left_budget, base]() {
         std::vector<A> buf2;
-        build_rec(b, cut, stem_idx * 2, level + 1, left_budget, base, buf2);
+        build_rec(b, cut, left, left_budget, base, buf2);
       });
-      build_rec(b + cut, len - cut, stem_idx * 2 + 1, level + 1, right_budget, base + cut, buf);
+      build_rec(b + cut, len - cut, right, right_budget, base + cut, buf);
       th.join();
     } else {
-      build_rec(b, cut, stem_idx * 2, level + 1, left_budget, base, buf);
-      build_rec(b + cut, len - cut, stem_idx * 2 + 1, level + 1, right_budget, base + cut, buf);
+      build_rec(b, cut, left, left_budget, base, buf);
+      build_rec(b + cut, len - cut, right, right_budget, base + cut, buf);
     }
   }
 };
@@ -181,7 +229,8 @@ void write_leaf(uint8_t* dst, const A* pts, const uint32_t* items, const uint32_
 
 template <typename A>
 void build_layout(Layout& L, const A* pts, const uint32_t* items, uint64_t n, int K,
-                  int nthreads) {
+                  uint32_t bh, int nthreads) {
+  L.block_height = bh;
   L.dtype = sizeof(A) == 8 ? 1 : 0;
   L.dims = K;
   L.size = n;
@@ -203,14 +252,35 @@ void build_layout(Layout& L, const A* pts, const uint32_t* items, uint64_t n, in
   } else {
     uint32_t depth = 0;
     while ((uint64_t(1) << depth) < leaf_node_count) ++depth;
+    const uint32_t leaf_bits = depth;
+    // Block strategies pad the stem tree at the root to a multiple of bh
+    // levels; the padding levels are walked to the left (construction.rs:
+    // 431-446) and carry no stems.
+    const uint32_t pad = bh && depth % bh ? bh - depth % bh : 0;
+    depth += pad;
+    NodePos root;
+    root.stem = bh ? 0u : 1u;  // Eytzinger root 1, Donnelly root 0
+    for (uint32_t i = 0; i < pad; ++i) {
+      NodePos l, r;
+      node_children(root, K, bh, l, r);
+      root = l;
+    }
     const uint64_t budget = uint64_t(1) << depth;
-    const size_t stem_count = (size_t(1) << (depth + 1));
+    // stem count: the index of the node reached by walking `depth` levels to
+    // the right from the root, plus one, padded to 8 (construction.rs:448-469)
+    NodePos far_right = root;
+    for (uint32_t i = 0; i < depth; ++i) {
+      NodePos l, r;
+      node_children(far_right, K, bh, l, r);
+      far_right = r;
+    }
+    const size_t stem_count = size_t(far_right.stem) + 1;
     const size_t padded = (stem_count + 7) / 8 * 8;
     L.stems_bytes.resize(padded * sizeof(A));
     A* stems = reinterpret_cast<A*>(L.stems_bytes.data());
     for (size_t i = 0; i < padded; ++i) stems[i] = std::numeric_limits<A>::infinity();
-    leaf_begin.assign(budget, 0);
-    leaf_len.assign(budget, 0);
+    leaf_begin.assign(uint64_t(1) << leaf_bits, 0);
+    leaf_len.assign(uint64_t(1) << leaf_bits, 0);
 
     SoftBuilder<A> sb;
     sb.K = K;
@@ -229,7 +299,9 @@ void build_layout(Layout& L, const A* pts, const uint32_t* items, uint64_t n, in
     int spawn = 0;
     while ((1 << spawn) < std::max(1, nthreads)) ++spawn;
     sb.spawn_levels = spawn + 1;
-    sb.build(idx.data(), n, 1, 0, budget, 0);
+    sb.bh = bh;
+    sb.root_level = root.level;
+    sb.build(idx.data(), n, root, budget, 0);
     L.max_stem_level = int(depth) - 1;
   }
   if (leaf_node_count < 2) std::sort(idx.begin(), idx.end());
@@ -256,16 +328,19 @@ void build_layout(Layout& L, const A* pts, const uint32_t* items, uint64_t n, in
 }  // namespace
 
 int build_layout_any(Layout& L, int dtype, int K, const void* pts, const uint32_t* items,
-                     uint64_t n, int nthreads) {
+                     uint64_t n, int nthreads, uint32_t block_height) {
   if (K < 1 || K > kMaxDims) return set_error(KGPU_EUNSUPPORTED, "dims must be 1..4");
+  if (block_height != 0 && block_height != 3 && block_height != 4)
+    return set_error(KGPU_EUNSUPPORTED, "Donnelly block height must be 3 or 4");
   if (n > 0 && !pts) return set_error(KGPU_EINVAL, "points is NULL");
   if (n > 0xFFFFFFFFull) return set_error(KGPU_EOVERFLOW, "more than 2^32 points");
   if (nthreads <= 0) nthreads = int(std::max(1u, std::thread::hardware_concurrency()));
   try {
     if (dtype == KGPU_F32)
-      build_layout<float>(L, static_cast<const float*>(pts), items, n, K, nthreads);
+      build_layout<float>(L, static_cast<const float*>(pts), items, n, K, block_height, nthreads);
     else if (dtype == KGPU_F64)
-      build_layout<double>(L, static_cast<const double*>(pts), items, n, K, nthreads);
+      build_layout<double>(L, static_cast<const double*>(pts), items, n, K, block_height,
+                           nthreads);
     else
       return set_error(KGPU_EINVAL, "dtype must be KGPU_F32 or KGPU_F64");
   } catch (const std::bad_alloc&) {

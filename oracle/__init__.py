@@ -49,8 +49,13 @@ def lib():
         vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
         L.kor_build.restype = vp
         L.kor_build.argtypes = [i32, i32, vp, vp, u64]
+        L.kor_build_ex.restype = vp
+        L.kor_build_ex.argtypes = [i32, i32, vp, vp, u64, ctypes.c_uint32]
         L.kor_from_layout.restype = vp
         L.kor_from_layout.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64, u64]
+        L.kor_from_layout_ex.restype = vp
+        L.kor_from_layout_ex.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64,
+                                         u64, ctypes.c_uint32]
         L.kor_free.argtypes = [vp]
         L.kor_layout_info.argtypes = [vp, vp]
         L.kor_copy_layout.argtypes = [vp, vp, vp, vp]
@@ -59,6 +64,7 @@ def lib():
                                       i32, i32, vp, vp, vp, vp, i32, vp]
         L.kor_query_radius.restype = vp
         L.kor_query_radius.argtypes = [vp, i32, i32, vp, u64, ctypes.c_double, i32, i32, vp, i32, vp]
+        L.kor_donnelly_path.argtypes = [ctypes.c_uint32, vp, u64, vp]
         L.kor_radius_total.restype = u64
         L.kor_radius_total.argtypes = [vp]
         L.kor_radius_copy.argtypes = [vp, vp, vp, vp]
@@ -72,9 +78,13 @@ def _ptr(a):
 
 
 class Layout:
-    """The reference's own ImmutableKdTree layout (stems, arena bytes, extents)."""
+    """A tree layout as the reference stores it (stems, arena bytes, extents);
+    block_height 0 for the Eytzinger stem order (ImmutableKdTree), > 0 for
+    Donnelly<block_height>."""
 
-    def __init__(self, dtype, k, stems, leaf_bytes, extents, max_stem_level, size, max_leaf_len):
+    def __init__(self, dtype, k, stems, leaf_bytes, extents, max_stem_level, size, max_leaf_len,
+                 block_height=0):
+        self.block_height = int(block_height)
         self.dtype = np.dtype(dtype)
         self.k = k
         self.stems = stems
@@ -98,12 +108,14 @@ class OracleTree:
         self.k = k
 
     @classmethod
-    def build(cls, points, items=None):
+    def build(cls, points, items=None, block_height=0):
+        """Soft construction; block_height > 0 builds a Donnelly<block_height> tree."""
         points = np.ascontiguousarray(points)
         assert points.dtype in (np.float32, np.float64) and points.ndim == 2
         n, k = points.shape
         it = None if items is None else np.ascontiguousarray(items, dtype=np.uint32)
-        h = lib().kor_build(0 if points.dtype == np.float32 else 1, k, _ptr(points), _ptr(it), n)
+        h = lib().kor_build_ex(0 if points.dtype == np.float32 else 1, k, _ptr(points), _ptr(it), n,
+                               int(block_height))
         if not h:
             raise ValueError("unsupported dtype/dimension for the oracle")
         return cls(h, points.dtype, k)
@@ -114,8 +126,9 @@ class OracleTree:
         stems = np.ascontiguousarray(lay.stems, dtype=lay.dtype)
         lb = np.ascontiguousarray(lay.leaf_bytes, dtype=np.uint8)
         ex = np.ascontiguousarray(lay.extents, dtype=np.uint64)
-        h = lib().kor_from_layout(dt, lay.k, _ptr(stems), stems.size, _ptr(lb), lb.size, _ptr(ex),
-                                  ex.shape[0], lay.max_stem_level, lay.size, lay.max_leaf_len)
+        h = lib().kor_from_layout_ex(dt, lay.k, _ptr(stems), stems.size, _ptr(lb), lb.size,
+                                     _ptr(ex), ex.shape[0], lay.max_stem_level, lay.size,
+                                     lay.max_leaf_len, getattr(lay, "block_height", 0))
         return cls(h, lay.dtype, lay.k)
 
     def __del__(self):
@@ -124,13 +137,13 @@ class OracleTree:
             self._h = None
 
     def layout(self) -> Layout:
-        info = np.zeros(6, dtype=np.int64)
+        info = np.zeros(7, dtype=np.int64)
         lib().kor_layout_info(self._h, _ptr(info))
         stems = np.empty(int(info[0]), dtype=self.dtype)
         lb = np.empty(int(info[1]), dtype=np.uint8)
         ex = np.empty((int(info[2]), 2), dtype=np.uint64)
         lib().kor_copy_layout(self._h, _ptr(stems), _ptr(lb), _ptr(ex))
-        return Layout(self.dtype, self.k, stems, lb, ex, info[3], info[4], info[5])
+        return Layout(self.dtype, self.k, stems, lb, ex, info[3], info[4], info[5], info[6])
 
     def _q(self, queries):
         q = np.ascontiguousarray(queries, dtype=self.dtype)
@@ -153,9 +166,11 @@ class OracleTree:
         st = np.zeros(3, dtype=np.uint64) if stats else None
         nth = threads if threads > 0 else (os.cpu_count() or 1)
         bx = self._box(box)
-        lib().kor_query_fixed(self._h, family, METRICS[metric], _ptr(q), nq, kk, float(radius),
-                              int(exclusive), int(sorted), _ptr(bx), _ptr(d), _ptr(it), _ptr(c),
-                              nth, _ptr(st))
+        rc = lib().kor_query_fixed(self._h, family, METRICS[metric], _ptr(q), nq, kk,
+                                   float(radius), int(exclusive), int(sorted), _ptr(bx), _ptr(d),
+                                   _ptr(it), _ptr(c), nth, _ptr(st))
+        if rc != 0:
+            raise ValueError("query family not supported on this tree by the oracle")
         out = (d.reshape(nq, kk), it.reshape(nq, kk), c)
         return out + (st,) if stats else out
 
@@ -168,6 +183,8 @@ class OracleTree:
         bx = self._box(box)
         r = lib().kor_query_radius(self._h, family, METRICS[metric], _ptr(q), nq, float(radius),
                                    int(exclusive), int(sorted), _ptr(bx), nth, _ptr(st))
+        if not r:
+            raise ValueError("query family not supported on this tree by the oracle")
         total = lib().kor_radius_total(r)
         off = np.empty(nq + 1, dtype=np.uint64)
         d = np.empty(total, dtype=self.dtype)
@@ -213,3 +230,12 @@ class OracleTree:
                         sorted=True, **kw):
         return self.query_radius(FAM_PERIODIC_WITHIN, queries, radius, metric=metric,
                                  exclusive=exclusive, sorted=sorted, box=box, **kw)
+
+
+def donnelly_path(bh, bits):
+    """(stem index after traverse() along `bits`, (left, right) children of the
+    node branch_relative() reaches along `bits`) in a Donnelly<bh> stem tree."""
+    b = np.ascontiguousarray(np.asarray(bits, dtype=np.uint8))
+    out = np.zeros(3, dtype=np.uint32)
+    lib().kor_donnelly_path(int(bh), _ptr(b) if b.size else None, b.size, _ptr(out))
+    return int(out[0]), (int(out[1]), int(out[2]))

@@ -62,13 +62,15 @@ inline A inf_value() { return std::numeric_limits<A>::infinity(); }
 // ---------------------------------------------------------------------------
 template <typename A, int K>
 struct Tree {
-  std::vector<A> stems;              // Eytzinger order, index 0 unused, +inf = "no split"
+  std::vector<A> stems;              // stem order of the strategy, +inf = "no split"
   std::vector<uint8_t> leaf_bytes;   // VecOfArenas arena
   std::vector<uint64_t> extents;     // (byte offset, len) pairs per leaf
   int32_t max_stem_level = -1;
   uint64_t size = 0;
   uint64_t max_leaf_len = 0;
   uint32_t stems_depth = 0;
+  int stem_strategy = 0;  // 0 Eytzinger, 1 Donnelly<bh>
+  uint32_t bh = 0;        // Donnelly block height
 
   size_t leaf_count() const { return extents.size() / 2; }
   uint64_t leaf_offset(size_t l) const { return extents[2 * l]; }
@@ -128,6 +130,100 @@ void append_leaf(Tree<A, K>& t, const A* pts, const uint32_t* items, const size_
 }
 
 // ---------------------------------------------------------------------------
+// Stem orderings (traits/stem_strategy.rs): the position of a node in the
+// stem array, its level, its split dimension and its leaf-index prefix.
+// ---------------------------------------------------------------------------
+// Eytzinger (stem_strategy/eytzinger/mod.rs:81-186): root 1, children 2i and
+// 2i + 1, dim = level % K.
+template <int K>
+struct EytzingerCursor {
+  uint32_t stem_idx = 1;
+  int level = 0;
+  int dim() const { return level % K; }
+  EytzingerCursor branch() {  // self -> left child, returns the right child
+    EytzingerCursor r = *this;
+    stem_idx *= 2;
+    ++level;
+    r.stem_idx = stem_idx + 1;
+    r.level = level;
+    return r;
+  }
+};
+
+// DonnellyCore<BH> (stem_strategy/donnelly/core.rs:35-154, 254-290, 400-428):
+// stems packed in minor triangles of BH levels, each a 0-based heap inside a
+// line of 2^BH slots; the child triangles of a triangle's bottom row start at
+// line (line_base + 1 + 2 * col + is_right) << BH, col = min_idx - minor - 1.
+// dim advances once per level (wrapping at K); leaf_idx accumulates the path
+// bits, which is the arithmetic leaf index of an immutable tree
+// (kd_tree/mod.rs:164-178).
+template <int K>
+struct DonnellyCursor {
+  uint32_t bh = 3;
+  uint32_t stem_idx = 0;
+  int level = 0;
+  uint32_t minor = 0;
+  uint64_t leaf_idx = 0;
+  int dim_ = 0;
+  int dim() const { return dim_; }
+  uint32_t line_mask() const { return (1u << bh) - 1u; }
+
+  // step_pure (core.rs:254-290)
+  void traverse(bool is_right) {
+    const uint32_t r = is_right ? 1u : 0u;
+    const uint32_t min_idx = stem_idx & line_mask();
+    const uint32_t min_col = min_idx - minor - 1u;
+    const uint32_t base_no_right = (stem_idx & ~line_mask()) + 1u;
+    const uint32_t next_base = (base_no_right + (min_col << 1)) << bh;
+    const uint32_t same = base_no_right + r + (min_idx << 1);
+    const uint32_t next = next_base + (r << bh);
+    const bool inc_major = minor + 1u == bh;
+    stem_idx = inc_major ? next : same;
+    minor = inc_major ? 0u : minor + 1u;
+    advance(is_right);
+  }
+  // both_children_pure (core.rs:400-428)
+  void children(uint32_t& left, uint32_t& right) const {
+    const uint32_t min_idx = stem_idx & line_mask();
+    const uint32_t min_row = min_idx - minor - 1u;
+    const bool inc_major = minor + 1u == bh;
+    const uint32_t base_no_right = (stem_idx & ~line_mask()) + 1u;
+    const uint32_t same_left = base_no_right + (min_idx << 1);
+    const uint32_t next_left = (base_no_right + (min_row << 1)) << bh;
+    left = inc_major ? next_left : same_left;
+    right = inc_major ? next_left + (1u << bh) : same_left + 1u;
+  }
+  // branch (core.rs:124-148): self -> left child, returns the right child
+  DonnellyCursor branch() {
+    uint32_t l, r;
+    children(l, r);
+    stem_idx = l;
+    minor = minor + 1u == bh ? 0u : minor + 1u;
+    advance(false);
+    DonnellyCursor right = *this;
+    right.stem_idx = r;
+    right.leaf_idx = leaf_idx | 1u;
+    return right;
+  }
+  // branch_relative (traits/stem_strategy.rs:110-118): self -> near child,
+  // returns the far one
+  DonnellyCursor branch_relative(bool is_right) {
+    DonnellyCursor right = branch();
+    if (!is_right) return right;
+    DonnellyCursor left = *this;
+    *this = right;
+    return left;
+  }
+
+ private:
+  void advance(bool is_right) {
+    ++level;
+    dim_ = dim_ == K - 1 ? 0 : dim_ + 1;
+    leaf_idx = (leaf_idx << 1) | (is_right ? 1u : 0u);
+  }
+};
+
+// ---------------------------------------------------------------------------
 // Construction: soft-bucket bulk build (construction.rs:413-539, 868-968)
 // ---------------------------------------------------------------------------
 template <typename A, int K>
@@ -178,19 +274,20 @@ struct Builder {
     std::copy(tmp.begin(), tmp.begin() + len, idx);
   }
 
-  // populate_recursive_soft (construction.rs:868-968) with Eytzinger indices
-  // (stem_strategy/eytzinger/mod.rs:131-168: child = 2i + is_right,
-  // dim = level % K).
-  void populate(size_t* idx, size_t len, uint32_t stem_idx, int level, int max_stem_level,
-                uint64_t leaf_budget) {
+  // populate_recursive_soft (construction.rs:868-968), generic over the stem
+  // ordering as the reference is (EytzingerCursor / DonnellyCursor).
+  template <typename Cursor>
+  void populate(size_t* idx, size_t len, Cursor cur, int max_stem_level, uint64_t leaf_budget) {
     if (leaf_budget == 0) return;
+    const int level = cur.level;
+    const uint32_t stem_idx = cur.stem_idx;
     if (level > max_stem_level) {
       // write_leaf_from_sort_index (construction.rs:641-670)
       t->max_leaf_len = std::max<uint64_t>(t->max_leaf_len, len);
       append_leaf(*t, pts, items, idx, len);
       return;
     }
-    const int dim = level % K;
+    const int dim = cur.dim();
     t->max_stem_level = std::max(t->max_stem_level, level);
     if (stem_idx >= t->stems.size()) t->stems.resize(stem_idx + 1, inf_value<A>());
 
@@ -223,18 +320,23 @@ struct Builder {
       t->stems[stem_idx] = m;
     }
     const size_t split = std::min(pivot, len);
-    populate(idx, split, stem_idx * 2, level + 1, max_stem_level, left_budget);
-    populate(idx + split, len - split, stem_idx * 2 + 1, level + 1, max_stem_level,
-             right_budget);
+    Cursor right = cur.branch();
+    populate(idx, split, cur, max_stem_level, left_budget);
+    populate(idx + split, len - split, right, max_stem_level, right_budget);
   }
 };
 
 // KdTree::new_from_entries / new_from_slice -> new_from_source_with
-// (construction.rs:278-303, 403-409, 413-539, 540-589).
+// (construction.rs:278-303, 403-409, 413-539, 540-589).  bh == 0 builds the
+// Eytzinger layout (ImmutableKdTree); bh > 0 builds Donnelly<bh>, whose stem
+// tree is padded at the root to a multiple of bh levels (construction.rs:
+// 431-446) and sized by walking to the right-most leaf (:448-469).
 template <typename A, int K>
-Tree<A, K> build(const A* pts, const uint32_t* items, size_t n) {
+Tree<A, K> build(const A* pts, const uint32_t* items, size_t n, uint32_t bh = 0) {
   Tree<A, K> t;
   t.size = n;
+  t.stem_strategy = bh ? 1 : 0;
+  t.bh = bh;
   const size_t leaf_node_count = (n + kBucket - 1) / kBucket;
   std::vector<size_t> idx(n);
   std::iota(idx.begin(), idx.end(), size_t(0));
@@ -246,18 +348,33 @@ Tree<A, K> build(const A* pts, const uint32_t* items, size_t n) {
     append_leaf(t, pts, items, idx.data(), n);
     return t;
   }
-  // stems_depth = log2(next_power_of_two(leaf_node_count)); Eytzinger block size 1.
+  // stems_depth = log2(next_power_of_two(leaf_node_count))
   uint32_t depth = 0;
   while ((size_t(1) << depth) < leaf_node_count) ++depth;
-  t.stems_depth = depth;
-  const uint64_t budget = uint64_t(1) << depth;
-  // stem_node_count: index of the right-most represented leaf + 1, padded to 8.
-  const size_t stem_node_count = (size_t(1) << (depth + 1));
-  const size_t padded = (stem_node_count + 7) / 8 * 8;
-  t.stems.assign(padded, inf_value<A>());
-  t.max_stem_level = -1;
   Builder<A, K> b{pts, items, &t, {}};
-  b.populate(idx.data(), n, 1, 0, int(depth) - 1, budget);
+  t.max_stem_level = -1;
+  if (!bh) {
+    t.stems_depth = depth;
+    const uint64_t budget = uint64_t(1) << depth;
+    // stem_node_count: index of the right-most represented leaf + 1, padded to 8.
+    const size_t stem_node_count = (size_t(1) << (depth + 1));
+    const size_t padded = (stem_node_count + 7) / 8 * 8;
+    t.stems.assign(padded, inf_value<A>());
+    b.populate(idx.data(), n, EytzingerCursor<K>{}, int(depth) - 1, budget);
+    return t;
+  }
+  uint32_t padding = depth % bh ? bh - depth % bh : 0;
+  depth += padding;
+  t.stems_depth = depth;
+  DonnellyCursor<K> root;
+  root.bh = bh;
+  for (uint32_t i = 0; i < padding; ++i) root.traverse(false);
+  const uint64_t budget = uint64_t(1) << depth;
+  DonnellyCursor<K> right_most = root;
+  for (int bit = int(depth) - 1; bit >= 0; --bit) right_most.traverse(((budget - 1) >> bit) & 1u);
+  const size_t stem_node_count = size_t(right_most.stem_idx) + 1;
+  t.stems.assign((stem_node_count + 7) / 8 * 8, inf_value<A>());
+  b.populate(idx.data(), n, root, int(depth) - 1, budget);
   return t;
 }
 
@@ -388,9 +505,87 @@ void arithmetic_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_
   }
 }
 
+// Scalar backtracking with an explicit stack, the path of every strategy
+// whose BLOCK_SIZE != 1 (Donnelly; orchestrator/mod.rs:214-345, 607-669,
+// traits/stem_strategy.rs:209-325, query_stack.rs:124-200).  A frame holds
+// the far child's stem state, the dimension to restore, the off value to put
+// there and the far child's rd.  The prune test is made when a frame is
+// popped; on the way down `rd` stays the popped frame's, and the far child is
+// pushed when rd_far is not greater than max_dist() as read when the descent
+// started.  Only the popped frame's own dimension of `off` is reset, so
+// values set under deeper subtrees carry over, as in the reference.
+template <typename A, int K, typename M, typename Ctx, typename Leaf>
+void scalar_backtracking_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_leaf,
+                               Stats* st) {
+  if (t.size == 0) return;
+  struct Frame {
+    DonnellyCursor<K> s;
+    int restore_dim;  // -1: the popped state's own dimension
+    A old_off;
+    A rd;
+  };
+  std::vector<Frame> stack;
+  DonnellyCursor<K> root;
+  root.bh = t.bh;
+  stack.push_back({root, -1, A(0), A(0)});
+  A off[K];
+  for (int d = 0; d < K; ++d) off[d] = A(0);
+  const A INF = inf_value<A>();
+  while (!stack.empty()) {
+    Frame f = stack.back();
+    stack.pop_back();
+    DonnellyCursor<K> s = f.s;
+    int dim = s.dim();
+    const int restore_dim = f.restore_dim < 0 ? dim : f.restore_dim;
+    const A md = ctx.max_dist();
+    if (f.rd > md || (ctx.prune_on_equal() && f.rd == md)) continue;
+    off[restore_dim] = f.old_off;
+    const A best = ctx.max_dist();
+    const A rd = f.rd;
+    while (s.level <= t.max_stem_level) {
+      if (st) st->stem_visits++;
+      const A pivot = s.stem_idx < t.stems.size() ? t.stems[s.stem_idx] : INF;
+      if (pivot < INF) {
+        const bool is_right = q[dim] >= pivot;
+        DonnellyCursor<K> far = s.branch_relative(is_right);
+        const A new_off = std::fabs(q[dim] - pivot);  // Axis::saturating_dist
+        const A rd_far = M::rect_after_update(rd, off[dim], new_off);
+        if (!(rd_far > best)) stack.push_back({far, dim, new_off, rd_far});
+      } else {
+        s.traverse(false);
+      }
+      dim = s.dim();
+    }
+    const size_t leaf = size_t(s.leaf_idx);
+    if (st) { st->leaf_visits++; st->points_scanned += t.leaf_len(leaf); }
+    process_leaf(leaf);
+  }
+}
+
+// The traversal the reference runs for this tree's strategy
+// (orchestrator/mod.rs:214-255): arithmetic DFS for Eytzinger, scalar
+// backtracking for Donnelly.
+template <typename A, int K, typename M, typename Ctx, typename Leaf>
+void tree_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_leaf, Stats* st) {
+  if (t.stem_strategy == 1)
+    scalar_backtracking_query<A, K, M>(t, q, ctx, process_leaf, st);
+  else
+    arithmetic_query<A, K, M>(t, q, ctx, process_leaf, st);
+}
+
 // Straight descent (orchestrator/mod.rs:143-151, traits/stem_strategy.rs:182-200)
 template <typename A, int K>
 size_t get_leaf_idx(const Tree<A, K>& t, const A* q, Stats* st) {
+  if (t.stem_strategy == 1) {
+    DonnellyCursor<K> s;
+    s.bh = t.bh;
+    while (s.level <= t.max_stem_level) {
+      if (st) st->stem_visits++;
+      const A pivot = s.stem_idx < t.stems.size() ? t.stems[s.stem_idx] : inf_value<A>();
+      s.traverse(q[s.dim()] >= pivot);
+    }
+    return size_t(s.leaf_idx);
+  }
   uint32_t stem_idx = 1;
   int level = 0;
   while (level <= t.max_stem_level) {
@@ -468,7 +663,7 @@ std::pair<A, uint32_t> nearest_one(const Tree<A, K>& t, const A* q, Stats* st) {
     bool prune_on_equal() const { return true; }
   } ctx{inf_value<A>()};
   uint32_t best_item = 0;
-  arithmetic_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
+  tree_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
     t.for_each_point(leaf, [&](const A* c, uint32_t item) {
       A d = point_dist<M, A, K>(c, q);
       if (d < ctx.best) { ctx.best = d; best_item = item; }
@@ -512,7 +707,7 @@ std::vector<Hit<A>> nearest_n_within(const Tree<A, K>& t, const A* q, A max_dist
     bool initial_bound_is_unbounded() const { return r == inf_value<A>(); }
     bool prune_on_equal() const { return excl; }
   } ctx{&res, max_dist, exclusive};
-  arithmetic_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
+  tree_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
     const A leaf_max = ctx.max_dist();
     t.for_each_point(leaf, [&](const A* c, uint32_t item) {
       A d = point_dist<M, A, K>(c, q);
@@ -541,7 +736,7 @@ std::vector<Hit<A>> within(const Tree<A, K>& t, const A* q, A radius, bool exclu
     bool prune_on_equal() const { return excl; }
   } ctx{radius, exclusive};
   uint64_t seq = 0;
-  arithmetic_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
+  tree_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
     t.for_each_point(leaf, [&](const A* c, uint32_t item) {
       A d = point_dist<M, A, K>(c, q);
       bool ok = exclusive ? (d < radius) : (d <= radius);
@@ -573,7 +768,7 @@ std::vector<Hit<A>> best_n_within(const Tree<A, K>& t, const A* q, A radius, siz
   auto less = [](const Hit<A>& a, const Hit<A>& b) {
     return a.item < b.item || (a.item == b.item && a.seq < b.seq);
   };
-  arithmetic_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
+  tree_query<A, K, M>(t, q, ctx, [&](size_t leaf) {
     const bool full_at_entry = heap.size() >= n;
     const uint32_t threshold_item = full_at_entry ? heap.back().item : 0;
     t.for_each_point(leaf, [&](const A* c, uint32_t item) {

@@ -210,8 +210,13 @@ auto dispatch(int dtype, int k, F&& f) -> decltype(f(float(), std::integral_cons
 extern "C" {
 
 // Build a tree with the restated soft construction.  `items` may be null, in
-// which case item = source index (new_from_slice).
-void* kor_build(int dtype, int k, const void* pts, const uint32_t* items, uint64_t n) {
+// which case item = source index (new_from_slice).  bh == 0: Eytzinger
+// (ImmutableKdTree); bh > 0: Donnelly<bh>.
+void* kor_build_ex(int dtype, int k, const void* pts, const uint32_t* items, uint64_t n,
+                   uint32_t bh) {
+  // Donnelly block heights the reference uses (3 for f64, 4 for f32 trees);
+  // the core's bottom-row column min_idx - minor - 1 underflows below 3.
+  if (bh != 0 && bh != 3 && bh != 4) return nullptr;
   return dispatch(dtype, k, [&](auto a, auto kk) -> void* {
     using A = decltype(a);
     constexpr int K = decltype(kk)::value;
@@ -224,17 +229,21 @@ void* kor_build(int dtype, int k, const void* pts, const uint32_t* items, uint64
     auto* h = new TreeHolder<A, K>();
     h->dtype = dtype;
     h->k = K;
-    h->t = build<A, K>(static_cast<const A*>(pts), items, n);
+    h->t = build<A, K>(static_cast<const A*>(pts), items, n, bh);
     return static_cast<TreeBase*>(h);
   });
 }
 
+void* kor_build(int dtype, int k, const void* pts, const uint32_t* items, uint64_t n) {
+  return kor_build_ex(dtype, k, pts, items, n, 0);
+}
+
 // Wrap an externally produced layout (for example the one the product builder
 // made) so the oracle's queries can run on exactly those bytes.
-void* kor_from_layout(int dtype, int k, const void* stems, uint64_t stems_len,
-                      const uint8_t* bytes, uint64_t bytes_len, const uint64_t* extents,
-                      uint64_t leaf_count, int32_t max_stem_level, uint64_t size,
-                      uint64_t max_leaf_len) {
+void* kor_from_layout_ex(int dtype, int k, const void* stems, uint64_t stems_len,
+                         const uint8_t* bytes, uint64_t bytes_len, const uint64_t* extents,
+                         uint64_t leaf_count, int32_t max_stem_level, uint64_t size,
+                         uint64_t max_leaf_len, uint32_t bh) {
   return dispatch(dtype, k, [&](auto a, auto kk) -> void* {
     using A = decltype(a);
     constexpr int K = decltype(kk)::value;
@@ -248,13 +257,24 @@ void* kor_from_layout(int dtype, int k, const void* stems, uint64_t stems_len,
     h->t.max_stem_level = max_stem_level;
     h->t.size = size;
     h->t.max_leaf_len = max_leaf_len;
+    h->t.stem_strategy = bh ? 1 : 0;
+    h->t.bh = bh;
     return static_cast<TreeBase*>(h);
   });
 }
 
+void* kor_from_layout(int dtype, int k, const void* stems, uint64_t stems_len,
+                      const uint8_t* bytes, uint64_t bytes_len, const uint64_t* extents,
+                      uint64_t leaf_count, int32_t max_stem_level, uint64_t size,
+                      uint64_t max_leaf_len) {
+  return kor_from_layout_ex(dtype, k, stems, stems_len, bytes, bytes_len, extents, leaf_count,
+                            max_stem_level, size, max_leaf_len, 0);
+}
+
 void kor_free(void* h) { delete static_cast<TreeBase*>(h); }
 
-// layout[0..5] = stems_len, leaf_bytes_len, leaf_count, max_stem_level, size, max_leaf_len
+// layout[0..6] = stems_len, leaf_bytes_len, leaf_count, max_stem_level, size, max_leaf_len,
+// block height (0: Eytzinger)
 void kor_layout_info(void* hp, int64_t* info) {
   auto* b = static_cast<TreeBase*>(hp);
   dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
@@ -267,6 +287,7 @@ void kor_layout_info(void* hp, int64_t* info) {
     info[3] = t.max_stem_level;
     info[4] = int64_t(t.size);
     info[5] = int64_t(t.max_leaf_len);
+    info[6] = int64_t(t.bh);
     return 0;
   });
 }
@@ -296,6 +317,9 @@ int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint6
     constexpr int K = decltype(kk)::value;
     auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
     const A r = A(radius);
+    if (t.stem_strategy == 1 && (family == FAM_PERIODIC_NEAREST_ONE ||
+                                 family == FAM_PERIODIC_NEAREST_N))
+      return -2;  // the periodic restatement follows the Eytzinger traversal only
     if (metric == 0)
       return query_fixed_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, k,
                                               r, exclusive, sorted,
@@ -317,6 +341,7 @@ void* kor_query_radius(void* hp, int family, int metric, const void* queries, ui
     constexpr int K = decltype(kk)::value;
     auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
     const A r = A(radius);
+    if (t.stem_strategy == 1 && family == FAM_PERIODIC_WITHIN) return nullptr;
     if (metric == 0)
       return query_radius_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, r,
                                                exclusive, sorted, static_cast<const A*>(box),
@@ -325,6 +350,21 @@ void* kor_query_radius(void* hp, int family, int metric, const void* queries, ui
                                            exclusive, sorted, static_cast<const A*>(box),
                                            nthreads, stats3);
   });
+}
+
+// Test hook for the Donnelly index math: walks `n` path bits from the root of
+// a Donnelly<bh> stem tree.  out[0] = stem index after traverse() per bit;
+// out[1], out[2] = the two children of the node reached by branch_relative()
+// per bit (the two ways the reference moves a stem state).
+void kor_donnelly_path(uint32_t bh, const uint8_t* bits, uint64_t n, uint32_t* out) {
+  DonnellyCursor<3> a, b;
+  a.bh = b.bh = bh;
+  for (uint64_t i = 0; i < n; ++i) {
+    a.traverse(bits[i] != 0);
+    b.branch_relative(bits[i] != 0);
+  }
+  out[0] = a.stem_idx;
+  b.children(out[1], out[2]);
 }
 
 uint64_t kor_radius_total(void* r) {

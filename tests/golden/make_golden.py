@@ -23,6 +23,30 @@ def issue_258_points(src: str):
     return [[float(a), float(b)] for a, b in pairs]
 
 
+def donnelly_cases(src: str):
+    """src/stem_strategy/donnelly/core.rs tests: the rstest cases of
+    donnelly_core_get_child_idx_produces_correct_values (path -> stem index) and
+    donnelly_core_get_both_child_idxs_produces_correct_values (path -> both
+    children), all for DonnellyCore::<3>."""
+    paths, children = [], []
+    for block in src.split("#[rstest]")[1:]:
+        m = re.search(r"fn (\w+)\(", block)
+        if not m:
+            continue
+        name = m.group(1)
+        head = block[:m.start()]
+        if name == "donnelly_core_get_child_idx_produces_correct_values":
+            for v, e in re.findall(r"#\[case\(vec!\[([a-z, ]*)\],\s*(\d+)\)\]", head):
+                path = [x.strip() == "true" for x in v.split(",") if x.strip()]
+                paths.append({"bh": 3, "path": path, "stem_idx": int(e)})
+        elif name == "donnelly_core_get_both_child_idxs_produces_correct_values":
+            for v, l, r in re.findall(
+                    r"#\[case\(vec!\[([a-z, ]*)\],\s*\((\d+),\s*(\d+)\)\)\]", head):
+                path = [x.strip() == "true" for x in v.split(",") if x.strip()]
+                children.append({"bh": 3, "path": path, "children": [int(l), int(r)]})
+    return paths, children
+
+
 def main(ref_root: str):
     within_rs = open(os.path.join(ref_root, "src/kd_tree/query/within.rs")).read()
     p258 = issue_258_points(within_rs)
@@ -91,9 +115,13 @@ def main(ref_root: str):
             "name": f"tile_boundary_{n}", "dtype": "f32", "points": pts, "items": None,
             "checks": [{"family": "within_brute", "metric": "manhattan", "radius": 0.35,
                         "query": [0.31, 0.47, 0.59]}]})
+    core_rs = open(os.path.join(ref_root, "src/stem_strategy/donnelly/core.rs")).read()
+    dpaths, dchildren = donnelly_cases(core_rs)
+    assert len(dpaths) >= 40 and len(dchildren) >= 40, (len(dpaths), len(dchildren))
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kats.json")
     with open(out, "w") as f:
-        json.dump({"source": "kiddo v6.0.0-alpha.3 literal tests", "kats": kats}, f, indent=1)
+        json.dump({"source": "kiddo v6.0.0-alpha.3 literal tests", "kats": kats,
+                   "donnelly_paths": dpaths, "donnelly_children": dchildren}, f, indent=1)
     print(out)
 
 

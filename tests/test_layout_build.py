@@ -59,3 +59,29 @@ def test_explicit_items():
     P = rng.random((5000, 3)).astype(np.float32)
     items = rng.permutation(5000).astype(np.uint32) * 3 + 7
     same_layout(P, items)
+
+
+@pytest.mark.parametrize("bh", [3, 4])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("n", [0, 1, 33, 64, 65, 1000, 5000, 100_000])
+def test_donnelly_layouts(bh, dtype, n):
+    """Donnelly<bh> stems (stem_strategy/donnelly/core.rs, construction.rs:431-469):
+    the product builder writes the oracle's bytes, padding levels included."""
+    P = np.random.default_rng(n * 3 + bh).random((n, 3)).astype(dtype)
+    t = kb.ImmutableKdTree.new_from_slice(P, block_height=bh)
+    o = oracle.OracleTree.build(P, block_height=bh).layout()
+    assert t.block_height() == bh and o.block_height == bh
+    assert t.max_stem_level() == o.max_stem_level
+    assert t.max_leaf_len() == o.max_leaf_len
+    assert np.array_equal(t.stems().view(np.uint8), o.stems.view(np.uint8))
+    assert np.array_equal(t.leaf_extents(), o.extents)
+    assert np.array_equal(t.leaf_bytes(), o.leaf_bytes)
+    if o.max_stem_level >= 0:
+        assert (o.max_stem_level + 1) % bh == 0
+
+
+def test_donnelly_rejects_other_block_heights():
+    P = np.random.default_rng(0).random((100, 3))
+    for bh in (1, 2, 5):
+        with pytest.raises(Exception):
+            kb.ImmutableKdTree.new_from_slice(P, block_height=bh)

@@ -1,5 +1,8 @@
 """Pin the CPU oracle: the reference's literal known-answer tests and its own
 brute-force parity rules (tests/kd_tree_fuzz_v6.rs:244-340, 682-734, 960-1029)."""
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -119,3 +122,62 @@ def test_oracle_periodic_vs_brute_force():
         assert abs(d[j] - bd.min()) <= 1e-12 * bd.min()
         sel = np.sort(bd[bd <= 0.01])[:32]
         assert np.array_equal(np.sort(dn[j, :cn[j]]), sel)
+
+
+# ---------------------------------------------------------------------------
+# Donnelly stem strategy (stem_strategy/donnelly/core.rs)
+# ---------------------------------------------------------------------------
+def test_donnelly_index_math_matches_reference_cases():
+    """The reference's own DonnellyCore::<3> cases (core.rs tests, extracted by
+    tests/golden/make_golden.py): stem index after a path, and both children
+    of the node a path reaches."""
+    kats = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "kats.json")))
+    for c in kats["donnelly_paths"]:
+        idx, _ = oracle.donnelly_path(c["bh"], c["path"])
+        assert idx == c["stem_idx"], c
+    for c in kats["donnelly_children"]:
+        _, ch = oracle.donnelly_path(c["bh"], c["path"])
+        assert list(ch) == c["children"], c
+
+
+@pytest.mark.parametrize("bh", [3, 4])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_donnelly_tree_matches_brute_force_and_eytzinger(bh, dtype):
+    """A Donnelly<bh> tree answers every family like brute force and like the
+    Eytzinger tree of the same points (equal-distance groups as multisets, the
+    reference's fuzz rule kd_tree_fuzz_v6.rs:244-340)."""
+    rng = np.random.default_rng(100 + bh)
+    for n in (1, 31, 33, 100, 2000, 7000):
+        P = rng.random((n, 3)).astype(dtype)
+        Q = np.concatenate([rng.random((300, 3)).astype(dtype), P[:50]])
+        don = oracle.OracleTree.build(P, block_height=bh)
+        eyt = oracle.OracleTree.build(P)
+        lay = don.layout()
+        assert lay.block_height == bh
+        dd, di = don.nearest_one(Q)
+        ed, ei = eyt.nearest_one(Q)
+        assert np.array_equal(dd, ed)
+        bd = ((Q[:, None, :].astype(np.float64) - P[None, :, :]) ** 2).sum(-1)
+        assert np.allclose(dd, bd.min(1), rtol=1e-5, atol=1e-12)
+        for k in (1, 5, 16):
+            d1, i1, c1 = don.nearest_n(Q, k)
+            d2, i2, c2 = eyt.nearest_n(Q, k)
+            assert np.array_equal(d1, d2) and np.array_equal(c1, c2)
+            for a, b, dist in zip(i1, i2, d1):
+                # items may differ only inside equal-distance groups
+                for v in np.unique(dist):
+                    m = dist == v
+                    assert sorted(a[m]) == sorted(b[m])
+        r = 0.05 if dtype == np.float32 else 0.05
+        o1, wd1, wi1 = don.within(Q, r)
+        o2, wd2, wi2 = eyt.within(Q, r)
+        assert np.array_equal(o1, o2)
+        for j in range(len(Q)):
+            s1 = sorted(zip(wd1[o1[j]:o1[j + 1]].tolist(), wi1[o1[j]:o1[j + 1]].tolist()))
+            s2 = sorted(zip(wd2[o2[j]:o2[j + 1]].tolist(), wi2[o2[j]:o2[j + 1]].tolist()))
+            assert s1 == s2
+        b1 = don.best_n_within(Q, r, 4)
+        b2 = eyt.best_n_within(Q, r, 4)
+        assert np.array_equal(b1[1], b2[1]) and np.array_equal(b1[2], b2[2])
+        a1 = don.approx_nearest_one(Q)[0]
+        assert np.all(a1 >= dd)
