@@ -468,10 +468,30 @@ def forest_workload(scale, seed=3):
 
 
 def run_forest(args, rank, world):
+    """One job of 256 catalogues and 64M queries.  With N > 1 GPUs every tree
+    has one owner rank (multi.partition_trees on points x queries) that holds
+    it and answers its queries (strong scaling: the job is fixed); the time is
+    the max over ranks."""
     import torch
     import kiddo_b200 as kb
+    from kiddo_b200 import multi
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        multi.init_process_group("nccl")
     pts, items, Q, tree_of, radii, family = forest_workload(args.scale)
+    nq_total = len(Q)
+    if world > 1:
+        counts = np.bincount(tree_of, minlength=len(pts))
+        owner = np.asarray(multi.partition_trees([len(p) * max(int(c), 1) for p, c in
+                                                  zip(pts, counts)], world))
+        mine = np.nonzero(owner == rank)[0]
+        local = np.full(len(pts), -1, np.int64)
+        local[mine] = np.arange(len(mine))
+        keep = owner[tree_of] == rank
+        Q, radii, family = Q[keep], radii[keep], family[keep]
+        tree_of = local[tree_of[keep]].astype(np.int32)
+        pts = [pts[i] for i in mine]
+        items = [items[i] for i in mine]
     trees = [kb.ImmutableKdTree.new_from_entries(it, p) for it, p in zip(items, pts)]
     forest = kb.Forest(trees)
     stream = torch.cuda.Stream()
@@ -509,6 +529,7 @@ def run_forest(args, rank, world):
             for _ in range(args.warmup):
                 fn()
             torch.cuda.synchronize()
+            multi.barrier()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -516,16 +537,25 @@ def run_forest(args, rank, world):
                 fn()
             e1.record(stream)
             torch.cuda.synchronize()
-            return e0.elapsed_time(e1) / steps
+            return multi.max_over_ranks(e0.elapsed_time(e1) / steps)
 
         l0 = kb.launch_count()
         ms_batched = timed(batched, args.steps)
         launches = (kb.launch_count() - l0) // (args.warmup + args.steps)
         ms_per_tree = timed(per_tree, max(1, args.steps // 2))
-    nq = len(Q)
+    nq = nq_total
+    hits = [int(multi.fixed_order_sum(torch.tensor([h], dtype=torch.float64,
+                                                   device="cuda"))[0].item()) for h in hits]
+    if rank != 0:
+        multi.barrier()
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
     line = {"metric": METRIC, "value": nq / (ms_batched / 1e3), "unit": "queries/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_batched, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": ms_batched, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "c3_forest", "trees": len(trees),
                        "points": int(sum(len(p) for p in pts)), "queries": nq,
@@ -535,7 +565,13 @@ def run_forest(args, rank, world):
             "per_tree_launch": {"ms_per_step": ms_per_tree, "value": nq / (ms_per_tree / 1e3)},
             "batched_over_per_tree": ms_per_tree / ms_batched,
             "gpu_launches": int(launches)}
+    if world > 1:
+        line["config"]["parallelism"] = f"trees partitioned over {world} ranks"
     print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        multi.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -562,11 +598,23 @@ def chamfer_workload(scale, seed=4):
 
 
 def run_chamfer(args, rank, world):
+    """Forward + backward over 64 cloud pairs.  With N > 1 GPUs every pair has
+    one owner rank (multi.partition_trees on source x target sizes); a pair's
+    gradients stay on its owner and the loss partials are added in rank order
+    (multi.fixed_order_sum), so the job is fixed (strong scaling)."""
     import torch
     import kiddo_b200 as kb
+    from kiddo_b200 import multi
     from kiddo_b200.chamfer import chamfer_backward, chamfer_forward
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        multi.init_process_group("nccl")
     pairs = chamfer_workload(args.scale)
+    n_src_total = sum(len(s) for s, _ in pairs)
+    n_tgt_total = sum(len(t) for _, t in pairs)
+    if world > 1:
+        owner = multi.partition_trees([len(s) * 5.0 for s, _ in pairs], world)
+        pairs = [pr for pr, o in zip(pairs, owner) if o == rank]
     trees = [kb.ImmutableKdTree.new_from_slice(t) for _, t in pairs]
     forest = kb.Forest(trees)
     src = torch.from_numpy(np.concatenate([s for s, _ in pairs])).cuda()
@@ -578,10 +626,12 @@ def run_chamfer(args, rank, world):
     for k in (8, 1):
         def step():
             loss, ctx = chamfer_forward(forest, src, tgt, k, 0.01, tree_of, base)
-            return loss, chamfer_backward(ctx)
+            grads = chamfer_backward(ctx)
+            return multi.fixed_order_sum(loss), grads
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
+        multi.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         l0 = kb.launch_count()
@@ -590,18 +640,25 @@ def run_chamfer(args, rank, world):
             step()
         e1.record()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
+        ms = multi.max_over_ranks(e0.elapsed_time(e1) / args.steps)
         out[k] = (ms, (kb.launch_count() - l0) // args.steps)
     ms8 = out[8][0]
     line = {"metric": METRIC, "value": 64 / (ms8 / 1e3), "unit": "cloud pairs/s (fwd+bwd)",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms8,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "c4_chamfer", "pairs": 64, "k": 8, "sigma": 0.01,
-                       "source_points": int(src.shape[0]), "target_points": int(tgt.shape[0])},
+                       "source_points": int(n_src_total), "target_points": int(n_tgt_total)},
             "k1": {"ms_per_step": out[1][0], "value": 64 / (out[1][0] / 1e3)},
             "gpu_launches": int(out[8][1])}
-    print(json.dumps(line), flush=True)
+    if world > 1:
+        line["config"]["parallelism"] = f"cloud pairs partitioned over {world} ranks"
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        multi.barrier()
+        dist.destroy_process_group()
     return 0
 
 

@@ -77,6 +77,21 @@ def chamfer_backward(ctx: ChamferContext, grad_scale: float = 1.0, recompute: bo
     return g_src, g_tgt
 
 
+def chamfer_step_sharded(target, src_shard, tgt_points, k, sigma, tree_of=None, tgt_base=None,
+                         recompute=False):
+    """One Chamfer forward + backward with the source points sharded over the
+    ranks of the process group (each rank holds every target tree and its own
+    slice of sources).  The loss and the target gradient are sums over all
+    sources, so their per-rank partials are combined with
+    ``multi.fixed_order_sum`` (gathered, added in rank order): the same bits on
+    every rank and every run.  The source gradient is per source and stays on
+    its rank.  Returns (loss, grad of this rank's sources, grad of targets)."""
+    from . import multi
+    loss, ctx = chamfer_forward(target, src_shard, tgt_points, k, sigma, tree_of, tgt_base)
+    g_src, g_tgt = chamfer_backward(ctx, recompute=recompute)
+    return multi.fixed_order_sum(loss), g_src, multi.fixed_order_sum(g_tgt)
+
+
 def _autograd_function():
     import torch
 

@@ -1,10 +1,19 @@
-"""Multi-GPU plumbing: one process per GPU, each holding a replica of the tree.
+"""Multi-GPU plumbing: one process per GPU.
 
 Queries are independent (the reference parallelises them with a rayon par_iter over
-`.execute()`, benches/query.rs:36-52), so a batch shards by contiguous query
-ranges with no data-path collective.  The only collectives are the timing
-barrier and the max-over-ranks reduction of elapsed times, and optional result
-gathering for callers that want every rank's answers on rank 0.
+`.execute()`, benches/query.rs:36-52), so a batch shards with no data-path
+collective:
+
+* one tree: every rank holds a replica and answers a contiguous query range
+  (``shard_range``);
+* many trees: every tree has one owner rank (``partition_trees``, balanced by
+  points x queries) that holds it and answers its queries;
+* sums that span ranks (a Chamfer loss, the target-point gradient when sources
+  are sharded) are combined by ``fixed_order_sum``: gathered, then added in
+  rank order, so every rank gets the same bits on every run.
+
+The other collectives are the timing barrier, the max-over-ranks reduction of
+elapsed times and optional result gathering on rank 0.
 """
 from __future__ import annotations
 
@@ -60,3 +69,34 @@ def gather_to_rank0(arr):
     out = [None] * dist.get_world_size()
     dist.all_gather_object(out, arr)
     return np.concatenate(out) if dist.get_rank() == 0 else None
+
+
+def partition_trees(weights, world_size: int):
+    """Owner rank of each tree: longest-first greedy on `weights` (for
+    example points x queries of each tree), each tree to the least-loaded rank,
+    ties to the lower tree index and the lower rank.  Every rank computes the
+    same map from the same weights."""
+    n = len(weights)
+    order = sorted(range(n), key=lambda i: (-float(weights[i]), i))
+    load = [0.0] * world_size
+    owner = [0] * n
+    for i in order:
+        r = min(range(world_size), key=lambda j: (load[j], j))
+        owner[i] = r
+        load[r] += float(weights[i])
+    return owner
+
+
+def fixed_order_sum(t):
+    """Elementwise sum of tensor `t` over the ranks, added in rank order
+    0, 1, ..., N-1 on every rank (all-gather, then a fixed sequence of adds),
+    so the result does not depend on the collective's reduction order."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return t.clone()
+    parts = [t.new_empty(t.shape) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, t.contiguous())
+    acc = parts[0].clone()
+    for p in parts[1:]:
+        acc += p
+    return acc
