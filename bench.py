@@ -243,7 +243,7 @@ def l2_note(n, nq, itemsize):
 
 def kernel_name(fam, engine):
     if fam.startswith("periodic"):
-        return "k_periodic_fixed<nearest_n>"
+        return "k_tperiodic_nn" if engine != "warp" else "k_periodic_fixed<nearest_n>"
     f = {"nearest_n": "nearest_n", "approx": "approx", "nearest_one": "nearest_one"}[fam]
     return f"k_tfixed<{f}>" if engine != "warp" else f"k_fixed<{f}>"
 

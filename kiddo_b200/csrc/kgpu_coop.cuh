@@ -176,6 +176,84 @@ struct CNearestNRow {
   __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
 
+  // Chunks with this many candidates are merged at once instead of inserted
+  // one by one.
+  static constexpr int kMergeFrom = 6;
+
+  // All candidates of a chunk at once.  The candidates are bitonic-sorted by
+  // (distance, lane) -- lane order is arrival order -- with non-candidates
+  // behind them; then every held entry and every candidate learns its place in
+  // the merged sequence by a binary search of the other sorted sequence (held
+  // entries ahead of candidates of equal distance, since they arrived first),
+  // the first k are written to the row, and the row is read back.  This is
+  // the list the one-by-one inserts would leave: the k smallest by (distance,
+  // arrival) of the held entries and the candidates.
+  __device__ __forceinline__ void merge_chunk(bool pass, A d, uint32_t it, int cnt, int& nn, A& kk,
+                                              A& Ld, uint32_t& Li, A* __restrict__ ld,
+                                              uint32_t* __restrict__ li, int lane) const {
+    A sd = d;
+    uint32_t si = it;
+    uint32_t tag = (pass ? 0u : 32u) | uint32_t(lane);  // non-candidates sort last
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const A od = __shfl_xor_sync(FULL, sd, stride);
+        const uint32_t ot = __shfl_xor_sync(FULL, tag, stride);
+        const uint32_t oi = __shfl_xor_sync(FULL, si, stride);
+        const bool up = (lane & size) == 0;
+        const bool lower = (lane & stride) == 0;
+        // key order: candidates first, then distance, then lane
+        const bool other_less =
+            (ot >> 5) != (tag >> 5) ? (ot >> 5) < (tag >> 5) : (od < sd || (od == sd && ot < tag));
+        const bool take = lower ? (up ? other_less : !other_less) : (up ? !other_less : other_less);
+        if (take) {
+          sd = od;
+          tag = ot;
+          si = oi;
+        }
+      }
+    }
+    // rank of a held entry among the candidates (strictly closer ones) and of
+    // a candidate among the held entries (not farther ones)
+    int lo = 0, hi = cnt;
+    int lo2 = 0, hi2 = nn;
+#pragma unroll
+    for (int step = 0; step < 6; ++step) {
+      const int mid = (lo + hi) >> 1;
+      const A v = shfl(sd, mid & 31);
+      if (lo < hi) {
+        if (v < Ld) lo = mid + 1;
+        else hi = mid;
+      }
+      const int mid2 = (lo2 + hi2) >> 1;
+      const A v2 = shfl(Ld, mid2 & 31);
+      if (lo2 < hi2) {
+        if (v2 <= sd) lo2 = mid2 + 1;
+        else hi2 = mid2;
+      }
+    }
+    const int pos_held = lane + lo, pos_cand = lane + lo2;
+    if (lane < nn && pos_held < k) {
+      ld[pos_held] = Ld;
+      li[pos_held] = Li;
+    }
+    if (lane < cnt && pos_cand < k) {
+      ld[pos_cand] = sd;
+      li[pos_cand] = si;
+    }
+    __syncwarp();
+    nn = nn + cnt < k ? nn + cnt : k;
+    Ld = inf_of<A>();
+    Li = 0;
+    if (lane < nn) {
+      Ld = ld[lane];
+      Li = li[lane];
+    }
+    if (nn == k) kk = shfl(Ld, k - 1);
+    __syncwarp();
+  }
+
   __device__ __forceinline__ void leaf(int o, uint64_t qo, const CoopLeaf<A, K>& L, int lane) {
     int nn = __shfl_sync(FULL, n, o);
     A kk = shfl(kth, o);
@@ -202,6 +280,11 @@ struct CNearestNRow {
           Li = li[lane];
         }
         loaded = true;
+      }
+      const int cnt = __popc(m);
+      if (cnt >= kMergeFrom) {
+        merge_chunk(pass, d, it, cnt, nn, kk, Ld, Li, ld, li, lane);
+        continue;
       }
       while (m) {
         const int c = __ffs(m) - 1;

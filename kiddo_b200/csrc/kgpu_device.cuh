@@ -163,6 +163,48 @@ __device__ __forceinline__ A point_dist(const A (&c)[K], const A (&q)[K]) {
   return acc;
 }
 
+// Packed pairs of f32 (sm_100 f32x2 arithmetic): each half of a packed sub or
+// mul rounds exactly like scalar __fsub_rn / __fmul_rn.  Only sub and mul are
+// used packed: the sums stay scalar __fadd_rn in the reference's order (a
+// packed multiply followed by a packed add did not reproduce the scalar
+// rounding when measured on B200).
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2_pack(float a, float b) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(F2 x, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+}
+__device__ __forceinline__ F2 f2_sub(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 f2_mul(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 f2_abs(F2 a) {  // fabsf on both halves: clear the sign bits
+  F2 r;
+  r.v = a.v & 0x7fffffff7fffffffull;
+  return r;
+}
+
+// Largest value below x (x >= 0 or +inf): "d < x" is "d <= below(x)" for
+// every non-negative, non-NaN d.
+__device__ __forceinline__ float below(float x) {
+  return x > 0.f ? __int_as_float(__float_as_int(x) - 1) : -__int_as_float(1);
+}
+__device__ __forceinline__ double below(double x) {
+  return x > 0.0 ? __longlong_as_double(__double_as_longlong(x) - 1)
+                 : -__longlong_as_double(1ll);
+}
+
 // Point-to-query distance of the Cartesian families.
 template <typename A, int K, typename M>
 struct CartesianDist {

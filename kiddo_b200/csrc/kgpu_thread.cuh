@@ -48,15 +48,10 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
       for (int d = 0; d < K; ++d) c0[d] = __ldg(col + d);
       d0 = d1 = dist(c0);
     } else if constexpr (sizeof(A) == 4) {
-      A c0[K], c1[K];
+      float2 v[K];
 #pragma unroll
-      for (int d = 0; d < K; ++d) {
-        const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
-        c0[d] = v.x;
-        c1[d] = v.y;
-      }
-      d0 = dist(c0);
-      d1 = dist(c1);
+      for (int d = 0; d < K; ++d) v[d] = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
+      dist.pair(v, d0, d1);
     } else {
       A c0[K], c1[K];
 #pragma unroll
@@ -117,15 +112,10 @@ __device__ __forceinline__ uint32_t leaf_chunk_mask(const uint8_t* __restrict__ 
       for (int d = 0; d < K; ++d) c[d] = __ldg(col + d);
       d0 = d1 = dist(c);
     } else if constexpr (sizeof(A) == 4) {
-      A c0v[K], c1v[K];
+      float2 v[K];
 #pragma unroll
-      for (int d = 0; d < K; ++d) {
-        const float2 v = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
-        c0v[d] = v.x;
-        c1v[d] = v.y;
-      }
-      d0 = dist(c0v);
-      d1 = dist(c1v);
+      for (int d = 0; d < K; ++d) v[d] = __ldg(reinterpret_cast<const float2*>(col + d * w + i));
+      dist.pair(v, d0, d1);
     } else {
       A c0v[K], c1v[K];
 #pragma unroll
@@ -483,6 +473,24 @@ struct CartesianQ {
   __device__ __forceinline__ A operator()(const A (&c)[K]) const {
     return point_dist<M, A, K>(c, q);
   }
+  // Both points of an f32 pair (v[d] = {axis d of point 0, of point 1}):
+  // dist1 packed, the sum scalar in the order of point_dist.
+  __device__ __forceinline__ void pair(const float2 (&v)[K], float& d0, float& d1) const {
+    float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+    for (int d = 0; d < K; ++d) {
+      const F2 t = f2_sub(f2_pack(v[d].x, v[d].y), f2_pack(q[d], q[d]));
+      F2 m;
+      if constexpr (std::is_same<M, SqEuclidean>::value) m = f2_mul(t, t);
+      else m = f2_abs(t);
+      float m0, m1;
+      f2_unpack(m, m0, m1);
+      a0 = d ? __fadd_rn(a0, m0) : m0;
+      a1 = d ? __fadd_rn(a1, m1) : m1;
+    }
+    d0 = a0;
+    d1 = a1;
+  }
 };
 template <typename A, int K, typename M>
 struct TNearestOne {
@@ -573,17 +581,23 @@ struct TNearestN {
   // kth.  The add() calls are the sequential ones minus those add() would
   // reject, so the list is the same.
   __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
-    const A bound = max_dist();
-    const bool full0 = n == k;
-    const A kth0 = kth;
+    // The mark "d within the leaf-start bound, and below kth when the list
+    // started full" as one test d <= gate: strict comparisons become <= on
+    // the next value down.
+    A gate;
+    if (n < k) {
+      gate = kExclusive ? below(radius) : radius;
+    } else if (kExclusive) {
+      gate = below(kth < radius ? kth : radius);
+    } else {
+      gate = kth <= radius ? below(kth) : radius;
+    }
     const CartesianQ<A, K, M> dist{q};
     const uint2 ex = __ldg(tv.extents + l);
     const uint8_t* base = tv.arena + size_t(ex.x) * 8;
     const uint32_t len = ex.y;
     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
-      uint32_t mask = leaf_chunk_mask<A, K>(base, len, c0, dist, [&](A d) {
-        return (kExclusive ? (d < bound) : (d <= bound)) && (!full0 || d < kth0);
-      });
+      uint32_t mask = leaf_chunk_mask<A, K>(base, len, c0, dist, [&](A d) { return d <= gate; });
       while (mask) {
         const uint32_t p = c0 + uint32_t(__ffs(mask) - 1);
         mask &= mask - 1;

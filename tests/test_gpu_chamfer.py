@@ -41,8 +41,11 @@ def test_chamfer_gradient_vs_fp64(k, kind):
     r_src, r_tgt = ref.gradient(src, tgt, items, counts, k, SIGMA)
     gs, gt = g_src.cpu().numpy(), g_tgt.cpu().numpy()
     # relative error of the gradient vectors (f32 engine vs FP64 oracle)
-    assert np.linalg.norm(gs - r_src) <= 1e-5 * np.linalg.norm(r_src)
-    assert np.linalg.norm(gt - r_tgt) <= 1e-5 * np.linalg.norm(r_tgt)
+    e_src = np.linalg.norm(gs - r_src) / np.linalg.norm(r_src)
+    e_tgt = np.linalg.norm(gt - r_tgt) / np.linalg.norm(r_tgt)
+    print(f"chamfer k={k} {kind}: loss rel err {abs(float(loss) - l64) / abs(l64):.2e}, "
+          f"grad rel err src {e_src:.2e} tgt {e_tgt:.2e}")
+    assert e_src <= 1e-5 and e_tgt <= 1e-5
     # f64 central differences on 1,000 sampled coordinates away from ties
     picks = rng.choice(len(src), 500, replace=False)
     for i in picks[:500]:
