@@ -319,7 +319,9 @@ def main():
     n = args.points or n
     nq = args.queries or nq
     P, Q = make_data(args.workload, rank, n, nq)
+    t_host = time.perf_counter()
     tree = kb.ImmutableKdTree.new_from_slice(P)
+    host_build_s = time.perf_counter() - t_host
     gtree = tree.to_gpu()
     stream = torch.cuda.current_stream(dev)
     dq = torch.from_numpy(Q).to(dev)
@@ -369,6 +371,19 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = multi.max_over_ranks(e0.elapsed_time(e1))
 
+    # the same tree built on the device from device points (same bytes)
+    dP = torch.from_numpy(P).to(dev)
+    kb.GpuTree.build(dP)
+    torch.cuda.synchronize()
+    b0 = torch.cuda.Event(enable_timing=True)
+    b1 = torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    kb.GpuTree.build(dP, stream=stream)
+    b1.record(stream)
+    torch.cuda.synchronize()
+    device_build_ms = b0.elapsed_time(b1)
+    del dP
+
     w = k if fam in ("nearest_n", "periodic_nearest_n_within") else 1
     h2d = nq * 3 * Q.itemsize
     d2h = nq * w * (Q.itemsize + 4) + (nq * 4)
@@ -404,6 +419,8 @@ def main():
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
+        "tree_build": {"host_s": host_build_s, "host_threads": os.cpu_count(),
+                       "device_ms": device_build_ms},
         "traversal_per_query": {"stems": float(stats[0]) / len(sub),
                                 "leaves": float(stats[1]) / len(sub),
                                 "points": float(stats[2]) / len(sub)},

@@ -156,6 +156,19 @@ int32_t kgpu_layout_free(kgpu_layout* layout);
  * are re-encoded as 32-bit (offset / 8, len) pairs. */
 int32_t kgpu_tree_create(const kgpu_tree_desc* desc, void* stream, kgpu_tree** out);
 int32_t kgpu_tree_destroy(kgpu_tree* tree);
+/* Builds the ImmutableKdTree of `n` points on the current device: `points` (n rows
+ * of `dims` values of `dtype`) and `items` (NULL: item = source index) are DEVICE
+ * pointers.  The resulting layout is byte-identical to kgpu_layout_build's (the
+ * reference's soft construction, src/kd_tree/construction.rs:413-539, 868-968,
+ * 1089-1175), built level by level on the GPU.  Synchronizes `stream` before
+ * returning.  At most 2^31 - 1 points. */
+int32_t kgpu_tree_build(int32_t dtype, uint32_t dims, const void* points, const uint32_t* items,
+                        uint64_t n, void* stream, kgpu_tree** out);
+/* Copies a device tree's layout to host arrays: stems (stem_count values), the
+ * leaf arena (leaf_bytes_len bytes) and the extents as (byte offset, len) u64
+ * pairs, leaf_count of them (sizes from kgpu_tree_info).  Any pointer may be NULL. */
+int32_t kgpu_tree_read_layout(const kgpu_tree* tree, void* stems, uint8_t* leaf_bytes,
+                              uint64_t* extents, void* stream);
 /* info[0..7] = dtype, dims, size, leaf_count, max_stem_level, stem_count,
  *              leaf_bytes_len, device bytes held */
 int32_t kgpu_tree_info(const kgpu_tree* tree, int64_t* info);

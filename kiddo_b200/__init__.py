@@ -216,16 +216,61 @@ class _LayoutHandle:
 
 
 class GpuTree:
-    """A tree resident in HBM (kgpu_tree_create)."""
+    """A tree resident in HBM: uploaded from a host layout (kgpu_tree_create),
+    or built on the device from device points (``GpuTree.build``)."""
 
-    def __init__(self, host: ImmutableKdTree, stream=None):
-        L = C.lib()
+    def __init__(self, host: Optional[ImmutableKdTree], stream=None, _handle=None, dtype=None,
+                 dims=None):
         self.host = host
+        if _handle is not None:
+            self._h = _handle
+            self.dtype = np.dtype(dtype)
+            self.dims = int(dims)
+            return
+        L = C.lib()
         self.dtype = host.dtype
         self.dims = host.dims
         h = ctypes.c_void_p()
         C.check(L.kgpu_tree_create(ctypes.byref(host._desc), _stream_ptr(stream), ctypes.byref(h)))
         self._h = h
+
+    @classmethod
+    def build(cls, points, items=None, stream=None) -> "GpuTree":
+        """The ImmutableKdTree of CUDA tensor `points` ([n, dims], float32 or
+        float64) built on the device (kgpu_tree_build): the same layout, byte for
+        byte, as ``ImmutableKdTree.new_from_slice`` / ``new_from_entries``
+        (`items`: uint32 values in an int32 CUDA tensor) build on the host."""
+        import torch
+        if not (isinstance(points, torch.Tensor) and points.is_cuda and points.dim() == 2):
+            raise TypeError("points must be a 2-D CUDA tensor")
+        if points.dtype not in (torch.float32, torch.float64):
+            raise TypeError("points must be float32 or float64")
+        pts = points.contiguous()
+        it = None
+        if items is not None:
+            it = items.contiguous()
+            if it.shape[0] != pts.shape[0] or it.element_size() != 4:
+                raise ValueError("items must be one 32-bit value per point")
+        h = ctypes.c_void_p()
+        dt = np.float32 if pts.dtype == torch.float32 else np.float64
+        C.check(C.lib().kgpu_tree_build(C.F32 if dt == np.float32 else C.F64, pts.shape[1],
+                                        ctypes.c_void_p(pts.data_ptr()),
+                                        None if it is None else ctypes.c_void_p(it.data_ptr()),
+                                        pts.shape[0], _stream_ptr(stream), ctypes.byref(h)))
+        return cls(None, _handle=h, dtype=dt, dims=pts.shape[1])
+
+    def read_layout(self):
+        """(stems, leaf_bytes, extents) copied back from the device; extents as
+        (byte offset, len) pairs like the reference's leaf_extents."""
+        inf = self.info()
+        stems = np.empty(int(inf["stem_count"]), dtype=self.dtype)
+        lb = np.empty(int(inf["leaf_bytes_len"]), dtype=np.uint8)
+        ex = np.empty((int(inf["leaf_count"]), 2), dtype=np.uint64)
+        C.check(C.lib().kgpu_tree_read_layout(self._h, _vp(stems), _vp(lb), _vp(ex), None))
+        return stems, lb, ex
+
+    def size(self) -> int:
+        return int(self.info()["size"])
 
     def __del__(self):
         if getattr(self, "_h", None) and C._lib is not None:

@@ -31,7 +31,7 @@ FLAG_NO_SPATIAL_ORDER = 0x10
 # Every symbol include/kiddo_gpu.h declares.
 EXPORTED_SYMBOLS = [
     "kgpu_last_error", "kgpu_status_string", "kgpu_abi_version", "kgpu_layout_build",
-    "kgpu_layout_build_stems",
+    "kgpu_layout_build_stems", "kgpu_tree_build", "kgpu_tree_read_layout",
     "kgpu_layout_describe", "kgpu_layout_free", "kgpu_tree_create", "kgpu_tree_destroy",
     "kgpu_tree_info", "kgpu_query", "kgpu_query_radius_count", "kgpu_query_radius_fill",
     "kgpu_launch_count", "kgpu_query_stats", "kgpu_query_radius_count_noalloc",
@@ -89,6 +89,10 @@ def lib():
     L.kgpu_abi_version.restype = u32
     L.kgpu_layout_build.restype = i32
     L.kgpu_layout_build.argtypes = [i32, u32, vp, vp, u64, i32, ctypes.POINTER(vp)]
+    L.kgpu_tree_build.restype = i32
+    L.kgpu_tree_build.argtypes = [i32, u32, vp, vp, u64, vp, ctypes.POINTER(vp)]
+    L.kgpu_tree_read_layout.restype = i32
+    L.kgpu_tree_read_layout.argtypes = [vp, vp, vp, vp, vp]
     L.kgpu_layout_build_stems.restype = i32
     L.kgpu_layout_build_stems.argtypes = [i32, u32, vp, vp, u64, i32, u32, i32, ctypes.POINTER(vp)]
     L.kgpu_layout_describe.restype = i32

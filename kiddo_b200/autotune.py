@@ -53,7 +53,7 @@ def key_for(builder) -> str:
     import torch
     tree = builder.tree
     dev = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
-    size = tree.host.size() if hasattr(tree, "host") else 0
+    size = tree.size() if hasattr(tree, "size") else 0
     size_bucket = int(math.log2(max(size, 1))) // 2 * 2
     k = builder.max_qty if builder.max_qty else 1
     return "|".join(str(x) for x in (dev, tree.dtype, tree.dims, builder.family, builder.metric,

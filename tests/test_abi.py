@@ -28,6 +28,21 @@ def test_exports_every_declared_symbol():
     assert sorted(C.EXPORTED_SYMBOLS) == syms
 
 
+def test_no_device_only_code_reached_from_host():
+    """nvcc gives a device-only function called from host code (through
+    --expt-relaxed-constexpr or a template) a host body of exit(1), which ends
+    the caller's process with no message.  The library must import no exit."""
+    import shutil
+    import subprocess
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not available")
+    out = subprocess.run([nm, "-D", "--undefined-only", C.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    names = {line.split()[-1].split("@")[0] for line in out.splitlines() if line.strip()}
+    assert "exit" not in names and "_exit" not in names
+
+
 def test_version_and_status_strings():
     L = C.lib()
     assert L.kgpu_abi_version() == C.ABI_VERSION
