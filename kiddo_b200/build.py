@@ -35,8 +35,7 @@ CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kgpu_forest.cu"
               "kernels_f64_radius.cu",
               ]
 CXX_SOURCES = ["layout_build.cpp"]
-HEADERS = ["kgpu_device.cuh", "kgpu_kernels.cuh", "kgpu_launch.h", "kgpu_launch_impl.cuh",
-           "kgpu_internal.h", "kgpu_tree_impl.h", "kgpu_thread.cuh"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 
 
 def _nvcc() -> str:

@@ -64,8 +64,6 @@ size_t leaf_encoded_bytes(uint64_t len, int K, size_t sa) {
   return total;
 }
 
-// RAII device buffer allocated on a stream (stream-ordered allocator).
-
 }  // namespace
 }  // namespace kgpu
 
@@ -86,6 +84,29 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
     cached_devices.fetch_or(bit, std::memory_order_relaxed);
   }
   return cudaMallocAsync(p, bytes, s);
+}
+
+void release_tree_arrays(DeviceTree& dt) {
+  if (dt.pooled) {
+    // the arrays came from the device's stream-ordered pool: wait for every
+    // stream, as cudaFree would, then return them to the pool
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dt.device) cudaSetDevice(dt.device);
+    cudaDeviceSynchronize();
+    if (dt.stems) cudaFreeAsync(dt.stems, nullptr);
+    if (dt.arena) cudaFreeAsync(dt.arena, nullptr);
+    if (dt.extents) cudaFreeAsync(dt.extents, nullptr);
+    cudaStreamSynchronize(nullptr);
+    if (cur != dt.device) cudaSetDevice(cur);
+  } else {
+    cudaFree(dt.stems);
+    cudaFree(dt.arena);
+    cudaFree(dt.extents);
+  }
+  dt.stems = nullptr;
+  dt.arena = nullptr;
+  dt.extents = nullptr;
 }
 
 }  // namespace kgpu
@@ -256,6 +277,10 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
   for (uint64_t l = 0; l < d->leaf_count; ++l) {
     const uint64_t off = d->leaf_extents[2 * l], len = d->leaf_extents[2 * l + 1];
     if (off % 8) return set_error(KGPU_EINVAL, "leaf offset not 8-byte aligned");
+    // f32 3-D leaves are 16 bytes per point, so the reference's offsets are
+    // multiples of 16; the device reads them as aligned 16-byte rows
+    if (d->dtype == KGPU_F32 && K == 3 && off % 16)
+      return set_error(KGPU_EINVAL, "f32 3-D leaf offset not a multiple of 16 bytes");
     if (len > 1024) return set_error(KGPU_EINVAL, "leaf longer than 1024 points");
     if (off + leaf_encoded_bytes(len, K, sa) > d->leaf_bytes_len)
       return set_error(KGPU_EINVAL, "leaf extent outside the arena");
@@ -295,10 +320,16 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
   }
   dt.device_bytes = stem_bytes + arena_bytes + ex_bytes;
   if (d->stem_count) e = cudaMemcpyAsync(dt.stems, d->stems, d->stem_count * sa, cudaMemcpyHostToDevice, s);
+  // f32 3-D leaves are staged as tiles and re-encoded as rows on the device
+  const bool rows = d->dtype == KGPU_F32 && K == 3 && d->leaf_bytes_len;
+  DevBuf tiles;
+  if (e == cudaSuccess && rows) e = tiles.alloc(d->leaf_bytes_len, s);
   if (e == cudaSuccess && d->leaf_bytes_len)
-    e = cudaMemcpyAsync(dt.arena, d->leaf_bytes, d->leaf_bytes_len, cudaMemcpyHostToDevice, s);
+    e = cudaMemcpyAsync(rows ? tiles.as<uint8_t>() : dt.arena, d->leaf_bytes, d->leaf_bytes_len,
+                        cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && !ex.empty())
     e = cudaMemcpyAsync(dt.extents, ex.data(), ex.size() * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && rows) e = convert_leaf_layout(dt, tiles.as<uint8_t>(), dt.arena, true, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // `ex` is a local
   if (e != cudaSuccess) {
     kgpu_tree_destroy(t);
@@ -310,9 +341,7 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
 
 int32_t kgpu_tree_destroy(kgpu_tree* t) {
   if (!t) return KGPU_OK;
-  cudaFree(t->dt.stems);
-  cudaFree(t->dt.arena);
-  cudaFree(t->dt.extents);
+  release_tree_arrays(t->dt);
   delete t;
   return KGPU_OK;
 }

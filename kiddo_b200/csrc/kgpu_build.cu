@@ -206,6 +206,46 @@ __global__ void k_write_leaves(const A* __restrict__ pts, const uint32_t* __rest
   }
 }
 
+// Tiles <-> rows for the leaves held as rows on the device (RowLeaves: f32,
+// 3-D), one warp per leaf; same offsets, same bytes per point.
+__global__ void k_leaf_tiles_to_rows(const uint8_t* __restrict__ tiles, uint8_t* __restrict__ rows,
+                                     const uint2* __restrict__ extents, uint64_t leaves) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t l = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; l < leaves;
+       l += (uint64_t(gridDim.x) * blockDim.x) >> 5) {
+    const uint2 ex = extents[l];
+    const size_t o = size_t(ex.x) * 8;
+    for (uint32_t p = lane; p < ex.y; p += 32) {
+      uint32_t toff, w, i;
+      tile_slot_cols<float, 3>(ex.y, p, toff, w, i);
+      const float* col = reinterpret_cast<const float*>(tiles + o + toff);
+      const uint32_t it = reinterpret_cast<const uint32_t*>(tiles + o + toff + 3 * w * 4)[i];
+      reinterpret_cast<float4*>(rows + o)[p] =
+          make_float4(col[i], col[w + i], col[2 * w + i], __uint_as_float(it));
+    }
+  }
+}
+
+__global__ void k_leaf_rows_to_tiles(const uint8_t* __restrict__ rows, uint8_t* __restrict__ tiles,
+                                     const uint2* __restrict__ extents, uint64_t leaves) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t l = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; l < leaves;
+       l += (uint64_t(gridDim.x) * blockDim.x) >> 5) {
+    const uint2 ex = extents[l];
+    const size_t o = size_t(ex.x) * 8;
+    for (uint32_t p = lane; p < ex.y; p += 32) {
+      uint32_t toff, w, i;
+      tile_slot_cols<float, 3>(ex.y, p, toff, w, i);
+      const float4 v = reinterpret_cast<const float4*>(rows + o)[p];
+      float* col = reinterpret_cast<float*>(tiles + o + toff);
+      col[i] = v.x;
+      col[w + i] = v.y;
+      col[2 * w + i] = v.z;
+      reinterpret_cast<uint32_t*>(tiles + o + toff + 3 * w * 4)[i] = __float_as_uint(v.w);
+    }
+  }
+}
+
 inline unsigned blocks_for(uint64_t n, unsigned threads = 256) {
   const uint64_t b = (n + threads - 1) / threads;
   return unsigned(std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 64)));
@@ -260,8 +300,11 @@ int build_on_device(const A* pts, const uint32_t* items, uint64_t n, cudaStream_
       return cuda_fail_b(e, "sorting an axis");
   }
 
-  // stems (+inf = no split)
-  if ((e = cudaMalloc(&dt.stems, std::max<size_t>(16, stem_count * sizeof(A)))) != cudaSuccess)
+  // stems (+inf = no split); the tree's arrays come from the stream-ordered
+  // pool, so rebuilding a tree of similar size reuses cached memory
+  dt.pooled = true;
+  if ((e = scratch_alloc(&dt.stems, std::max<size_t>(16, stem_count * sizeof(A)), s)) !=
+      cudaSuccess)
     return cuda_fail_b(e, "stems");
   if (stem_count) {
     k_fill<A><<<blocks_for(stem_count), 256, 0, s>>>(static_cast<A*>(dt.stems), stem_count,
@@ -379,9 +422,9 @@ int build_on_device(const A* pts, const uint32_t* items, uint64_t n, cudaStream_
   }
   dt.leaf_bytes_len = arena_bytes;
   dt.max_leaf_len = max_leaf;
-  if ((e = cudaMalloc(reinterpret_cast<void**>(&dt.arena), std::max<size_t>(16, arena_bytes + 16))) !=
-          cudaSuccess ||
-      (e = cudaMalloc(&dt.extents, std::max<size_t>(16, leaves * 8))) != cudaSuccess)
+  if ((e = scratch_alloc(reinterpret_cast<void**>(&dt.arena), std::max<size_t>(16, arena_bytes + 16),
+                         s)) != cudaSuccess ||
+      (e = scratch_alloc(&dt.extents, std::max<size_t>(16, leaves * 8), s)) != cudaSuccess)
     return cuda_fail_b(e, "tree arrays");
   if ((e = cudaMemsetAsync(dt.arena, 0, arena_bytes + 16, s)) != cudaSuccess)
     return cuda_fail_b(e, "arena");
@@ -396,6 +439,23 @@ int build_on_device(const A* pts, const uint32_t* items, uint64_t n, cudaStream_
   dt.device_bytes = std::max<size_t>(16, stem_count * sizeof(A)) + arena_bytes + 16 + leaves * 8;
   return KGPU_OK;
 }
+
+}  // namespace
+
+cudaError_t convert_leaf_layout(const DeviceTree& dt, const uint8_t* src, uint8_t* dst,
+                                bool to_rows, cudaStream_t s) {
+  if (dt.leaf_count == 0) return cudaSuccess;
+  const unsigned grid = blocks_for(uint64_t(dt.leaf_count) * 32);
+  const uint2* ex = static_cast<const uint2*>(dt.extents);
+  if (to_rows)
+    k_leaf_tiles_to_rows<<<grid, 256, 0, s>>>(src, dst, ex, dt.leaf_count);
+  else
+    k_leaf_rows_to_tiles<<<grid, 256, 0, s>>>(src, dst, ex, dt.leaf_count);
+  g_launches++;
+  return cudaGetLastError();
+}
+
+namespace {
 
 template <typename A>
 int build_any_dims(int K, const void* pts, const uint32_t* items, uint64_t n, cudaStream_t s,
@@ -434,9 +494,7 @@ int32_t kgpu_tree_build(int32_t dtype, uint32_t dims, const void* points, const 
                      : build_any_dims<float>(int(dims), points, items, n, s, t->dt);
   if (st != KGPU_OK) {
     cudaStreamSynchronize(s);
-    cudaFree(t->dt.stems);
-    cudaFree(t->dt.arena);
-    cudaFree(t->dt.extents);
+    release_tree_arrays(t->dt);
     delete t;
     return st;
   }
@@ -452,11 +510,21 @@ int32_t kgpu_tree_read_layout(const kgpu_tree* t, void* stems, uint8_t* leaf_byt
   const size_t sa = dt.dtype == KGPU_F64 ? 8 : 4;
   std::vector<uint32_t> ex(2 * size_t(dt.leaf_count));
   cudaError_t e;
+  // leaves held as rows go back to the reference's tiles first
+  DevBuf tiles;
+  const uint8_t* arena = dt.arena;
+  if (leaf_bytes && dt.leaf_bytes_len && dt.dtype == KGPU_F32 && dt.dims == 3) {
+    if ((e = tiles.alloc(dt.leaf_bytes_len, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(tiles.p, 0, dt.leaf_bytes_len, s)) != cudaSuccess ||
+        (e = convert_leaf_layout(dt, dt.arena, tiles.as<uint8_t>(), false, s)) != cudaSuccess)
+      return cuda_fail_b(e, "reading the layout");
+    arena = tiles.as<uint8_t>();
+  }
   if ((stems && dt.stem_count &&
        (e = cudaMemcpyAsync(stems, dt.stems, dt.stem_count * sa, cudaMemcpyDeviceToHost, s)) !=
            cudaSuccess) ||
       (leaf_bytes && dt.leaf_bytes_len &&
-       (e = cudaMemcpyAsync(leaf_bytes, dt.arena, dt.leaf_bytes_len, cudaMemcpyDeviceToHost, s)) !=
+       (e = cudaMemcpyAsync(leaf_bytes, arena, dt.leaf_bytes_len, cudaMemcpyDeviceToHost, s)) !=
            cudaSuccess) ||
       (dt.leaf_count &&
        (e = cudaMemcpyAsync(ex.data(), dt.extents, ex.size() * 4, cudaMemcpyDeviceToHost, s)) !=

@@ -16,6 +16,11 @@ namespace kgpu {
 // the same caching.
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 
+struct DeviceTree;
+// Frees a tree's stems, arena and extents, from the pool (DeviceTree::pooled)
+// or from cudaMalloc, after the device's pending work.
+void release_tree_arrays(DeviceTree& dt);
+
 // RAII scratch buffer, released on its stream.
 struct DevBuf {
   void* p = nullptr;

@@ -108,11 +108,22 @@ __device__ __forceinline__ void donnelly_children(uint32_t stem, uint32_t minor,
   }
 }
 
+// Leaf encoding on the device.  The reference stores a leaf as tiles of 32,
+// then 8, 4, 2, 1 points, each tile its K coordinate columns then its items
+// (leaf_strategy/vec_of_arenas.rs:292-323).  f32 3-D leaves are held on the
+// device instead as one 16-byte row per point, (x, y, z, item bits), in the
+// same point order: 3 x 4 + 4 bytes per point either way, so every leaf keeps
+// its size and its offset, and a point is one aligned 16-byte load instead of
+// a tile decode and four loads.  The arena is converted on upload and back on
+// read-back; other shapes keep the tiles.
+template <typename A, int K>
+struct RowLeaves : std::integral_constant<bool, std::is_same<A, float>::value && K == 3> {};
+
 // Byte offset inside the leaf, tile width and index in tile of point p of a
 // leaf of `len` points laid out as tiles of 32, then 8, then 4, 2, 1.
 template <typename A, int K>
-__device__ __forceinline__ void tile_slot(uint32_t len, uint32_t p, uint32_t& off, uint32_t& w,
-                                          uint32_t& i) {
+__host__ __device__ __forceinline__ void tile_slot_cols(uint32_t len, uint32_t p, uint32_t& off,
+                                                        uint32_t& w, uint32_t& i) {
   constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
   const uint32_t n32 = len >> 5;
   if (p < (n32 << 5)) {
@@ -141,9 +152,30 @@ __device__ __forceinline__ void tile_slot(uint32_t len, uint32_t p, uint32_t& of
   w = 1; i = 0; off = base;
 }
 
+// The slot of point p in the device encoding: a row is a tile of width 1.
+template <typename A, int K>
+__device__ __forceinline__ void tile_slot(uint32_t len, uint32_t p, uint32_t& off, uint32_t& w,
+                                          uint32_t& i) {
+  if constexpr (RowLeaves<A, K>::value) {
+    off = p * uint32_t(K * sizeof(A) + sizeof(uint32_t));
+    w = 1;
+    i = 0;
+  } else {
+    tile_slot_cols<A, K>(len, p, off, w, i);
+  }
+}
+
 template <typename A, int K>
 __device__ __forceinline__ void load_point(const uint8_t* __restrict__ leaf, uint32_t len,
                                            uint32_t p, A (&c)[K], uint32_t& item) {
+  if constexpr (RowLeaves<A, K>::value) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(leaf) + p);
+    c[0] = v.x;
+    c[1] = v.y;
+    c[2] = v.z;
+    item = __float_as_uint(v.w);
+    return;
+  }
   uint32_t off, w, i;
   tile_slot<A, K>(len, p, off, w, i);
   const A* col = reinterpret_cast<const A*>(leaf + off);

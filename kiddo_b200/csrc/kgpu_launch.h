@@ -22,6 +22,7 @@ struct DeviceTree {
   uint64_t max_leaf_len = 0;
   size_t device_bytes = 0;
   uint32_t bh = 0;             // 0: Eytzinger stems; 3 or 4: Donnelly<bh>
+  bool pooled = false;         // arrays from the stream-ordered pool (device-built trees)
 };
 
 struct QueryLaunch {
@@ -95,5 +96,10 @@ cudaError_t launch_exclusive_scan(const uint64_t* counts, uint64_t* offsets, uin
                                   void* tmp, cudaStream_t s);
 
 int sm_count();
+
+// Re-encodes a tree's leaves between the reference's tiles and the device's
+// rows (RowLeaves); src and dst are arenas laid out by dt's extents.
+cudaError_t convert_leaf_layout(const DeviceTree& dt, const uint8_t* src, uint8_t* dst,
+                                bool to_rows, cudaStream_t s);
 
 }  // namespace kgpu

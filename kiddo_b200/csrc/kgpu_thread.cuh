@@ -35,6 +35,17 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
   constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
   const uint2 ex = __ldg(tv.extents + leaf);
   const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+  if constexpr (RowLeaves<A, K>::value) {
+    // rows: one 16-byte load per point
+    const float4* rows = reinterpret_cast<const float4*>(base);
+    for (uint32_t p = 0; p < ex.y; ++p) {
+      const float4 v = __ldg(rows + p);
+      const A c[K] = {v.x, v.y, v.z};
+      const A d0 = dist(c);
+      if (pass(d0)) f(d0, __float_as_uint(v.w));
+    }
+    return ex.y;
+  }
   uint32_t rem = ex.y;
   uint32_t boff = 0, i = 0;
   uint32_t w = rem >= 32 ? 32 : rem >= 8 ? 8 : rem >= 4 ? 4 : rem >= 2 ? 2 : 1;
@@ -92,6 +103,17 @@ template <typename A, int K, typename D, typename P>
 __device__ __forceinline__ uint32_t leaf_chunk_mask(const uint8_t* __restrict__ base, uint32_t len,
                                                     uint32_t c0, const D& dist, P&& pass) {
   constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
+  if constexpr (RowLeaves<A, K>::value) {
+    const float4* rows = reinterpret_cast<const float4*>(base);
+    const uint32_t end = len < c0 + 32 ? len : c0 + 32;
+    uint32_t mask = 0;
+    for (uint32_t p = c0; p < end; ++p) {
+      const float4 v = __ldg(rows + p);
+      const A c[K] = {v.x, v.y, v.z};
+      mask |= (pass(dist(c)) ? 1u : 0u) << (p - c0);
+    }
+    return mask;
+  }
   const uint32_t full = len & ~31u;
   uint32_t boff, rem;
   if (c0 < full) {
