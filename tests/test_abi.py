@@ -82,6 +82,21 @@ def test_tree_create_rejects_bad_layouts_before_touching_the_device():
         assert C.lib().kgpu_last_error()
 
 
+def test_tree_create_rejects_f32_3d_offsets_off_16_bytes():
+    """f32 3-D leaves take 16 bytes per point, so the reference's leaf offsets
+    are multiples of 16, and the device reads each point as one aligned
+    16-byte row; an offset that is only 8-byte aligned is rejected."""
+    t = kb.ImmutableKdTree.new_from_slice(
+        np.random.default_rng(1).random((1000, 3)).astype(np.float32))
+    ex = t.leaf_extents().astype(np.uint64).copy()
+    assert ex.shape[0] >= 2 and all(int(o) % 16 == 0 for o in ex[:, 0])
+    ex[1, 0] += 8
+    d = _desc_of(t)
+    d.leaf_extents = ex.ctypes.data
+    assert _create(d) == C.KGPU_EINVAL
+    assert b"multiple of 16" in C.lib().kgpu_last_error()
+
+
 def test_layout_build_rejects_bad_arguments():
     L = C.lib()
     h = ctypes.c_void_p()

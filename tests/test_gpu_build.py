@@ -86,3 +86,17 @@ def test_device_build_rejects_overlong_leaves():
     P = np.full((5000, 3), 0.25, dtype=np.float32)
     with pytest.raises(Exception):
         kb.GpuTree.build(torch.from_numpy(P).cuda())
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("dims", [1, 2, 3, 4])
+def test_uploaded_tree_reads_back_the_reference_bytes(dtype, dims):
+    """A tree uploaded from the reference's layout reads back unchanged, also
+    where the device re-encodes the leaves (f32 3-D rows)."""
+    rng = np.random.default_rng(dims)
+    for n in (0, 7, 33, 5000, 100_000):
+        host = kb.ImmutableKdTree.new_from_slice(rng.random((n, dims)).astype(dtype))
+        stems, lb, ex = host.to_gpu().read_layout()
+        assert np.array_equal(lb, host.leaf_bytes())
+        assert np.array_equal(ex, host.leaf_extents())
+        assert np.array_equal(stems.view(np.uint8), host.stems().view(np.uint8))
