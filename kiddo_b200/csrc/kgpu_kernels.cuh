@@ -464,16 +464,16 @@ __global__ void __launch_bounds__(256, FAM == KF_BEST_N ? 3 : KGPU_TFIXED_MIN_BL
     });
   } else if constexpr (FAM == KF_NEAREST_N || !KGPU_BESTN_COOP) {
     // lists in shared-memory columns: entry j of thread t at j * blockDim + t
-    A* list_d = reinterpret_cast<A*>(lists) + threadIdx.x;
-    uint32_t* list_i =
-        reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(lists) + size_t(k) * stride) +
-        threadIdx.x;
     if constexpr (FAM == KF_NEAREST_N) {
-      TNearestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius0);
+      TNearestN<A, K, M, EXCL> pol(lists, stride, k, radius0);
       thread_drive<A, K, M>(tv0, b, radius0, wk, pol, slot, stride, st, [&](uint64_t qi) {
         pol.write(qi, out_d, out_i, out_c, arrival_order != 0);
       });
     } else {
+      A* list_d = reinterpret_cast<A*>(lists) + threadIdx.x;
+      uint32_t* list_i =
+          reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(lists) + size_t(k) * stride) +
+          threadIdx.x;
       TBestN<A, K, M, EXCL> pol(list_d, list_i, stride, k, radius0);
       thread_drive<A, K, M>(tv0, b, radius0, wk, pol, slot, stride, st,
                             [&](uint64_t qi) { pol.write(qi, out_d, out_i, out_c); });

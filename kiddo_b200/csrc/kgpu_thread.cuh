@@ -17,6 +17,8 @@
 // results as the per-level restore/far stacks of the reference.
 #pragma once
 
+#include <type_traits>
+
 #include "kgpu_device.cuh"
 
 namespace kgpu {
@@ -545,53 +547,81 @@ struct TNearestOne {
 template <typename A, int K, typename M, bool kExclusive>
 struct TNearestN {
   static constexpr bool kPruneOnEqual = kExclusive;
-  A* __restrict__ ld;
-  uint32_t* __restrict__ li;
+  // The list sits in shared-memory columns, entry j of thread t at j * stride + t.
+  // For f32 an entry is one 8-byte (distance, item bits) pair, so moving an
+  // entry is one 64-bit load and one 64-bit store; f64 keeps a distance column
+  // and an item column.
+  static constexpr bool kPacked = sizeof(A) == 4;
+  using E = typename std::conditional<kPacked, float2, A>::type;
+  E* __restrict__ le;
+  uint32_t* __restrict__ li;  // f64 items
   int stride;
   int n, k;
   A radius, kth;
-  __device__ TNearestN(A* d, uint32_t* i, int s, int k_, A r)
-      : ld(d), li(i), stride(s), n(0), k(k_), radius(r), kth(inf_of<A>()) {}
+  // `lists` holds k * stride entries (k * stride * (sizeof(A) + 4) bytes)
+  __device__ TNearestN(unsigned char* lists, int s, int k_, A r)
+      : le(reinterpret_cast<E*>(lists) + threadIdx.x),
+        li(reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(lists) + size_t(k_) * s) +
+           threadIdx.x),
+        stride(s), n(0), k(k_), radius(r), kth(inf_of<A>()) {}
   __device__ __forceinline__ void reset(A r) { n = 0; radius = r; kth = inf_of<A>(); }
   __device__ __forceinline__ A max_dist() const { return (n == k && kth < radius) ? kth : radius; }
   __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
 
-  // stable insertion sort of the m held entries
-  __device__ __forceinline__ void sort_held(int m) {
-    for (int a = 1; a < m; ++a) {
-      const A d = ld[a * stride];
-      const uint32_t it = li[a * stride];
-      int j = a;
-      while (j > 0 && ld[(j - 1) * stride] > d) {
-        ld[j * stride] = ld[(j - 1) * stride];
+  __device__ __forceinline__ A dist_at(int j) const {
+    if constexpr (kPacked) return le[j * stride].x;
+    else return le[j * stride];
+  }
+  __device__ __forceinline__ uint32_t item_at(int j) const {
+    if constexpr (kPacked) return __float_as_uint(le[j * stride].y);
+    else return li[j * stride];
+  }
+  __device__ __forceinline__ void put(int j, A d, uint32_t it) {
+    if constexpr (kPacked) {
+      le[j * stride] = make_float2(d, __uint_as_float(it));
+    } else {
+      le[j * stride] = d;
+      li[j * stride] = it;
+    }
+  }
+  // Shifts the entries before position j that are above d one place up and
+  // stores (d, it) in the gap: the stable insertion step (equal distances stay
+  // ahead of the new entry).
+  __device__ __forceinline__ void insert_below(int j, A d, uint32_t it) {
+    if constexpr (kPacked) {
+      while (j > 0) {
+        const float2 e = le[(j - 1) * stride];
+        if (!(e.x > d)) break;
+        le[j * stride] = e;
+        --j;
+      }
+    } else {
+      while (j > 0 && le[(j - 1) * stride] > d) {
+        le[j * stride] = le[(j - 1) * stride];
         li[j * stride] = li[(j - 1) * stride];
         --j;
       }
-      ld[j * stride] = d;
-      li[j * stride] = it;
     }
+    put(j, d, it);
+  }
+
+  // stable insertion sort of the m held entries
+  __device__ __forceinline__ void sort_held(int m) {
+    for (int a = 1; a < m; ++a) insert_below(a, dist_at(a), item_at(a));
   }
 
   __device__ __forceinline__ void add(A d, uint32_t it) {
     if (n < k) {
-      ld[n * stride] = d;
-      li[n * stride] = it;
+      put(n, d, it);
       if (++n == k) {
         sort_held(k);
-        kth = ld[(k - 1) * stride];
+        kth = dist_at(k - 1);
       }
       return;
     }
     if (!(d < kth)) return;
-    int j = k - 1;
-    while (j > 0 && ld[(j - 1) * stride] > d) {
-      ld[j * stride] = ld[(j - 1) * stride];
-      li[j * stride] = li[(j - 1) * stride];
-      --j;
-    }
-    ld[j * stride] = d;
-    li[j * stride] = it;
-    kth = ld[(k - 1) * stride];
+    insert_below(k - 1, d, it);
+    kth = dist_at(k - 1);
   }
 
   // The leaf filter of leaf_view_chunked/nearest_n_within/fallback.rs:37-95
@@ -639,8 +669,8 @@ struct TNearestN {
     A* od = out_d + size_t(qi) * k;
     uint32_t* oi = out_i + size_t(qi) * k;
     for (int j = 0; j < k; ++j) {
-      od[j] = j < n ? ld[j * stride] : inf_of<A>();
-      oi[j] = j < n ? li[j * stride] : 0xffffffffu;
+      od[j] = j < n ? dist_at(j) : inf_of<A>();
+      oi[j] = j < n ? item_at(j) : 0xffffffffu;
     }
     if (out_c) out_c[qi] = uint32_t(n);
   }
