@@ -112,7 +112,7 @@ __device__ __forceinline__ uint32_t leaf_chunk_mask(const uint8_t* __restrict__ 
     for (uint32_t p = c0; p < end; ++p) {
       const float4 v = __ldg(rows + p);
       const A c[K] = {v.x, v.y, v.z};
-      mask |= (pass(dist(c)) ? 1u : 0u) << (p - c0);
+      if (pass(dist(c))) mask |= 1u << (p - c0);
     }
     return mask;
   }
@@ -650,13 +650,38 @@ struct TNearestN {
     const uint32_t len = ex.y;
     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
       uint32_t mask = leaf_chunk_mask<A, K>(base, len, c0, dist, [&](A d) { return d <= gate; });
-      while (mask) {
-        const uint32_t p = c0 + uint32_t(__ffs(mask) - 1);
-        mask &= mask - 1;
-        A c[K];
-        uint32_t it;
-        load_point<A, K>(base, len, p, c, it);
-        add(dist(c), it);
+      if constexpr (RowLeaves<A, K>::value) {
+        // The next candidate's row is requested before the current one is
+        // added, so its load overlaps the insertion (the kernel waits on load
+        // latency more than on issue slots here).
+        const float4* rows = reinterpret_cast<const float4*>(base);
+        if (mask) {
+          uint32_t p = c0 + uint32_t(__ffs(mask) - 1);
+          mask &= mask - 1;
+          float4 v = __ldg(rows + p);
+          for (;;) {
+            const bool more = mask != 0;
+            float4 nv = v;
+            if (more) {
+              p = c0 + uint32_t(__ffs(mask) - 1);
+              mask &= mask - 1;
+              nv = __ldg(rows + p);
+            }
+            const A c[K] = {v.x, v.y, v.z};
+            add(dist(c), __float_as_uint(v.w));
+            if (!more) break;
+            v = nv;
+          }
+        }
+      } else {
+        while (mask) {
+          const uint32_t p = c0 + uint32_t(__ffs(mask) - 1);
+          mask &= mask - 1;
+          A c[K];
+          uint32_t it;
+          load_point<A, K>(base, len, p, c, it);
+          add(dist(c), it);
+        }
       }
     }
     return len;
