@@ -29,7 +29,7 @@ from . import _capi as C
 from ._capi import KiddoGpuError, launch_count
 
 __all__ = ["ImmutableKdTree", "GpuTree", "Forest", "CapturedGraph", "SquaredEuclidean",
-           "Manhattan", "KiddoGpuError", "NearestOneResult", "NearestNResult", "WithinResult",
+           "Manhattan", "Chebyshev", "KiddoGpuError", "NearestOneResult", "NearestNResult", "WithinResult",
            "launch_count"]
 
 
@@ -43,12 +43,20 @@ class Manhattan:
     code = C.MANHATTAN
 
 
+class Chebyshev:
+    """dist/chebyshev/mod.rs:19-59 — the largest per-axis |difference|; not
+    with periodic boundary conditions."""
+    code = C.CHEBYSHEV
+
+
 def _metric_code(m) -> int:
     if m in (SquaredEuclidean, "sqeuclidean", "squared_euclidean"):
         return C.SQUARED_EUCLIDEAN
     if m in (Manhattan, "manhattan"):
         return C.MANHATTAN
-    raise TypeError(f"unsupported metric {m!r} (SquaredEuclidean or Manhattan)")
+    if m in (Chebyshev, "chebyshev"):
+        return C.CHEBYSHEV
+    raise TypeError(f"unsupported metric {m!r} (SquaredEuclidean, Manhattan or Chebyshev)")
 
 
 def _vp(a: np.ndarray):

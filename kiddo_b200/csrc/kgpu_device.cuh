@@ -52,7 +52,39 @@ __device__ __forceinline__ uint32_t shfl_up(uint32_t v, int d) { return __shfl_u
 // ---------------------------------------------------------------------------
 // Metrics (dist/distance_metric_core.rs:12-105)
 // ---------------------------------------------------------------------------
-struct SqEuclidean {
+// Element d of a small register array, read and written without local memory.
+template <typename A, int K>
+__device__ __forceinline__ A sel(const A (&v)[K], int d) {
+  A r = v[0];
+#pragma unroll
+  for (int j = 1; j < K; ++j)
+    if (d == j) r = v[j];
+  return r;
+}
+template <typename A, int K>
+__device__ __forceinline__ void put(A (&v)[K], int d, A x) {
+#pragma unroll
+  for (int j = 0; j < K; ++j)
+    if (d == j) v[j] = x;
+}
+
+// The additive metrics: combine_component is acc + component, and the
+// rectangle distance after one axis offset changes is the O(1) update of
+// rect() (distance_metric_core.rs:38-44, 86-96).  These also run periodic
+// queries.
+template <typename Self>
+struct Additive {
+  static constexpr bool kPeriodic = true;
+  template <typename A> __device__ __forceinline__ static A combine(A acc, A comp) {
+    return add_rn(acc, comp);
+  }
+  template <typename A, int K>
+  __device__ __forceinline__ static A rect_k(A rd, const A (&off)[K], int dim, A new_off) {
+    return Self::template rect<A>(rd, sel(off, dim), new_off);
+  }
+};
+
+struct SqEuclidean : Additive<SqEuclidean> {
   // dist1(a, b) = (a - b)^2   (dist/squared_euclidean/mod.rs:35-38)
   template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
     const A d = sub_rn(a, b);
@@ -64,7 +96,7 @@ struct SqEuclidean {
   }
 };
 
-struct Manhattan {
+struct Manhattan : Additive<Manhattan> {
   // |a - b|   (dist/manhattan/mod.rs:35-38)
   template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
     return abs_val(sub_rn(a, b));
@@ -72,6 +104,28 @@ struct Manhattan {
   // (rd - old) + new   (dist/manhattan/mod.rs:40-48)
   template <typename A> __device__ __forceinline__ static A rect(A rd, A old_off, A new_off) {
     return add_rn(sub_rn(rd, old_off), new_off);
+  }
+};
+
+// Chebyshev / L-infinity (dist/chebyshev/mod.rs:19-59): dist1 = |a - b|,
+// combine_component keeps the larger value (a component that is not greater,
+// NaN included, leaves the accumulator as it is), and the rectangle distance
+// is re-scanned from zero over every axis offset, the changed axis taking its
+// new offset.  Periodic queries take the additive metrics only.
+struct Chebyshev {
+  static constexpr bool kPeriodic = false;
+  template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
+    return abs_val(sub_rn(a, b));
+  }
+  template <typename A> __device__ __forceinline__ static A combine(A acc, A comp) {
+    return comp > acc ? comp : acc;
+  }
+  template <typename A, int K>
+  __device__ __forceinline__ static A rect_k(A, const A (&off)[K], int dim, A new_off) {
+    A acc = A(0);
+#pragma unroll
+    for (int d = 0; d < K; ++d) acc = combine(acc, d == dim ? new_off : off[d]);
+    return acc;
   }
 };
 
@@ -189,10 +243,18 @@ __device__ __forceinline__ void load_point(const uint8_t* __restrict__ leaf, uin
 // exact and is left out.
 template <typename M, typename A, int K>
 __device__ __forceinline__ A point_dist(const A (&c)[K], const A (&q)[K]) {
-  A acc = M::template dist1<A>(c[0], q[0]);
+  if constexpr (M::kPeriodic) {
+    A acc = M::template dist1<A>(c[0], q[0]);
 #pragma unroll
-  for (int d = 1; d < K; ++d) acc = add_rn(acc, M::template dist1<A>(c[d], q[d]));
-  return acc;
+    for (int d = 1; d < K; ++d) acc = M::combine(acc, M::template dist1<A>(c[d], q[d]));
+    return acc;
+  } else {
+    // from zero: the first component is combined like the others
+    A acc = A(0);
+#pragma unroll
+    for (int d = 0; d < K; ++d) acc = M::combine(acc, M::template dist1<A>(c[d], q[d]));
+    return acc;
+  }
 }
 
 // Packed pairs of f32 (sm_100 f32x2 arithmetic): each half of a packed sub or
@@ -264,20 +326,6 @@ struct PeriodicDist {
   }
 };
 
-template <typename A, int K>
-__device__ __forceinline__ A sel(const A (&v)[K], int d) {
-  A r = v[0];
-#pragma unroll
-  for (int j = 1; j < K; ++j)
-    if (d == j) r = v[j];
-  return r;
-}
-template <typename A, int K>
-__device__ __forceinline__ void put(A (&v)[K], int d, A x) {
-#pragma unroll
-  for (int j = 0; j < K; ++j)
-    if (d == j) v[j] = x;
-}
 
 // ---------------------------------------------------------------------------
 // The arithmetic traversal, one warp per query.
@@ -321,7 +369,7 @@ __device__ __forceinline__ void warp_arith_query(const TreeView<A>& tv, const A 
         const A qd = sel(q, dim);
         const bool is_right = qd >= pivot;
         const A new_off = abs_val(sub_rn(qd, pivot));
-        const A rd_far = M::template rect<A>(rd, oo, new_off);
+        const A rd_far = M::template rect_k<A, K>(rd, off, dim, new_off);
         const bool cand = !check_bound || !(rd_far > pol.max_dist());
         if (lane == level) { s_old = oo; s_far = new_off; s_rd = rd_far; }
         has_far = cand ? (has_far | bit) : (has_far & ~bit);

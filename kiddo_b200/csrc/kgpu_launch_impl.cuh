@@ -49,6 +49,7 @@ inline cudaError_t with_dims(int dims, F&& f) {
 template <typename F>
 inline cudaError_t with_metric(int metric, F&& f) {
   if (metric == KGPU_MANHATTAN) return f(Manhattan());
+  if (metric == KGPU_CHEBYSHEV) return f(Chebyshev());
   return f(SqEuclidean());
 }
 
@@ -100,8 +101,10 @@ cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
       using M = decltype(m);
       return with_excl(q.exclusive, [&](auto ex) {
         constexpr bool EX = decltype(ex)::value;
-        if (q.periodic) {
-          const BoxArg<A, K> box = make_box<A, K>(q);
+        if constexpr (!M::kPeriodic) {
+          if (q.periodic) return cudaErrorInvalidValue;  // rejected by the entry points
+        } else if (q.periodic) {
+          const auto box = make_box<A, K>(q);
           auto runp = [&](auto kern) {
             const int grid = grid_for(kern, 0, q.nq);
             kern<<<grid, 256, 0, q.stream>>>(tv, b, box, q.k, radius, static_cast<A*>(q.out_d),
@@ -164,7 +167,8 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
         using M = decltype(m);
         return with_excl(q.exclusive, [&](auto ex) {
           constexpr bool EX = decltype(ex)::value;
-          if (STEMS == 0 && q.periodic) {
+          if (!M::kPeriodic && q.periodic) return cudaErrorInvalidValue;
+          if constexpr (M::kPeriodic) if (STEMS == 0 && q.periodic) {
             // periodic nearest_n: per-thread walk, cooperative leaf scans,
             // lists in the output rows
             const auto box = make_box<A, K>(q);
@@ -225,7 +229,8 @@ cudaError_t launch_within_pass_stems(const DeviceTree& t, const QueryLaunch& q, 
       using M = decltype(m);
       return with_excl(q.exclusive, [&](auto ex) -> cudaError_t {
         constexpr bool EX = decltype(ex)::value;
-        if constexpr (thread_engine_dims(K)) {
+        if (!M::kPeriodic && q.periodic) return cudaErrorInvalidValue;
+        if constexpr (thread_engine_dims(K) && M::kPeriodic) {
           if (q.periodic && q.engine != 1) {
             const auto box = make_box<A, K>(q);
             const size_t smem = thread_smem<A>(t);
@@ -239,8 +244,8 @@ cudaError_t launch_within_pass_stems(const DeviceTree& t, const QueryLaunch& q, 
             return cudaGetLastError();
           }
         }
-        if (q.periodic) {
-          const BoxArg<A, K> box = make_box<A, K>(q);
+        if constexpr (M::kPeriodic) if (q.periodic) {
+          const auto box = make_box<A, K>(q);
           if (!offsets) {
             auto kern = k_periodic_within_count<A, K, M, EX>;
             kern<<<grid_for(kern, 0, q.nq), 256, 0, q.stream>>>(tv, b, box, radius, counts,

@@ -197,7 +197,7 @@ struct ThreadWalk {
         const A qd = sel(q, dim);
         const bool is_right = qd >= pivot;
         const A new_off = abs_val(sub_rn(qd, pivot));
-        const A rd_far = M::template rect<A>(rd, sel(off, dim), new_off);
+        const A rd_far = M::template rect_k<A, K>(rd, off, dim, new_off);
         if (!check_bound || !(rd_far > pol.max_dist())) {
           slot[level * stride] = rd_far;
           pending |= 1u << level;
@@ -297,7 +297,7 @@ struct DonnellyWalk {
         const A qd = sel(q, dim);
         const bool is_right = qd >= pivot;
         const A new_off = abs_val(sub_rn(qd, pivot));
-        const A rd_far = M::template rect<A>(rd, sel(off, dim), new_off);
+        const A rd_far = M::template rect_k<A, K>(rd, off, dim, new_off);
         if (!(rd_far > best)) {
           const int fl = level + 1;
           slot[fl * stride] = rd_far;
@@ -500,6 +500,17 @@ struct CartesianQ {
   // Both points of an f32 pair (v[d] = {axis d of point 0, of point 1}):
   // dist1 packed, the sum scalar in the order of point_dist.
   __device__ __forceinline__ void pair(const float2 (&v)[K], float& d0, float& d1) const {
+    if constexpr (!M::kPeriodic) {
+      float c0[K], c1[K];
+#pragma unroll
+      for (int d = 0; d < K; ++d) {
+        c0[d] = v[d].x;
+        c1[d] = v[d].y;
+      }
+      d0 = point_dist<M, float, K>(c0, q);
+      d1 = point_dist<M, float, K>(c1, q);
+      return;
+    }
     float a0 = 0.f, a1 = 0.f;
 #pragma unroll
     for (int d = 0; d < K; ++d) {

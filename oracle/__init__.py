@@ -26,7 +26,7 @@ FAM_PERIODIC_NEAREST_N = 5
 FAM_WITHIN = 10
 FAM_PERIODIC_WITHIN = 11
 
-METRICS = {"sqeuclidean": 0, "manhattan": 1}
+METRICS = {"sqeuclidean": 0, "manhattan": 1, "chebyshev": 2}
 
 
 def build_library(force: bool = False) -> str:
@@ -65,6 +65,8 @@ def lib():
         L.kor_query_radius.restype = vp
         L.kor_query_radius.argtypes = [vp, i32, i32, vp, u64, ctypes.c_double, i32, i32, vp, i32, vp]
         L.kor_donnelly_path.argtypes = [ctypes.c_uint32, vp, u64, vp]
+        L.kor_metric_f64x3.restype = i32
+        L.kor_metric_f64x3.argtypes = [i32, vp, vp, ctypes.c_double, vp, i32, ctypes.c_double, vp]
         L.kor_radius_total.restype = u64
         L.kor_radius_total.argtypes = [vp]
         L.kor_radius_copy.argtypes = [vp, vp, vp, vp]
@@ -239,3 +241,17 @@ def donnelly_path(bh, bits):
     out = np.zeros(3, dtype=np.uint32)
     lib().kor_donnelly_path(int(bh), _ptr(b) if b.size else None, b.size, _ptr(out))
     return int(out[0]), (int(out[1]), int(out[2]))
+
+
+def metric_f64x3(metric, a, b, rd, off, dim, new_off):
+    """(dist(a, b), rect_dist_after_update(rd, off, dim, new_off)) of `metric`
+    for f64 3-D points, the arithmetic the traversal uses."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    off = np.ascontiguousarray(off, dtype=np.float64)
+    out = np.zeros(2)
+    rc = lib().kor_metric_f64x3(METRICS[metric], _ptr(a), _ptr(b), float(rd), _ptr(off), int(dim),
+                                float(new_off), _ptr(out))
+    if rc != 0:
+        raise ValueError(f"unknown metric {metric}")
+    return float(out[0]), float(out[1])

@@ -383,7 +383,19 @@ Tree<A, K> build(const A* pts, const uint32_t* items, size_t n, uint32_t bh = 0)
 // dist/squared_euclidean/mod.rs:21-40, dist/manhattan/mod.rs:21-48,
 // traits/axis.rs:82-139)
 // ---------------------------------------------------------------------------
-struct SqEuclidean {
+// The additive metrics: combine_component is acc += component, and the
+// rectangle distance after one axis offset changes is the O(1) update
+// (rd - dist1(old, 0)) + dist1(new, 0) (distance_metric_core.rs:86-96).
+template <typename Self>
+struct Additive {
+  static constexpr bool kPeriodic = true;  // restated for periodic queries
+  template <typename A> static A combine(A acc, A component) { return acc + component; }
+  template <typename A, int K>
+  static A rect_k(A rd, const A* off, int dim, A new_off) {
+    return Self::rect_after_update(rd, off[dim], new_off);
+  }
+};
+struct SqEuclidean : Additive<SqEuclidean> {
   template <typename A> static A dist1(A a, A b) { A d = a - b; return d * d; }
   template <typename A> static A rect_after_update(A rd, A old_off, A new_off) {
     A new1 = dist1(new_off, A(0));
@@ -391,18 +403,36 @@ struct SqEuclidean {
     return (rd - old1) + new1;
   }
 };
-struct Manhattan {
+struct Manhattan : Additive<Manhattan> {
   template <typename A> static A dist1(A a, A b) { return std::fabs(a - b); }
   template <typename A> static A rect_after_update(A rd, A old_off, A new_off) {
     return (rd - old_off) + new_off;
   }
 };
+// Chebyshev / L-infinity (dist/chebyshev/mod.rs:19-59): dist1 = |a - b|
+// (Axis::saturating_dist), combine_component keeps the larger value (a
+// component that is not greater, NaN included, leaves acc unchanged), and the
+// rectangle distance is re-scanned from zero over every axis offset, the
+// changed axis taking its new offset.
+struct Chebyshev {
+  static constexpr bool kPeriodic = false;  // periodic queries are restated for + metrics only
+  template <typename A> static A dist1(A a, A b) { return std::fabs(a - b); }
+  template <typename A> static A combine(A acc, A component) {
+    return component > acc ? component : acc;
+  }
+  template <typename A, int K>
+  static A rect_k(A, const A* off, int dim, A new_off) {
+    A acc = A(0);
+    for (int axis = 0; axis < K; ++axis) acc = combine(acc, axis == dim ? new_off : off[axis]);
+    return acc;
+  }
+};
 
-// combine_component: acc += dist1(point, query), left to right from zero.
+// combine_component over dist1(point, query), left to right from zero.
 template <typename M, typename A, int K>
 inline A point_dist(const A* c, const A* q) {
   A acc = A(0);
-  for (int d = 0; d < K; ++d) acc += M::template dist1<A>(c[d], q[d]);
+  for (int d = 0; d < K; ++d) acc = M::combine(acc, M::template dist1<A>(c[d], q[d]));
   return acc;
 }
 
@@ -452,7 +482,7 @@ void arithmetic_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_
         const uint32_t far_idx = stem_idx * 2 + (is_right ? 0u : 1u);
         const A new_off = std::fabs(qd - pivot);  // Axis::saturating_dist
         const A old_off = off[dim];
-        const A rd_far = M::rect_after_update(rd, old_off, new_off);
+        const A rd_far = M::template rect_k<A, K>(rd, off, dim, new_off);
         bool far_is_candidate = true;
         if (check_bound) far_is_candidate = !(rd_far > ctx.max_dist());
         if (far_is_candidate) {
@@ -549,7 +579,7 @@ void scalar_backtracking_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&&
         const bool is_right = q[dim] >= pivot;
         DonnellyCursor<K> far = s.branch_relative(is_right);
         const A new_off = std::fabs(q[dim] - pivot);  // Axis::saturating_dist
-        const A rd_far = M::rect_after_update(rd, off[dim], new_off);
+        const A rd_far = M::template rect_k<A, K>(rd, off, dim, new_off);
         if (!(rd_far > best)) stack.push_back({far, dim, new_off, rd_far});
       } else {
         s.traverse(false);

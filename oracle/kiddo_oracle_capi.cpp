@@ -100,9 +100,11 @@ int query_fixed_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq
         break;
       }
       case FAM_PERIODIC_NEAREST_ONE: {
-        auto r = periodic_nearest_one<A, K, M>(t, q, box, sp);
-        out_d[qi] = r.first; out_i[qi] = r.second;
-        if (out_c) out_c[qi] = 1;
+        if constexpr (M::kPeriodic) {
+          auto r = periodic_nearest_one<A, K, M>(t, q, box, sp);
+          out_d[qi] = r.first; out_i[qi] = r.second;
+          if (out_c) out_c[qi] = 1;
+        }
         break;
       }
       case FAM_NEAREST_N:
@@ -113,7 +115,7 @@ int query_fixed_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq
           h = nearest_n_within<A, K, M>(t, q, radius, k, exclusive, sorted, sp);
         else if (family == FAM_BEST_N_WITHIN)
           h = best_n_within<A, K, M>(t, q, radius, k, exclusive, sp);
-        else
+        else if constexpr (M::kPeriodic)
           h = periodic_nearest<A, K, M>(t, q, box, radius, k, exclusive, sorted, sp);
         for (uint32_t j = 0; j < k; ++j) {
           if (j < h.size()) {
@@ -153,7 +155,7 @@ RadiusResult* query_radius_t(const Tree<A, K>& t, int family, const A* queries, 
     const A* q = queries + qi * K;
     if (family == FAM_WITHIN)
       per[qi] = within<A, K, M>(t, q, radius, exclusive, sorted, sp);
-    else
+    else if constexpr (M::kPeriodic)
       per[qi] = periodic_nearest<A, K, M>(t, q, box, radius, 0, exclusive, sorted, sp);
     if (want_stats) acc.add(s);
   });
@@ -305,7 +307,8 @@ void kor_copy_layout(void* hp, void* stems_out, uint8_t* bytes_out, uint64_t* ex
   });
 }
 
-// metric: 0 SquaredEuclidean, 1 Manhattan.  Outputs are dense [nq * k]
+// metric: 0 SquaredEuclidean, 1 Manhattan, 2 Chebyshev (not periodic: -2 /
+// nullptr).  Outputs are dense [nq * k]
 // (k = 1 for the nearest-one families); unused slots hold +inf / 0xFFFFFFFF.
 int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint64_t nq,
                     uint32_t k, double radius, int exclusive, int sorted, const void* box,
@@ -325,6 +328,13 @@ int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint6
                                               r, exclusive, sorted,
                                               static_cast<const A*>(box), static_cast<A*>(out_d),
                                               out_i, out_c, nthreads, stats3);
+    if (metric == 2) {
+      if (family == FAM_PERIODIC_NEAREST_ONE || family == FAM_PERIODIC_NEAREST_N) return -2;
+      return query_fixed_t<A, K, Chebyshev>(t, family, static_cast<const A*>(queries), nq, k, r,
+                                            exclusive, sorted, static_cast<const A*>(box),
+                                            static_cast<A*>(out_d), out_i, out_c, nthreads,
+                                            stats3);
+    }
     return query_fixed_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, k, r,
                                           exclusive, sorted, static_cast<const A*>(box),
                                           static_cast<A*>(out_d), out_i, out_c, nthreads,
@@ -346,10 +356,32 @@ void* kor_query_radius(void* hp, int family, int metric, const void* queries, ui
       return query_radius_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, r,
                                                exclusive, sorted, static_cast<const A*>(box),
                                                nthreads, stats3);
+    if (metric == 2) {
+      if (family == FAM_PERIODIC_WITHIN) return nullptr;
+      return query_radius_t<A, K, Chebyshev>(t, family, static_cast<const A*>(queries), nq, r,
+                                             exclusive, sorted, static_cast<const A*>(box),
+                                             nthreads, stats3);
+    }
     return query_radius_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, r,
                                            exclusive, sorted, static_cast<const A*>(box),
                                            nthreads, stats3);
   });
+}
+
+// Test hook for the metric arithmetic (f64, K = 3): out[0] = dist(a, b),
+// out[1] = rect_dist_after_update(rd, off, dim, new_off).
+int kor_metric_f64x3(int metric, const double* a, const double* b, double rd, const double* off,
+                     int dim, double new_off, double* out) {
+  auto run = [&](auto m) {
+    using M = decltype(m);
+    out[0] = point_dist<M, double, 3>(a, b);
+    out[1] = M::template rect_k<double, 3>(rd, off, dim, new_off);
+    return 0;
+  };
+  if (metric == 0) return run(SqEuclidean());
+  if (metric == 1) return run(Manhattan());
+  if (metric == 2) return run(Chebyshev());
+  return -1;
 }
 
 // Test hook for the Donnelly index math: walks `n` path bits from the root of

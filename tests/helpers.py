@@ -35,7 +35,11 @@ def brute_dists(points, q, metric="sqeuclidean"):
     acc = np.zeros(P.shape[0], dtype=P.dtype)
     for d in range(P.shape[1]):
         diff = (P[:, d] - q[d]).astype(P.dtype)
-        acc = (acc + (diff * diff if metric == "sqeuclidean" else np.abs(diff))).astype(P.dtype)
+        if metric == "chebyshev":
+            comp = np.abs(diff)
+            acc = np.where(comp > acc, comp, acc).astype(P.dtype)
+        else:
+            acc = (acc + (diff * diff if metric == "sqeuclidean" else np.abs(diff))).astype(P.dtype)
     return acc
 
 

@@ -36,13 +36,14 @@ def _pair(P, bh, items=None):
 
 
 def _metric(m):
-    return kb.SquaredEuclidean if m == "sqeuclidean" else kb.Manhattan
+    return {"sqeuclidean": kb.SquaredEuclidean, "manhattan": kb.Manhattan,
+            "chebyshev": kb.Chebyshev}[m]
 
 
 @pytest.mark.parametrize("bh", [3, 4])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("dims", [2, 3])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
 @pytest.mark.parametrize("data", ["uniform", "quantized", "clustered"])
 def test_fixed_families_donnelly(bh, dtype, dims, metric, data):
     rng = np.random.default_rng(zlib.crc32(f"don{bh}{dims}{metric}{data}".encode()))
@@ -56,7 +57,7 @@ def test_fixed_families_donnelly(bh, dtype, dims, metric, data):
     g = t.query(Q).nearest_one(M).approx().execute_gpu()
     od, oi = o.approx_nearest_one(Q, metric=metric)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "approx")
-    r = 0.001 if metric == "sqeuclidean" else 0.03
+    r = {"sqeuclidean": 0.001, "manhattan": 0.03, "chebyshev": 0.015}[metric]
     for k in (1, 5, 16, 32):
         g = t.query(Q).nearest_n(M, k).execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, k, metric=metric),
@@ -83,15 +84,16 @@ def test_fixed_families_donnelly(bh, dtype, dims, metric, data):
 
 @pytest.mark.parametrize("bh", [3, 4])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
 def test_within_families_donnelly(bh, dtype, metric):
     rng = np.random.default_rng(17 + bh)
     P = DATASETS["uniform"](rng, 30000, 3, dtype)
     Q = DATASETS["uniform"](rng, 2000, 3, dtype)
     t, o = _pair(P, bh)
     M = _metric(metric)
-    cases = ((1e-5, 2000), (3e-4, 2000), (4e-3, 2000), (0.15, 120)) if metric == "sqeuclidean" \
-        else ((0.005, 2000), (0.04, 2000), (0.2, 2000), (0.6, 120))
+    cases = {"sqeuclidean": ((1e-5, 2000), (3e-4, 2000), (4e-3, 2000), (0.15, 120)),
+             "manhattan": ((0.005, 2000), (0.04, 2000), (0.2, 2000), (0.6, 120)),
+             "chebyshev": ((0.003, 2000), (0.03, 2000), (0.1, 2000), (0.3, 120))}[metric]
     for r, nq in cases:
         Qr = Q[:nq]
         for excl in (False, True):

@@ -24,7 +24,8 @@ def _pair(P, items=None):
 
 
 def _metric(m):
-    return kb.SquaredEuclidean if m == "sqeuclidean" else kb.Manhattan
+    return {"sqeuclidean": kb.SquaredEuclidean, "manhattan": kb.Manhattan,
+            "chebyshev": kb.Chebyshev}[m]
 
 
 DATASETS = {
@@ -41,7 +42,7 @@ ENGINES = [None, "warp", "thread"]
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("dims", [2, 3])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
 @pytest.mark.parametrize("data", ["uniform", "quantized", "clustered"])
 def test_fixed_families(dtype, dims, metric, data, engine):
     rng = np.random.default_rng(zlib.crc32(f"{dims}{metric}{data}".encode()))
@@ -59,7 +60,7 @@ def test_fixed_families(dtype, dims, metric, data, engine):
     od, oi = o.approx_nearest_one(Q, metric=metric)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "approx")
     # nearest_n, sorted and unsorted, and .within
-    r = 0.001 if metric == "sqeuclidean" else 0.03
+    r = {"sqeuclidean": 0.001, "manhattan": 0.03, "chebyshev": 0.015}[metric]
     for k in (1, 5, 16, 32):
         g = t.query(Q).with_engine(engine).nearest_n(M, k).execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, k, metric=metric),
@@ -87,7 +88,7 @@ def test_fixed_families(dtype, dims, metric, data, engine):
 
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
 @pytest.mark.parametrize("data", ["uniform", "quantized"])
 def test_within_families(dtype, metric, data, engine):
     rng = np.random.default_rng(11)
@@ -97,8 +98,9 @@ def test_within_families(dtype, metric, data, engine):
     M = _metric(metric)
     # radii giving 0 .. ~7000 hits per query, so every segment-sort path runs
     # (one warp <= 32, shared memory <= 4096, global memory above)
-    cases = ((1e-5, 2000), (3e-4, 2000), (4e-3, 2000), (0.15, 120)) if metric == "sqeuclidean" \
-        else ((0.005, 2000), (0.04, 2000), (0.2, 2000), (0.6, 120))
+    cases = {"sqeuclidean": ((1e-5, 2000), (3e-4, 2000), (4e-3, 2000), (0.15, 120)),
+             "manhattan": ((0.005, 2000), (0.04, 2000), (0.2, 2000), (0.6, 120)),
+             "chebyshev": ((0.003, 2000), (0.03, 2000), (0.1, 2000), (0.3, 120))}[metric]
     for r, nq in cases:
         Qr = Q[:nq]
         for excl in (False, True):

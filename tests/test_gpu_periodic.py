@@ -95,3 +95,15 @@ def test_periodic_rejections():
     q = np.zeros((1, 3))
     with pytest.raises(TypeError):
         t.query(q).periodic_boundary_condition(np.ones(3)).nearest_one(kb.SquaredEuclidean).approx()
+
+
+def test_periodic_rejects_chebyshev():
+    """Periodic queries take the additive metrics (SquaredEuclidean,
+    Manhattan); a Chebyshev periodic query is refused with a status."""
+    rng = np.random.default_rng(3)
+    t = kb.ImmutableKdTree.new_from_slice(rng.random((2000, 3)))
+    Q = rng.random((10, 3))
+    with pytest.raises(kb.KiddoGpuError):
+        t.query(Q).periodic_boundary_condition(np.ones(3)).nearest_one(kb.Chebyshev).execute_gpu()
+    with pytest.raises(kb.KiddoGpuError):
+        t.query(Q).periodic_boundary_condition(np.ones(3)).within(kb.Chebyshev, 0.01).execute_gpu()

@@ -71,8 +71,23 @@ def test_oracle_known_answers(kat):
         verify(kat, chk, d, i)
 
 
+def test_metric_known_answers():
+    """The reference's metric unit tests (dist/mod.rs:1436-1490): point
+    distances and the rectangle update of each metric, f64 3-D."""
+    a, b = [1.0, 2.0, 3.0], [4.0, 2.0, -1.0]
+    assert oracle.metric_f64x3("sqeuclidean", a, b, 0, [0, 0, 0], 0, 0)[0] == 25.0
+    assert oracle.metric_f64x3("manhattan", a, b, 0, [0, 0, 0], 0, 0)[0] == 7.0
+    assert oracle.metric_f64x3("manhattan", a, b, 7.0, [0.0, 2.0, 5.0], 1, 4.0)[1] == 9.0
+    assert oracle.metric_f64x3("chebyshev", a, [4.0, 2.5, -1.0], 0, [0, 0, 0], 0, 0)[0] == 4.0
+    # Chebyshev re-scans every offset, the changed axis taking its new one
+    assert oracle.metric_f64x3("chebyshev", a, b, 5.0, [0.0, 2.0, 5.0], 2, 1.0)[1] == 2.0
+    assert oracle.metric_f64x3("chebyshev", a, b, 5.0, [0.0, 2.0, 5.0], 0, 6.0)[1] == 6.0
+    # a NaN component is not greater than the accumulator, so it is passed over
+    assert oracle.metric_f64x3("chebyshev", [np.nan, 2.0, 3.0], b, 0, [0, 0, 0], 0, 0)[0] == 4.0
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
 @pytest.mark.parametrize("n", [1, 31, 33, 1000, 20000])
 def test_oracle_vs_brute_force(dtype, metric, n):
     rng = np.random.default_rng(n)
@@ -82,7 +97,8 @@ def test_oracle_vs_brute_force(dtype, metric, n):
     d1, i1 = t.nearest_one(Q, metric=metric)
     k = 8
     dn, inn, cn = t.nearest_n(Q, k, metric=metric)
-    r = np.asarray(0.02 if metric == "sqeuclidean" else 0.2, dtype=dtype)
+    r = np.asarray({"sqeuclidean": 0.02, "manhattan": 0.2, "chebyshev": 0.08}[metric],
+                   dtype=dtype)
     off, dw, iw = t.within(Q, float(r), metric=metric)
     bd_, bi_, bc_ = t.best_n_within(Q, float(r), 5, metric=metric)
     for j in range(len(Q)):
