@@ -659,6 +659,11 @@ struct TNearestN {
     const uint2 ex = __ldg(tv.extents + l);
     const uint8_t* base = tv.arena + size_t(ex.x) * 8;
     const uint32_t len = ex.y;
+    // every 128-byte line of the leaf's rows requested up front, so the scan's
+    // one-row-per-step loads find them in L1
+    if constexpr (RowLeaves<A, K>::value)
+      for (uint32_t b = 0; b < len * 16u; b += 128u)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(base + b));
     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
       uint32_t mask = leaf_chunk_mask<A, K>(base, len, c0, dist, [&](A d) { return d <= gate; });
       if constexpr (RowLeaves<A, K>::value) {
