@@ -472,6 +472,9 @@ int out_width(const kgpu_query_desc* d) {
 #ifndef KGPU_HOST_CHUNK_LOG2
 #define KGPU_HOST_CHUNK_LOG2 21
 #endif
+#ifndef KGPU_HOST_EDGE_DIV
+#define KGPU_HOST_EDGE_DIV 8
+#endif
 // Host buffers: the batch goes through in 2M-query chunks on three internal
 // streams, each with its own device buffers, so the copy of one chunk's
 // queries in, another chunk's kernel and a third chunk's results out run at
@@ -508,10 +511,23 @@ int query_host_pipelined(const DeviceTree& dt, const kgpu_query_desc* d, const Q
         status = e == cudaErrorMemoryAllocation ? set_error(KGPU_ENOMEM, "device allocation failed")
                                                 : cuda_fail(e, "cudaMallocAsync");
     }
-    for (uint64_t c0 = 0, ci = 0; c0 < nq && status == KGPU_OK; c0 += chunk, ++ci) {
+    // The first and the last chunk are short (an eighth of a chunk): the first
+    // chunk's kernel runs before any result can leave, and the last chunk's
+    // results leave after every kernel, so shorter ends shorten the
+    // unoverlapped head and tail (kNN16 over 16M queries: 50.9 -> 47.1 ms).
+    const uint64_t edge = std::max<uint64_t>(1, chunk / KGPU_HOST_EDGE_DIV);
+    auto chunk_len = [&](uint64_t c0) -> uint64_t {
+      const uint64_t rem = nq - c0;
+      if (nslots == 1 || rem <= edge) return rem;
+      if (c0 == 0) return edge;
+      if (rem <= chunk + edge) return rem - edge;
+      return chunk;
+    };
+    uint64_t nc = 0;
+    for (uint64_t c0 = 0, ci = 0; c0 < nq && status == KGPU_OK; c0 += nc, ++ci) {
       const int slot = int(ci % nslots);
       cudaStream_t ss = st[slot];
-      const uint64_t nc = std::min(chunk, nq - c0);
+      nc = chunk_len(c0);
       QueryLaunch q = base;
       q.nq = nc;
       q.queries = bq[slot].p;

@@ -38,8 +38,10 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
   const uint2 ex = __ldg(tv.extents + leaf);
   const uint8_t* base = tv.arena + size_t(ex.x) * 8;
   if constexpr (RowLeaves<A, K>::value) {
-    // rows: one 16-byte load per point
+    // rows: one 16-byte load per point, the leaf's lines requested up front
     const float4* rows = reinterpret_cast<const float4*>(base);
+    for (uint32_t b = 0; b < ex.y * 16u; b += 128u)
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(base + b));
     for (uint32_t p = 0; p < ex.y; ++p) {
       const float4 v = __ldg(rows + p);
       const A c[K] = {v.x, v.y, v.z};
