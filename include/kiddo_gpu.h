@@ -107,6 +107,23 @@ typedef struct kgpu_tree_desc {
   uint64_t max_leaf_len;
 } kgpu_tree_desc;
 
+/* A FlatVec tree (src/leaf_strategy/flat_vec.rs:20-26). */
+typedef struct kgpu_flatvec_desc {
+  uint32_t abi_version;      /* KGPU_ABI_VERSION */
+  int32_t dtype;             /* kgpu_dtype of the axis type A */
+  uint32_t dims;             /* K, 1..4 */
+  int32_t stem_strategy;     /* kgpu_stem_strategy */
+  uint32_t block_height;     /* Donnelly BH; 0 for Eytzinger */
+  int32_t max_stem_level;    /* KdTree::max_stem_level, -1 for a stemless tree */
+  const void* stems;         /* stem_count values of type A */
+  uint64_t stem_count;
+  const void* columns[4];    /* leaf_points: `dims` arrays of `size` values of A */
+  const uint32_t* items;     /* leaf_items: `size` values */
+  const uint32_t* extents;   /* leaf_extents: leaf_count (start, end) pairs, in points */
+  uint64_t leaf_count;
+  uint64_t size;             /* number of points */
+} kgpu_flatvec_desc;
+
 typedef struct kgpu_query_desc {
   uint32_t abi_version;   /* KGPU_ABI_VERSION */
   int32_t family;         /* kgpu_family */
@@ -156,6 +173,13 @@ int32_t kgpu_layout_free(kgpu_layout* layout);
  * current CUDA device.  Stems and arena bytes are copied unchanged; extents
  * are re-encoded as 32-bit (offset / 8, len) pairs. */
 int32_t kgpu_tree_create(const kgpu_tree_desc* desc, void* stream, kgpu_tree** out);
+/* Uploads a tree whose leaves use the FlatVec strategy (KdTree<A, u32, SS,
+ * FlatVec<A, u32, K, 32>, K, 32>, src/leaf_strategy/flat_vec.rs:20-26): its
+ * stems as in kgpu_tree_desc, its K point columns, items and (start, end)
+ * leaf extents.  The leaves are re-encoded on the host in the VecOfArenas
+ * tiles (same points, same order per leaf) and uploaded as kgpu_tree_create
+ * does, so every query family runs on it unchanged. */
+int32_t kgpu_tree_create_flatvec(const kgpu_flatvec_desc* desc, void* stream, kgpu_tree** out);
 int32_t kgpu_tree_destroy(kgpu_tree* tree);
 /* Builds the ImmutableKdTree of `n` points on the current device: `points` (n rows
  * of `dims` values of `dtype`) and `items` (NULL: item = source index) are DEVICE

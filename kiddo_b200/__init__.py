@@ -243,6 +243,45 @@ class GpuTree:
         self._h = h
 
     @classmethod
+    def from_flatvec(cls, stems, leaf_points, leaf_items, leaf_extents, max_stem_level,
+                     block_height=0, stream=None) -> "GpuTree":
+        """A tree whose leaves use the FlatVec strategy
+        (src/leaf_strategy/flat_vec.rs:20-26): `stems` in the stem order of the
+        strategy (Eytzinger, or Donnelly<block_height>), `leaf_points` the K
+        point columns ([K, n] or K arrays), `leaf_items` n uint32 values and
+        `leaf_extents` one (start, end) pair of point indices per leaf
+        (kgpu_tree_create_flatvec)."""
+        cols = [np.ascontiguousarray(c) for c in leaf_points]
+        dt = cols[0].dtype if cols else np.dtype(np.float64)
+        if dt not in (np.float32, np.float64) or any(c.dtype != dt for c in cols):
+            raise TypeError("leaf_points must be K float32 or float64 columns of one dtype")
+        st = np.ascontiguousarray(stems, dtype=dt)
+        items = np.ascontiguousarray(leaf_items, dtype=np.uint32)
+        ext = np.ascontiguousarray(leaf_extents, dtype=np.uint32).reshape(-1, 2)
+        n = int(items.shape[0])
+        if any(c.shape != (n,) for c in cols):
+            raise ValueError("every leaf_points column needs one value per item")
+        d = C.FlatVecDesc()
+        d.abi_version = C.ABI_VERSION
+        d.dtype = C.F32 if dt == np.float32 else C.F64
+        d.dims = len(cols)
+        d.stem_strategy = C.STEM_DONNELLY if block_height else 0
+        d.block_height = int(block_height)
+        d.max_stem_level = int(max_stem_level)
+        d.stems = st.ctypes.data if st.size else None
+        d.stem_count = st.size
+        for j, c in enumerate(cols[:4]):
+            d.columns[j] = c.ctypes.data if c.size else None
+        d.items = items.ctypes.data if items.size else None
+        d.extents = ext.ctypes.data if ext.size else None
+        d.leaf_count = ext.shape[0]
+        d.size = n
+        h = ctypes.c_void_p()
+        C.check(C.lib().kgpu_tree_create_flatvec(ctypes.byref(d), _stream_ptr(stream),
+                                                 ctypes.byref(h)))
+        return cls(None, _handle=h, dtype=dt, dims=len(cols))
+
+    @classmethod
     def build(cls, points, items=None, stream=None) -> "GpuTree":
         """The ImmutableKdTree of CUDA tensor `points` ([n, dims], float32 or
         float64) built on the device (kgpu_tree_build): the same layout, byte for

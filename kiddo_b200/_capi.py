@@ -38,7 +38,7 @@ EXPORTED_SYMBOLS = [
     "kgpu_forest_create", "kgpu_forest_destroy", "kgpu_forest_query",
     "kgpu_forest_query_radius_count", "kgpu_forest_query_radius_fill", "kgpu_graph_begin",
     "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy", "kgpu_chamfer_loss",
-    "kgpu_chamfer_backward",
+    "kgpu_chamfer_backward", "kgpu_tree_create_flatvec",
 ]
 
 
@@ -53,6 +53,17 @@ class TreeDesc(ctypes.Structure):
         ("leaf_count", ctypes.c_uint64), ("max_stem_level", ctypes.c_int32),
         ("reserved0", ctypes.c_uint32), ("size", ctypes.c_uint64),
         ("max_leaf_len", ctypes.c_uint64),
+    ]
+
+
+class FlatVecDesc(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32), ("dtype", ctypes.c_int32), ("dims", ctypes.c_uint32),
+        ("stem_strategy", ctypes.c_int32), ("block_height", ctypes.c_uint32),
+        ("max_stem_level", ctypes.c_int32), ("stems", ctypes.c_void_p),
+        ("stem_count", ctypes.c_uint64), ("columns", ctypes.c_void_p * 4),
+        ("items", ctypes.c_void_p), ("extents", ctypes.c_void_p),
+        ("leaf_count", ctypes.c_uint64), ("size", ctypes.c_uint64),
     ]
 
 
@@ -101,6 +112,8 @@ def lib():
     L.kgpu_layout_free.argtypes = [vp]
     L.kgpu_tree_create.restype = i32
     L.kgpu_tree_create.argtypes = [ctypes.POINTER(TreeDesc), vp, ctypes.POINTER(vp)]
+    L.kgpu_tree_create_flatvec.restype = i32
+    L.kgpu_tree_create_flatvec.argtypes = [ctypes.POINTER(FlatVecDesc), vp, ctypes.POINTER(vp)]
     L.kgpu_tree_destroy.restype = i32
     L.kgpu_tree_destroy.argtypes = [vp]
     L.kgpu_tree_info.restype = i32

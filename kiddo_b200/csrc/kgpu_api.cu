@@ -339,6 +339,36 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
   return KGPU_OK;
 }
 
+int32_t kgpu_tree_create_flatvec(const kgpu_flatvec_desc* d, void* stream, kgpu_tree** out) {
+  if (!d || !out) return set_error(KGPU_EINVAL, "NULL argument");
+  *out = nullptr;
+  if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
+  Layout L;
+  const int st = flatvec_to_layout(L, d->dtype, int(d->dims), d->columns, d->items, d->extents,
+                                   d->leaf_count, d->size);
+  if (st != KGPU_OK) return st;
+  kgpu_tree_desc td;
+  std::memset(&td, 0, sizeof(td));
+  td.abi_version = KGPU_ABI_VERSION;
+  td.dtype = d->dtype;
+  td.dims = d->dims;
+  td.item_size = 4;
+  td.bucket_size = 32;
+  td.stem_strategy = d->stem_strategy;
+  td.block_height = d->block_height;
+  td.resolution = KGPU_RES_ARITHMETIC;
+  td.stems = d->stems;
+  td.stem_count = d->stem_count;
+  td.leaf_bytes = L.leaf_bytes.data();
+  td.leaf_bytes_len = L.leaf_bytes.size();
+  td.leaf_extents = L.extents.data();
+  td.leaf_count = d->leaf_count;
+  td.max_stem_level = d->max_stem_level;
+  td.size = d->size;
+  td.max_leaf_len = L.max_leaf_len;
+  return kgpu_tree_create(&td, stream, out);
+}
+
 int32_t kgpu_tree_destroy(kgpu_tree* t) {
   if (!t) return KGPU_OK;
   release_tree_arrays(t->dt);

@@ -32,6 +32,12 @@ int set_error(int status, const std::string& msg);
 int build_layout_any(Layout& L, int dtype, int K, const void* pts, const uint32_t* items,
                      uint64_t n, int nthreads, uint32_t block_height = 0);
 
+// The VecOfArenas arena and byte extents of a FlatVec tree's leaves: K point
+// columns, items and (start, end) extents in points.
+int flatvec_to_layout(Layout& L, int dtype, int K, const void* const* columns,
+                      const uint32_t* items, const uint32_t* extents, uint64_t leaf_count,
+                      uint64_t size);
+
 }  // namespace kgpu
 
 struct kgpu_layout {

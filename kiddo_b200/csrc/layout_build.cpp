@@ -327,6 +327,80 @@ void build_layout(Layout& L, const A* pts, const uint32_t* items, uint64_t n, in
 
 }  // namespace
 
+namespace {
+
+// FlatVec leaves (leaf_strategy/flat_vec.rs:20-26, 189-210) re-encoded in the
+// VecOfArenas tiles: leaf l holds points start..end of the K columns, in that
+// order, the same chunk VecOfArenas::append_leaf would have been given.
+template <typename A>
+void flatvec_arena(Layout& L, const void* const* columns, const uint32_t* items,
+                   const uint32_t* ext, uint64_t leaf_count, int K) {
+  L.extents.resize(2 * leaf_count);
+  uint64_t cursor = 0;
+  for (uint64_t l = 0; l < leaf_count; ++l) {
+    const uint64_t len = ext[2 * l + 1] - ext[2 * l];
+    cursor = (cursor + 7) & ~uint64_t(7);
+    L.extents[2 * l] = cursor;
+    L.extents[2 * l + 1] = len;
+    cursor += leaf_encoded_bytes<A>(len, K);
+    L.max_leaf_len = std::max<uint64_t>(L.max_leaf_len, len);
+  }
+  L.leaf_bytes.assign(cursor, 0);
+  for (uint64_t l = 0; l < leaf_count; ++l) {
+    uint8_t* dst = L.leaf_bytes.data() + L.extents[2 * l];
+    size_t len = L.extents[2 * l + 1], base = ext[2 * l], off = 0;
+    while (len) {
+      const size_t w = tile_width(len);
+      for (int d = 0; d < K; ++d) {
+        const A* src = static_cast<const A*>(columns[d]) + base;
+        std::memcpy(dst + off + d * w * sizeof(A), src, w * sizeof(A));
+      }
+      std::memcpy(dst + off + K * w * sizeof(A), items + base, w * sizeof(uint32_t));
+      off += w * (K * sizeof(A) + sizeof(uint32_t));
+      base += w;
+      len -= w;
+    }
+  }
+}
+
+}  // namespace
+
+int flatvec_to_layout(Layout& L, int dtype, int K, const void* const* columns,
+                      const uint32_t* items, const uint32_t* extents, uint64_t leaf_count,
+                      uint64_t size) {
+  if (K < 1 || K > kMaxDims) return set_error(KGPU_EUNSUPPORTED, "dims must be 1..4");
+  if (dtype != KGPU_F32 && dtype != KGPU_F64)
+    return set_error(KGPU_EINVAL, "dtype must be KGPU_F32 or KGPU_F64");
+  if (size > 0xFFFFFFFFull) return set_error(KGPU_EOVERFLOW, "more than 2^32 points");
+  if (size > 0) {
+    if (!items) return set_error(KGPU_EINVAL, "leaf_items is NULL");
+    for (int d = 0; d < K; ++d)
+      if (!columns[d]) return set_error(KGPU_EINVAL, "a leaf_points column is NULL");
+  }
+  if (leaf_count > 0 && !extents) return set_error(KGPU_EINVAL, "leaf_extents is NULL");
+  uint64_t total = 0;
+  for (uint64_t l = 0; l < leaf_count; ++l) {
+    const uint32_t a = extents[2 * l], b = extents[2 * l + 1];
+    if (a > b || b > size) return set_error(KGPU_EINVAL, "leaf extent outside the points");
+    if (b - a > 1024) return set_error(KGPU_EINVAL, "leaf longer than 1024 points");
+    total += b - a;
+  }
+  if (total != size) return set_error(KGPU_EINVAL, "sum of leaf lengths != size");
+  L.dtype = dtype == KGPU_F64 ? 1 : 0;
+  L.dims = K;
+  L.size = size;
+  L.max_leaf_len = 0;
+  try {
+    if (dtype == KGPU_F32)
+      flatvec_arena<float>(L, columns, items, extents, leaf_count, K);
+    else
+      flatvec_arena<double>(L, columns, items, extents, leaf_count, K);
+  } catch (const std::bad_alloc&) {
+    return set_error(KGPU_ENOMEM, "host allocation failed");
+  }
+  return KGPU_OK;
+}
+
 int build_layout_any(Layout& L, int dtype, int K, const void* pts, const uint32_t* items,
                      uint64_t n, int nthreads, uint32_t block_height) {
   if (K < 1 || K > kMaxDims) return set_error(KGPU_EUNSUPPORTED, "dims must be 1..4");

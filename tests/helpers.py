@@ -107,3 +107,32 @@ def compare_nearest_n_reference_rule(dists, items, exp_d, exp_i, k):
             assert len(lst) == len(egroups.get(key, []))
             continue
         assert sorted(lst) == sorted(egroups.get(key, [])), key
+
+
+def flatvec_parts(tree):
+    """The FlatVec form (src/leaf_strategy/flat_vec.rs:20-26, 189-210) of a
+    host ImmutableKdTree: K point columns, items and (start, end) extents,
+    read off its VecOfArenas tiles leaf by leaf."""
+    K = tree.dims
+    dt = np.dtype(tree.dtype)
+    lb = tree.leaf_bytes()
+    ex = tree.leaf_extents()
+    cols = [[] for _ in range(K)]
+    items = []
+    extents = []
+    start = 0
+    for off, ln in ex:
+        off, ln = int(off), int(ln)
+        rem, pos = ln, off
+        while rem:
+            w = next(t for t in (32, 8, 4, 2, 1) if rem >= t)
+            for d in range(K):
+                cols[d].append(np.frombuffer(lb, dtype=dt, count=w, offset=pos + d * w * dt.itemsize))
+            items.append(np.frombuffer(lb, dtype=np.uint32, count=w, offset=pos + K * w * dt.itemsize))
+            pos += w * (K * dt.itemsize + 4)
+            rem -= w
+        extents.append((start, start + ln))
+        start += ln
+    cols = [np.concatenate(c) if c else np.zeros(0, dt) for c in cols]
+    items = np.concatenate(items) if items else np.zeros(0, np.uint32)
+    return cols, items, np.asarray(extents, dtype=np.uint32).reshape(-1, 2)

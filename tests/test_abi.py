@@ -97,6 +97,52 @@ def test_tree_create_rejects_f32_3d_offsets_off_16_bytes():
     assert b"multiple of 16" in C.lib().kgpu_last_error()
 
 
+def test_flatvec_create_rejects_bad_layouts_before_touching_the_device():
+    """kgpu_tree_create_flatvec checks the FlatVec arrays on the host."""
+    L = C.lib()
+    n = 100
+    cols = [np.zeros(n, dtype=np.float32) for _ in range(3)]
+    items = np.arange(n, dtype=np.uint32)
+
+    def create(extents, size=n, columns=cols, it=items, dims=3):
+        ext = np.ascontiguousarray(extents, dtype=np.uint32).reshape(-1, 2)
+        d = C.FlatVecDesc()
+        d.abi_version = C.ABI_VERSION
+        d.dtype = C.F32
+        d.dims = dims
+        d.max_stem_level = -1
+        for j, c in enumerate(columns):
+            d.columns[j] = c.ctypes.data if c is not None else None
+        d.items = it.ctypes.data if it is not None else None
+        d.extents = ext.ctypes.data
+        d.leaf_count = ext.shape[0]
+        d.size = size
+        h = ctypes.c_void_p()
+        return L.kgpu_tree_create_flatvec(ctypes.byref(d), None, ctypes.byref(h))
+
+    assert create([(0, 60), (60, 101)]) == C.KGPU_EINVAL       # past the points
+    assert create([(0, 60), (50, 40)]) == C.KGPU_EINVAL        # start after end
+    assert create([(0, 60), (60, 90)]) == C.KGPU_EINVAL        # lengths do not sum to size
+    assert create([(0, 100)], columns=cols[:2] + [None]) == C.KGPU_EINVAL
+    assert create([(0, 100)], it=None) == C.KGPU_EINVAL
+    assert create([(0, 100)], dims=5) == C.KGPU_EUNSUPPORTED
+    big = [np.zeros(2000, dtype=np.float32) for _ in range(3)]
+    assert create([(0, 2000)], size=2000, columns=big,
+                  it=np.arange(2000, dtype=np.uint32)) == C.KGPU_EINVAL  # leaf over 1024
+    assert L.kgpu_last_error()
+
+
+def test_flatvec_parts_round_trip():
+    """The test helper's FlatVec form holds every point once, leaf by leaf."""
+    from helpers import flatvec_parts
+    P = np.random.default_rng(4).random((5000, 3))
+    t = kb.ImmutableKdTree.new_from_slice(P)
+    cols, items, ext = flatvec_parts(t)
+    assert ext.shape == (t.leaf_count(), 2) and int(ext[-1, 1]) == 5000
+    assert np.array_equal(np.sort(items), np.arange(5000, dtype=np.uint32))
+    assert np.array_equal(np.stack(cols, 1), P[items])
+
+
 def test_layout_build_rejects_bad_arguments():
     L = C.lib()
     h = ctypes.c_void_p()
