@@ -97,16 +97,19 @@ void release_tree_arrays(DeviceTree& dt) {
     if (dt.stems) cudaFreeAsync(dt.stems, nullptr);
     if (dt.arena) cudaFreeAsync(dt.arena, nullptr);
     if (dt.extents) cudaFreeAsync(dt.extents, nullptr);
+    if (dt.src_extents) cudaFreeAsync(dt.src_extents, nullptr);
     cudaStreamSynchronize(nullptr);
     if (cur != dt.device) cudaSetDevice(cur);
   } else {
     cudaFree(dt.stems);
     cudaFree(dt.arena);
     cudaFree(dt.extents);
+    cudaFree(dt.src_extents);
   }
   dt.stems = nullptr;
   dt.arena = nullptr;
   dt.extents = nullptr;
+  dt.src_extents = nullptr;
 }
 
 }  // namespace kgpu
@@ -304,31 +307,59 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
   dt.max_leaf_len = d->max_leaf_len;
   dt.bh = donnelly ? d->block_height : 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // 3-D leaves are re-encoded as rows on the device.  f64 rows take 32 bytes
+  // per point against 28 in the tiles, so they get offsets of their own (32 x
+  // the points before the leaf) and the reference's extents stay beside them.
+  const bool rows = K == 3 && d->leaf_bytes_len;
+  const bool moved = rows && d->dtype == KGPU_F64;
+  std::vector<uint32_t> rex;
+  if (moved) {
+    try {
+      rex.resize(ex.size());
+    } catch (const std::bad_alloc&) {
+      delete t;
+      return set_error(KGPU_ENOMEM, "host allocation failed");
+    }
+    uint64_t before = 0;
+    for (uint64_t l = 0; l < d->leaf_count; ++l) {
+      rex[2 * l] = uint32_t(before * 32 / 8);
+      rex[2 * l + 1] = ex[2 * l + 1];
+      before += ex[2 * l + 1];
+    }
+  }
+  if (moved && d->size * 32 / 8 >= (uint64_t(1) << 32)) {
+    delete t;
+    return set_error(KGPU_EOVERFLOW, "f64 3-D rows larger than 32 GiB");
+  }
   const size_t stem_bytes = std::max<size_t>(16, d->stem_count * sa);
-  const size_t arena_bytes = std::max<size_t>(16, d->leaf_bytes_len + 16);
+  const size_t arena_bytes = std::max<size_t>(16, (moved ? d->size * 32 : d->leaf_bytes_len) + 16);
   const size_t ex_bytes = std::max<size_t>(16, ex.size() * 4);
   cudaError_t e;
   if ((e = cudaMalloc(&dt.stems, stem_bytes)) != cudaSuccess ||
       (e = cudaMalloc(reinterpret_cast<void**>(&dt.arena), arena_bytes)) != cudaSuccess ||
-      (e = cudaMalloc(&dt.extents, ex_bytes)) != cudaSuccess) {
+      (e = cudaMalloc(&dt.extents, ex_bytes)) != cudaSuccess ||
+      (moved && (e = cudaMalloc(&dt.src_extents, ex_bytes)) != cudaSuccess)) {
     cudaFree(dt.stems);
     cudaFree(dt.arena);
     cudaFree(dt.extents);
+    cudaFree(dt.src_extents);
     delete t;
     if (e == cudaErrorMemoryAllocation) return set_error(KGPU_ENOMEM, "device allocation failed");
     return cuda_fail(e, "cudaMalloc");
   }
-  dt.device_bytes = stem_bytes + arena_bytes + ex_bytes;
+  dt.device_bytes = stem_bytes + arena_bytes + ex_bytes * (moved ? 2 : 1);
   if (d->stem_count) e = cudaMemcpyAsync(dt.stems, d->stems, d->stem_count * sa, cudaMemcpyHostToDevice, s);
-  // f32 3-D leaves are staged as tiles and re-encoded as rows on the device
-  const bool rows = d->dtype == KGPU_F32 && K == 3 && d->leaf_bytes_len;
+  // 3-D leaves are staged as tiles and re-encoded as rows on the device
   DevBuf tiles;
   if (e == cudaSuccess && rows) e = tiles.alloc(d->leaf_bytes_len, s);
   if (e == cudaSuccess && d->leaf_bytes_len)
     e = cudaMemcpyAsync(rows ? tiles.as<uint8_t>() : dt.arena, d->leaf_bytes, d->leaf_bytes_len,
                         cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && !ex.empty())
-    e = cudaMemcpyAsync(dt.extents, ex.data(), ex.size() * 4, cudaMemcpyHostToDevice, s);
+    e = cudaMemcpyAsync(dt.extents, moved ? rex.data() : ex.data(), ex.size() * 4,
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && moved)
+    e = cudaMemcpyAsync(dt.src_extents, ex.data(), ex.size() * 4, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && rows) e = convert_leaf_layout(dt, tiles.as<uint8_t>(), dt.arena, true, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // `ex` is a local
   if (e != cudaSuccess) {

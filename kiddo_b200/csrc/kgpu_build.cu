@@ -187,12 +187,19 @@ __global__ void k_write_leaves(const A* __restrict__ pts, const uint32_t* __rest
                                const uint32_t* __restrict__ sorted_ids,
                                const uint64_t* __restrict__ nb, const uint64_t* __restrict__ nl,
                                const uint64_t* __restrict__ off, uint64_t leaves,
-                               uint8_t* __restrict__ arena, uint2* __restrict__ extents) {
+                               uint8_t* __restrict__ arena, uint2* __restrict__ extents,
+                               uint2* __restrict__ src_extents) {
   const int lane = threadIdx.x & 31;
   for (uint64_t l = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; l < leaves;
        l += (uint64_t(gridDim.x) * blockDim.x) >> 5) {
-    const uint64_t b = nb[l], len = nl[l], o = off[l];
-    if (lane == 0) extents[l] = make_uint2(uint32_t(o / 8), uint32_t(len));
+    const uint64_t b = nb[l], len = nl[l];
+    // f64 rows sit at 32 bytes per point before them; other leaves at the
+    // reference's offsets
+    const uint64_t o = src_extents ? b * row_bytes<A>() : off[l];
+    if (lane == 0) {
+      extents[l] = make_uint2(uint32_t(o / 8), uint32_t(len));
+      if (src_extents) src_extents[l] = make_uint2(uint32_t(off[l] / 8), uint32_t(len));
+    }
     uint8_t* leaf = arena + o;
     for (uint64_t p = lane; p < len; p += 32) {
       const uint32_t id = sorted_ids[b + p];
@@ -206,42 +213,59 @@ __global__ void k_write_leaves(const A* __restrict__ pts, const uint32_t* __rest
   }
 }
 
-// Tiles <-> rows for the leaves held as rows on the device (RowLeaves: f32,
-// 3-D), one warp per leaf; same offsets, same bytes per point.
+// Tiles <-> rows for the 3-D leaves held as rows on the device (RowLeaves),
+// one warp per leaf: tiles at the reference's offsets (tex), rows at the
+// device's (rex), the same point order.
+template <typename A>
+__device__ __forceinline__ void put_row(uint8_t* rows, uint32_t p, A x, A y, A z, uint32_t it) {
+  if constexpr (sizeof(A) == 4) {
+    reinterpret_cast<float4*>(rows)[p] = make_float4(x, y, z, __uint_as_float(it));
+  } else {
+    double2* r = reinterpret_cast<double2*>(rows) + 2 * size_t(p);
+    r[0] = make_double2(x, y);
+    r[1] = make_double2(z, __longlong_as_double((long long)it));  // item, then 4 zero bytes
+  }
+}
+
+template <typename A>
 __global__ void k_leaf_tiles_to_rows(const uint8_t* __restrict__ tiles, uint8_t* __restrict__ rows,
-                                     const uint2* __restrict__ extents, uint64_t leaves) {
+                                     const uint2* __restrict__ tex, const uint2* __restrict__ rex,
+                                     uint64_t leaves) {
   const int lane = threadIdx.x & 31;
   for (uint64_t l = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; l < leaves;
        l += (uint64_t(gridDim.x) * blockDim.x) >> 5) {
-    const uint2 ex = extents[l];
-    const size_t o = size_t(ex.x) * 8;
-    for (uint32_t p = lane; p < ex.y; p += 32) {
+    const uint2 te = tex[l];
+    const size_t to = size_t(te.x) * 8, ro = size_t(rex[l].x) * 8;
+    for (uint32_t p = lane; p < te.y; p += 32) {
       uint32_t toff, w, i;
-      tile_slot_cols<float, 3>(ex.y, p, toff, w, i);
-      const float* col = reinterpret_cast<const float*>(tiles + o + toff);
-      const uint32_t it = reinterpret_cast<const uint32_t*>(tiles + o + toff + 3 * w * 4)[i];
-      reinterpret_cast<float4*>(rows + o)[p] =
-          make_float4(col[i], col[w + i], col[2 * w + i], __uint_as_float(it));
+      tile_slot_cols<A, 3>(te.y, p, toff, w, i);
+      const A* col = reinterpret_cast<const A*>(tiles + to + toff);
+      const uint32_t it = reinterpret_cast<const uint32_t*>(tiles + to + toff + 3 * w * sizeof(A))[i];
+      put_row<A>(rows + ro, p, col[i], col[w + i], col[2 * w + i], it);
     }
   }
 }
 
+template <typename A>
 __global__ void k_leaf_rows_to_tiles(const uint8_t* __restrict__ rows, uint8_t* __restrict__ tiles,
-                                     const uint2* __restrict__ extents, uint64_t leaves) {
+                                     const uint2* __restrict__ tex, const uint2* __restrict__ rex,
+                                     uint64_t leaves) {
   const int lane = threadIdx.x & 31;
   for (uint64_t l = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; l < leaves;
        l += (uint64_t(gridDim.x) * blockDim.x) >> 5) {
-    const uint2 ex = extents[l];
-    const size_t o = size_t(ex.x) * 8;
-    for (uint32_t p = lane; p < ex.y; p += 32) {
+    const uint2 te = tex[l];
+    const size_t to = size_t(te.x) * 8, ro = size_t(rex[l].x) * 8;
+    for (uint32_t p = lane; p < te.y; p += 32) {
       uint32_t toff, w, i;
-      tile_slot_cols<float, 3>(ex.y, p, toff, w, i);
-      const float4 v = reinterpret_cast<const float4*>(rows + o)[p];
-      float* col = reinterpret_cast<float*>(tiles + o + toff);
-      col[i] = v.x;
-      col[w + i] = v.y;
-      col[2 * w + i] = v.z;
-      reinterpret_cast<uint32_t*>(tiles + o + toff + 3 * w * 4)[i] = __float_as_uint(v.w);
+      tile_slot_cols<A, 3>(te.y, p, toff, w, i);
+      A c[3];
+      uint32_t it;
+      load_row<A, 3>(rows + ro, p, c, it);
+      A* col = reinterpret_cast<A*>(tiles + to + toff);
+      col[i] = c[0];
+      col[w + i] = c[1];
+      col[2 * w + i] = c[2];
+      reinterpret_cast<uint32_t*>(tiles + to + toff + 3 * w * sizeof(A))[i] = it;
     }
   }
 }
@@ -421,22 +445,29 @@ int build_on_device(const A* pts, const uint32_t* items, uint64_t n, cudaStream_
     arena_bytes = arena_bytes - ((raw + 7) & ~uint64_t(7)) + raw;
   }
   dt.leaf_bytes_len = arena_bytes;
+  // f64 3-D rows: 32 bytes per point, offsets of their own
+  const bool moved = RowLeaves<A, K>::value && sizeof(A) == 8;
+  const uint64_t dev_bytes = moved ? n * row_bytes<A>() : arena_bytes;
   dt.max_leaf_len = max_leaf;
-  if ((e = scratch_alloc(reinterpret_cast<void**>(&dt.arena), std::max<size_t>(16, arena_bytes + 16),
+  if ((e = scratch_alloc(reinterpret_cast<void**>(&dt.arena), std::max<size_t>(16, dev_bytes + 16),
                          s)) != cudaSuccess ||
-      (e = scratch_alloc(&dt.extents, std::max<size_t>(16, leaves * 8), s)) != cudaSuccess)
+      (e = scratch_alloc(&dt.extents, std::max<size_t>(16, leaves * 8), s)) != cudaSuccess ||
+      (moved && (e = scratch_alloc(&dt.src_extents, std::max<size_t>(16, leaves * 8), s)) !=
+                    cudaSuccess))
     return cuda_fail_b(e, "tree arrays");
-  if ((e = cudaMemsetAsync(dt.arena, 0, arena_bytes + 16, s)) != cudaSuccess)
+  if ((e = cudaMemsetAsync(dt.arena, 0, dev_bytes + 16, s)) != cudaSuccess)
     return cuda_fail_b(e, "arena");
   if (leaves) {
     k_write_leaves<A, K><<<blocks_for(leaves * 32), 256, 0, s>>>(
         pts, items, lids.as<uint32_t>(), nb.as<uint64_t>(), nl.as<uint64_t>(), loff.as<uint64_t>(),
-        leaves, dt.arena, static_cast<uint2*>(dt.extents));
+        leaves, dt.arena, static_cast<uint2*>(dt.extents),
+        static_cast<uint2*>(dt.src_extents));
     g_launches++;
   }
   if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return cuda_fail_b(e, "writing the leaves");
-  dt.device_bytes = std::max<size_t>(16, stem_count * sizeof(A)) + arena_bytes + 16 + leaves * 8;
+  dt.device_bytes = std::max<size_t>(16, stem_count * sizeof(A)) + dev_bytes + 16 +
+                    leaves * 8 * (moved ? 2 : 1);
   return KGPU_OK;
 }
 
@@ -446,11 +477,15 @@ cudaError_t convert_leaf_layout(const DeviceTree& dt, const uint8_t* src, uint8_
                                 bool to_rows, cudaStream_t s) {
   if (dt.leaf_count == 0) return cudaSuccess;
   const unsigned grid = blocks_for(uint64_t(dt.leaf_count) * 32);
-  const uint2* ex = static_cast<const uint2*>(dt.extents);
-  if (to_rows)
-    k_leaf_tiles_to_rows<<<grid, 256, 0, s>>>(src, dst, ex, dt.leaf_count);
-  else
-    k_leaf_rows_to_tiles<<<grid, 256, 0, s>>>(src, dst, ex, dt.leaf_count);
+  const uint2* rex = static_cast<const uint2*>(dt.extents);
+  const uint2* tex = dt.src_extents ? static_cast<const uint2*>(dt.src_extents) : rex;
+  if (dt.dtype == KGPU_F64) {
+    if (to_rows) k_leaf_tiles_to_rows<double><<<grid, 256, 0, s>>>(src, dst, tex, rex, dt.leaf_count);
+    else k_leaf_rows_to_tiles<double><<<grid, 256, 0, s>>>(src, dst, tex, rex, dt.leaf_count);
+  } else {
+    if (to_rows) k_leaf_tiles_to_rows<float><<<grid, 256, 0, s>>>(src, dst, tex, rex, dt.leaf_count);
+    else k_leaf_rows_to_tiles<float><<<grid, 256, 0, s>>>(src, dst, tex, rex, dt.leaf_count);
+  }
   g_launches++;
   return cudaGetLastError();
 }
@@ -513,7 +548,7 @@ int32_t kgpu_tree_read_layout(const kgpu_tree* t, void* stems, uint8_t* leaf_byt
   // leaves held as rows go back to the reference's tiles first
   DevBuf tiles;
   const uint8_t* arena = dt.arena;
-  if (leaf_bytes && dt.leaf_bytes_len && dt.dtype == KGPU_F32 && dt.dims == 3) {
+  if (leaf_bytes && dt.leaf_bytes_len && dt.dims == 3) {
     if ((e = tiles.alloc(dt.leaf_bytes_len, s)) != cudaSuccess ||
         (e = cudaMemsetAsync(tiles.p, 0, dt.leaf_bytes_len, s)) != cudaSuccess ||
         (e = convert_leaf_layout(dt, dt.arena, tiles.as<uint8_t>(), false, s)) != cudaSuccess)
@@ -527,8 +562,8 @@ int32_t kgpu_tree_read_layout(const kgpu_tree* t, void* stems, uint8_t* leaf_byt
        (e = cudaMemcpyAsync(leaf_bytes, arena, dt.leaf_bytes_len, cudaMemcpyDeviceToHost, s)) !=
            cudaSuccess) ||
       (dt.leaf_count &&
-       (e = cudaMemcpyAsync(ex.data(), dt.extents, ex.size() * 4, cudaMemcpyDeviceToHost, s)) !=
-           cudaSuccess))
+       (e = cudaMemcpyAsync(ex.data(), dt.src_extents ? dt.src_extents : dt.extents,
+                            ex.size() * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess))
     return cuda_fail_b(e, "reading the layout");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail_b(e, "reading the layout");
   if (extents)

@@ -164,14 +164,40 @@ __device__ __forceinline__ void donnelly_children(uint32_t stem, uint32_t minor,
 
 // Leaf encoding on the device.  The reference stores a leaf as tiles of 32,
 // then 8, 4, 2, 1 points, each tile its K coordinate columns then its items
-// (leaf_strategy/vec_of_arenas.rs:292-323).  f32 3-D leaves are held on the
-// device instead as one 16-byte row per point, (x, y, z, item bits), in the
-// same point order: 3 x 4 + 4 bytes per point either way, so every leaf keeps
-// its size and its offset, and a point is one aligned 16-byte load instead of
-// a tile decode and four loads.  The arena is converted on upload and back on
-// read-back; other shapes keep the tiles.
+// (leaf_strategy/vec_of_arenas.rs:292-323).  3-D leaves are held on the
+// device instead as one row per point, in the same point order:
+//  * f32: 16 bytes, (x, y, z, item bits).  A tile also spends 3 x 4 + 4
+//    bytes per point, so every leaf keeps its size and its offset;
+//  * f64: 32 bytes, (x, y, z, item bits, 4 zero bytes), against 28 in a tile,
+//    so the device arena has offsets of its own (leaf l at 32 x the points
+//    before it) and keeps the reference's extents beside them for read-back.
+// A point is then one or two aligned 16-byte loads instead of a tile decode
+// and four loads.  The arena is converted on upload and back on read-back;
+// other shapes keep the tiles.
 template <typename A, int K>
-struct RowLeaves : std::integral_constant<bool, std::is_same<A, float>::value && K == 3> {};
+struct RowLeaves : std::integral_constant<bool, K == 3> {};
+template <typename A>
+constexpr uint32_t row_bytes() { return sizeof(A) == 4 ? 16u : 32u; }
+
+// Point p of a leaf held as rows.
+template <typename A, int K>
+__device__ __forceinline__ void load_row(const uint8_t* __restrict__ leaf, uint32_t p,
+                                         A (&c)[K], uint32_t& item) {
+  if constexpr (sizeof(A) == 4) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(leaf) + p);
+    c[0] = v.x;
+    c[1] = v.y;
+    c[2] = v.z;
+    item = __float_as_uint(v.w);
+  } else {
+    const double2* r = reinterpret_cast<const double2*>(leaf) + 2 * size_t(p);
+    const double2 a = __ldg(r), b = __ldg(r + 1);
+    c[0] = a.x;
+    c[1] = a.y;
+    c[2] = b.x;
+    item = uint32_t(__double_as_longlong(b.y));
+  }
+}
 
 // Byte offset inside the leaf, tile width and index in tile of point p of a
 // leaf of `len` points laid out as tiles of 32, then 8, then 4, 2, 1.
@@ -211,7 +237,7 @@ template <typename A, int K>
 __device__ __forceinline__ void tile_slot(uint32_t len, uint32_t p, uint32_t& off, uint32_t& w,
                                           uint32_t& i) {
   if constexpr (RowLeaves<A, K>::value) {
-    off = p * uint32_t(K * sizeof(A) + sizeof(uint32_t));
+    off = p * row_bytes<A>();
     w = 1;
     i = 0;
   } else {
@@ -223,11 +249,7 @@ template <typename A, int K>
 __device__ __forceinline__ void load_point(const uint8_t* __restrict__ leaf, uint32_t len,
                                            uint32_t p, A (&c)[K], uint32_t& item) {
   if constexpr (RowLeaves<A, K>::value) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(leaf) + p);
-    c[0] = v.x;
-    c[1] = v.y;
-    c[2] = v.z;
-    item = __float_as_uint(v.w);
+    load_row<A, K>(leaf, p, c, item);
     return;
   }
   uint32_t off, w, i;

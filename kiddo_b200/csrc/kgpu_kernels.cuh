@@ -424,11 +424,20 @@ struct WalkOf<A, K, M, 1> {
 // idle, so lanes do not wait for the warp's slowest query.  nearest_one and
 // nearest_n scan their leaves per thread; best_n_within scans them
 // warp-cooperatively (kgpu_coop.cuh).  Each query's own traversal is unchanged.
+// Four 256-thread blocks per SM (64 registers) in general; three (80
+// registers, no spills) for best_n and for the f64 nearest_one / nearest_n
+// kernels, whose two 16-byte row loads per point would spill at 64.
 #ifndef KGPU_TFIXED_MIN_BLOCKS
 #define KGPU_TFIXED_MIN_BLOCKS 4
 #endif
+template <int FAM, typename A>
+constexpr int tfixed_min_blocks() {
+  return (FAM == KF_BEST_N || ((FAM == KF_NEAREST_N || FAM == KF_NEAREST_ONE) && sizeof(A) == 8))
+             ? 3
+             : KGPU_TFIXED_MIN_BLOCKS;
+}
 template <typename A, int K, typename M, int FAM, bool EXCL, int STEMS = 0>
-__global__ void __launch_bounds__(256, FAM == KF_BEST_N ? 3 : KGPU_TFIXED_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, tfixed_min_blocks<FAM, A>())
     k_tfixed(TreeView<A> tv0, Batch<A> b, int levels, int k, A radius0, int arrival_order,
              A* __restrict__ out_d, uint32_t* __restrict__ out_i, uint32_t* __restrict__ out_c,
              unsigned long long* __restrict__ stats) {

@@ -23,6 +23,9 @@ struct DeviceTree {
   size_t device_bytes = 0;
   uint32_t bh = 0;             // 0: Eytzinger stems; 3 or 4: Donnelly<bh>
   bool pooled = false;         // arrays from the stream-ordered pool (device-built trees)
+  // f64 3-D leaves are 32-byte rows with offsets of their own: the reference
+  // layout's extents, uint2 (offset / 8, len), for read-back; null otherwise
+  void* src_extents = nullptr;
 };
 
 struct QueryLaunch {
@@ -97,8 +100,9 @@ cudaError_t launch_exclusive_scan(const uint64_t* counts, uint64_t* offsets, uin
 
 int sm_count();
 
-// Re-encodes a tree's leaves between the reference's tiles and the device's
-// rows (RowLeaves); src and dst are arenas laid out by dt's extents.
+// Re-encodes a tree's 3-D leaves between the reference's tiles (at the
+// offsets of dt.src_extents, or of dt.extents when that is null) and the
+// device's rows (at the offsets of dt.extents).
 cudaError_t convert_leaf_layout(const DeviceTree& dt, const uint8_t* src, uint8_t* dst,
                                 bool to_rows, cudaStream_t s);
 

@@ -38,15 +38,15 @@ __device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv,
   const uint2 ex = __ldg(tv.extents + leaf);
   const uint8_t* base = tv.arena + size_t(ex.x) * 8;
   if constexpr (RowLeaves<A, K>::value) {
-    // rows: one 16-byte load per point, the leaf's lines requested up front
-    const float4* rows = reinterpret_cast<const float4*>(base);
-    for (uint32_t b = 0; b < ex.y * 16u; b += 128u)
+    // rows: one row per step, the leaf's lines requested up front
+    for (uint32_t b = 0; b < ex.y * row_bytes<A>(); b += 128u)
       asm volatile("prefetch.global.L1 [%0];" ::"l"(base + b));
     for (uint32_t p = 0; p < ex.y; ++p) {
-      const float4 v = __ldg(rows + p);
-      const A c[K] = {v.x, v.y, v.z};
+      A c[K];
+      uint32_t it;
+      load_row<A, K>(base, p, c, it);
       const A d0 = dist(c);
-      if (pass(d0)) f(d0, __float_as_uint(v.w));
+      if (pass(d0)) f(d0, it);
     }
     return ex.y;
   }
@@ -108,12 +108,12 @@ __device__ __forceinline__ uint32_t leaf_chunk_mask(const uint8_t* __restrict__ 
                                                     uint32_t c0, const D& dist, P&& pass) {
   constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
   if constexpr (RowLeaves<A, K>::value) {
-    const float4* rows = reinterpret_cast<const float4*>(base);
     const uint32_t end = len < c0 + 32 ? len : c0 + 32;
     uint32_t mask = 0;
     for (uint32_t p = c0; p < end; ++p) {
-      const float4 v = __ldg(rows + p);
-      const A c[K] = {v.x, v.y, v.z};
+      A c[K];
+      uint32_t it;
+      load_row<A, K>(base, p, c, it);
       if (pass(dist(c))) mask |= 1u << (p - c0);
     }
     return mask;
@@ -664,11 +664,11 @@ struct TNearestN {
     // every 128-byte line of the leaf's rows requested up front, so the scan's
     // one-row-per-step loads find them in L1
     if constexpr (RowLeaves<A, K>::value)
-      for (uint32_t b = 0; b < len * 16u; b += 128u)
+      for (uint32_t b = 0; b < len * row_bytes<A>(); b += 128u)
         asm volatile("prefetch.global.L1 [%0];" ::"l"(base + b));
     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
       uint32_t mask = leaf_chunk_mask<A, K>(base, len, c0, dist, [&](A d) { return d <= gate; });
-      if constexpr (RowLeaves<A, K>::value) {
+      if constexpr (RowLeaves<A, K>::value && sizeof(A) == 4) {
         // The next candidate's row is requested before the current one is
         // added, so its load overlaps the insertion (the kernel waits on load
         // latency more than on issue slots here).
