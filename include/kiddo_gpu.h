@@ -4,9 +4,11 @@
  *
  * The engine takes the reference builder's own layout — the Eytzinger stem
  * array, the VecOfArenas leaf arena bytes and the (offset, len) leaf extents —
- * uploads it unchanged to HBM and answers whole batches of queries with CUDA
- * kernels for sm_100a.  Results are bit-identical to the reference's scalar
- * `.execute()` path on the same tree and queries.
+ * uploads it to HBM (3-D leaves re-encoded as one row per point, the same
+ * points in the same order; the reference's bytes read back unchanged) and
+ * answers whole batches of queries with CUDA kernels for sm_100a.  Results
+ * are bit-identical to the reference's scalar `.execute()` path on the same
+ * tree and queries.
  *
  * Conventions
  *  - Every entry point returns a kgpu_status; nothing aborts or throws across
@@ -170,8 +172,11 @@ int32_t kgpu_layout_free(kgpu_layout* layout);
 
 /* ---- device trees --------------------------------------------------------
  * Upload a layout (one the reference built, or kgpu_layout_build's) to the
- * current CUDA device.  Stems and arena bytes are copied unchanged; extents
- * are re-encoded as 32-bit (offset / 8, len) pairs. */
+ * current CUDA device.  Stems are copied unchanged; extents are re-encoded as
+ * 32-bit (offset / 8, len) pairs; 3-D leaves are re-encoded as rows (f32: 16
+ * bytes per point at the same offsets, which must then be multiples of 16, as
+ * the reference's are; f64: 32 bytes per point at offsets of their own).
+ * kgpu_tree_read_layout returns the layout's original bytes. */
 int32_t kgpu_tree_create(const kgpu_tree_desc* desc, void* stream, kgpu_tree** out);
 /* Uploads a tree whose leaves use the FlatVec strategy (KdTree<A, u32, SS,
  * FlatVec<A, u32, K, 32>, K, 32>, src/leaf_strategy/flat_vec.rs:20-26): its
