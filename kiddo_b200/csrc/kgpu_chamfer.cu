@@ -9,14 +9,16 @@
 //     dL/dt_m = - sum_{(i, j) : nbr_ij = m} phi'(d_ij) * 2 (s_i - t_m)
 // Determinism without floating-point atomics: the loss is reduced in a fixed
 // tree order; a source sums its neighbours in rank order; the (source,
-// neighbour) pairs are bucketed by target with a counting sort (integer
-// atomics only), each bucket is put in pair-id order and summed in that order.
+// neighbour) pairs are bucketed by target with one stable radix sort of the
+// pair ids on their target, so every bucket holds its pairs in pair-id order
+// and is summed in that order (no atomics at all).
 // d_ij is recomputed from the coordinates with the same rounded operations as
 // the leaf scan ((0 + dx^2) + dy^2) + dz^2, so it equals the forward distance.
 #include <cmath>
 #include <cstdint>
 #include <string>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include "../../include/kiddo_gpu.h"
@@ -110,38 +112,32 @@ __global__ void k_grad_src(const float* __restrict__ src, const float* __restric
   }
 }
 
-__global__ void k_pair_histogram(const uint32_t* __restrict__ items,
-                                 const uint32_t* __restrict__ counts,
-                                 const uint32_t* __restrict__ tree_of,
-                                 const uint64_t* __restrict__ tgt_base, uint64_t n_src, int k,
-                                 unsigned long long* __restrict__ bucket) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_src;
-       i += uint64_t(gridDim.x) * blockDim.x) {
-    const int c = int(counts[i]);
-    for (int j = 0; j < c; ++j) atomicAdd(bucket + target_of(items, tree_of, tgt_base, i, k, j), 1ull);
+// Pair p = i * k + j (source i, rank j): its target when j < count_i, else
+// n_tgt, which sorts after every real target.
+__global__ void k_pair_keys(const uint32_t* __restrict__ items,
+                            const uint32_t* __restrict__ counts,
+                            const uint32_t* __restrict__ tree_of,
+                            const uint64_t* __restrict__ tgt_base, uint64_t np, int k,
+                            uint32_t n_tgt, uint32_t* __restrict__ key, uint32_t* __restrict__ id) {
+  for (uint64_t p = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < np;
+       p += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t i = p / uint32_t(k);
+    const int j = int(p - i * uint32_t(k));
+    key[p] = j < int(counts[i]) ? uint32_t(target_of(items, tree_of, tgt_base, i, k, j)) : n_tgt;
+    id[p] = uint32_t(p);
   }
 }
 
-// Bucket the pairs by target; inside a bucket the order is arbitrary here and
-// is fixed afterwards by sorting each bucket on the pair id (`key`, exact in
-// a double up to 2^53).
-__global__ void k_pair_scatter(const uint32_t* __restrict__ items,
-                               const uint32_t* __restrict__ counts,
-                               const uint32_t* __restrict__ tree_of,
-                               const uint64_t* __restrict__ tgt_base, uint64_t n_src, int k,
-                               const uint64_t* __restrict__ start,
-                               unsigned long long* __restrict__ cursor, double* __restrict__ key,
-                               uint32_t* __restrict__ pairs) {
-  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_src;
-       i += uint64_t(gridDim.x) * blockDim.x) {
-    const int c = int(counts[i]);
-    for (int j = 0; j < c; ++j) {
-      const uint64_t m = target_of(items, tree_of, tgt_base, i, k, j);
-      const unsigned long long pos = start[m] + atomicAdd(cursor + m, 1ull);
-      const uint32_t id = uint32_t(i * k + j);
-      pairs[pos] = id;
-      key[pos] = double(id);
-    }
+// start[m] = the first position of target m in the sorted keys, for m in
+// 0..n_tgt (start[n_tgt] = the number of real pairs): each position a sets
+// the targets after key[a - 1] up to key[a], and position np the rest.
+__global__ void k_bucket_starts(const uint32_t* __restrict__ key, uint64_t np, uint64_t n_tgt,
+                                uint64_t* __restrict__ start) {
+  for (uint64_t a = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; a <= np;
+       a += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t lo = a == 0 ? 0 : uint64_t(key[a - 1]) + 1;
+    const uint64_t hi = a == np ? n_tgt : uint64_t(key[a]);
+    for (uint64_t m = lo; m <= hi && m <= n_tgt; ++m) start[m] = a;
   }
 }
 
@@ -232,39 +228,36 @@ int32_t kgpu_chamfer_backward(const float* src, uint64_t n_src, const float* tgt
     g_launches++;
   }
   if (grad_tgt && n_tgt) {
-    DevBuf bucket, cursor, pairs, keys, skeys, spairs, tmp;
+    if (n_tgt >= 0xFFFFFFFFull) return set_error(KGPU_EOVERFLOW, "2^32 - 1 targets or more");
+    DevBuf start, kin, vin, kout, vout, sort_tmp;
     const uint64_t np = n_src * k;
-    if ((e = bucket.alloc((n_tgt + 1) * 8, s)) != cudaSuccess ||
-        (e = cursor.alloc(n_tgt * 8, s)) != cudaSuccess ||
-        (e = pairs.alloc(np * 4, s)) != cudaSuccess || (e = keys.alloc(np * 8, s)) != cudaSuccess ||
-        (e = spairs.alloc(np * 4, s)) != cudaSuccess || (e = skeys.alloc(np * 8, s)) != cudaSuccess ||
-        (e = tmp.alloc(scan_tmp_bytes(n_tgt), s)) != cudaSuccess)
+    int bits = 1;
+    while (bits < 32 && (uint64_t(1) << bits) <= n_tgt) ++bits;
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, kin.as<uint32_t>(), kout.as<uint32_t>(),
+                                    vin.as<uint32_t>(), vout.as<uint32_t>(), uint32_t(np), 0, bits,
+                                    s);
+    if ((e = start.alloc((n_tgt + 1) * 8, s)) != cudaSuccess ||
+        (e = kin.alloc(np * 4, s)) != cudaSuccess || (e = vin.alloc(np * 4, s)) != cudaSuccess ||
+        (e = kout.alloc(np * 4, s)) != cudaSuccess || (e = vout.alloc(np * 4, s)) != cudaSuccess ||
+        (e = sort_tmp.alloc(sort_bytes, s)) != cudaSuccess)
       return set_error(KGPU_ENOMEM, "device allocation failed");
-    if ((e = cudaMemsetAsync(bucket.p, 0, (n_tgt + 1) * 8, s)) != cudaSuccess ||
-        (e = cudaMemsetAsync(cursor.p, 0, n_tgt * 8, s)) != cudaSuccess)
-      return cuda_err(e, "memset");
-    if (n_src) {
-      k_pair_histogram<<<grid_of(n_src), 256, 0, s>>>(items, counts, tree_of, tgt_base, n_src,
-                                                      int(k), bucket.as<unsigned long long>());
+    if (np) {
+      k_pair_keys<<<grid_of(np), 256, 0, s>>>(items, counts, tree_of, tgt_base, np, int(k),
+                                             uint32_t(n_tgt), kin.as<uint32_t>(),
+                                             vin.as<uint32_t>());
       g_launches++;
+      if ((e = cub::DeviceRadixSort::SortPairs(sort_tmp.p, sort_bytes, kin.as<uint32_t>(),
+                                               kout.as<uint32_t>(), vin.as<uint32_t>(),
+                                               vout.as<uint32_t>(), uint32_t(np), 0, bits, s)) !=
+          cudaSuccess)
+        return cuda_err(e, "ordering the pairs");
     }
-    if ((e = launch_exclusive_scan(bucket.as<uint64_t>(), bucket.as<uint64_t>(), n_tgt, tmp.p, s)) !=
-        cudaSuccess)
-      return cuda_err(e, "scan");
-    if (n_src) {
-      k_pair_scatter<<<grid_of(n_src), 256, 0, s>>>(items, counts, tree_of, tgt_base, n_src,
-                                                    int(k), bucket.as<uint64_t>(),
-                                                    cursor.as<unsigned long long>(),
-                                                    keys.as<double>(), pairs.as<uint32_t>());
-      g_launches++;
-      e = launch_seg_sort<double>(bucket.as<uint64_t>(), n_tgt, np, keys.as<double>(),
-                                  pairs.as<uint32_t>(), skeys.as<double>(), spairs.as<uint32_t>(),
-                                  s);
-      if (e != cudaSuccess) return cuda_err(e, "ordering the pairs");
-    }
-    k_grad_tgt<<<grid_of(n_tgt), 256, 0, s>>>(src, tgt, bucket.as<uint64_t>(), pairs.as<uint32_t>(),
+    k_bucket_starts<<<grid_of(np + 1), 256, 0, s>>>(kout.as<uint32_t>(), np, n_tgt,
+                                                    start.as<uint64_t>());
+    k_grad_tgt<<<grid_of(n_tgt), 256, 0, s>>>(src, tgt, start.as<uint64_t>(), vout.as<uint32_t>(),
                                               n_tgt, int(k), inv2s2, grad_scale, grad_tgt);
-    g_launches++;
+    g_launches += 2;
   }
   e = cudaGetLastError();
   return e == cudaSuccess ? KGPU_OK : cuda_err(e, "chamfer backward");
