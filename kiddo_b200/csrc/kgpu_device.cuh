@@ -627,6 +627,115 @@ struct NearestNPolicy {
   }
 };
 
+// nearest_n for 32 < k <= kMaxBigK, one query per warp: the collector of
+// NearestNPolicy (ThresholdVec, result_collection.rs:136-215: the k smallest
+// by (distance, arrival)), with the list in this warp's shared-memory region
+// instead of one entry per lane: distances, items and arrival numbers, kept
+// sorted.  An insertion finds its place with one ballot per 32 entries and
+// moves the entries above it up by one, 32 at a time from the top.
+template <typename A, int K, typename M, bool kExclusive,
+          typename PD = CartesianDist<A, K, M>>
+struct NearestNBigPolicy {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  PD dist;
+  A* __restrict__ ld;
+  uint32_t* __restrict__ li;
+  uint32_t* __restrict__ ls;  // arrival number of each entry
+  int n, k;
+  A radius, kth;
+  uint32_t seq;
+  __device__ NearestNBigPolicy(A* d, uint32_t* i, uint32_t* s, int k_, A r, PD pd = PD())
+      : dist(pd), ld(d), li(i), ls(s), n(0), k(k_), radius(r), kth(inf_of<A>()), seq(0) {}
+  __device__ __forceinline__ A max_dist() const {
+    return (n == k && kth < radius) ? kth : radius;
+  }
+  __device__ __forceinline__ bool unbounded_start() const { return radius == inf_of<A>(); }
+
+  __device__ __forceinline__ void insert(A cd, uint32_t ci, int lane) {
+    int pos = 0;  // entries not above cd: the new one goes after its equals
+    for (int c0 = 0; c0 < n; c0 += 32) {
+      const int j = c0 + lane;
+      pos += __popc(__ballot_sync(FULL, j < n && !(ld[j] > cd)));
+    }
+    // entries pos..last move to pos+1..last+1; a full list drops its last
+    const int last = n < k ? n - 1 : k - 2;
+    if (last >= pos) {
+      for (int c0 = last & ~31; c0 >= (pos & ~31); c0 -= 32) {
+        const int j = c0 + lane;
+        const bool mv = j >= pos && j <= last;
+        A d = A(0);
+        uint32_t it = 0, sq = 0;
+        if (mv) {
+          d = ld[j];
+          it = li[j];
+          sq = ls[j];
+        }
+        __syncwarp();
+        if (mv) {
+          ld[j + 1] = d;
+          li[j + 1] = it;
+          ls[j + 1] = sq;
+        }
+        __syncwarp();
+      }
+    }
+    if (lane == 0) {
+      ld[pos] = cd;
+      li[pos] = ci;
+      ls[pos] = seq;
+    }
+    __syncwarp();
+    ++seq;
+    if (n < k) ++n;
+    if (n == k) kth = ld[k - 1];
+  }
+
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
+                                           int lane) {
+    const uint2 ex = __ldg(tv.extents + l);
+    const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+    const uint32_t len = ex.y;
+    const A bound = max_dist();
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t p = b + lane;
+      A dd = inf_of<A>();
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < len) {
+        A c[K];
+        load_point<A, K>(base, len, p, c, it);
+        dd = dist(c, q);
+        pass = kExclusive ? (dd < bound) : (dd <= bound);
+      }
+      uint32_t mask = __ballot_sync(FULL, pass);
+      if (n == k) mask &= __ballot_sync(FULL, dd < kth);
+      while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        insert(shfl(dd, src), shfl(it, src), lane);
+        if (n == k) mask &= __ballot_sync(FULL, dd < kth);
+      }
+    }
+    return len;
+  }
+
+  // Sorted rows; with `arrival_order` a list that never filled goes out in
+  // arrival order (nothing was evicted, so its arrival numbers are 0..n-1).
+  __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
+                                        uint32_t* __restrict__ out_i,
+                                        uint32_t* __restrict__ out_c, bool arrival_order,
+                                        int lane) const {
+    for (int j = lane; j < k; j += 32) {
+      const bool valid = j < n;
+      const int slot = (valid && arrival_order && n < k) ? int(ls[j]) : j;
+      const size_t o = size_t(qi) * k + slot;
+      out_d[o] = valid ? ld[j] : inf_of<A>();
+      out_i[o] = valid ? li[j] : 0xffffffffu;
+    }
+    if (lane == 0 && out_c) out_c[qi] = uint32_t(n);
+  }
+};
+
 // best_n_within: n smallest items among hits, ties by arrival
 // (kd_tree/query/best_n_within.rs:88-196, ctx :281-306; leaf filter
 // leaf_view_chunked/best_n_within/fallback.rs:40-104; heap replace-if-smaller

@@ -148,6 +148,34 @@ __global__ void __launch_bounds__(256) k_fixed(TreeView<A> tv0, Batch<A> b, int 
   });
 }
 
+// nearest_n with 32 < k <= kMaxBigK, one query per warp, each warp's list in
+// its own region of dynamic shared memory: k distances, then (after every
+// warp's distances) k items and k arrival numbers per warp.
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_fixed_bign(TreeView<A> tv0, Batch<A> b, int k, A radius0,
+                                                    int arrival_order, A* __restrict__ out_d,
+                                                    uint32_t* __restrict__ out_i,
+                                                    uint32_t* __restrict__ out_c,
+                                                    unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char bsmem[];
+  const int lane = threadIdx.x & 31;
+  const size_t warps = blockDim.x >> 5, w = threadIdx.x >> 5;
+  A* ld = reinterpret_cast<A*>(bsmem) + w * k;
+  uint32_t* li = reinterpret_cast<uint32_t*>(reinterpret_cast<A*>(bsmem) + warps * k) + w * k;
+  uint32_t* ls = li + warps * k;
+  for_each_query_warp(b, [&](uint64_t qi) {
+    const TreeView<A> tv = b.tree(tv0, qi);
+    A q[K];
+    b.query(qi, q);
+    TravStats st;
+    NearestNBigPolicy<A, K, M, EXCL> pol(ld, li, ls, k, b.radius(radius0, qi));
+    warp_arith_query<A, K, M>(tv, q, pol, lane, st);
+    pol.write(qi, out_d, out_i, out_c, arrival_order != 0, lane);
+    __syncwarp();
+    if (stats && lane == 0) add_stats(stats, st);
+  });
+}
+
 // ---------------------------------------------------------------------------
 // Radius families: count pass, exclusive scan, fill pass, segmented sort.
 // The fill pass writes at most `cap` hits per query; a query whose count

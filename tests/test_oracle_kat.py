@@ -119,6 +119,23 @@ def test_oracle_vs_brute_force(dtype, metric, n):
         assert bi_[j, :bc_[j]].tolist() == exp_best
 
 
+@pytest.mark.parametrize("k", [33, 100, 256])
+def test_oracle_large_k_vs_brute_force(k):
+    """nearest_n beyond the fixed-size lists (ThresholdVec up to 192, BinaryHeap
+    above): the k smallest by the reference's brute-force rule
+    (tests/kd_tree_fuzz_v6.rs:272-340)."""
+    rng = np.random.default_rng(k)
+    P = rng.random((20000, 3))
+    Q = rng.random((40, 3))
+    t = oracle.OracleTree.build(P)
+    dn, inn, cn = t.nearest_n(Q, k)
+    for j in range(len(Q)):
+        bd = brute_dists(P, Q[j])
+        order = np.lexsort((np.arange(len(P)), bd))
+        compare_nearest_n_reference_rule(dn[j, :cn[j]], inn[j, :cn[j]], bd[order[:k]],
+                                         order[:k], k)
+
+
 def test_oracle_periodic_vs_brute_force():
     rng = np.random.default_rng(7)
     P = rng.random((5000, 3))
