@@ -130,8 +130,8 @@ typedef struct kgpu_query_desc {
   uint32_t abi_version;   /* KGPU_ABI_VERSION */
   int32_t family;         /* kgpu_family */
   int32_t metric;         /* kgpu_metric */
-  uint32_t max_qty;       /* k for nearest_n* (1..256; above 32 only for Eytzinger trees
-                             and Cartesian queries), n for best_n_within (1..32) */
+  uint32_t max_qty;       /* k for nearest_n*, n for best_n_within: 1..256 (above 32
+                             only for Eytzinger trees and Cartesian queries) */
   double radius;          /* metric units (squared distance for SquaredEuclidean); cast to A */
   int32_t exclusive;      /* .exclusive_boundaries(): strict `< radius` */
   int32_t sorted;         /* 1 = default sorted output, 0 = .unsorted() */

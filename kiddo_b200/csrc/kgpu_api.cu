@@ -444,14 +444,14 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
       return set_error(KGPU_EINVAL, "family is not a fixed-size family");
     if (f == KGPU_NEAREST_N || f == KGPU_NEAREST_N_WITHIN || f == KGPU_BEST_N_WITHIN) {
       if (d->max_qty == 0) return set_error(KGPU_EINVAL, "max_qty must be >= 1");
-      // nearest_n takes k up to 256 (above 32 on the warp engine, Eytzinger
-      // trees, Cartesian queries); best_n_within n up to 32
-      const bool big = f != KGPU_BEST_N_WITHIN && !t->dt.bh && !d->periodic_box;
+      // k (nearest_n) and n (best_n_within) up to 256; above 32 on the warp
+      // engine, so for Eytzinger trees and Cartesian queries
+      const bool big = !t->dt.bh && !d->periodic_box;
       if (d->max_qty > uint32_t(big ? kMaxBigK : kMaxK))
         return set_error(KGPU_EUNSUPPORTED,
-                         big ? "k above 256 is not supported"
-                             : "max_qty above 32 is not supported here (best_n_within, "
-                               "Donnelly trees and periodic queries)");
+                         big ? "max_qty above 256 is not supported"
+                             : "max_qty above 32 is not supported for Donnelly trees and "
+                               "periodic queries");
     }
   }
   if (t->dt.bh) {
@@ -499,7 +499,8 @@ template <typename A>
 cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   // thread engine for 2-D/3-D trees; periodic nearest_one stays on the warp
   // engine (home query plus images)
-  const bool big_k = (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN) &&
+  const bool big_k = (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
+                      q.family == KGPU_BEST_N_WITHIN) &&
                      q.k > kMaxK;
   const bool thread = (t.bh || q.engine != 1) && (t.dims == 2 || t.dims == 3) &&
                       (!q.periodic || q.family != KGPU_NEAREST_ONE) && !big_k;

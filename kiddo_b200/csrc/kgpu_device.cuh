@@ -806,6 +806,100 @@ struct BestNPolicy {
   }
 };
 
+// best_n_within for 32 < n <= kMaxBigK, one query per warp: the collector of
+// BestNPolicy (the n smallest items among the hits, by (item, arrival);
+// best_n_within.rs:88-196) with the list in this warp's shared-memory region,
+// kept sorted by item and shifted 32 entries at a time like NearestNBigPolicy.
+template <typename A, int K, typename M, bool kExclusive>
+struct BestNBigPolicy {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  A* __restrict__ ld;
+  uint32_t* __restrict__ li;
+  int n, k;
+  A radius;
+  __device__ BestNBigPolicy(A* d, uint32_t* i, uint32_t*, int k_, A r)
+      : ld(d), li(i), n(0), k(k_), radius(r) {}
+  __device__ __forceinline__ A max_dist() const { return radius; }
+  __device__ __forceinline__ bool unbounded_start() const { return false; }
+
+  __device__ __forceinline__ void insert(A cd, uint32_t ci, int lane) {
+    int pos = 0;  // entries with an item not above ci: the new one goes after them
+    for (int c0 = 0; c0 < n; c0 += 32) {
+      const int j = c0 + lane;
+      pos += __popc(__ballot_sync(FULL, j < n && li[j] <= ci));
+    }
+    const int last = n < k ? n - 1 : k - 2;
+    if (last >= pos) {
+      for (int c0 = last & ~31; c0 >= (pos & ~31); c0 -= 32) {
+        const int j = c0 + lane;
+        const bool mv = j >= pos && j <= last;
+        A d = A(0);
+        uint32_t it = 0;
+        if (mv) {
+          d = ld[j];
+          it = li[j];
+        }
+        __syncwarp();
+        if (mv) {
+          ld[j + 1] = d;
+          li[j + 1] = it;
+        }
+        __syncwarp();
+      }
+    }
+    if (lane == 0) {
+      ld[pos] = cd;
+      li[pos] = ci;
+    }
+    __syncwarp();
+    if (n < k) ++n;
+  }
+
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K],
+                                           int lane) {
+    const uint2 ex = __ldg(tv.extents + l);
+    const uint8_t* base = tv.arena + size_t(ex.x) * 8;
+    const uint32_t len = ex.y;
+    const bool full_at_entry = n == k;
+    const uint32_t thr_item = full_at_entry ? li[k - 1] : 0u;
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t p = b + lane;
+      A dd = inf_of<A>();
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < len) {
+        A c[K];
+        load_point<A, K>(base, len, p, c, it);
+        dd = point_dist<M, A, K>(c, q);
+        pass = kExclusive ? (dd < radius) : (dd <= radius);
+        if (full_at_entry && it >= thr_item) pass = false;
+      }
+      uint32_t mask = __ballot_sync(FULL, pass);
+      while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const A cd = shfl(dd, src);
+        const uint32_t ci = shfl(it, src);
+        if (n == k && !(ci < li[k - 1])) continue;
+        insert(cd, ci, lane);
+      }
+    }
+    return len;
+  }
+
+  __device__ __forceinline__ void write(uint64_t qi, A* __restrict__ out_d,
+                                        uint32_t* __restrict__ out_i,
+                                        uint32_t* __restrict__ out_c, bool, int lane) const {
+    for (int j = lane; j < k; j += 32) {
+      const bool valid = j < n;
+      const size_t o = size_t(qi) * k + j;
+      out_d[o] = valid ? ld[j] : inf_of<A>();
+      out_i[o] = valid ? li[j] : 0xffffffffu;
+    }
+    if (lane == 0 && out_c) out_c[qi] = uint32_t(n);
+  }
+};
+
 // within / within().unsorted(): constant bound r (within.rs:18-41,
 // within_unsorted.rs:133-157); counting pass and filling pass.
 template <typename A, int K, typename M, bool kExclusive, typename PD = CartesianDist<A, K, M>>

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "kgpu_device.cuh"
@@ -148,10 +149,10 @@ __global__ void __launch_bounds__(256) k_fixed(TreeView<A> tv0, Batch<A> b, int 
   });
 }
 
-// nearest_n with 32 < k <= kMaxBigK, one query per warp, each warp's list in
-// its own region of dynamic shared memory: k distances, then (after every
-// warp's distances) k items and k arrival numbers per warp.
-template <typename A, int K, typename M, bool EXCL>
+// nearest_n and best_n_within with 32 < k <= kMaxBigK, one query per warp,
+// each warp's list in its own region of dynamic shared memory: k distances,
+// then (after every warp's distances) k items and k arrival numbers per warp.
+template <typename A, int K, typename M, int FAM, bool EXCL>
 __global__ void __launch_bounds__(256) k_fixed_bign(TreeView<A> tv0, Batch<A> b, int k, A radius0,
                                                     int arrival_order, A* __restrict__ out_d,
                                                     uint32_t* __restrict__ out_i,
@@ -168,7 +169,9 @@ __global__ void __launch_bounds__(256) k_fixed_bign(TreeView<A> tv0, Batch<A> b,
     A q[K];
     b.query(qi, q);
     TravStats st;
-    NearestNBigPolicy<A, K, M, EXCL> pol(ld, li, ls, k, b.radius(radius0, qi));
+    using Pol = typename std::conditional<FAM == KF_BEST_N, BestNBigPolicy<A, K, M, EXCL>,
+                                          NearestNBigPolicy<A, K, M, EXCL>>::type;
+    Pol pol(ld, li, ls, k, b.radius(radius0, qi));
     warp_arith_query<A, K, M>(tv, q, pol, lane, st);
     pol.write(qi, out_d, out_i, out_c, arrival_order != 0, lane);
     __syncwarp();

@@ -135,7 +135,7 @@ cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
           case KGPU_NEAREST_N_WITHIN:
             if (q.k > kMaxK) {
               const size_t smem = size_t(8) * q.k * (sizeof(A) + 8);
-              auto kern = k_fixed_bign<A, K, M, EX>;
+              auto kern = k_fixed_bign<A, K, M, KF_NEAREST_N, EX>;
               cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
               const int grid = grid_for(kern, smem, q.nq);
               kern<<<grid, 256, smem, q.stream>>>(tv, b, q.k, radius, q.sorted ? 0 : 1,
@@ -146,6 +146,16 @@ cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q) {
             }
             return run(k_fixed<A, K, M, KF_NEAREST_N, EX>);
           case KGPU_BEST_N_WITHIN:
+            if (q.k > kMaxK) {
+              const size_t smem = size_t(8) * q.k * (sizeof(A) + 8);
+              auto kern = k_fixed_bign<A, K, M, KF_BEST_N, EX>;
+              cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+              const int grid = grid_for(kern, smem, q.nq);
+              kern<<<grid, 256, smem, q.stream>>>(tv, b, q.k, radius, 0, static_cast<A*>(q.out_d),
+                                                  q.out_i, q.out_c, q.stats);
+              g_launches++;
+              return cudaGetLastError();
+            }
             return run(k_fixed<A, K, M, KF_BEST_N, EX>);
         }
         return cudaErrorInvalidValue;

@@ -1,8 +1,9 @@
-"""nearest_n with k above 32 (up to 256): the warp engine with each warp's
-list in shared memory, bit-exact with the oracle's collector (the reference's
-ThresholdVec, results/result_collection.rs:136-215: the k smallest by
-(distance, arrival order), arrival order kept for an unsorted list that never
-filled)."""
+"""nearest_n and best_n_within with k above 32 (up to 256): the warp engine
+with each warp's list in shared memory, bit-exact with the oracle's
+collectors (the reference's ThresholdVec, results/result_collection.rs:136-215:
+the k smallest by (distance, arrival order), arrival order kept for an
+unsorted list that never filled; best_n_within.rs:88-196: the n smallest
+items among the hits)."""
 import numpy as np
 import pytest
 
@@ -38,6 +39,25 @@ def test_large_k_matches_the_oracle(dtype, dims):
                               f"within k={k} excl={excl}")
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_large_best_n_matches_the_oracle(dtype):
+    rng = np.random.default_rng(21)
+    P = rng.random((30000, 3)).astype(dtype)
+    items = (rng.permutation(30000) % 9000).astype(np.uint32)  # repeated items
+    Q = rng.random((800, 3)).astype(dtype)
+    t = kb.ImmutableKdTree.new_from_entries(items, P)
+    o = oracle.OracleTree.build(P, items)
+    for n in (33, 100, 256):
+        for excl in (False, True):
+            b = t.query(Q).best_n_within(kb.SquaredEuclidean, 0.004, n)
+            if excl:
+                b = b.exclusive_boundaries()
+            g = b.execute_gpu()
+            assert_same_fixed(g.distances, g.items, g.counts,
+                              *o.best_n_within(Q, 0.004, n, exclusive=excl),
+                              f"best_n({n}) excl={excl}")
+
+
 def test_large_k_small_trees_and_counters():
     rng = np.random.default_rng(5)
     for n in (0, 1, 40, 300):
@@ -62,10 +82,12 @@ def test_large_k_limits():
     with pytest.raises(kb.KiddoGpuError):
         t.query(Q).nearest_n(kb.SquaredEuclidean, 257).execute_gpu()
     with pytest.raises(kb.KiddoGpuError):
-        t.query(Q).best_n_within(kb.SquaredEuclidean, 0.1, 33).execute_gpu()
+        t.query(Q).best_n_within(kb.SquaredEuclidean, 0.1, 257).execute_gpu()
     with pytest.raises(kb.KiddoGpuError):
         t.query(Q).periodic_boundary_condition(np.ones(3)).nearest_n(
             kb.SquaredEuclidean, 64).execute_gpu()
     d = kb.ImmutableKdTree.new_from_slice(P, block_height=3)
     with pytest.raises(kb.KiddoGpuError):
         d.query(Q).nearest_n(kb.SquaredEuclidean, 64).execute_gpu()
+    with pytest.raises(kb.KiddoGpuError):
+        d.query(Q).best_n_within(kb.SquaredEuclidean, 0.1, 64).execute_gpu()

@@ -134,6 +134,11 @@ def test_oracle_large_k_vs_brute_force(k):
         order = np.lexsort((np.arange(len(P)), bd))
         compare_nearest_n_reference_rule(dn[j, :cn[j]], inn[j, :cn[j]], bd[order[:k]],
                                          order[:k], k)
+    # best_n_within: the within-set sorted by item, truncated (fuzz_v6.rs:1020-1029)
+    bd_, bi_, bc_ = t.best_n_within(Q, 0.01, k)
+    for j in range(len(Q)):
+        sel = np.nonzero(brute_dists(P, Q[j]) <= 0.01)[0]
+        assert bi_[j, :bc_[j]].tolist() == sorted(sel.tolist())[:k]
 
 
 def test_oracle_periodic_vs_brute_force():
