@@ -656,7 +656,6 @@ int32_t kgpu_query(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, 
   if (nq == 0) return KGPU_OK;
   if (!queries || !out_dists || !out_items) return set_error(KGPU_EINVAL, "NULL buffer");
   const DeviceTree& dt = t->dt;
-  const size_t sa = dt.dtype == KGPU_F64 ? 8 : 4;
   const int w = out_width(d);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   QueryLaunch q;
