@@ -602,11 +602,26 @@ struct TNearestN {
   // ahead of the new entry).
   __device__ __forceinline__ void insert_below(int j, A d, uint32_t it) {
     if constexpr (kPacked) {
-      while (j > 0) {
-        const float2 e = le[(j - 1) * stride];
-        if (!(e.x > d)) break;
-        le[j * stride] = e;
-        --j;
+      // two entries read per step, so the shift waits on half as many
+      // dependent shared-memory loads
+      while (j > 1) {
+        const float2 e1 = le[(j - 1) * stride];
+        const float2 e2 = le[(j - 2) * stride];
+        if (!(e1.x > d)) break;
+        le[j * stride] = e1;
+        if (!(e2.x > d)) {
+          --j;
+          break;
+        }
+        le[(j - 1) * stride] = e2;
+        j -= 2;
+      }
+      if (j == 1) {
+        const float2 e = le[0];
+        if (e.x > d) {
+          le[stride] = e;
+          j = 0;
+        }
       }
     } else {
       while (j > 0 && le[(j - 1) * stride] > d) {
