@@ -600,7 +600,11 @@ struct TNearestN {
   // Shifts the entries before position j that are above d one place up and
   // stores (d, it) in the gap: the stable insertion step (equal distances stay
   // ahead of the new entry).
-  __device__ __forceinline__ void insert_below(int j, A d, uint32_t it) {
+  // Returns the distance now held at the starting position j: the entry that
+  // moved into it, or d if d went there.
+  __device__ __forceinline__ A insert_below(int j, A d, uint32_t it) {
+    const int j0 = j;
+    A top = d;
     if constexpr (kPacked) {
       // two entries read per step, so the shift waits on half as many
       // dependent shared-memory loads
@@ -609,6 +613,7 @@ struct TNearestN {
         const float2 e2 = le[(j - 2) * stride];
         if (!(e1.x > d)) break;
         le[j * stride] = e1;
+        if (j == j0) top = e1.x;
         if (!(e2.x > d)) {
           --j;
           break;
@@ -620,6 +625,7 @@ struct TNearestN {
         const float2 e = le[0];
         if (e.x > d) {
           le[stride] = e;
+          if (j == j0) top = e.x;
           j = 0;
         }
       }
@@ -627,10 +633,12 @@ struct TNearestN {
       while (j > 0 && le[(j - 1) * stride] > d) {
         le[j * stride] = le[(j - 1) * stride];
         li[j * stride] = li[(j - 1) * stride];
+        if (j == j0) top = le[j * stride];
         --j;
       }
     }
     put(j, d, it);
+    return top;
   }
 
   // stable insertion sort of the m held entries
@@ -648,8 +656,7 @@ struct TNearestN {
       return;
     }
     if (!(d < kth)) return;
-    insert_below(k - 1, d, it);
-    kth = dist_at(k - 1);
+    kth = insert_below(k - 1, d, it);
   }
 
   // The leaf filter of leaf_view_chunked/nearest_n_within/fallback.rs:37-95
