@@ -65,7 +65,9 @@ typedef enum kgpu_resolution {
 typedef enum kgpu_metric {
   KGPU_SQUARED_EUCLIDEAN = 0, /* src/dist/squared_euclidean/mod.rs:21-40 */
   KGPU_MANHATTAN = 1,         /* src/dist/manhattan/mod.rs:21-48 */
-  KGPU_CHEBYSHEV = 2          /* src/dist/chebyshev/mod.rs:19-59; not with periodic boxes */
+  KGPU_CHEBYSHEV = 2,         /* src/dist/chebyshev/mod.rs:19-59; not with periodic boxes */
+  KGPU_MINKOWSKI3 = 3,        /* Minkowski<3>, src/dist/minkowski/mod.rs:19-58; not periodic */
+  KGPU_MINKOWSKI4 = 4         /* Minkowski<4>; not periodic */
 } kgpu_metric;
 
 typedef enum kgpu_family {

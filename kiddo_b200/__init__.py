@@ -29,8 +29,8 @@ from . import _capi as C
 from ._capi import KiddoGpuError, launch_count
 
 __all__ = ["ImmutableKdTree", "GpuTree", "Forest", "CapturedGraph", "SquaredEuclidean",
-           "Manhattan", "Chebyshev", "KiddoGpuError", "NearestOneResult", "NearestNResult", "WithinResult",
-           "launch_count"]
+           "Manhattan", "Chebyshev", "Minkowski", "KiddoGpuError", "NearestOneResult",
+           "NearestNResult", "WithinResult", "launch_count"]
 
 
 class SquaredEuclidean:
@@ -49,6 +49,27 @@ class Chebyshev:
     code = C.CHEBYSHEV
 
 
+class _Minkowski3:
+    """dist/minkowski/mod.rs:19-58 with P = 3: the sum of |dx|^3."""
+    code = C.MINKOWSKI3
+
+
+class _Minkowski4:
+    """dist/minkowski/mod.rs:19-58 with P = 4: the sum of |dx|^4."""
+    code = C.MINKOWSKI4
+
+
+def Minkowski(p: int):
+    """The Minkowski<P> metric (the sum of |dx|^P, without the root) for P = 3
+    or 4; not with periodic boundary conditions."""
+    if p == 3:
+        return _Minkowski3
+    if p == 4:
+        return _Minkowski4
+    raise ValueError("Minkowski<P> is served for P = 3 and 4 (use Manhattan for 1, "
+                     "SquaredEuclidean for 2)")
+
+
 def _metric_code(m) -> int:
     if m in (SquaredEuclidean, "sqeuclidean", "squared_euclidean"):
         return C.SQUARED_EUCLIDEAN
@@ -56,7 +77,12 @@ def _metric_code(m) -> int:
         return C.MANHATTAN
     if m in (Chebyshev, "chebyshev"):
         return C.CHEBYSHEV
-    raise TypeError(f"unsupported metric {m!r} (SquaredEuclidean, Manhattan or Chebyshev)")
+    if m in (_Minkowski3, "minkowski3"):
+        return C.MINKOWSKI3
+    if m in (_Minkowski4, "minkowski4"):
+        return C.MINKOWSKI4
+    raise TypeError(f"unsupported metric {m!r} (SquaredEuclidean, Manhattan, Chebyshev or "
+                    "Minkowski(3|4))")
 
 
 def _vp(a: np.ndarray):

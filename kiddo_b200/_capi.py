@@ -19,7 +19,7 @@ KGPU_OK, KGPU_EINVAL, KGPU_EUNSUPPORTED, KGPU_ENOMEM, KGPU_ECUDA, KGPU_ETIMEDOUT
 F32, F64 = 0, 1
 STEM_EYTZINGER, STEM_DONNELLY = 0, 1
 RES_ARITHMETIC, RES_MAPPED, RES_PRISTINE = 0, 1, 2
-SQUARED_EUCLIDEAN, MANHATTAN, CHEBYSHEV = 0, 1, 2
+SQUARED_EUCLIDEAN, MANHATTAN, CHEBYSHEV, MINKOWSKI3, MINKOWSKI4 = 0, 1, 2, 3, 4
 NEAREST_ONE, APPROX_NEAREST_ONE, NEAREST_N, NEAREST_N_WITHIN, WITHIN, WITHIN_UNSORTED, \
     BEST_N_WITHIN = range(7)
 FLAG_HOST_BUFFERS = 0x1

@@ -428,12 +428,11 @@ namespace kgpu {
 int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_family) {
   if (!t || !d) return set_error(KGPU_EINVAL, "NULL argument");
   if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
-  if (d->metric != KGPU_SQUARED_EUCLIDEAN && d->metric != KGPU_MANHATTAN &&
-      d->metric != KGPU_CHEBYSHEV)
+  if (d->metric < KGPU_SQUARED_EUCLIDEAN || d->metric > KGPU_MINKOWSKI4)
     return set_error(KGPU_EINVAL, "unknown metric");
-  if (d->metric == KGPU_CHEBYSHEV && d->periodic_box)
+  if (d->metric >= KGPU_CHEBYSHEV && d->periodic_box)
     return set_error(KGPU_EUNSUPPORTED,
-                     "periodic queries take SquaredEuclidean or Manhattan, not Chebyshev");
+                     "periodic queries take SquaredEuclidean or Manhattan");
   const int f = d->family;
   if (radius_family) {
     if (f != KGPU_WITHIN && f != KGPU_WITHIN_UNSORTED)

@@ -107,6 +107,25 @@ struct Manhattan : Additive<Manhattan> {
   }
 };
 
+// Minkowski<P> (dist/minkowski/mod.rs:19-58): dist1 = |a - b|.powi(P), summed
+// without the final root.  Rust's powi is llvm.powi, expanded by binary
+// exponentiation (result times the running square, low bit first), so
+// x^3 = x * (x * x) and x^4 = (x * x) * (x * x), each product rounded.  P = 3
+// and 4; periodic queries take SquaredEuclidean and Manhattan.
+template <int P>
+struct Minkowski : Additive<Minkowski<P>> {
+  static_assert(P == 3 || P == 4, "Minkowski<3> and Minkowski<4>");
+  static constexpr bool kPeriodic = false;
+  template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
+    const A x = abs_val(sub_rn(a, b));
+    const A x2 = mul_rn(x, x);
+    return P == 3 ? mul_rn(x, x2) : mul_rn(x2, x2);
+  }
+  template <typename A> __device__ __forceinline__ static A rect(A rd, A old_off, A new_off) {
+    return add_rn(sub_rn(rd, dist1(old_off, A(0))), dist1(new_off, A(0)));
+  }
+};
+
 // Chebyshev / L-infinity (dist/chebyshev/mod.rs:19-59): dist1 = |a - b|,
 // combine_component keeps the larger value (a component that is not greater,
 // NaN included, leaves the accumulator as it is), and the rectangle distance

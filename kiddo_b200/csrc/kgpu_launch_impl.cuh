@@ -51,6 +51,8 @@ template <typename F>
 inline cudaError_t with_metric(int metric, F&& f) {
   if (metric == KGPU_MANHATTAN) return f(Manhattan());
   if (metric == KGPU_CHEBYSHEV) return f(Chebyshev());
+  if (metric == KGPU_MINKOWSKI3) return f(Minkowski<3>());
+  if (metric == KGPU_MINKOWSKI4) return f(Minkowski<4>());
   return f(SqEuclidean());
 }
 

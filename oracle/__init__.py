@@ -26,7 +26,7 @@ FAM_PERIODIC_NEAREST_N = 5
 FAM_WITHIN = 10
 FAM_PERIODIC_WITHIN = 11
 
-METRICS = {"sqeuclidean": 0, "manhattan": 1, "chebyshev": 2}
+METRICS = {"sqeuclidean": 0, "manhattan": 1, "chebyshev": 2, "minkowski3": 3, "minkowski4": 4}
 
 
 def build_library(force: bool = False) -> str:

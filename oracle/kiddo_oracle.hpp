@@ -428,6 +428,47 @@ struct Chebyshev {
   }
 };
 
+// Minkowski<P> (dist/minkowski/mod.rs:19-58): dist1 = |a - b|.powi(P), the
+// sum of powered differences without the final root.  Rust's powi is LLVM's
+// llvm.powi, which is expanded by binary exponentiation (result times the
+// running square, low bit first): x^3 = x * (x * x), x^4 = (x * x) * (x * x).
+// Restated for P = 3 and 4; periodic queries are restated for the other
+// metrics.
+template <int P>
+inline double powi_binary(double x) {
+  double res = 1.0, cur = x;
+  bool have = false;
+  for (int e = P; e; e >>= 1) {
+    if (e & 1) {
+      res = have ? res * cur : cur;
+      have = true;
+    }
+    if (e >> 1) cur = cur * cur;
+  }
+  return res;
+}
+template <int P>
+inline float powi_binary(float x) {
+  float res = 1.f, cur = x;
+  bool have = false;
+  for (int e = P; e; e >>= 1) {
+    if (e & 1) {
+      res = have ? res * cur : cur;
+      have = true;
+    }
+    if (e >> 1) cur = cur * cur;
+  }
+  return res;
+}
+template <int P>
+struct Minkowski : Additive<Minkowski<P>> {
+  static constexpr bool kPeriodic = false;
+  template <typename A> static A dist1(A a, A b) { return powi_binary<P>(std::fabs(a - b)); }
+  template <typename A> static A rect_after_update(A rd, A old_off, A new_off) {
+    return (rd - dist1(old_off, A(0))) + dist1(new_off, A(0));
+  }
+};
+
 // combine_component over dist1(point, query), left to right from zero.
 template <typename M, typename A, int K>
 inline A point_dist(const A* c, const A* q) {

@@ -307,8 +307,8 @@ void kor_copy_layout(void* hp, void* stems_out, uint8_t* bytes_out, uint64_t* ex
   });
 }
 
-// metric: 0 SquaredEuclidean, 1 Manhattan, 2 Chebyshev (not periodic: -2 /
-// nullptr).  Outputs are dense [nq * k]
+// metric: 0 SquaredEuclidean, 1 Manhattan, 2 Chebyshev, 3 / 4 Minkowski<3> /
+// Minkowski<4> (the last three not periodic: -2 / nullptr).  Outputs are dense [nq * k]
 // (k = 1 for the nearest-one families); unused slots hold +inf / 0xFFFFFFFF.
 int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint64_t nq,
                     uint32_t k, double radius, int exclusive, int sorted, const void* box,
@@ -328,12 +328,18 @@ int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint6
                                               r, exclusive, sorted,
                                               static_cast<const A*>(box), static_cast<A*>(out_d),
                                               out_i, out_c, nthreads, stats3);
-    if (metric == 2) {
+    if (metric >= 2) {
       if (family == FAM_PERIODIC_NEAREST_ONE || family == FAM_PERIODIC_NEAREST_N) return -2;
-      return query_fixed_t<A, K, Chebyshev>(t, family, static_cast<const A*>(queries), nq, k, r,
-                                            exclusive, sorted, static_cast<const A*>(box),
-                                            static_cast<A*>(out_d), out_i, out_c, nthreads,
-                                            stats3);
+      auto run = [&](auto m) {
+        return query_fixed_t<A, K, decltype(m)>(t, family, static_cast<const A*>(queries), nq, k,
+                                                r, exclusive, sorted, static_cast<const A*>(box),
+                                                static_cast<A*>(out_d), out_i, out_c, nthreads,
+                                                stats3);
+      };
+      if (metric == 2) return run(Chebyshev());
+      if (metric == 3) return run(Minkowski<3>());
+      if (metric == 4) return run(Minkowski<4>());
+      return -1;
     }
     return query_fixed_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, k, r,
                                           exclusive, sorted, static_cast<const A*>(box),
@@ -356,11 +362,17 @@ void* kor_query_radius(void* hp, int family, int metric, const void* queries, ui
       return query_radius_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, r,
                                                exclusive, sorted, static_cast<const A*>(box),
                                                nthreads, stats3);
-    if (metric == 2) {
+    if (metric >= 2) {
       if (family == FAM_PERIODIC_WITHIN) return nullptr;
-      return query_radius_t<A, K, Chebyshev>(t, family, static_cast<const A*>(queries), nq, r,
-                                             exclusive, sorted, static_cast<const A*>(box),
-                                             nthreads, stats3);
+      auto run = [&](auto m) {
+        return query_radius_t<A, K, decltype(m)>(t, family, static_cast<const A*>(queries), nq, r,
+                                                 exclusive, sorted, static_cast<const A*>(box),
+                                                 nthreads, stats3);
+      };
+      if (metric == 2) return run(Chebyshev());
+      if (metric == 3) return run(Minkowski<3>());
+      if (metric == 4) return run(Minkowski<4>());
+      return nullptr;
     }
     return query_radius_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, r,
                                            exclusive, sorted, static_cast<const A*>(box),
@@ -381,6 +393,8 @@ int kor_metric_f64x3(int metric, const double* a, const double* b, double rd, co
   if (metric == 0) return run(SqEuclidean());
   if (metric == 1) return run(Manhattan());
   if (metric == 2) return run(Chebyshev());
+  if (metric == 3) return run(Minkowski<3>());
+  if (metric == 4) return run(Minkowski<4>());
   return -1;
 }
 

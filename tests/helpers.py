@@ -38,6 +38,11 @@ def brute_dists(points, q, metric="sqeuclidean"):
         if metric == "chebyshev":
             comp = np.abs(diff)
             acc = np.where(comp > acc, comp, acc).astype(P.dtype)
+        elif metric in ("minkowski3", "minkowski4"):
+            a = np.abs(diff)
+            sq = (a * a).astype(P.dtype)
+            comp = (a * sq) if metric == "minkowski3" else (sq * sq)  # llvm.powi expansion
+            acc = (acc + comp.astype(P.dtype)).astype(P.dtype)
         else:
             acc = (acc + (diff * diff if metric == "sqeuclidean" else np.abs(diff))).astype(P.dtype)
     return acc

@@ -37,13 +37,15 @@ def _pair(P, bh, items=None):
 
 def _metric(m):
     return {"sqeuclidean": kb.SquaredEuclidean, "manhattan": kb.Manhattan,
-            "chebyshev": kb.Chebyshev}[m]
+            "chebyshev": kb.Chebyshev, "minkowski3": kb.Minkowski(3),
+            "minkowski4": kb.Minkowski(4)}[m]
 
 
 @pytest.mark.parametrize("bh", [3, 4])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("dims", [2, 3])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev",
+                                    "minkowski3", "minkowski4"])
 @pytest.mark.parametrize("data", ["uniform", "quantized", "clustered"])
 def test_fixed_families_donnelly(bh, dtype, dims, metric, data):
     rng = np.random.default_rng(zlib.crc32(f"don{bh}{dims}{metric}{data}".encode()))
@@ -57,7 +59,8 @@ def test_fixed_families_donnelly(bh, dtype, dims, metric, data):
     g = t.query(Q).nearest_one(M).approx().execute_gpu()
     od, oi = o.approx_nearest_one(Q, metric=metric)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "approx")
-    r = {"sqeuclidean": 0.001, "manhattan": 0.03, "chebyshev": 0.015}[metric]
+    r = {"sqeuclidean": 0.001, "manhattan": 0.03, "chebyshev": 0.015, "minkowski3": 3e-5,
+         "minkowski4": 1e-6}[metric]
     for k in (1, 5, 16, 32):
         g = t.query(Q).nearest_n(M, k).execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, k, metric=metric),
@@ -84,7 +87,8 @@ def test_fixed_families_donnelly(bh, dtype, dims, metric, data):
 
 @pytest.mark.parametrize("bh", [3, 4])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev",
+                                    "minkowski3", "minkowski4"])
 def test_within_families_donnelly(bh, dtype, metric):
     rng = np.random.default_rng(17 + bh)
     P = DATASETS["uniform"](rng, 30000, 3, dtype)
@@ -93,7 +97,9 @@ def test_within_families_donnelly(bh, dtype, metric):
     M = _metric(metric)
     cases = {"sqeuclidean": ((1e-5, 2000), (3e-4, 2000), (4e-3, 2000), (0.15, 120)),
              "manhattan": ((0.005, 2000), (0.04, 2000), (0.2, 2000), (0.6, 120)),
-             "chebyshev": ((0.003, 2000), (0.03, 2000), (0.1, 2000), (0.3, 120))}[metric]
+             "chebyshev": ((0.003, 2000), (0.03, 2000), (0.1, 2000), (0.3, 120)),
+             "minkowski3": ((3e-8, 2000), (5e-6, 2000), (2.5e-4, 2000), (0.06, 120)),
+             "minkowski4": ((1e-10, 2000), (8e-8, 2000), (1.6e-5, 2000), (0.023, 120))}[metric]
     for r, nq in cases:
         Qr = Q[:nq]
         for excl in (False, True):

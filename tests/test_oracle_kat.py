@@ -84,10 +84,15 @@ def test_metric_known_answers():
     assert oracle.metric_f64x3("chebyshev", a, b, 5.0, [0.0, 2.0, 5.0], 0, 6.0)[1] == 6.0
     # a NaN component is not greater than the accumulator, so it is passed over
     assert oracle.metric_f64x3("chebyshev", [np.nan, 2.0, 3.0], b, 0, [0, 0, 0], 0, 0)[0] == 4.0
+    # Minkowski<3>: sum of |dx|^3 (dist/mod.rs:1497-1507)
+    assert oracle.metric_f64x3("minkowski3", a, [4.0, 2.5, -1.0], 0, [0, 0, 0], 0, 0)[0] == 91.125
+    assert oracle.metric_f64x3("minkowski4", a, [4.0, 2.5, -1.0], 0, [0, 0, 0], 0, 0)[0] == \
+        81.0 + 0.0625 + 256.0
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev", "minkowski3",
+                                    "minkowski4"])
 @pytest.mark.parametrize("n", [1, 31, 33, 1000, 20000])
 def test_oracle_vs_brute_force(dtype, metric, n):
     rng = np.random.default_rng(n)
@@ -97,8 +102,8 @@ def test_oracle_vs_brute_force(dtype, metric, n):
     d1, i1 = t.nearest_one(Q, metric=metric)
     k = 8
     dn, inn, cn = t.nearest_n(Q, k, metric=metric)
-    r = np.asarray({"sqeuclidean": 0.02, "manhattan": 0.2, "chebyshev": 0.08}[metric],
-                   dtype=dtype)
+    r = np.asarray({"sqeuclidean": 0.02, "manhattan": 0.2, "chebyshev": 0.08,
+                    "minkowski3": 0.002, "minkowski4": 0.0002}[metric], dtype=dtype)
     off, dw, iw = t.within(Q, float(r), metric=metric)
     bd_, bi_, bc_ = t.best_n_within(Q, float(r), 5, metric=metric)
     for j in range(len(Q)):
