@@ -498,9 +498,14 @@ template <typename A>
 cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   // thread engine for 2-D/3-D trees; periodic nearest_one stays on the warp
   // engine (home query plus images)
-  const bool big_k = (q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
-                      q.family == KGPU_BEST_N_WITHIN) &&
-                     q.k > kMaxK;
+  // lists above 32 entries: nearest_n up to kMaxThreadK stays on the thread
+  // engine (per-thread lists in 128-thread blocks: 136M against 62M queries/s
+  // at k = 33 on C2's data, 42M against 36M at 64); larger k (the warp engine
+  // was faster from k = 100), and best_n_within above 32, run on the warp
+  // engine's shared-memory lists
+  const bool nn = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN;
+  const bool big_k = q.k > kMaxK && (q.family == KGPU_BEST_N_WITHIN ||
+                                     (nn && (q.k > kMaxThreadK || q.periodic)));
   const bool thread = (t.bh || q.engine != 1) && (t.dims == 2 || t.dims == 3) &&
                       (!q.periodic || q.family != KGPU_NEAREST_ONE) && !big_k;
   return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);

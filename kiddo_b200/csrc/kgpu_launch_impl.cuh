@@ -24,15 +24,16 @@ inline TreeView<A> make_view(const DeviceTree& t) {
   return v;
 }
 
-// Persistent grid: as many 256-thread blocks as fit on all SMs at once.
+// Persistent grid: as many blocks of `threads` threads as fit on all SMs at once.
 template <typename Kern>
-inline int grid_for(Kern kern, size_t smem, uint64_t work_warps) {
+inline int grid_for(Kern kern, size_t smem, uint64_t work_warps, int threads = 256) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const uint64_t full = uint64_t(per_sm) * sm_count();
-  const uint64_t need = (work_warps + 7) / 8;
+  const uint64_t warps = uint64_t(threads) / 32;
+  const uint64_t need = (work_warps + warps - 1) / warps;
   return int(need < full ? (need > 0 ? need : 1) : full);
 }
 
@@ -180,8 +181,11 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
   const int levels = t.max_stem_level + 2;
   const bool list = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
                     q.family == KGPU_BEST_N_WITHIN;
-  const size_t walk = size_t(levels) * 256 * (STEMS ? 2 * sizeof(A) + 4 : sizeof(A));
-  const size_t smem = walk + (list ? size_t(q.k) * 256 * (sizeof(A) + sizeof(uint32_t)) : 0);
+  // nearest_n lists of 33..kMaxThreadK entries fit in shared memory with
+  // 128-thread blocks (up to 96 KB of lists per block)
+  const int threads = (list && q.k > kMaxK) ? 128 : 256;
+  const size_t walk = size_t(levels) * threads * (STEMS ? 2 * sizeof(A) + 4 : sizeof(A));
+  const size_t smem = walk + (list ? size_t(q.k) * threads * (sizeof(A) + sizeof(uint32_t)) : 0);
   return with_dims(t.dims, [&](auto kk) -> cudaError_t {
     constexpr int K = decltype(kk)::value;
     if constexpr (!thread_engine_dims(K)) {
@@ -208,8 +212,8 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
           }
           auto runt = [&](auto kern) {
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
-            kern<<<grid, 256, smem, q.stream>>>(tv, b, levels, q.k, radius, q.sorted ? 0 : 1,
+            const int grid = grid_for(kern, smem, (q.nq + 31) / 32, threads);
+            kern<<<grid, threads, smem, q.stream>>>(tv, b, levels, q.k, radius, q.sorted ? 0 : 1,
                                                 static_cast<A*>(q.out_d), q.out_i, q.out_c,
                                                 q.stats);
             g_launches++;

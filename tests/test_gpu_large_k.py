@@ -25,6 +25,13 @@ def test_large_k_matches_the_oracle(dtype, dims):
     for k in (33, 64, 100, 192, 256):
         g = t.query(Q).nearest_n(kb.SquaredEuclidean, k).execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, k), f"k={k}")
+    if dims in (2, 3):
+        # up to k = 64 both engines serve it: per-thread lists (128-thread
+        # blocks) by default, warp lists on request
+        for engine in ("thread", "warp"):
+            g = t.query(Q).with_engine(engine).nearest_n(kb.SquaredEuclidean, 48).execute_gpu()
+            assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, 48),
+                              f"k=48 engine={engine}")
     for k in (48, 200):
         g = t.query(Q).nearest_n(kb.Manhattan, k).unsorted().execute_gpu()
         assert_same_fixed(g.distances, g.items, g.counts,
