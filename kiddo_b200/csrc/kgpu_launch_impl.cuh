@@ -182,7 +182,7 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
   const bool list = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN ||
                     q.family == KGPU_BEST_N_WITHIN;
   // nearest_n lists of 33..kMaxThreadK entries fit in shared memory with
-  // 128-thread blocks (up to 96 KB of lists per block)
+  // 128-thread blocks (at k = 64: 64 KB of lists per block, 96 KB in f64)
   const int threads = (list && q.k > kMaxK) ? 128 : 256;
   const size_t walk = size_t(levels) * threads * (STEMS ? 2 * sizeof(A) + 4 : sizeof(A));
   const size_t smem = walk + (list ? size_t(q.k) * threads * (sizeof(A) + sizeof(uint32_t)) : 0);
