@@ -206,6 +206,28 @@ int32_t kgpu_tree_read_layout(const kgpu_tree* tree, void* stems, uint8_t* leaf_
  *              leaf_bytes_len, device bytes held */
 int32_t kgpu_tree_info(const kgpu_tree* tree, int64_t* info);
 
+/* ---- iteration order and stored points -------------------------------------
+ * The tree's entries in the reference's iteration order (KdTreeIter,
+ * src/kd_tree/iter.rs:54-90; KdTree::iter, src/kd_tree/mod.rs:481): leaf 0 to
+ * leaf_count - 1, each leaf's entries in stored order.  An entry's position
+ * in that sequence is its rank.  Device pointers; the tree's device must be
+ * current.
+ * kgpu_tree_iter writes out_items[size] and out_points[size * dims] (values
+ * of the tree's dtype) in rank order; either may be NULL.
+ * kgpu_tree_project backs QueryBuilder::with_points
+ * (src/kd_tree/query/builder.rs:1982-1987, 2175-2305): for each of n result
+ * items it writes the entry's rank to out_ranks[n] and its stored point to
+ * out_points[n * dims] (either may be NULL); an item not in the tree, such as
+ * the 0xFFFFFFFF of an unused result slot, gives rank 0xFFFFFFFF and a zero
+ * point.  An item must name one entry: KGPU_EUNSUPPORTED when two entries of
+ * the tree share an item, or for trees of 2^32 - 1 entries or more.  The
+ * first call for a tree builds its table (the points in rank order and the
+ * items sorted: dims values of the dtype + 8 bytes per entry, held until
+ * kgpu_tree_destroy) and synchronizes `stream`. */
+int32_t kgpu_tree_iter(kgpu_tree* tree, uint32_t* out_items, void* out_points, void* stream);
+int32_t kgpu_tree_project(kgpu_tree* tree, const uint32_t* items, uint64_t n, uint32_t* out_ranks,
+                          void* out_points, void* stream);
+
 /* ---- fixed-size families --------------------------------------------------
  * KGPU_NEAREST_ONE, KGPU_APPROX_NEAREST_ONE: out_dists/out_items hold nq
  * entries.  KGPU_NEAREST_N, KGPU_NEAREST_N_WITHIN, KGPU_BEST_N_WITHIN: they

@@ -356,6 +356,43 @@ class GpuTree:
         return dict(zip(["dtype", "dims", "size", "leaf_count", "max_stem_level", "stem_count",
                          "leaf_bytes_len", "device_bytes"], a.tolist()))
 
+    def iter(self, stream=None):
+        """The tree's entries as CUDA tensors (items [size] int32 holding the
+        uint32 values, points [size, dims]) in the reference's iteration order
+        (KdTree::iter, src/kd_tree/iter.rs:64-90): leaf by leaf, each leaf's
+        entries in stored order (kgpu_tree_iter)."""
+        import torch
+        n = self.size()
+        tdt = torch.float32 if self.dtype == np.float32 else torch.float64
+        items = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+        pts = torch.empty((max(n, 1), self.dims), dtype=tdt, device="cuda")
+        st = stream if stream is not None else torch.cuda.current_stream()
+        C.check(C.lib().kgpu_tree_iter(self._h, ctypes.c_void_p(items.data_ptr()),
+                                       ctypes.c_void_p(pts.data_ptr()), _stream_ptr(st)))
+        return items[:n], pts[:n]
+
+    def project(self, items, stream=None):
+        """(ranks, points) of result items (a CUDA int32 tensor of any shape):
+        each item's position in iteration order (-1 as int32 when the item is
+        not in the tree) and its stored point (kgpu_tree_project).  Needs
+        distinct items in the tree."""
+        import torch
+        tdt = torch.float32 if self.dtype == np.float32 else torch.float64
+        it = items.contiguous()
+        ranks = torch.empty(it.shape, dtype=torch.int32, device=it.device)
+        pts = torch.empty(tuple(it.shape) + (self.dims,), dtype=tdt, device=it.device)
+        st = stream if stream is not None else torch.cuda.current_stream(it.device)
+        C.check(C.lib().kgpu_tree_project(self._h, ctypes.c_void_p(it.data_ptr()), it.numel(),
+                                          ctypes.c_void_p(ranks.data_ptr()),
+                                          ctypes.c_void_p(pts.data_ptr()), _stream_ptr(st)))
+        return ranks, pts
+
+    def _self_forest(self):
+        f = getattr(self, "_forest", None)
+        if f is None:
+            f = self._forest = Forest([self])
+        return f
+
     def query(self, queries) -> "QueryBuilder":
         return QueryBuilder(self, queries)
 
@@ -372,6 +409,7 @@ def _stream_ptr(stream):
 class NearestOneResult:
     distances: object
     items: object
+    points: object = None  # with_points(): [nq, dims]
 
 
 @dataclass
@@ -379,6 +417,7 @@ class NearestNResult:
     distances: object
     items: object
     counts: object
+    points: object = None  # with_points(): [nq, max_qty, dims], zeros in unused slots
 
 
 @dataclass
@@ -386,12 +425,15 @@ class WithinResult:
     offsets: object
     distances: object
     items: object
+    points: object = None  # with_points(): [total, dims]
 
     def __len__(self):
         return len(self.offsets) - 1
 
     def __getitem__(self, i):
         a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+        if self.points is not None:
+            return self.distances[a:b], self.items[a:b], self.points[a:b]
         return self.distances[a:b], self.items[a:b]
 
 
@@ -411,11 +453,16 @@ class QueryBuilder:
         self.spatial_order = None  # None: the library decides
         self.engine = None
         self.stream = None
+        self.points = False
+        self.want_items = True
+        self.want_distances = True
 
     # ---- space --------------------------------------------------------------
     def periodic_boundary_condition(self, box_size) -> "QueryBuilder":
         if self.family is not None:
             raise TypeError("periodic_boundary_condition must be chosen before the query type")
+        if self.points:
+            raise TypeError("with_points() is available only for non-periodic queries")
         box = np.ascontiguousarray(box_size, dtype=self.tree.dtype).reshape(-1)
         if box.size != self.tree.dims:
             raise ValueError("box_size must have one entry per axis")
@@ -478,6 +525,56 @@ class QueryBuilder:
         if self.family not in (C.WITHIN, C.WITHIN_UNSORTED, C.NEAREST_N_WITHIN, C.BEST_N_WITHIN):
             raise TypeError("exclusive_boundaries() applies to radius-bounded queries")
         self.exclusive = True
+        return self
+
+    # ---- projections ----------------------------------------------------------
+    def with_points(self) -> "QueryBuilder":
+        """Return each hit's stored point too (QueryBuilder::with_points,
+        src/kd_tree/query/builder.rs:1982-1987; non-periodic queries only).
+
+        The reference answers these queries by scanning the tree in iteration
+        order (builder.rs:2175-2305), and so does the result here:
+          * nearest_one (and approx, which the scan makes exact): the first
+            entry in iteration order at the least distance;
+          * within().unsorted(): the hits in iteration order;
+          * within, nearest_n, nearest_n().within (sorted or not): by distance,
+            equal distances in iteration order.  The reference sorts with
+            slice::sort_unstable, whose order of equal distances, and choice
+            among equal distances at the max_qty cut, Rust leaves unspecified;
+            here the cut follows nearest_n's own rule;
+          * best_n_within: ascending item.
+        Items must be distinct (KGPU_EUNSUPPORTED otherwise); nearest_one takes
+        Eytzinger trees."""
+        if self.box is not None:
+            raise TypeError("with_points() is available only for non-periodic queries")
+        self.points = True
+        return self
+
+    def without_points(self) -> "QueryBuilder":
+        """Leave the stored points out again (builder.rs:1926-1933)."""
+        self.points = False
+        return self
+
+    def with_items(self) -> "QueryBuilder":
+        """Include the items in the results (builder.rs:1935-1942), the default."""
+        self.want_items = True
+        return self
+
+    def without_items(self) -> "QueryBuilder":
+        """Leave the items out of the results: ``items`` is None
+        (builder.rs:1944-1951).  The query itself is unchanged."""
+        self.want_items = False
+        return self
+
+    def with_distances(self) -> "QueryBuilder":
+        """Include the distances in the results (builder.rs:1953-1960), the default."""
+        self.want_distances = True
+        return self
+
+    def without_distances(self) -> "QueryBuilder":
+        """Leave the distances out of the results: ``distances`` is None
+        (builder.rs:1962-1969).  The query itself is unchanged."""
+        self.want_distances = False
         return self
 
     def with_spatial_order(self, on: Optional[bool] = True) -> "QueryBuilder":
@@ -551,9 +648,115 @@ class QueryBuilder:
     def execute_gpu(self):
         if self.family is None:
             raise TypeError("choose a query type before execute_gpu()")
-        if _is_torch_cuda(self.queries):
-            return self._execute_device()
-        return self._execute_host()
+        if self.points:
+            res = self._execute_points()
+        elif _is_torch_cuda(self.queries):
+            res = self._execute_device()
+        else:
+            res = self._execute_host()
+        if not self.want_items:
+            res.items = None
+        if not self.want_distances:
+            res.distances = None
+        return res
+
+    def _sub(self, family, queries):
+        """A copy of this builder without projections, for another family."""
+        b = QueryBuilder(self.tree, queries)
+        b.__dict__.update({k: v for k, v in self.__dict__.items() if k != "queries"})
+        b.points = False
+        b.want_items = b.want_distances = True
+        b.family = family
+        return b
+
+    def _execute_points(self):
+        import torch
+        host = not _is_torch_cuda(self.queries)
+        if host:
+            qh = np.ascontiguousarray(self.queries, dtype=self.tree.dtype)
+            if qh.ndim == 1:
+                qh = qh.reshape(1, -1)
+            q = torch.from_numpy(qh).cuda()
+        else:
+            q = self.queries.contiguous()
+        if q.shape[1] != self.tree.dims:
+            raise ValueError("query dimensionality does not match the tree")
+        nq = q.shape[0]
+        stream = self.stream if self.stream is not None else torch.cuda.current_stream(q.device)
+        fam = self.family
+        if fam in (C.NEAREST_ONE, C.APPROX_NEAREST_ONE):
+            res = self._points_nearest_one(q, stream)
+        elif fam in (C.WITHIN, C.WITHIN_UNSORTED):
+            r = self._sub(C.WITHIN_UNSORTED, q)._execute_device()
+            ranks, pts = self.tree.project(r.items, stream)
+            off = r.offsets
+            rows = torch.repeat_interleave(torch.arange(nq, device=q.device),
+                                           off[1:] - off[:-1], output_size=r.items.shape[0])
+            # iteration order inside each row; then by distance, stably, when sorted
+            order = torch.argsort(rows.to(torch.int64) * (1 << 32) +
+                                  ranks.to(torch.int64).remainder(1 << 32), stable=True)
+            if fam == C.WITHIN:
+                o2 = torch.argsort(r.distances[order], stable=True)
+                order = order[o2][torch.argsort(rows[order][o2], stable=True)]
+            res = WithinResult(off, r.distances[order], r.items[order], pts[order])
+        else:
+            r = self._sub(fam, q)
+            if fam != C.BEST_N_WITHIN:
+                r.sorted = True
+            r = r._execute_device()
+            ranks, pts = self.tree.project(r.items, stream)
+            if fam == C.BEST_N_WITHIN:
+                res = NearestNResult(r.distances, r.items, r.counts, pts)
+            else:
+                # by distance, equal distances in iteration order; unused slots
+                # (rank 0xFFFFFFFF, distance +inf) stay last
+                key = ranks.to(torch.int64).remainder(1 << 32)
+                o1 = torch.argsort(key, dim=1, stable=True)
+                o2 = torch.argsort(torch.gather(r.distances, 1, o1), dim=1, stable=True)
+                order = torch.gather(o1, 1, o2)
+                res = NearestNResult(torch.gather(r.distances, 1, order),
+                                     torch.gather(r.items, 1, order), r.counts,
+                                     pts[torch.arange(nq, device=q.device)[:, None], order])
+        if not host:
+            return res
+        torch.cuda.synchronize()
+        out = {}
+        for k, v in res.__dict__.items():
+            a = v.cpu().numpy() if v is not None else None
+            if a is not None and k in ("items", "counts") and a.dtype == np.int32:
+                a = a.view(np.uint32)
+            if a is not None and k == "offsets":
+                a = a.astype(np.uint64)
+            out[k] = a
+        return type(res)(**out)
+
+    def _points_nearest_one(self, q, stream):
+        """scan_projected_nearest_one (builder.rs:2175-2212): the first entry in
+        iteration order at the least distance.  The least distance comes from
+        the nearest_one traversal, every entry at that distance from a radius
+        query with one radius per query, and the earliest of them by rank."""
+        import torch
+        nq, K = q.shape[0], self.tree.dims
+        tdt = q.dtype
+        if self.tree.size() == 0:
+            return NearestOneResult(torch.full((nq,), float("inf"), dtype=tdt, device=q.device),
+                                    torch.zeros(nq, dtype=torch.int32, device=q.device),
+                                    torch.zeros((nq, K), dtype=tdt, device=q.device))
+        best = self._sub(C.NEAREST_ONE, q)._execute_device().distances
+        fq = self.tree._self_forest().query(q, torch.zeros(nq, dtype=torch.int32, device=q.device),
+                                            best)
+        fq.stream = self.stream
+        fq.family, fq.metric = C.WITHIN_UNSORTED, self.metric
+        fq.radius = float("inf")
+        r = fq.execute_gpu()
+        ranks, pts = self.tree.project(r.items, stream)
+        off = r.offsets
+        rows = torch.repeat_interleave(torch.arange(nq, device=q.device), off[1:] - off[:-1],
+                                       output_size=r.items.shape[0])
+        key = rows.to(torch.int64) * (1 << 32) + ranks.to(torch.int64).remainder(1 << 32)
+        order = torch.argsort(key, stable=True)
+        first = order[off[:-1]]  # each row's least rank
+        return NearestOneResult(r.distances[first], r.items[first], pts[first])
 
     def _execute_host(self):
         L = C.lib()

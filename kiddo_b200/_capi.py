@@ -33,7 +33,8 @@ EXPORTED_SYMBOLS = [
     "kgpu_last_error", "kgpu_status_string", "kgpu_abi_version", "kgpu_layout_build",
     "kgpu_layout_build_stems", "kgpu_tree_build", "kgpu_tree_read_layout",
     "kgpu_layout_describe", "kgpu_layout_free", "kgpu_tree_create", "kgpu_tree_destroy",
-    "kgpu_tree_info", "kgpu_query", "kgpu_query_radius_count", "kgpu_query_radius_fill",
+    "kgpu_tree_info", "kgpu_tree_iter", "kgpu_tree_project", "kgpu_query",
+    "kgpu_query_radius_count", "kgpu_query_radius_fill",
     "kgpu_launch_count", "kgpu_query_stats", "kgpu_query_radius_count_noalloc",
     "kgpu_forest_create", "kgpu_forest_destroy", "kgpu_forest_query",
     "kgpu_forest_query_radius_count", "kgpu_forest_query_radius_fill", "kgpu_graph_begin",
@@ -118,6 +119,10 @@ def lib():
     L.kgpu_tree_destroy.argtypes = [vp]
     L.kgpu_tree_info.restype = i32
     L.kgpu_tree_info.argtypes = [vp, vp]
+    L.kgpu_tree_iter.restype = i32
+    L.kgpu_tree_iter.argtypes = [vp, vp, vp, vp]
+    L.kgpu_tree_project.restype = i32
+    L.kgpu_tree_project.argtypes = [vp, vp, u64, vp, vp, vp]
     L.kgpu_query.restype = i32
     L.kgpu_query.argtypes = [vp, ctypes.POINTER(QueryDesc), vp, u64, vp, vp, vp, vp]
     L.kgpu_query_radius_count.restype = i32

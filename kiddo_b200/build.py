@@ -25,6 +25,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]
 CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kgpu_forest.cu",
               "kgpu_build.cu",
               "kgpu_chamfer.cu",
+              "kgpu_points.cu",
               "kernels_f32_warp.cu",
               "kernels_f32_thread.cu",
               "kernels_f32_donnelly.cu",

@@ -87,6 +87,13 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
 }
 
 void release_tree_arrays(DeviceTree& dt) {
+  cudaFree(dt.iter_points);
+  cudaFree(dt.sorted_items);
+  cudaFree(dt.sorted_ranks);
+  dt.iter_points = nullptr;
+  dt.sorted_items = nullptr;
+  dt.sorted_ranks = nullptr;
+  dt.items_distinct = -1;
   if (dt.pooled) {
     // the arrays came from the device's stream-ordered pool: wait for every
     // stream, as cudaFree would, then return them to the pool

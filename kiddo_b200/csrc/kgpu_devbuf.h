@@ -17,7 +17,7 @@ namespace kgpu {
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 
 struct DeviceTree;
-// Frees a tree's stems, arena and extents, from the pool (DeviceTree::pooled)
+// Frees a tree's stems, arena, extents and point table, from the pool (DeviceTree::pooled)
 // or from cudaMalloc, after the device's pending work.
 void release_tree_arrays(DeviceTree& dt);
 

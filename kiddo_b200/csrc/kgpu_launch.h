@@ -26,6 +26,12 @@ struct DeviceTree {
   // f64 3-D leaves are 32-byte rows with offsets of their own: the reference
   // layout's extents, uint2 (offset / 8, len), for read-back; null otherwise
   void* src_extents = nullptr;
+  // stored points of query results (kgpu_tree_project), built on first use:
+  // the entries' points in iteration order, and (item, rank) sorted by item
+  void* iter_points = nullptr;
+  uint32_t* sorted_items = nullptr;
+  uint32_t* sorted_ranks = nullptr;
+  int items_distinct = -1;     // -1: not checked yet; 0: two entries share an item; 1: distinct
 };
 
 struct QueryLaunch {

@@ -2,11 +2,14 @@
 // translation units that launch queries on it.
 #pragma once
 
+#include <mutex>
+
 #include "../../include/kiddo_gpu.h"
 #include "kgpu_launch.h"
 
 struct kgpu_tree {
   kgpu::DeviceTree dt;
+  std::mutex points_mu;  // guards the lazily built point table (kgpu_tree_project)
 };
 
 namespace kgpu {

@@ -57,6 +57,7 @@ def lib():
         L.kor_from_layout_ex.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64,
                                          u64, ctypes.c_uint32]
         L.kor_free.argtypes = [vp]
+        L.kor_iter.argtypes = [vp, vp, vp]
         L.kor_layout_info.argtypes = [vp, vp]
         L.kor_copy_layout.argtypes = [vp, vp, vp, vp]
         L.kor_query_fixed.restype = i32
@@ -146,6 +147,18 @@ class OracleTree:
         ex = np.empty((int(info[2]), 2), dtype=np.uint64)
         lib().kor_copy_layout(self._h, _ptr(stems), _ptr(lb), _ptr(ex))
         return Layout(self.dtype, self.k, stems, lb, ex, info[3], info[4], info[5], info[6])
+
+    def iter(self):
+        """(items[size], points[size, K]) in KdTreeIter order
+        (src/kd_tree/iter.rs:64-90): leaf by leaf, each leaf's entries by
+        position."""
+        lay = self.layout()
+        n = int(lay.size)
+        items = np.empty(n, dtype=np.uint32)
+        pts = np.empty((n, self.k), dtype=self.dtype)
+        if n:
+            lib().kor_iter(self._h, _ptr(items), _ptr(pts))
+        return items, pts
 
     def _q(self, queries):
         q = np.ascontiguousarray(queries, dtype=self.dtype)
@@ -255,3 +268,78 @@ def metric_f64x3(metric, a, b, rd, off, dim, new_off):
     if rc != 0:
         raise ValueError(f"unknown metric {metric}")
     return float(out[0]), float(out[1])
+
+
+# ---------------------------------------------------------------------------
+# Point-projected queries (QueryBuilder::with_points).  The reference answers
+# them with a scan of the whole tree in iteration order
+# (src/kd_tree/query/builder.rs:2175-2305), not with the traversal; these
+# functions restate those scans over ``OracleTree.iter()``.
+# ---------------------------------------------------------------------------
+
+def scan_dists(points, q, metric="sqeuclidean"):
+    """D::dist(point, query) for every point (dist/*/mod.rs): components in
+    axis order, accumulated from the first one, in the points' dtype."""
+    P = np.asarray(points)
+    q = np.asarray(q, dtype=P.dtype)
+    acc = np.zeros(P.shape[0], dtype=P.dtype)
+    for d in range(P.shape[1]):
+        diff = (P[:, d] - q[d]).astype(P.dtype)
+        if metric == "chebyshev":
+            comp = np.abs(diff)
+            acc = np.where(comp > acc, comp, acc).astype(P.dtype)
+        elif metric in ("minkowski3", "minkowski4"):
+            a = np.abs(diff)
+            sq = (a * a).astype(P.dtype)
+            comp = (a * sq) if metric == "minkowski3" else (sq * sq)  # llvm.powi expansion
+            acc = (acc + comp.astype(P.dtype)).astype(P.dtype)
+        else:
+            acc = (acc + (diff * diff if metric == "sqeuclidean" else np.abs(diff))).astype(P.dtype)
+    return acc
+
+
+def _accepts(d, radius, exclusive):
+    # boundary_accepts: inclusive d <= r, exclusive d < r
+    return d < radius if exclusive else d <= radius
+
+
+def projected_nearest_one(tree, query, metric="sqeuclidean"):
+    """scan_projected_nearest_one (builder.rs:2175-2212): the first entry in
+    iteration order whose distance is below every earlier one's.  Returns
+    (distance, item, point, rank); an empty tree gives (inf, 0, zeros, None)."""
+    items, pts = tree.iter()
+    if items.size == 0:
+        return tree.dtype.type(np.inf), 0, np.zeros(tree.k, tree.dtype), None
+    d = scan_dists(pts, query, metric)
+    r = int(np.argmin(d))  # first occurrence of the minimum
+    return d[r], int(items[r]), pts[r].copy(), r
+
+
+def projected_nearest(tree, query, metric="sqeuclidean", radius=None, max_qty=None,
+                      sorted=True, exclusive=False):
+    """scan_projected_nearest_results (builder.rs:2214-2260): every entry in
+    iteration order that the radius accepts; sorted by distance when asked or
+    when max_qty is given, then cut to max_qty.  The reference sorts with
+    slice::sort_unstable, which leaves the order of equal distances
+    unspecified; this restatement keeps them in iteration order.  Returns
+    (distances, items, points, ranks)."""
+    items, pts = tree.iter()
+    d = scan_dists(pts, query, metric)
+    keep = np.arange(items.size) if radius is None else np.nonzero(
+        _accepts(d, tree.dtype.type(radius), exclusive))[0]
+    if sorted or max_qty is not None:
+        keep = keep[np.argsort(d[keep], kind="stable")]
+        if max_qty is not None:
+            keep = keep[:max_qty]
+    return d[keep], items[keep], pts[keep], keep
+
+
+def projected_best(tree, query, radius, max_qty, metric="sqeuclidean", exclusive=False):
+    """scan_projected_best_results (builder.rs:2262-2305): the max_qty entries
+    with the smallest (item, distance) among those the radius accepts, as the
+    heap's set; returned sorted by (item, distance)."""
+    items, pts = tree.iter()
+    d = scan_dists(pts, query, metric)
+    keep = np.nonzero(_accepts(d, tree.dtype.type(radius), exclusive))[0]
+    keep = keep[np.lexsort((d[keep], items[keep]))][:max_qty]
+    return d[keep], items[keep], pts[keep], keep

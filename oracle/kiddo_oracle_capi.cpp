@@ -275,6 +275,27 @@ void* kor_from_layout(int dtype, int k, const void* stems, uint64_t stems_len,
 
 void kor_free(void* h) { delete static_cast<TreeBase*>(h); }
 
+// KdTreeIter::next (src/kd_tree/iter.rs:64-90): leaf 0 to leaf_count - 1,
+// each leaf's entries by position (leaf_point_item), which for VecOfArenas is
+// the tile order of for_each_point.  Writes size items and size * K points.
+void kor_iter(void* hp, uint32_t* items_out, void* points_out) {
+  auto* b = static_cast<TreeBase*>(hp);
+  dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    A* pts = static_cast<A*>(points_out);
+    uint64_t r = 0;
+    for (size_t l = 0; l < t.leaf_count(); ++l)
+      t.for_each_point(l, [&](const A (&c)[K], uint32_t item) {
+        items_out[r] = item;
+        for (int d = 0; d < K; ++d) pts[r * K + d] = c[d];
+        ++r;
+      });
+    return 0;
+  });
+}
+
 // layout[0..6] = stems_len, leaf_bytes_len, leaf_count, max_stem_level, size, max_leaf_len,
 // block height (0: Eytzinger)
 void kor_layout_info(void* hp, int64_t* info) {

@@ -30,22 +30,8 @@ def load_kats():
 
 def brute_dists(points, q, metric="sqeuclidean"):
     """Per-point distance with the reference's accumulation order."""
-    P = np.asarray(points)
-    q = np.asarray(q, dtype=P.dtype)
-    acc = np.zeros(P.shape[0], dtype=P.dtype)
-    for d in range(P.shape[1]):
-        diff = (P[:, d] - q[d]).astype(P.dtype)
-        if metric == "chebyshev":
-            comp = np.abs(diff)
-            acc = np.where(comp > acc, comp, acc).astype(P.dtype)
-        elif metric in ("minkowski3", "minkowski4"):
-            a = np.abs(diff)
-            sq = (a * a).astype(P.dtype)
-            comp = (a * sq) if metric == "minkowski3" else (sq * sq)  # llvm.powi expansion
-            acc = (acc + comp.astype(P.dtype)).astype(P.dtype)
-        else:
-            acc = (acc + (diff * diff if metric == "sqeuclidean" else np.abs(diff))).astype(P.dtype)
-    return acc
+    import oracle
+    return oracle.scan_dists(points, q, metric)
 
 
 def gaussian_mixture(n, centres, sigma, background_frac, rng, dtype=np.float32):

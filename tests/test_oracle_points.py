@@ -1,0 +1,71 @@
+"""The oracle's iteration order and point-projected scans, pinned to the
+reference's own known answers (CPU only).
+
+KdTree::iter's documented results (src/kd_tree/construction.rs:255-271,
+:385-400, :1236-1251) fix the iteration order of small trees: a single leaf
+yields its entries in source order.  The projected scans restate
+builder.rs:2175-2305 over that order.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+
+def test_iter_known_answers():
+    # construction.rs:255-271: new_from_slice, f64 3-D
+    t = oracle.OracleTree.build(np.array([[1.0, 2.0, 3.0], [4.0, 5.0, 6.0]]))
+    items, pts = t.iter()
+    assert items.tolist() == [0, 1]
+    assert pts.tolist() == [[1.0, 2.0, 3.0], [4.0, 5.0, 6.0]]
+    # construction.rs:385-400: new_from_entries, f32 2-D
+    t = oracle.OracleTree.build(np.array([[0.0, 1.0], [2.0, 3.0]], np.float32),
+                                np.array([42, 7], np.uint32))
+    items, pts = t.iter()
+    assert items.tolist() == [42, 7]
+    assert pts.tolist() == [[0.0, 1.0], [2.0, 3.0]]
+    # construction.rs:1236-1251 (before its replace_item): f64 2-D entries
+    t = oracle.OracleTree.build(np.array([[1.0, 10.0], [2.0, 20.0], [3.0, 30.0]]),
+                                np.array([20, 21, 22], np.uint32))
+    items, pts = t.iter()
+    assert items.tolist() == [20, 21, 22]
+    assert pts.tolist() == [[1.0, 10.0], [2.0, 20.0], [3.0, 30.0]]
+
+
+@pytest.mark.parametrize("dims", [1, 2, 3, 4])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_iter_is_a_permutation_in_leaf_order(dims, dtype):
+    rng = np.random.default_rng(dims)
+    P = rng.random((3000, dims)).astype(dtype)
+    t = oracle.OracleTree.build(P)
+    items, pts = t.iter()
+    assert sorted(items.tolist()) == list(range(3000))
+    assert np.array_equal(pts, P[items])
+    lay = t.layout()
+    assert int(lay.extents[:, 1].astype(np.int64).sum()) == 3000
+
+
+def test_projected_scans_against_brute_force():
+    rng = np.random.default_rng(5)
+    P = (np.floor(rng.random((2000, 3)) * 8) / 8)  # many equal distances
+    t = oracle.OracleTree.build(P)
+    items, pts = t.iter()
+    q = np.array([0.3, 0.55, 0.7])
+    d = oracle.scan_dists(pts, q)
+    dist, item, point, rank = oracle.projected_nearest_one(t, q)
+    assert rank == int(np.nonzero(d == d.min())[0][0]) and item == items[rank]
+    assert np.array_equal(point, pts[rank])
+    dd, ii, pp, rr = oracle.projected_nearest(t, q, radius=0.05, sorted=False)
+    assert np.all(np.diff(rr) > 0) and np.all(dd <= 0.05)  # iteration order
+    dd, ii, pp, rr = oracle.projected_nearest(t, q, max_qty=40)
+    assert len(dd) == 40 and np.all(np.diff(dd) >= 0)
+    tie = dd[:-1] == dd[1:]
+    assert np.all(rr[:-1][tie] < rr[1:][tie])  # equal distances in iteration order
+    dd, ii, pp, rr = oracle.projected_best(t, q, 0.1, 5)
+    assert np.all(np.diff(ii.astype(np.int64)) > 0) and np.all(dd <= 0.1)
+
+
+def test_empty_tree_nearest_one():
+    t = oracle.OracleTree.build(np.zeros((0, 2), np.float32))
+    dist, item, point, rank = oracle.projected_nearest_one(t, np.zeros(2, np.float32))
+    assert np.isinf(dist) and item == 0 and rank is None and point.tolist() == [0.0, 0.0]
