@@ -436,6 +436,24 @@ class WithinResult:
             return self.distances[a:b], self.items[a:b], self.points[a:b]
         return self.distances[a:b], self.items[a:b]
 
+    def iter(self):
+        """Yields (query index, distance, item, point) per hit, query by query,
+        each query's hits in the result's order; fields left out by
+        without_distances / without_items / no with_points are None."""
+        off = self.offsets
+        for i in range(len(off) - 1):
+            for j in range(int(off[i]), int(off[i + 1])):
+                yield (i,
+                       None if self.distances is None else self.distances[j],
+                       None if self.items is None else self.items[j],
+                       None if self.points is None else self.points[j])
+
+    def visit(self, visitor):
+        """Calls visitor(query index, distance, item, point) once per hit, in
+        the order of ``iter()``."""
+        for hit in self.iter():
+            visitor(*hit)
+
 
 class QueryBuilder:
     """Runtime mirror of the typestate QueryBuilder (builder.rs:1373-1398)."""
@@ -659,6 +677,24 @@ class QueryBuilder:
         if not self.want_distances:
             res.distances = None
         return res
+
+    def visit(self, visitor):
+        """within().unsorted().visit (builder.rs:1643-1665, 5136-5184) for the
+        batch: runs the query, then calls visitor(query index, distance, item,
+        point) per hit, each query's hits in the reference's visiting order
+        (traversal order; iteration order with with_points())."""
+        self._check_streaming()
+        self.execute_gpu().visit(visitor)
+
+    def iter(self):
+        """within().unsorted().iter (builder.rs:5187-5230) for the batch: the
+        hits of ``visit`` as an iterator over the batch's result."""
+        self._check_streaming()
+        return self.execute_gpu().iter()
+
+    def _check_streaming(self):
+        if self.family != C.WITHIN_UNSORTED:
+            raise TypeError("visit() and iter() follow within(...).unsorted()")
 
     def _sub(self, family, queries):
         """A copy of this builder without projections, for another family."""

@@ -69,3 +69,26 @@ def test_empty_tree_nearest_one():
     t = oracle.OracleTree.build(np.zeros((0, 2), np.float32))
     dist, item, point, rank = oracle.projected_nearest_one(t, np.zeros(2, np.float32))
     assert np.isinf(dist) and item == 0 and rank is None and point.tolist() == [0.0, 0.0]
+
+
+def test_within_result_streaming_on_the_host():
+    """QueryBuilder.visit/iter walk the CSR result of within().unsorted(): each
+    query's hits in order, fields that a projection left out as None."""
+    import kiddo_b200 as kb
+    from kiddo_b200 import _capi as C
+    res = kb.WithinResult(np.array([0, 2, 2, 3], np.uint64),
+                          np.array([0.5, 0.25, 0.125], np.float32),
+                          np.array([7, 3, 9], np.uint32), None)
+    assert [(i, float(d), int(it), p) for i, d, it, p in res.iter()] == \
+        [(0, 0.5, 7, None), (0, 0.25, 3, None), (2, 0.125, 9, None)]
+    seen = []
+    res.visit(lambda i, d, it, p: seen.append((i, int(it))))
+    assert seen == [(0, 7), (0, 3), (2, 9)]
+
+    b = kb.QueryBuilder.__new__(kb.QueryBuilder)
+    b.__dict__.update(family=C.WITHIN_UNSORTED)
+    b.execute_gpu = lambda: res
+    assert len(list(b.iter())) == 3
+    b.family = C.WITHIN
+    with pytest.raises(TypeError):
+        b.visit(print)
