@@ -128,6 +128,26 @@ typedef struct kgpu_flatvec_desc {
   uint64_t size;             /* number of points */
 } kgpu_flatvec_desc;
 
+/* A VecOfArrays tree (src/leaf_strategy/vec_of_arrays.rs:51-97): one LeafNode
+ * per leaf, `bucket` (B) slots each, its first `size` slots live. */
+typedef struct kgpu_vecofarrays_desc {
+  uint32_t abi_version;      /* KGPU_ABI_VERSION */
+  int32_t dtype;             /* kgpu_dtype of the axis type A */
+  uint32_t dims;             /* K, 1..4 */
+  int32_t stem_strategy;     /* kgpu_stem_strategy */
+  uint32_t block_height;     /* Donnelly BH; 0 for Eytzinger */
+  int32_t max_stem_level;    /* KdTree::max_stem_level, -1 for a stemless tree */
+  const void* stems;         /* stem_count values of type A */
+  uint64_t stem_count;
+  uint32_t bucket;           /* B, 1..65536 */
+  uint32_t reserved0;
+  const void* content_points; /* leaf_count * dims * bucket values of A: leaf l's
+                                 content_points[d][i] at (l * dims + d) * bucket + i */
+  const uint32_t* content_items; /* leaf_count * bucket values: leaf l's slot i at l * bucket + i */
+  const uint64_t* sizes;     /* leaf_count live-entry counts, each <= bucket */
+  uint64_t leaf_count;
+} kgpu_vecofarrays_desc;
+
 typedef struct kgpu_query_desc {
   uint32_t abi_version;   /* KGPU_ABI_VERSION */
   int32_t family;         /* kgpu_family */
@@ -181,6 +201,13 @@ int32_t kgpu_layout_free(kgpu_layout* layout);
  * the reference's are; f64: 32 bytes per point at offsets of their own).
  * kgpu_tree_read_layout returns the layout's original bytes. */
 int32_t kgpu_tree_create(const kgpu_tree_desc* desc, void* stream, kgpu_tree** out);
+/* Uploads a VecOfArrays tree (KdTree<A, u32, SS, VecOfArrays<A, u32, K, B>, K, B>,
+ * src/leaf_strategy/vec_of_arrays.rs:51-97, append_leaf :249-275): its stems and
+ * each leaf's live slots, in slot order.  Construction hands every leaf
+ * strategy the same leaf chunks in the same order, so the leaves are re-encoded
+ * on the host as VecOfArenas tiles and uploaded as kgpu_tree_create does. */
+int32_t kgpu_tree_create_vecofarrays(const kgpu_vecofarrays_desc* desc, void* stream,
+                                     kgpu_tree** out);
 /* Uploads a tree whose leaves use the FlatVec strategy (KdTree<A, u32, SS,
  * FlatVec<A, u32, K, 32>, K, 32>, src/leaf_strategy/flat_vec.rs:20-26): its
  * stems as in kgpu_tree_desc, its K point columns, items and (start, end)

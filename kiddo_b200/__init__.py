@@ -308,6 +308,40 @@ class GpuTree:
         return cls(None, _handle=h, dtype=dt, dims=len(cols))
 
     @classmethod
+    def from_vec_of_arrays(cls, stems, content_points, content_items, sizes, max_stem_level,
+                           block_height=0, stream=None) -> "GpuTree":
+        """A tree whose leaves use the VecOfArrays strategy
+        (src/leaf_strategy/vec_of_arrays.rs:51-97): `stems` in the stem order of
+        the strategy, each leaf's `content_points` ([leaf_count, K, B]) and
+        `content_items` ([leaf_count, B], uint32) and its live-entry count in
+        `sizes` ([leaf_count]) (kgpu_tree_create_vecofarrays)."""
+        pts = np.ascontiguousarray(content_points)
+        if pts.dtype not in (np.float32, np.float64) or pts.ndim != 3:
+            raise TypeError("content_points must be a float32 or float64 [leaf_count, K, B] array")
+        L_, K, B = pts.shape
+        items = np.ascontiguousarray(content_items, dtype=np.uint32).reshape(L_, B)
+        sz = np.ascontiguousarray(sizes, dtype=np.uint64).reshape(L_)
+        st = np.ascontiguousarray(stems, dtype=pts.dtype)
+        d = C.VecOfArraysDesc()
+        d.abi_version = C.ABI_VERSION
+        d.dtype = C.F32 if pts.dtype == np.float32 else C.F64
+        d.dims = K
+        d.stem_strategy = C.STEM_DONNELLY if block_height else 0
+        d.block_height = int(block_height)
+        d.max_stem_level = int(max_stem_level)
+        d.stems = st.ctypes.data if st.size else None
+        d.stem_count = st.size
+        d.bucket = B
+        d.content_points = pts.ctypes.data if pts.size else None
+        d.content_items = items.ctypes.data if items.size else None
+        d.sizes = sz.ctypes.data if sz.size else None
+        d.leaf_count = L_
+        h = ctypes.c_void_p()
+        C.check(C.lib().kgpu_tree_create_vecofarrays(ctypes.byref(d), _stream_ptr(stream),
+                                                     ctypes.byref(h)))
+        return cls(None, _handle=h, dtype=pts.dtype, dims=K)
+
+    @classmethod
     def build(cls, points, items=None, stream=None) -> "GpuTree":
         """The ImmutableKdTree of CUDA tensor `points` ([n, dims], float32 or
         float64) built on the device (kgpu_tree_build): the same layout, byte for

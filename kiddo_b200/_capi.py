@@ -39,7 +39,7 @@ EXPORTED_SYMBOLS = [
     "kgpu_forest_create", "kgpu_forest_destroy", "kgpu_forest_query",
     "kgpu_forest_query_radius_count", "kgpu_forest_query_radius_fill", "kgpu_graph_begin",
     "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy", "kgpu_chamfer_loss",
-    "kgpu_chamfer_backward", "kgpu_tree_create_flatvec",
+    "kgpu_chamfer_backward", "kgpu_tree_create_flatvec", "kgpu_tree_create_vecofarrays",
 ]
 
 
@@ -65,6 +65,18 @@ class FlatVecDesc(ctypes.Structure):
         ("stem_count", ctypes.c_uint64), ("columns", ctypes.c_void_p * 4),
         ("items", ctypes.c_void_p), ("extents", ctypes.c_void_p),
         ("leaf_count", ctypes.c_uint64), ("size", ctypes.c_uint64),
+    ]
+
+
+class VecOfArraysDesc(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32), ("dtype", ctypes.c_int32), ("dims", ctypes.c_uint32),
+        ("stem_strategy", ctypes.c_int32), ("block_height", ctypes.c_uint32),
+        ("max_stem_level", ctypes.c_int32), ("stems", ctypes.c_void_p),
+        ("stem_count", ctypes.c_uint64), ("bucket", ctypes.c_uint32),
+        ("reserved0", ctypes.c_uint32), ("content_points", ctypes.c_void_p),
+        ("content_items", ctypes.c_void_p), ("sizes", ctypes.c_void_p),
+        ("leaf_count", ctypes.c_uint64),
     ]
 
 
@@ -115,6 +127,9 @@ def lib():
     L.kgpu_tree_create.argtypes = [ctypes.POINTER(TreeDesc), vp, ctypes.POINTER(vp)]
     L.kgpu_tree_create_flatvec.restype = i32
     L.kgpu_tree_create_flatvec.argtypes = [ctypes.POINTER(FlatVecDesc), vp, ctypes.POINTER(vp)]
+    L.kgpu_tree_create_vecofarrays.restype = i32
+    L.kgpu_tree_create_vecofarrays.argtypes = [ctypes.POINTER(VecOfArraysDesc), vp,
+                                               ctypes.POINTER(vp)]
     L.kgpu_tree_destroy.restype = i32
     L.kgpu_tree_destroy.argtypes = [vp]
     L.kgpu_tree_info.restype = i32

@@ -407,6 +407,59 @@ int32_t kgpu_tree_create_flatvec(const kgpu_flatvec_desc* d, void* stream, kgpu_
   return kgpu_tree_create(&td, stream, out);
 }
 
+int32_t kgpu_tree_create_vecofarrays(const kgpu_vecofarrays_desc* d, void* stream,
+                                     kgpu_tree** out) {
+  if (!d || !out) return set_error(KGPU_EINVAL, "NULL argument");
+  *out = nullptr;
+  if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
+  if (d->dtype != KGPU_F32 && d->dtype != KGPU_F64) return set_error(KGPU_EINVAL, "unknown dtype");
+  if (d->dims < 1 || d->dims > uint32_t(kMaxDims))
+    return set_error(KGPU_EINVAL, "dims must be 1..4");
+  if (d->bucket < 1 || d->bucket > 65536) return set_error(KGPU_EINVAL, "bucket must be 1..65536");
+  if (d->leaf_count && (!d->content_points || !d->content_items || !d->sizes))
+    return set_error(KGPU_EINVAL, "NULL leaf arrays");
+  const uint64_t B = d->bucket;
+  const uint32_t K = d->dims;
+  uint64_t n = 0;
+  for (uint64_t l = 0; l < d->leaf_count; ++l) {
+    if (d->sizes[l] > B) return set_error(KGPU_EINVAL, "a leaf's size exceeds its bucket");
+    n += d->sizes[l];
+  }
+  if (n >= 0xFFFFFFFFull) return set_error(KGPU_EOVERFLOW, "2^32 - 1 points or more");
+  // gather the live slots into the FlatVec form: K columns, items, (start, end)
+  const size_t esz = d->dtype == KGPU_F64 ? 8 : 4;
+  std::vector<std::vector<uint8_t>> cols(K, std::vector<uint8_t>(n * esz));
+  std::vector<uint32_t> items(n);
+  std::vector<uint32_t> ext(2 * d->leaf_count);
+  const uint8_t* pts = static_cast<const uint8_t*>(d->content_points);
+  uint64_t at = 0;
+  for (uint64_t l = 0; l < d->leaf_count; ++l) {
+    const uint64_t len = d->sizes[l];
+    for (uint32_t k = 0; k < K; ++k)
+      std::memcpy(cols[k].data() + at * esz, pts + ((l * K + k) * B) * esz, len * esz);
+    std::memcpy(items.data() + at, d->content_items + l * B, len * 4);
+    ext[2 * l] = uint32_t(at);
+    ext[2 * l + 1] = uint32_t(at + len);
+    at += len;
+  }
+  kgpu_flatvec_desc f;
+  std::memset(&f, 0, sizeof(f));
+  f.abi_version = KGPU_ABI_VERSION;
+  f.dtype = d->dtype;
+  f.dims = K;
+  f.stem_strategy = d->stem_strategy;
+  f.block_height = d->block_height;
+  f.max_stem_level = d->max_stem_level;
+  f.stems = d->stems;
+  f.stem_count = d->stem_count;
+  for (uint32_t k = 0; k < K; ++k) f.columns[k] = cols[k].data();
+  f.items = items.data();
+  f.extents = ext.data();
+  f.leaf_count = d->leaf_count;
+  f.size = n;
+  return kgpu_tree_create_flatvec(&f, stream, out);
+}
+
 int32_t kgpu_tree_destroy(kgpu_tree* t) {
   if (!t) return KGPU_OK;
   release_tree_arrays(t->dt);

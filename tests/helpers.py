@@ -127,3 +127,23 @@ def flatvec_parts(tree):
     cols = [np.concatenate(c) if c else np.zeros(0, dt) for c in cols]
     items = np.concatenate(items) if items else np.zeros(0, np.uint32)
     return cols, items, np.asarray(extents, dtype=np.uint32).reshape(-1, 2)
+
+
+def vecofarrays_parts(tree, bucket=32):
+    """The VecOfArrays form (src/leaf_strategy/vec_of_arrays.rs:51-97,
+    append_leaf :249-275) of a host ImmutableKdTree: per leaf, content_points
+    [K, B] and content_items [B] with the live entries first (zeros after) and
+    the live-entry count."""
+    cols, items, ext = flatvec_parts(tree)
+    K = tree.dims
+    L = ext.shape[0]
+    pts = np.zeros((L, K, bucket), dtype=np.dtype(tree.dtype))
+    its = np.zeros((L, bucket), dtype=np.uint32)
+    sizes = np.zeros(L, dtype=np.uint64)
+    for l, (a, b) in enumerate(ext):
+        a, b = int(a), int(b)
+        for d in range(K):
+            pts[l, d, :b - a] = cols[d][a:b]
+        its[l, :b - a] = items[a:b]
+        sizes[l] = b - a
+    return pts, its, sizes

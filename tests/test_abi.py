@@ -188,3 +188,31 @@ def test_query_builder_typestate_errors():
         kb.QueryBuilder(b.tree, q).nearest_one(kb.SquaredEuclidean).exclusive_boundaries()
     with pytest.raises(TypeError):
         kb.QueryBuilder(b.tree, q).execute_gpu()
+
+
+def test_vecofarrays_create_rejects_bad_leaves_before_touching_the_device():
+    """kgpu_tree_create_vecofarrays checks the leaf arrays on the host."""
+    import ctypes
+    from kiddo_b200 import _capi as C
+    L = C.lib()
+    pts = np.zeros((2, 3, 4), np.float32)
+    its = np.zeros((2, 4), np.uint32)
+
+    def create(sizes, bucket=4, dims=3):
+        sz = np.ascontiguousarray(sizes, dtype=np.uint64)
+        d = C.VecOfArraysDesc()
+        d.abi_version = C.ABI_VERSION
+        d.dtype = C.F32
+        d.dims = dims
+        d.max_stem_level = 0
+        d.bucket = bucket
+        d.content_points = pts.ctypes.data
+        d.content_items = its.ctypes.data
+        d.sizes = sz.ctypes.data
+        d.leaf_count = 2
+        h = ctypes.c_void_p()
+        return L.kgpu_tree_create_vecofarrays(ctypes.byref(d), None, ctypes.byref(h))
+
+    assert create([4, 5]) == C.KGPU_EINVAL     # a leaf larger than its bucket
+    assert create([1, 1], bucket=0) == C.KGPU_EINVAL
+    assert create([1, 1], dims=5) == C.KGPU_EINVAL

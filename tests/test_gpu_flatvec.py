@@ -12,7 +12,7 @@ import pytest
 
 import kiddo_b200 as kb
 import oracle
-from helpers import assert_same_csr, assert_same_fixed, flatvec_parts
+from helpers import assert_same_csr, assert_same_fixed, flatvec_parts, vecofarrays_parts
 
 pytestmark = pytest.mark.gpu
 
@@ -56,3 +56,24 @@ def test_flatvec_tree_answers_like_the_oracle(dtype, bh):
     r = g.query(Q).within(kb.Chebyshev, 0.02).execute_gpu()
     assert_same_csr((r.offsets, r.distances, r.items), o.within(Q, 0.02, metric="chebyshev"),
                     "within")
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("dims", [2, 3])
+def test_vecofarrays_upload_reads_back_and_answers(dtype, dims):
+    """A VecOfArrays tree (vec_of_arrays.rs:51-97) of the same points holds the
+    same leaf chunks; kgpu_tree_create_vecofarrays re-encodes its live slots as
+    VecOfArenas tiles, so it reads back as the ImmutableKdTree's bytes."""
+    rng = np.random.default_rng(40 + dims)
+    for n in (0, 5, 20000):
+        P = rng.random((n, dims)).astype(dtype)
+        host = kb.ImmutableKdTree.new_from_slice(P)
+        pts, its, sizes = vecofarrays_parts(host)
+        g = kb.GpuTree.from_vec_of_arrays(host.stems(), pts, its, sizes, host.max_stem_level())
+        stems, lb, ex = g.read_layout()
+        assert np.array_equal(lb, host.leaf_bytes())
+        assert np.array_equal(ex, host.leaf_extents())
+    Q = np.concatenate([rng.random((1000, dims)).astype(dtype), P[:50]])
+    o = oracle.OracleTree.build(P)
+    r = g.query(Q).nearest_n(kb.SquaredEuclidean, 8).execute_gpu()
+    assert_same_fixed(r.distances, r.items, r.counts, *o.nearest_n(Q, 8), "nearest_n(8)")
