@@ -216,3 +216,33 @@ def test_vecofarrays_create_rejects_bad_leaves_before_touching_the_device():
     assert create([4, 5]) == C.KGPU_EINVAL     # a leaf larger than its bucket
     assert create([1, 1], bucket=0) == C.KGPU_EINVAL
     assert create([1, 1], dims=5) == C.KGPU_EINVAL
+
+
+def test_descriptor_layouts_match_the_header(tmp_path):
+    """Every ctypes mirror of a descriptor struct has the C header's size and
+    field offsets (gcc compiles a probe against include/kiddo_gpu.h)."""
+    import shutil
+    import subprocess
+    from kiddo_b200 import _capi as C
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    pairs = {"kgpu_tree_desc": C.TreeDesc, "kgpu_flatvec_desc": C.FlatVecDesc,
+             "kgpu_vecofarrays_desc": C.VecOfArraysDesc, "kgpu_query_desc": C.QueryDesc}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "kiddo_gpu.h"',
+             "int main(void) {"]
+    for cname, cls in pairs.items():
+        lines.append(f'  printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in out.splitlines():
+        cname, fname, value = line.split()
+        cls = pairs[cname]
+        want = ctypes.sizeof(cls) if fname == "sizeof" else getattr(cls, fname).offset
+        assert int(value) == want, (cname, fname, int(value), want)
