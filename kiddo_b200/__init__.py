@@ -422,10 +422,9 @@ class GpuTree:
         return ranks, pts
 
     def _self_forest(self):
-        f = getattr(self, "_forest", None)
-        if f is None:
-            f = self._forest = Forest([self])
-        return f
+        # made per call: a forest cached on the tree would hold the tree in a
+        # reference cycle and keep its device memory until a garbage-collector pass
+        return Forest([self])
 
     def query(self, queries) -> "QueryBuilder":
         return QueryBuilder(self, queries)
