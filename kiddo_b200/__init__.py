@@ -488,6 +488,32 @@ class WithinResult:
             visitor(*hit)
 
 
+def _csr_order(offsets, ranks, dists=None):
+    """Permutation of a CSR result's entries that orders each row by
+    iteration rank, or by (distance, rank) when `dists` is given; rows keep
+    their places.  Ranks are int32 holding uint32 values."""
+    import torch
+    nq = offsets.shape[0] - 1
+    rows = torch.repeat_interleave(torch.arange(nq, device=offsets.device),
+                                   offsets[1:] - offsets[:-1], output_size=ranks.shape[0])
+    order = torch.argsort(rows.to(torch.int64) * (1 << 32) +
+                          ranks.to(torch.int64).remainder(1 << 32), stable=True)
+    if dists is not None:
+        o2 = torch.argsort(dists[order], stable=True)
+        order = order[o2][torch.argsort(rows[order][o2], stable=True)]
+    return order
+
+
+def _row_order(dists, ranks):
+    """Per row of [nq, k] results, the column order by distance, equal
+    distances by iteration rank; unused slots (rank 0xFFFFFFFF, distance +inf)
+    stay last."""
+    import torch
+    o1 = torch.argsort(ranks.to(torch.int64).remainder(1 << 32), dim=1, stable=True)
+    o2 = torch.argsort(torch.gather(dists, 1, o1), dim=1, stable=True)
+    return torch.gather(o1, 1, o2)
+
+
 class QueryBuilder:
     """Runtime mirror of the typestate QueryBuilder (builder.rs:1373-1398)."""
 
@@ -758,16 +784,8 @@ class QueryBuilder:
         elif fam in (C.WITHIN, C.WITHIN_UNSORTED):
             r = self._sub(C.WITHIN_UNSORTED, q)._execute_device()
             ranks, pts = self.tree.project(r.items, stream)
-            off = r.offsets
-            rows = torch.repeat_interleave(torch.arange(nq, device=q.device),
-                                           off[1:] - off[:-1], output_size=r.items.shape[0])
-            # iteration order inside each row; then by distance, stably, when sorted
-            order = torch.argsort(rows.to(torch.int64) * (1 << 32) +
-                                  ranks.to(torch.int64).remainder(1 << 32), stable=True)
-            if fam == C.WITHIN:
-                o2 = torch.argsort(r.distances[order], stable=True)
-                order = order[o2][torch.argsort(rows[order][o2], stable=True)]
-            res = WithinResult(off, r.distances[order], r.items[order], pts[order])
+            order = _csr_order(r.offsets, ranks, r.distances if fam == C.WITHIN else None)
+            res = WithinResult(r.offsets, r.distances[order], r.items[order], pts[order])
         else:
             r = self._sub(fam, q)
             if fam != C.BEST_N_WITHIN:
@@ -777,12 +795,7 @@ class QueryBuilder:
             if fam == C.BEST_N_WITHIN:
                 res = NearestNResult(r.distances, r.items, r.counts, pts)
             else:
-                # by distance, equal distances in iteration order; unused slots
-                # (rank 0xFFFFFFFF, distance +inf) stay last
-                key = ranks.to(torch.int64).remainder(1 << 32)
-                o1 = torch.argsort(key, dim=1, stable=True)
-                o2 = torch.argsort(torch.gather(r.distances, 1, o1), dim=1, stable=True)
-                order = torch.gather(o1, 1, o2)
+                order = _row_order(r.distances, ranks)
                 res = NearestNResult(torch.gather(r.distances, 1, order),
                                      torch.gather(r.items, 1, order), r.counts,
                                      pts[torch.arange(nq, device=q.device)[:, None], order])
@@ -819,12 +832,7 @@ class QueryBuilder:
         fq.radius = float("inf")
         r = fq.execute_gpu()
         ranks, pts = self.tree.project(r.items, stream)
-        off = r.offsets
-        rows = torch.repeat_interleave(torch.arange(nq, device=q.device), off[1:] - off[:-1],
-                                       output_size=r.items.shape[0])
-        key = rows.to(torch.int64) * (1 << 32) + ranks.to(torch.int64).remainder(1 << 32)
-        order = torch.argsort(key, stable=True)
-        first = order[off[:-1]]  # each row's least rank
+        first = _csr_order(r.offsets, ranks)[r.offsets[:-1]]  # each row's least rank
         return NearestOneResult(r.distances[first], r.items[first], pts[first])
 
     def _execute_host(self):

@@ -92,3 +92,31 @@ def test_within_result_streaming_on_the_host():
     b.family = C.WITHIN
     with pytest.raises(TypeError):
         b.visit(print)
+
+
+def test_projection_ordering_rules_on_the_host():
+    """The orderings with_points applies to device results, run here on CPU
+    tensors against numpy's lexsort: CSR rows by rank or (distance, rank),
+    fixed rows by (distance, rank) with unused slots last."""
+    import torch
+    import kiddo_b200 as kb
+    rng = np.random.default_rng(8)
+    counts = rng.integers(0, 25, 60)
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    n = int(off[-1])
+    dist = np.floor(rng.random(n) * 6).astype(np.float32)  # many ties
+    ranks = rng.permutation(1 << 20)[:n].astype(np.int32)
+    rows = np.repeat(np.arange(60), counts)
+    got = kb._csr_order(torch.from_numpy(off), torch.from_numpy(ranks)).numpy()
+    assert np.array_equal(got, np.lexsort((ranks, rows)))
+    got = kb._csr_order(torch.from_numpy(off), torch.from_numpy(ranks),
+                        torch.from_numpy(dist)).numpy()
+    assert np.array_equal(got, np.lexsort((ranks, dist, rows)))
+    D = np.floor(rng.random((40, 12)) * 4).astype(np.float32)
+    R = rng.integers(0, 1000, (40, 12)).astype(np.int32)
+    D[:, 9:] = np.inf
+    R[:, 9:] = -1  # unused slots: rank 0xFFFFFFFF
+    got = kb._row_order(torch.from_numpy(D), torch.from_numpy(R)).numpy()
+    key = R.astype(np.int64) % (1 << 32)
+    for j in range(40):
+        assert np.array_equal(got[j], np.lexsort((key[j], D[j])))
