@@ -12,11 +12,19 @@ synthetic arrays (no dataset); the tree (256 MB arena) and the queries
 (192 MB) are both larger than the 126 MB L2, so no flush is needed between
 steps.
 
+On one GPU the default run measures every term of the metric in the same
+process after the headline: approx on the same tree, the f64 nearest_one and
+periodic configurations, the 256-catalogue forest batched against one launch
+per tree, and Chamfer forward + backward; each becomes a sub-object of the
+headline line (``--headline-only`` skips them).  Every timed result is sampled
+(100,000 rows) against the oracle inside the run (``parity_sample``).
+
 Under torchrun each rank owns one GPU, holds its own replica of the tree and
 answers its own 16M queries (weak scaling, no data-path collective); timing is
 the max over ranks of the CUDA-event time.  `--impl reference` times the CPU
 restatement of the reference path (the oracle; the Rust reference cannot be
-built here) on all host cores.
+built here), built -O3 -march=native on the host it runs on, on all host
+threads; it loads nothing of the product package.
 """
 from __future__ import annotations
 
@@ -71,6 +79,9 @@ def periodic_particles(n, rng, dtype, clumps=4096, sigma=0.002, clumped=0.7):
     pts[pts >= 1.0] = 0.0  # np.mod can round up to the box edge
     return pts[rng.permutation(n)].astype(dtype)
 
+
+# rows of each timed result compared with the oracle inside the run
+SAMPLE_ROWS = 100_000
 
 # radius argument of the periodic neighbour lists, in the metric's own units
 # (SquaredEuclidean: 0.01 = a Euclidean radius of 0.1), as within(0.01) takes it
@@ -188,26 +199,30 @@ def profile_traffic(workload):
         return None
 
 
-def cpu_baseline(tree, Q, workload, target_seconds=12.0, threads=0):
-    """The CPU restatement of the reference path on the host cores, on a
-    bounded sample of the same queries (test infrastructure: the oracle)."""
+def cpu_info():
     import oracle
-    lay = oracle.Layout(tree.dtype, tree.dims, tree.stems(), tree.leaf_bytes(),
-                        tree.leaf_extents(), tree.max_stem_level(), tree.size(),
-                        tree.max_leaf_len())
-    ot = oracle.OracleTree.from_layout(lay)
-    nthreads = threads if threads > 0 else (os.cpu_count() or 1)
+    model, logical, physical = oracle.host_cpu()
+    return {"cpu_model": model, "logical_cpus": logical, "physical_cores": physical}
+
+
+def oracle_family(workload):
+    import oracle
     _, _, _, fam, k = WORKLOADS[workload]
-    famcode = {"nearest_n": oracle.FAM_NEAREST_N, "approx": oracle.FAM_APPROX,
-               "nearest_one": oracle.FAM_NEAREST_ONE,
-               "periodic_nearest_n_within": oracle.FAM_PERIODIC_NEAREST_N}[fam]
-    extra = {}
-    if fam == "periodic_nearest_n_within":
-        extra = {"radius": C5_RADIUS, "box": np.ones(3)}
+    code = {"nearest_n": oracle.FAM_NEAREST_N, "approx": oracle.FAM_APPROX,
+            "nearest_one": oracle.FAM_NEAREST_ONE,
+            "periodic_nearest_n_within": oracle.FAM_PERIODIC_NEAREST_N}[fam]
+    extra = {"radius": C5_RADIUS, "box": np.ones(3)} if fam == "periodic_nearest_n_within" else {}
+    return code, k, extra
+
+
+def time_cpu(ot, Q, workload, target_seconds, threads):
+    """Queries/s of the oracle tree `ot` on a bounded sample of Q: a first
+    pass of 20,000 queries sizes a sample of about `target_seconds`."""
+    fam, k, extra = oracle_family(workload)
 
     def run(m):
         t0 = time.perf_counter()
-        ot.query_fixed(famcode, Q[:m], k=k, threads=nthreads, **extra)
+        ot.query_fixed(fam, Q[:m], k=k, threads=threads, **extra)
         return time.perf_counter() - t0
 
     m = min(len(Q), 20000)
@@ -221,9 +236,54 @@ def cpu_baseline(tree, Q, workload, target_seconds=12.0, threads=0):
         # the whole batch is quick: repeat it for a sample of about target_seconds
         reps = int(min(1000, max(2, target_seconds / max(dt, 1e-6))))
         dt = sum(run(m) for _ in range(reps))
-    return {"value": m * reps / dt, "unit": "queries/s", "cores": nthreads, "kind": "port",
-            "sample": f"{m} of the {len(Q)} queries x {reps}, {fam}(k={k}), {nthreads} threads, "
-                      f"{dt:.1f} s, oracle (C++ restatement of the reference scalar path)"}
+    return m, reps, dt
+
+
+def timing_tree_from(tree):
+    """The oracle's -O3 -march=native build (built on this host) over the
+    product tree's layout, for the CPU baseline leg of our own arm."""
+    import oracle
+    lay = oracle.Layout(tree.dtype, tree.dims, tree.stems(), tree.leaf_bytes(),
+                        tree.leaf_extents(), tree.max_stem_level(), tree.size(),
+                        tree.max_leaf_len())
+    return oracle.OracleTree.from_layout(lay, L=oracle.timing_lib())
+
+
+def cpu_baseline(tree, Q, workload, target_seconds=12.0, threads=0):
+    """The CPU restatement of the reference path on all host cores, on a
+    bounded sample of the same queries (test infrastructure: the oracle)."""
+    ot = timing_tree_from(tree)
+    nthreads = threads if threads > 0 else (os.cpu_count() or 1)
+    _, _, _, fam, k = WORKLOADS[workload]
+    m, reps, dt = time_cpu(ot, Q, workload, target_seconds, nthreads)
+    return dict({"value": m * reps / dt, "unit": "queries/s", "cores": nthreads, "kind": "port",
+                 "sample": f"{m} of the {len(Q)} queries x {reps}, {fam}(k={k}), {nthreads} "
+                           f"threads, {dt:.1f} s; the oracle (C++ restatement of the reference "
+                           f"scalar path) built -O3 -march=native -ffp-contract=off on this host"},
+                **cpu_info())
+
+
+def parity_sample(tree, Q, res, workload, n=SAMPLE_ROWS, seed=0):
+    """Compare `n` seeded sampled rows of a timed result with the oracle (the
+    checker build) on the same tree layout, bit for bit."""
+    import oracle
+    fam, k, extra = oracle_family(workload)
+    rows = np.sort(np.random.default_rng(seed).choice(len(Q), size=min(n, len(Q)),
+                                                      replace=False))
+    lay = oracle.Layout(tree.dtype, tree.dims, tree.stems(), tree.leaf_bytes(),
+                        tree.leaf_extents(), tree.max_stem_level(), tree.size(),
+                        tree.max_leaf_len())
+    ot = oracle.OracleTree.from_layout(lay)
+    od, oi, oc = ot.query_fixed(fam, Q[rows], k=k, **extra)
+    idx = __import__("torch").from_numpy(rows).to(res.distances.device)
+    gd = res.distances.index_select(0, idx).cpu().numpy().reshape(len(rows), -1)
+    gi = res.items.index_select(0, idx).cpu().numpy().view(np.uint32).reshape(len(rows), -1)
+    same = np.all((gd == od) | (np.isnan(gd) & np.isnan(od)), axis=1) & np.all(gi == oi, axis=1)
+    if getattr(res, "counts", None) is not None:
+        gc = res.counts.index_select(0, idx).cpu().numpy().astype(np.uint32)
+        same &= gc == oc
+    return {"n": int(len(rows)), "mismatches": int((~same).sum()),
+            "rule": "bit-exact distances, items and counts against the oracle, seeded rows"}
 
 
 def bytes_per_query(stats, nq, dtype_size, k):
@@ -248,33 +308,204 @@ def kernel_name(fam, engine):
     return f"k_tfixed<{f}>" if engine != "warp" else f"k_fixed<{f}>"
 
 
+def config_for(workload, n, nq, world):
+    """The workload's description, identical in both arms' lines."""
+    dt, _, _, fam, k = WORKLOADS[workload]
+    cfg = {"workload": workload, "points": n, "queries_per_gpu": nq, "family": fam, "k": k,
+           "metric": "SquaredEuclidean", "parallelism": f"replicas{world}",
+           "l2": l2_note(n, nq, 4 if dt == "f32" else 8)}
+    if fam == "periodic_nearest_n_within":
+        cfg.update({"radius": C5_RADIUS, "periodic_box": [1.0, 1.0, 1.0]})
+    return cfg
+
+
 def run_reference(args, rank, world):
+    """The reference arm: the oracle (a C++ restatement of the reference's
+    scalar path; the Rust crate cannot be built here), built -O3
+    -march=native on this host, timed on all host threads over the same
+    workload and config.  It loads nothing of the product package."""
     if rank != 0:
         return 0
-    P, Q = make_data(args.workload, 0)
-    import kiddo_b200 as kb
-    tree = kb.ImmutableKdTree.new_from_slice(P)
-    _, _, _, fam, k = WORKLOADS[args.workload]
+    import oracle
+    dtype_name, n, nq, fam, k = WORKLOADS[args.workload]
+    n = args.points or n
+    nq = args.queries or nq
+    P, Q = make_data(args.workload, 0, n, nq)
+    ot = oracle.OracleTree.build(P, L=oracle.timing_lib())
+    nthreads = os.cpu_count() or 1
+    # one sample size for every step: about 3 s of CPU work
+    m, _, dt0 = time_cpu(ot, Q, args.workload, 3.0, nthreads)
+    code, kk, extra = oracle_family(args.workload)
     times = []
-    base = None
     for s in range(args.warmup + args.steps):
-        cb = cpu_baseline(tree, Q, args.workload, target_seconds=8.0)
+        t0 = time.perf_counter()
+        ot.query_fixed(code, Q[:m], k=kk, threads=nthreads, **extra)
         if s >= args.warmup:
-            times.append(cb["value"])
-            base = cb
-    val = statistics.median(times)
+            times.append(time.perf_counter() - t0)
+    val = m / statistics.median(times)
+    sample = (f"{m} of the {len(Q)} queries per step, {fam}(k={k}), {nthreads} threads, "
+              f"median of {args.steps} steps; the oracle (C++ restatement of the reference "
+              f"scalar path) built -O3 -march=native -ffp-contract=off on this host")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "queries/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.median(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": WORKLOADS[args.workload][0], "data": "synthetic",
-            "config": {"workload": args.workload, "points": len(P), "queries": len(Q),
-                       "family": fam, "k": k},
-            "cpu_baseline": {"value": val, "unit": "queries/s", "cores": base["cores"],
-                             "kind": "port", "sample": base["sample"]},
+            "dtype": dtype_name, "data": "synthetic",
+            "config": config_for(args.workload, n, nq, world),
+            "cpu_baseline": dict({"value": val, "unit": "queries/s", "cores": nthreads,
+                                  "kind": "port", "sample": sample}, **cpu_info()),
             "e2e": {"value": val, "unit": "queries/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_tree_workload(args, workload, rank, world, steps, warmup, points=0, queries=0,
+                      with_cpu=True, parity_rows=SAMPLE_ROWS):
+    """One single-tree workload (C1, C2, C5): the line's fields, measured
+    with the queries resident in HBM (`value`) and through host buffers
+    (`e2e`), with the roofline of the dominant kernel."""
+    import torch
+    import kiddo_b200 as kb
+    from kiddo_b200 import multi
+
+    local = torch.cuda.current_device()
+    dev = torch.device("cuda", local)
+    dtype_name, n, nq, fam, k = WORKLOADS[workload]
+    n = points or n
+    nq = queries or nq
+    P, Q = make_data(workload, rank, n, nq)
+    t_host = time.perf_counter()
+    tree = kb.ImmutableKdTree.new_from_slice(P)
+    host_build_s = time.perf_counter() - t_host
+    gtree = tree.to_gpu()
+    stream = torch.cuda.current_stream(dev)
+    dq = torch.from_numpy(Q).to(dev)
+
+    def step():
+        b = builder_for(gtree, dq, workload).with_engine(args.engine)
+        return b.with_spatial_order(args.spatial_order).execute_gpu()
+
+    # algorithmic bytes per query from the engine's own traversal counters,
+    # which the tests hold equal to the oracle's (the reference traversal)
+    sub = Q[: min(nq, 2_000_000)]
+    stats = builder_for(gtree, sub, workload).traversal_stats()
+    bpq = bytes_per_query(stats, len(sub), Q.itemsize, k)
+
+    with ClockSampler(local) as clk:
+        clk.wait_first()
+        for _ in range(warmup):
+            res = step()
+        torch.cuda.synchronize()
+        multi.barrier()
+        l0 = kb.launch_count()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for s in range(steps):
+            res = step()
+            ev[s + 1].record(stream)
+        torch.cuda.synchronize()
+        launches = kb.launch_count() - l0
+    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+    total_ms = sum(step_ms)
+    total_ms_max = multi.max_over_ranks(total_ms)
+    multi.barrier()
+    # the last timed step's own output, sampled against the oracle
+    check = parity_sample(tree, Q, res, workload, parity_rows) if parity_rows else None
+    del res
+
+    # end to end through the C ABI with pinned host buffers
+    hq = torch.from_numpy(Q).pin_memory().numpy()
+    for _ in range(max(1, warmup // 2)):
+        builder_for(gtree, hq, workload).execute_gpu()
+    torch.cuda.synchronize()
+    multi.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(steps, 3))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        builder_for(gtree, hq, workload).execute_gpu()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = multi.max_over_ranks(e0.elapsed_time(e1))
+    del hq
+
+    # the same tree built on the device from device points (same bytes); the
+    # call synchronizes, so it is timed on the host clock: median of 3 after one
+    dP = torch.from_numpy(P).to(dev)
+    builds = []
+    for _ in range(4):
+        torch.cuda.synchronize()
+        t_dev = time.perf_counter()
+        g_dev = kb.GpuTree.build(dP, stream=stream)
+        torch.cuda.synchronize()
+        builds.append((time.perf_counter() - t_dev) * 1e3)
+        del g_dev
+    device_build_ms = float(np.median(builds[1:]))
+    del dP, dq
+
+    w = k if fam in ("nearest_n", "periodic_nearest_n_within") else 1
+    h2d = nq * 3 * Q.itemsize
+    d2h = nq * w * (Q.itemsize + 4) + (nq * 4 if w > 1 else 0)
+    value = world * nq * steps / (total_ms_max / 1e3)
+    e2e_val = world * nq * e2e_steps / (e2e_ms / 1e3)
+    kern_ms = total_ms / steps
+    achieved = bpq * nq / (kern_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profile_traffic(workload)
+    # compulsory bytes: the whole tree once, the queries once, the results once
+    tree_bytes = sum(a.nbytes for a in (tree.stems(), tree.leaf_bytes(), tree.leaf_extents()))
+    compulsory = tree_bytes + h2d + d2h
+    comp_gbs = compulsory / (kern_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": total_ms_max / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": dtype_name, "data": "synthetic",
+        "config": config_for(workload, n, nq, world),
+        "path": {"spatial_order": "auto" if args.spatial_order is None else args.spatial_order,
+                 "engine": args.engine or "auto"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "bytes_per_query": bpq,
+                     "traffic": (traffic or {}).get("dram_bytes_per_launch"),
+                     "compulsory": {"bytes": int(compulsory), "achieved": comp_gbs,
+                                    "frac": comp_gbs / peak},
+                     "kernel": kernel_name(fam, args.engine)},
+        "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "tree_build": {"host_s": host_build_s, "host_threads": os.cpu_count(),
+                       "device_ms": device_build_ms},
+        "traversal_per_query": {"stems": float(stats[0]) / len(sub),
+                                "leaves": float(stats[1]) / len(sub),
+                                "points": float(stats[2]) / len(sub)},
+        "step_ms": step_ms,
+    }
+    if check is not None:
+        line["parity_sample"] = check
+    if rank == 0 and world == 1 and with_cpu:
+        line["cpu_baseline"] = cpu_baseline(tree, Q, workload)
+    del gtree, tree
+    return line
+
+
+# the other configurations, measured in the same run as the headline (one
+# GPU): their own lines' main fields, as sub-objects of the headline line
+SUB_KEYS = ("value", "unit", "ms_per_step", "steps", "warmup", "dtype", "config", "roofline",
+            "e2e", "gpu_launches", "clocks", "parity_sample", "cpu_baseline",
+            "traversal_per_query")
+
+
+def _free_device():
+    import gc
+    import torch
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
 
 
 def main():
@@ -287,6 +518,9 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="scale the c3/c4 workloads (tests and profiling only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="measure the chosen workload alone, without the other configurations")
+    ap.add_argument("--no-parity-sample", action="store_true")
     ap.add_argument("--spatial-order", default=None, action="store_true",
                     help="force leaf-grouped processing (default: the library decides)")
     ap.add_argument("--no-spatial-order", dest="spatial_order", action="store_false")
@@ -308,127 +542,35 @@ def main():
 
     import torch
     import torch.distributed as dist
-    import kiddo_b200 as kb
     from kiddo_b200 import multi
 
     torch.cuda.set_device(local)
     if world > 1:
         multi.init_process_group("nccl")
-    dev = torch.device("cuda", local)
-    dtype_name, n, nq, fam, k = WORKLOADS[args.workload]
-    n = args.points or n
-    nq = args.queries or nq
-    P, Q = make_data(args.workload, rank, n, nq)
-    t_host = time.perf_counter()
-    tree = kb.ImmutableKdTree.new_from_slice(P)
-    host_build_s = time.perf_counter() - t_host
-    gtree = tree.to_gpu()
-    stream = torch.cuda.current_stream(dev)
-    dq = torch.from_numpy(Q).to(dev)
-
-    def step():
-        b = builder_for(gtree, dq, args.workload).with_engine(args.engine)
-        return b.with_spatial_order(args.spatial_order).execute_gpu()
-
-    # algorithmic bytes per query from the engine's own traversal counters
-    sub = Q[: min(nq, 2_000_000)]
-    stats = builder_for(gtree, sub, args.workload).traversal_stats()
-    bpq = bytes_per_query(stats, len(sub), Q.itemsize, k)
-
-    with ClockSampler(local) as clk:
-        clk.wait_first()
-        for _ in range(args.warmup):
-            step()
-        torch.cuda.synchronize()
-        multi.barrier()
-        l0 = kb.launch_count()
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-        torch.cuda.synchronize()
-        ev[0].record(stream)
-        for s in range(args.steps):
-            step()
-            ev[s + 1].record(stream)
-        torch.cuda.synchronize()
-        launches = kb.launch_count() - l0
-    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    total_ms = sum(step_ms)
-    total_ms_max = multi.max_over_ranks(total_ms)
-    multi.barrier()
-
-    # end to end through the C ABI with pinned host buffers
-    hq = torch.from_numpy(Q).pin_memory().numpy()
-    for _ in range(max(1, args.warmup // 2)):
-        builder_for(gtree, hq, args.workload).execute_gpu()
-    torch.cuda.synchronize()
-    multi.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(1, min(args.steps, 3))
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        builder_for(gtree, hq, args.workload).execute_gpu()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = multi.max_over_ranks(e0.elapsed_time(e1))
-
-    # the same tree built on the device from device points (same bytes); the
-    # call synchronizes, so it is timed on the host clock: median of 3 after one
-    dP = torch.from_numpy(P).to(dev)
-    builds = []
-    for _ in range(4):
-        torch.cuda.synchronize()
-        t_dev = time.perf_counter()
-        g_dev = kb.GpuTree.build(dP, stream=stream)
-        torch.cuda.synchronize()
-        builds.append((time.perf_counter() - t_dev) * 1e3)
-        del g_dev
-    device_build_ms = float(np.median(builds[1:]))
-    del dP
-
-    w = k if fam in ("nearest_n", "periodic_nearest_n_within") else 1
-    h2d = nq * 3 * Q.itemsize
-    d2h = nq * w * (Q.itemsize + 4) + (nq * 4)
-    value = world * nq * args.steps / (total_ms_max / 1e3)
-    e2e_val = world * nq * e2e_steps / (e2e_ms / 1e3)
-    kern_ms = total_ms / args.steps
-    achieved = bpq * nq / (kern_ms / 1e3) / 1e9
-    peak, peak_kind = measured_peaks()
-    traffic = profile_traffic(args.workload)
-    # compulsory bytes: the whole tree once, the queries once, the results once
-    tree_bytes = sum(a.nbytes for a in (tree.stems(), tree.leaf_bytes(), tree.leaf_extents()))
-    out_bytes = nq * w * (Q.itemsize + 4) + (nq * 4 if w > 1 else 0)
-    compulsory = tree_bytes + nq * 3 * Q.itemsize + out_bytes
-    comp_gbs = compulsory / (kern_ms / 1e3) / 1e9
-    line = {
-        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if dtype_name == "f32" else "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "points": n, "queries_per_gpu": nq, "family": fam,
-                   "k": k, "metric": "SquaredEuclidean", "parallelism": f"replicas{world}",
-                   "l2": l2_note(n, nq, Q.itemsize),
-                   "spatial_order": "auto" if args.spatial_order is None else args.spatial_order,
-                   "engine": args.engine or "auto"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "bytes_per_query": bpq,
-                     "traffic": (traffic or {}).get("dram_bytes_per_launch"),
-                     "compulsory": {"bytes": int(compulsory), "achieved": comp_gbs,
-                                    "frac": comp_gbs / peak},
-                     "kernel": kernel_name(fam, args.engine)},
-        "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(launches),
-        "clocks": clk.summary(),
-        "tree_build": {"host_s": host_build_s, "host_threads": os.cpu_count(),
-                       "device_ms": device_build_ms},
-        "traversal_per_query": {"stems": float(stats[0]) / len(sub),
-                                "leaves": float(stats[1]) / len(sub),
-                                "points": float(stats[2]) / len(sub)},
-        "step_ms": step_ms,
-    }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(tree, Q, args.workload)
+    parity_rows = 0 if args.no_parity_sample else SAMPLE_ROWS
+    line = run_tree_workload(args, args.workload, rank, world, args.steps, args.warmup,
+                             args.points, args.queries, not args.no_cpu_baseline, parity_rows)
+    full = (args.workload == "c2_knn16" and world == 1 and not args.headline_only
+            and not (args.points or args.queries))
+    if full:
+        # every term of the metric in the one run: approx and the f64
+        # configurations on single trees, the batched-vs-per-tree forest, and
+        # Chamfer forward + backward
+        sub_steps, sub_warm = max(1, min(args.steps, 10)), max(3, min(args.warmup, 5))
+        for wl in ("c2_approx", "c1_nn1", "c5_periodic"):
+            _free_device()
+            sub = run_tree_workload(args, wl, rank, world, sub_steps, sub_warm,
+                                    with_cpu=not args.no_cpu_baseline, parity_rows=parity_rows)
+            line[wl] = {k: sub[k] for k in SUB_KEYS if k in sub}
+        _free_device()
+        fa = argparse.Namespace(**vars(args))
+        fa.steps, fa.warmup = sub_steps, sub_warm
+        line["c3_batched_vs_per_tree"] = forest_measure(fa, rank, world, parity_rows)
+        _free_device()
+        line["c4_chamfer"] = chamfer_measure(fa, rank, world)
+        line["gpu_launches_all_workloads"] = line["gpu_launches"] + sum(
+            line[w].get("gpu_launches", 0) for w in ("c2_approx", "c1_nn1", "c5_periodic",
+                                                     "c3_batched_vs_per_tree", "c4_chamfer"))
     if rank == 0:
         print(json.dumps(line), flush=True)
     multi.barrier()
@@ -471,12 +613,21 @@ def forest_workload(scale, seed=3):
     share = rng.dirichlet(np.full(n_trees, 0.5))
     per_tree = np.floor(share * n_q).astype(np.int64)
     per_tree[0] += n_q - per_tree.sum()
-    pts, items, qs = [], [], []
-    for t in range(n_trees):
+
+    def one_tree(t):
+        # every tree draws from its own seeded generator, so the threads give
+        # the same arrays in any order
         trng = np.random.default_rng(seed * 1000 + t)
-        pts.append(sphere_catalogue(int(sizes[t]), trng))
-        items.append(pareto_ranks(int(sizes[t]), trng))
-        qs.append(sphere_catalogue(int(per_tree[t]), trng))
+        p = sphere_catalogue(int(sizes[t]), trng)
+        it = pareto_ranks(int(sizes[t]), trng)
+        return p, it, sphere_catalogue(int(per_tree[t]), trng)
+
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        parts = list(ex.map(one_tree, range(n_trees)))
+    pts = [p for p, _, _ in parts]
+    items = [it for _, it, _ in parts]
+    qs = [q for _, _, q in parts]
     tree_of = np.repeat(np.arange(n_trees, dtype=np.int32), per_tree)
     Q = np.concatenate(qs)
     chord = np.exp(rng.uniform(np.log(1e-4), np.log(1e-2), n_q))
@@ -485,17 +636,76 @@ def forest_workload(scale, seed=3):
     return pts, items, Q, tree_of, radii, family
 
 
-def run_forest(args, rank, world):
-    """One job of 256 catalogues and 64M queries.  With N > 1 GPUs every tree
-    has one owner rank (multi.partition_trees on points x queries) that holds
-    it and answers its queries (strong scaling: the job is fixed); the time is
-    the max over ranks."""
+def forest_parity_sample(trees, parts, results, n=SAMPLE_ROWS, seed=0):
+    """Sampled rows of each family's batched result against the oracle tree
+    of the query's catalogue (checker build, the same layouts), bit for bit."""
+    import oracle
+    import torch
+    rng = np.random.default_rng(seed)
+    mism, total = 0, 0
+    ots = {}
+
+    def ot(t):
+        if t not in ots:
+            tr = trees[t]
+            ots[t] = oracle.OracleTree.from_layout(oracle.Layout(
+                tr.dtype, tr.dims, tr.stems(), tr.leaf_bytes(), tr.leaf_extents(),
+                tr.max_stem_level(), tr.size(), tr.max_leaf_len()))
+        return ots[t]
+
+    for fam, ((q, _, r, host_t), res) in enumerate(zip(parts, results)):
+        nq = q.shape[0]
+        if nq == 0:
+            continue
+        rows = np.sort(rng.choice(nq, size=min(n // 3, nq), replace=False))
+        sel = torch.from_numpy(rows).to(q.device)
+        qh = q.index_select(0, sel).cpu().numpy()
+        rh = r.index_select(0, sel).cpu().numpy()
+        idx = sel
+        if fam < 2:
+            # every sampled row's hits in one gather: row j at [goff[j], goff[j + 1])
+            off = res.offsets.cpu().numpy().astype(np.int64)
+            lens = off[rows + 1] - off[rows]
+            goff = np.concatenate([[0], np.cumsum(lens)])
+            hit = np.repeat(off[rows] - goff[:-1], lens) + np.arange(goff[-1])
+            th = torch.from_numpy(hit).to(q.device)
+            gd = res.distances.index_select(0, th).cpu().numpy()
+            gi = res.items.index_select(0, th).cpu().numpy().view(np.uint32)
+        else:
+            gd = res.distances.index_select(0, idx).cpu().numpy()
+            gi = res.items.index_select(0, idx).cpu().numpy().view(np.uint32)
+            gc = res.counts.index_select(0, idx).cpu().numpy()
+        tof = host_t[rows]
+        for t in np.unique(tof):
+            m = np.nonzero(tof == t)[0]
+            if fam < 2:
+                oo, od, oi = ot(int(t)).within(qh[m], rh[m], sorted=(fam == 0))
+                for j, p in enumerate(m):
+                    a, b = goff[p], goff[p + 1]
+                    oa, ob = int(oo[j]), int(oo[j + 1])
+                    ok = (b - a) == (ob - oa) and np.array_equal(gd[a:b], od[oa:ob]) and \
+                        np.array_equal(gi[a:b], oi[oa:ob])
+                    mism += int(not ok)
+            else:
+                od, oi, oc = ot(int(t)).best_n_within(qh[m], rh[m], 5)
+                same = (np.all(gd[m] == od, axis=1) & np.all(gi[m] == oi, axis=1) &
+                        (gc[m].astype(np.uint32) == oc))
+                mism += int((~same).sum())
+            total += len(m)
+    return {"n": int(total), "mismatches": int(mism),
+            "rule": "bit-exact CSR rows / best_n rows against the oracle, seeded rows per family"}
+
+
+def forest_measure(args, rank, world, parity_rows=SAMPLE_ROWS):
+    """One job of 256 catalogues and 64M queries, batched (one persistent
+    launch per family) and per tree (one launch per tree and family).  With
+    N > 1 GPUs every tree has one owner rank (multi.partition_trees on points x
+    queries) that holds it and answers its queries (strong scaling: the job is
+    fixed); the time is the max over ranks.  Returns the measured fields on
+    rank 0 (None elsewhere)."""
     import torch
     import kiddo_b200 as kb
     from kiddo_b200 import multi
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    if world > 1:
-        multi.init_process_group("nccl")
     pts, items, Q, tree_of, radii, family = forest_workload(args.scale)
     nq_total = len(Q)
     if world > 1:
@@ -510,7 +720,9 @@ def run_forest(args, rank, world):
         tree_of = local[tree_of[keep]].astype(np.int32)
         pts = [pts[i] for i in mine]
         items = [items[i] for i in mine]
+    n_points = int(sum(len(p) for p in pts))
     trees = [kb.ImmutableKdTree.new_from_entries(it, p) for it, p in zip(items, pts)]
+    del pts, items
     forest = kb.Forest(trees)
     stream = torch.cuda.Stream()
     parts = []
@@ -518,6 +730,7 @@ def run_forest(args, rank, world):
         sel = np.nonzero(family == fam)[0]  # queries stay grouped by tree
         parts.append((torch.from_numpy(Q[sel]).cuda(), torch.from_numpy(tree_of[sel]).cuda(),
                       torch.from_numpy(radii[sel]).cuda(), tree_of[sel]))
+    del Q
     SE = kb.SquaredEuclidean
 
     def builders(q, t, r):
@@ -542,6 +755,8 @@ def run_forest(args, rank, world):
         res = batched()
         torch.cuda.synchronize()
         hits = [int(x.offsets[-1].item()) for x in res[:2]]
+        check = forest_parity_sample(trees, parts, res, parity_rows) if parity_rows else None
+        del res
 
         def timed(fn, steps):
             for _ in range(args.warmup):
@@ -560,32 +775,50 @@ def run_forest(args, rank, world):
         l0 = kb.launch_count()
         ms_batched = timed(batched, args.steps)
         launches = (kb.launch_count() - l0) // (args.warmup + args.steps)
-        ms_per_tree = timed(per_tree, max(1, args.steps // 2))
-    nq = nq_total
+        per_tree_steps = max(1, args.steps // 2)
+        ms_per_tree = timed(per_tree, per_tree_steps)
     hits = [int(multi.fixed_order_sum(torch.tensor([h], dtype=torch.float64,
                                                    device="cuda"))[0].item()) for h in hits]
+    del parts, forest, trees
     if rank != 0:
-        multi.barrier()
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return 0
-    line = {"metric": METRIC, "value": nq / (ms_batched / 1e3), "unit": "queries/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_batched, "higher_is_better": True,
-            "scaling": "strong" if world > 1 else "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "c3_forest", "trees": len(trees),
-                       "points": int(sum(len(p) for p in pts)), "queries": nq,
-                       "families": "within sorted / within unsorted / best_n_within(5), thirds",
-                       "radii": "chord log-uniform [1e-4, 1e-2], squared",
-                       "hits": {"within_sorted": hits[0], "within_unsorted": hits[1]}},
-            "per_tree_launch": {"ms_per_step": ms_per_tree, "value": nq / (ms_per_tree / 1e3)},
-            "batched_over_per_tree": ms_per_tree / ms_batched,
-            "gpu_launches": int(launches)}
+        return None
+    out = {"value": nq_total / (ms_batched / 1e3), "unit": "queries/s",
+           "ms_per_step": ms_batched, "steps": args.steps, "warmup": args.warmup,
+           "config": {"workload": "c3_forest", "trees": 256, "points": n_points,
+                      "queries": nq_total,
+                      "families": "within sorted / within unsorted / best_n_within(5), thirds",
+                      "radii": "chord log-uniform [1e-4, 1e-2], squared",
+                      "hits": {"within_sorted": hits[0], "within_unsorted": hits[1]}},
+           "per_tree_launch": {"ms_per_step": ms_per_tree, "steps": per_tree_steps,
+                               "value": nq_total / (ms_per_tree / 1e3)},
+           "batched_over_per_tree": ms_per_tree / ms_batched,
+           "gpu_launches": int(launches)}
+    if check is not None:
+        out["parity_sample"] = check
+    return out
+
+
+def run_forest(args, rank, world):
+    """The forest configuration as its own line (``--workload c3_forest``)."""
+    import torch
+    from kiddo_b200 import multi
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     if world > 1:
-        line["config"]["parallelism"] = f"trees partitioned over {world} ranks"
-    print(json.dumps(line), flush=True)
+        multi.init_process_group("nccl")
+    local = torch.cuda.current_device()
+    with ClockSampler(local) as clk:
+        clk.wait_first()
+        m = forest_measure(args, rank, world,
+                           0 if getattr(args, "no_parity_sample", False) else SAMPLE_ROWS)
+    if rank == 0:
+        line = {"metric": METRIC, "n_gpus": world, "higher_is_better": True,
+                "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic"}
+        line.update(m)
+        line["clocks"] = clk.summary()
+        if world > 1:
+            line["config"]["parallelism"] = f"trees partitioned over {world} ranks"
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         multi.barrier()
@@ -615,18 +848,16 @@ def chamfer_workload(scale, seed=4):
     return pairs
 
 
-def run_chamfer(args, rank, world):
-    """Forward + backward over 64 cloud pairs.  With N > 1 GPUs every pair has
-    one owner rank (multi.partition_trees on source x target sizes); a pair's
-    gradients stay on its owner and the loss partials are added in rank order
-    (multi.fixed_order_sum), so the job is fixed (strong scaling)."""
+def chamfer_measure(args, rank, world):
+    """Forward + backward over 64 cloud pairs at k = 8 and k = 1.  With N > 1
+    GPUs every pair has one owner rank (multi.partition_trees on source x
+    target sizes); a pair's gradients stay on its owner and the loss partials
+    are added in rank order (multi.fixed_order_sum), so the job is fixed
+    (strong scaling).  Returns the measured fields on rank 0 (None elsewhere)."""
     import torch
     import kiddo_b200 as kb
     from kiddo_b200 import multi
     from kiddo_b200.chamfer import chamfer_backward, chamfer_forward
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    if world > 1:
-        multi.init_process_group("nccl")
     pairs = chamfer_workload(args.scale)
     n_src_total = sum(len(s) for s, _ in pairs)
     n_tgt_total = sum(len(t) for _, t in pairs)
@@ -660,18 +891,36 @@ def run_chamfer(args, rank, world):
         torch.cuda.synchronize()
         ms = multi.max_over_ranks(e0.elapsed_time(e1) / args.steps)
         out[k] = (ms, (kb.launch_count() - l0) // args.steps)
+    del forest, trees, src, tgt
+    if rank != 0:
+        return None
     ms8 = out[8][0]
-    line = {"metric": METRIC, "value": 64 / (ms8 / 1e3), "unit": "cloud pairs/s (fwd+bwd)",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms8,
-            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+    return {"value": 64 / (ms8 / 1e3), "unit": "cloud pairs/s (fwd+bwd)", "ms_per_step": ms8,
+            "steps": args.steps, "warmup": args.warmup,
             "config": {"workload": "c4_chamfer", "pairs": 64, "k": 8, "sigma": 0.01,
                        "source_points": int(n_src_total), "target_points": int(n_tgt_total)},
             "k1": {"ms_per_step": out[1][0], "value": 64 / (out[1][0] / 1e3)},
             "gpu_launches": int(out[8][1])}
+
+
+def run_chamfer(args, rank, world):
+    """The Chamfer configuration as its own line (``--workload c4_chamfer``)."""
+    import torch
+    from kiddo_b200 import multi
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     if world > 1:
-        line["config"]["parallelism"] = f"cloud pairs partitioned over {world} ranks"
+        multi.init_process_group("nccl")
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        clk.wait_first()
+        m = chamfer_measure(args, rank, world)
     if rank == 0:
+        line = {"metric": METRIC, "n_gpus": world, "higher_is_better": True,
+                "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic"}
+        line.update(m)
+        line["clocks"] = clk.summary()
+        if world > 1:
+            line["config"]["parallelism"] = f"cloud pairs partitioned over {world} ranks"
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -298,7 +298,9 @@ int32_t kgpu_query_radius_fill(kgpu_tree* tree, const kgpu_query_desc* desc,
  * loading the library holds until exit.  Limit: nq <= 16,777,216 queries
  * (KGPU_EOVERFLOW beyond).  The tree's device must be current.  The first
  * call on each device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * (cudaGetSymbolAddress), and so does the first call after cudaDeviceReset
+ * has made the device's context anew; make that first call before any
+ * stream capture.
  * All calls share the one array, so calls that overlap on the GPU (on
  * different streams or from different threads) race and must be serialised
  * by the caller. */
@@ -382,6 +384,20 @@ int32_t kgpu_graph_destroy(kgpu_graph* graph);
  * Number of CUDA kernels this library has launched in the process so far
  * (all threads).  Lets a caller count the launches inside a timed region. */
 uint64_t kgpu_launch_count(void);
+
+/* ---- scratch memory ----------------------------------------------------
+ * No counterpart in the reference (its queries allocate on the host heap).
+ * The entry points take their scratch (staging buffers, scan tiles, sort
+ * buffers) from a stream-ordered memory pool of the library's own, one per
+ * device, which keeps freed scratch cached between calls; the device's default
+ * pool and other users of cudaMallocAsync are not touched.
+ * kgpu_scratch_stats: out[0] bytes in use, out[1] the high-water mark of bytes
+ * in use, out[2] bytes the pool holds from the driver, on `device` (zeros if
+ * the library has not used that device).  kgpu_scratch_trim waits for the
+ * device, returns every cached byte not in use to the driver and resets the
+ * high-water mark to the bytes in use. */
+int32_t kgpu_scratch_stats(int32_t device, uint64_t out[3]);
+int32_t kgpu_scratch_trim(int32_t device);
 
 #ifdef __cplusplus
 }

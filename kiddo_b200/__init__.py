@@ -504,6 +504,54 @@ def _csr_order(offsets, ranks, dists=None):
     return order
 
 
+def _metric_dist(points, q, metric):
+    """D::dist(point, query) row by row (dist/*/mod.rs): components in axis
+    order, accumulated from zero in the points' dtype."""
+    import torch
+    acc = torch.zeros(points.shape[0], dtype=points.dtype, device=points.device)
+    for d in range(points.shape[1]):
+        diff = points[:, d] - q[:, d]
+        if metric == C.CHEBYSHEV:
+            a = diff.abs()
+            acc = torch.where(a > acc, a, acc)
+        elif metric in (C.MINKOWSKI3, C.MINKOWSKI4):
+            a = diff.abs()
+            sq = a * a
+            acc = acc + (a * sq if metric == C.MINKOWSKI3 else sq * sq)
+        else:
+            acc = acc + (diff * diff if metric == C.SQUARED_EUCLIDEAN else diff.abs())
+    return acc
+
+
+def _first_by_rank(r, ranks, pts, q, metric, tree, stream):
+    """scan_projected_nearest_one's answer from a radius result holding every
+    entry at each query's least distance: the row's entry of least rank.  A
+    row with no entry is a query whose distance to every entry is NaN (a NaN
+    coordinate): no candidate is below the first one, so the scan keeps the
+    first entry in iteration order, at its own (NaN) distance."""
+    import torch
+    order = _csr_order(r.offsets, ranks)
+    nq = r.offsets.shape[0] - 1
+    nonempty = r.offsets[1:] > r.offsets[:-1]
+    total = int(order.shape[0])
+    if total == 0:
+        first = torch.zeros(nq, dtype=torch.int64, device=q.device)
+        d, it, p = (torch.zeros(nq, dtype=q.dtype, device=q.device),
+                    torch.zeros(nq, dtype=torch.int32, device=q.device),
+                    torch.zeros((nq, q.shape[1]), dtype=q.dtype, device=q.device))
+    else:
+        first = order[r.offsets[:-1].clamp(max=total - 1)]  # each row's least rank
+        d, it, p = r.distances[first], r.items[first], pts[first]
+    if bool(nonempty.all()):
+        return NearestOneResult(d, it, p)
+    items0, pts0 = tree.iter(stream)
+    p0 = pts0[:1].expand(nq, -1)
+    d0 = _metric_dist(p0, q, metric)
+    keep = nonempty[:, None]
+    return NearestOneResult(torch.where(nonempty, d, d0), torch.where(nonempty, it, items0[0]),
+                            torch.where(keep, p, p0))
+
+
 def _row_order(dists, ranks):
     """Per row of [nq, k] results, the column order by distance, equal
     distances by iteration rank; unused slots (rank 0xFFFFFFFF, distance +inf)
@@ -832,8 +880,7 @@ class QueryBuilder:
         fq.radius = float("inf")
         r = fq.execute_gpu()
         ranks, pts = self.tree.project(r.items, stream)
-        first = _csr_order(r.offsets, ranks)[r.offsets[:-1]]  # each row's least rank
-        return NearestOneResult(r.distances[first], r.items[first], pts[first])
+        return _first_by_rank(r, ranks, pts, q, self.metric, self.tree, stream)
 
     def _execute_host(self):
         L = C.lib()

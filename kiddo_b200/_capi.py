@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = [
     "kgpu_forest_query_radius_count", "kgpu_forest_query_radius_fill", "kgpu_graph_begin",
     "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy", "kgpu_chamfer_loss",
     "kgpu_chamfer_backward", "kgpu_tree_create_flatvec", "kgpu_tree_create_vecofarrays",
+    "kgpu_scratch_stats", "kgpu_scratch_trim",
 ]
 
 
@@ -171,6 +172,10 @@ def lib():
     L.kgpu_graph_destroy.argtypes = [vp]
     L.kgpu_chamfer_loss.restype = i32
     L.kgpu_chamfer_loss.argtypes = [vp, vp, u64, u32, ctypes.c_double, vp, vp, vp]
+    L.kgpu_scratch_stats.restype = i32
+    L.kgpu_scratch_stats.argtypes = [ctypes.c_int32, vp]
+    L.kgpu_scratch_trim.restype = i32
+    L.kgpu_scratch_trim.argtypes = [ctypes.c_int32]
     L.kgpu_chamfer_backward.restype = i32
     L.kgpu_chamfer_backward.argtypes = [vp, u64, vp, u64, vp, vp, u32, vp, vp, ctypes.c_double,
                                         ctypes.c_float, vp, vp, vp]
@@ -188,3 +193,17 @@ def check(status):
 
 def launch_count() -> int:
     return int(lib().kgpu_launch_count())
+
+
+def scratch_stats(device: int = 0):
+    """(bytes in use, high-water mark, bytes held) of the library's own
+    scratch pool on `device`."""
+    import numpy as np
+    out = np.zeros(3, dtype=np.uint64)
+    check(lib().kgpu_scratch_stats(int(device), ctypes.c_void_p(out.ctypes.data)))
+    return tuple(int(x) for x in out)
+
+
+def scratch_trim(device: int = 0):
+    """Give the scratch pool's cached bytes on `device` back to the driver."""
+    check(lib().kgpu_scratch_trim(int(device)))

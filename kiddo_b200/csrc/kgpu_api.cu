@@ -69,21 +69,82 @@ size_t leaf_encoded_bytes(uint64_t len, int K, size_t sa) {
 
 namespace kgpu {
 
+uint64_t current_context_id() {
+  // cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points, so
+  // the library needs no link-time dependency on the driver library
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult r;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &r) ==
+            cudaSuccess && r == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &r) ==
+            cudaSuccess && r == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+namespace {
+// One stream-ordered pool per device, private to the library: its release
+// threshold is at its maximum, so freed scratch stays cached across stream
+// synchronizations instead of going back to the driver at each one (and being
+// mapped again, milliseconds later, by the next call).  Being the library's
+// own, the setting leaves the device's default pool (and every other
+// cudaMallocAsync user in the process) as it was.  A pool belongs to a
+// context: after cudaDeviceReset the next call makes a new one.
+struct ScratchPool {
+  uint64_t ctx_id = 0;
+  cudaMemPool_t pool = nullptr;
+};
+constexpr int kPoolDevices = 64;
+std::mutex g_pool_mu;
+ScratchPool g_pools[kPoolDevices];
+}  // namespace
+
+cudaError_t library_pool(int dev, cudaMemPool_t* out) {
+  if (dev < 0 || dev >= kPoolDevices) return cudaErrorInvalidDevice;
+  const uint64_t ctx = current_context_id();
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  ScratchPool& sp = g_pools[dev];
+  if (!sp.pool || sp.ctx_id != ctx) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = ~uint64_t(0);
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return e;
+    }
+    sp.pool = pool;
+    sp.ctx_id = ctx;
+  }
+  *out = sp.pool;
+  return cudaSuccess;
+}
+
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
-  static std::atomic<uint64_t> cached_devices{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
-  if (bit && !(cached_devices.load(std::memory_order_relaxed) & bit)) {
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      uint64_t keep = ~uint64_t(0);
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-    cached_devices.fetch_or(bit, std::memory_order_relaxed);
-  }
-  return cudaMallocAsync(p, bytes, s);
+  cudaMemPool_t pool = nullptr;
+  if ((e = library_pool(dev, &pool)) != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 
 void release_tree_arrays(DeviceTree& dt) {
@@ -144,6 +205,55 @@ const char* kgpu_status_string(int32_t s) {
 uint32_t kgpu_abi_version(void) { return KGPU_ABI_VERSION; }
 
 uint64_t kgpu_launch_count(void) { return g_launches.load(); }
+
+namespace {
+// The library's pool on `device` if one was made in the device's current
+// context (nullptr otherwise), with that device current until `restore`.
+struct PoolOnDevice {
+  int prev = -1;
+  cudaMemPool_t pool = nullptr;
+  cudaError_t err = cudaSuccess;
+  explicit PoolOnDevice(int device) {
+    if ((err = cudaGetDevice(&prev)) != cudaSuccess) return;
+    if (prev != device && (err = cudaSetDevice(device)) != cudaSuccess) return;
+    const uint64_t ctx = current_context_id();
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    if (g_pools[device].ctx_id == ctx) pool = g_pools[device].pool;
+  }
+  ~PoolOnDevice() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
+int32_t kgpu_scratch_stats(int32_t device, uint64_t out[3]) {
+  if (!out) return set_error(KGPU_EINVAL, "out is NULL");
+  out[0] = out[1] = out[2] = 0;
+  if (device < 0 || device >= kPoolDevices) return set_error(KGPU_EINVAL, "bad device index");
+  PoolOnDevice pd(device);
+  if (pd.err != cudaSuccess) return cuda_fail(pd.err, "selecting the device");
+  if (!pd.pool) return KGPU_OK;
+  const cudaMemPoolAttr attrs[3] = {cudaMemPoolAttrUsedMemCurrent, cudaMemPoolAttrUsedMemHigh,
+                                    cudaMemPoolAttrReservedMemCurrent};
+  for (int i = 0; i < 3; ++i) {
+    cudaError_t e = cudaMemPoolGetAttribute(pd.pool, attrs[i], &out[i]);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolGetAttribute");
+  }
+  return KGPU_OK;
+}
+
+int32_t kgpu_scratch_trim(int32_t device) {
+  if (device < 0 || device >= kPoolDevices) return set_error(KGPU_EINVAL, "bad device index");
+  PoolOnDevice pd(device);
+  if (pd.err != cudaSuccess) return cuda_fail(pd.err, "selecting the device");
+  if (!pd.pool) return KGPU_OK;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemPoolTrimTo(pd.pool, 0);
+  uint64_t zero = 0;  // the high-water mark restarts from the bytes in use
+  if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pd.pool, cudaMemPoolAttrUsedMemHigh, &zero);
+  return e == cudaSuccess ? KGPU_OK : cuda_fail(e, "trimming the scratch pool");
+}
 
 // ---- host construction ----------------------------------------------------
 int32_t kgpu_layout_build(int32_t dtype, uint32_t dims, const void* points, const uint32_t* items,

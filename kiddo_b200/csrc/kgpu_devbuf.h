@@ -7,14 +7,16 @@
 
 namespace kgpu {
 
-// cudaMallocAsync from the current device's default memory pool.  On a
-// device's first use the pool's release threshold is raised to its maximum,
-// so that freed scratch stays cached in the pool across stream
-// synchronizations instead of going back to the driver at each one (and being
-// mapped again, milliseconds later, by the next call).  This is a setting of
-// the process's default pool: other cudaMallocAsync users in the process see
-// the same caching.
+// Stream-ordered allocation from the library's own memory pool on the current
+// device (one per device and context, created on first use).  The pool keeps
+// freed scratch cached across stream synchronizations (release threshold at
+// its maximum), so a call does not map memory that the previous call just
+// gave back; the device's default pool is left as it was.  kgpu_scratch_trim
+// returns the cached memory to the driver.
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+
+// The pool scratch_alloc draws from on `dev` (made if needed).
+cudaError_t library_pool(int dev, cudaMemPool_t* out);
 
 struct DeviceTree;
 // Frees a tree's stems, arena, extents and point table, from the pool (DeviceTree::pooled)

@@ -28,6 +28,12 @@ struct Layout {
   std::vector<uint64_t> extents;     // (offset, len) pairs
 };
 
+// A process-unique id of the calling thread's current CUDA context (cuCtxGetId),
+// or 0 if there is none.  It changes when a context is destroyed and made
+// again (cudaDeviceReset), which invalidates device addresses cached per
+// device.
+uint64_t current_context_id();
+
 // Records `msg` as the calling thread's last error and returns `status`.
 int set_error(int status, const std::string& msg);
 

@@ -39,13 +39,21 @@ static __device__ __align__(256) unsigned long long g_noalloc_scan_tiles[kNoAllo
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
+struct CachedAddress {
+  uint64_t ctx_id = 0;  // the context the address was looked up in
+  void* addr = nullptr;
+};
+CachedAddress g_scratch_addr[kMaxDevices];
 
-// Device address of g_noalloc_scan_tiles on the current device (looked up once
-// per device).  Returns nullptr and sets the error message on failure.
+// Device address of g_noalloc_scan_tiles on the current device.  It is looked
+// up once per device and context: cudaDeviceReset destroys the context that
+// holds the array, and the next call looks the address up again in the new
+// one.  Returns nullptr and sets the error message on failure.
 void* scratch_address(int dev) {
+  const uint64_t ctx = current_context_id();
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[dev]) {
+  CachedAddress& c = g_scratch_addr[dev];
+  if (!c.addr || c.ctx_id != ctx) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scan_tiles);
     if (e != cudaSuccess || !p) {
@@ -53,9 +61,10 @@ void* scratch_address(int dev) {
                                 cudaGetErrorString(e));
       return nullptr;
     }
-    g_scratch_addr[dev] = p;
+    c.addr = p;
+    c.ctx_id = ctx;
   }
-  return g_scratch_addr[dev];
+  return c.addr;
 }
 
 }  // namespace

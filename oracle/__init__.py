@@ -15,7 +15,10 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libkiddo_oracle.so")
+_TIMING_PATH = os.path.join(_HERE, "libkiddo_oracle_timing.so")
+_TIMING_STAMP = _TIMING_PATH + ".host"
 _lib = None
+_timing_lib = None
 
 FAM_NEAREST_ONE = 0
 FAM_APPROX = 1
@@ -40,40 +43,98 @@ def build_library(force: bool = False) -> str:
     return _LIB_PATH
 
 
+def host_cpu():
+    """(CPU model name, logical CPUs, physical cores) of this host."""
+    model, cores = "unknown", set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            phys = core = None
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name":
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+            if phys is not None:
+                cores.add((phys, core))
+    except OSError:
+        pass
+    logical = os.cpu_count() or 1
+    return model, logical, len(cores) or logical
+
+
+def timing_lib():
+    """The timed CPU baseline: the oracle's source built -O3 -march=native for
+    THIS host (``make timing``), 3-D SquaredEuclidean trees only.  It is
+    rebuilt when the library was built on another CPU model, so the
+    instructions it uses always exist here.  Same API as ``lib()``."""
+    global _timing_lib
+    if _timing_lib is None:
+        model = host_cpu()[0]
+        src = [os.path.join(_HERE, f) for f in ("kiddo_oracle_capi.cpp", "kiddo_oracle.hpp")]
+        stamp = None
+        if os.path.exists(_TIMING_STAMP):
+            with open(_TIMING_STAMP) as f:
+                stamp = f.read().strip()
+        if (stamp != model or not os.path.exists(_TIMING_PATH)
+                or any(os.path.getmtime(p) > os.path.getmtime(_TIMING_PATH) for p in src)):
+            subprocess.run(["make", "-s", "-C", _HERE, "timing"], check=True)
+            with open(_TIMING_STAMP, "w") as f:
+                f.write(model + "\n")
+        _timing_lib = _declare(ctypes.CDLL(_TIMING_PATH))
+    return _timing_lib
+
+
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(_LIB_PATH):
             build_library()
-        L = ctypes.CDLL(_LIB_PATH)
-        vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
-        L.kor_build.restype = vp
-        L.kor_build.argtypes = [i32, i32, vp, vp, u64]
-        L.kor_build_ex.restype = vp
-        L.kor_build_ex.argtypes = [i32, i32, vp, vp, u64, ctypes.c_uint32]
-        L.kor_from_layout.restype = vp
-        L.kor_from_layout.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64, u64]
-        L.kor_from_layout_ex.restype = vp
-        L.kor_from_layout_ex.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64,
-                                         u64, ctypes.c_uint32]
-        L.kor_free.argtypes = [vp]
-        L.kor_iter.argtypes = [vp, vp, vp]
-        L.kor_layout_info.argtypes = [vp, vp]
-        L.kor_copy_layout.argtypes = [vp, vp, vp, vp]
-        L.kor_query_fixed.restype = i32
-        L.kor_query_fixed.argtypes = [vp, i32, i32, vp, u64, ctypes.c_uint32, ctypes.c_double,
-                                      i32, i32, vp, vp, vp, vp, i32, vp]
-        L.kor_query_radius.restype = vp
-        L.kor_query_radius.argtypes = [vp, i32, i32, vp, u64, ctypes.c_double, i32, i32, vp, i32, vp]
-        L.kor_donnelly_path.argtypes = [ctypes.c_uint32, vp, u64, vp]
-        L.kor_metric_f64x3.restype = i32
-        L.kor_metric_f64x3.argtypes = [i32, vp, vp, ctypes.c_double, vp, i32, ctypes.c_double, vp]
-        L.kor_radius_total.restype = u64
-        L.kor_radius_total.argtypes = [vp]
-        L.kor_radius_copy.argtypes = [vp, vp, vp, vp]
-        L.kor_radius_free.argtypes = [vp]
-        _lib = L
+        _lib = _declare(ctypes.CDLL(_LIB_PATH))
     return _lib
+
+
+def _declare(L):
+    """ctypes signatures of the oracle's C API on library ``L``."""
+    vp, u64, i32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int
+    L.kor_build.restype = vp
+    L.kor_build.argtypes = [i32, i32, vp, vp, u64]
+    L.kor_build_ex.restype = vp
+    L.kor_build_ex.argtypes = [i32, i32, vp, vp, u64, ctypes.c_uint32]
+    L.kor_from_layout.restype = vp
+    L.kor_from_layout.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64, u64]
+    L.kor_from_layout_ex.restype = vp
+    L.kor_from_layout_ex.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64,
+                                     u64, ctypes.c_uint32]
+    L.kor_free.argtypes = [vp]
+    L.kor_iter.argtypes = [vp, vp, vp]
+    L.kor_layout_info.argtypes = [vp, vp]
+    L.kor_copy_layout.argtypes = [vp, vp, vp, vp]
+    L.kor_query_fixed.restype = i32
+    L.kor_query_fixed.argtypes = [vp, i32, i32, vp, u64, ctypes.c_uint32, ctypes.c_double,
+                                  i32, i32, vp, vp, vp, vp, i32, vp]
+    L.kor_query_radius.restype = vp
+    L.kor_query_radius.argtypes = [vp, i32, i32, vp, u64, ctypes.c_double, i32, i32, vp, i32, vp]
+    L.kor_query_fixed_r.restype = i32
+    L.kor_query_fixed_r.argtypes = [vp, i32, i32, vp, u64, ctypes.c_uint32, ctypes.c_double,
+                                    vp, i32, i32, vp, vp, vp, vp, i32, vp]
+    L.kor_query_radius_r.restype = vp
+    L.kor_query_radius_r.argtypes = [vp, i32, i32, vp, u64, ctypes.c_double, vp, i32, i32, vp,
+                                     i32, vp]
+    L.kor_donnelly_path.argtypes = [ctypes.c_uint32, vp, u64, vp]
+    L.kor_metric_f64x3.restype = i32
+    L.kor_metric_f64x3.argtypes = [i32, vp, vp, ctypes.c_double, vp, i32, ctypes.c_double, vp]
+    L.kor_radius_total.restype = u64
+    L.kor_radius_total.argtypes = [vp]
+    L.kor_radius_copy.argtypes = [vp, vp, vp, vp]
+    L.kor_radius_free.argtypes = [vp]
+    return L
 
 
 def _ptr(a):
@@ -105,47 +166,54 @@ class Layout:
 class OracleTree:
     """ImmutableKdTree<A, K> built and queried by the CPU restatement."""
 
-    def __init__(self, handle, dtype, k):
+    def __init__(self, handle, dtype, k, L=None):
         self._h = handle
         self.dtype = np.dtype(dtype)
         self.k = k
+        self._L = L if L is not None else lib()
 
     @classmethod
-    def build(cls, points, items=None, block_height=0):
-        """Soft construction; block_height > 0 builds a Donnelly<block_height> tree."""
+    def build(cls, points, items=None, block_height=0, L=None):
+        """Soft construction; block_height > 0 builds a Donnelly<block_height> tree.
+        ``L`` picks the library (default the checker, ``lib()``; the timed
+        baseline passes ``timing_lib()``)."""
+        L = L if L is not None else lib()
         points = np.ascontiguousarray(points)
         assert points.dtype in (np.float32, np.float64) and points.ndim == 2
         n, k = points.shape
         it = None if items is None else np.ascontiguousarray(items, dtype=np.uint32)
-        h = lib().kor_build_ex(0 if points.dtype == np.float32 else 1, k, _ptr(points), _ptr(it), n,
-                               int(block_height))
+        h = L.kor_build_ex(0 if points.dtype == np.float32 else 1, k, _ptr(points), _ptr(it), n,
+                           int(block_height))
         if not h:
             raise ValueError("unsupported dtype/dimension for the oracle")
-        return cls(h, points.dtype, k)
+        return cls(h, points.dtype, k, L)
 
     @classmethod
-    def from_layout(cls, lay: Layout):
+    def from_layout(cls, lay: Layout, L=None):
+        L = L if L is not None else lib()
         dt = 0 if lay.dtype == np.float32 else 1
         stems = np.ascontiguousarray(lay.stems, dtype=lay.dtype)
         lb = np.ascontiguousarray(lay.leaf_bytes, dtype=np.uint8)
         ex = np.ascontiguousarray(lay.extents, dtype=np.uint64)
-        h = lib().kor_from_layout_ex(dt, lay.k, _ptr(stems), stems.size, _ptr(lb), lb.size,
-                                     _ptr(ex), ex.shape[0], lay.max_stem_level, lay.size,
-                                     lay.max_leaf_len, getattr(lay, "block_height", 0))
-        return cls(h, lay.dtype, lay.k)
+        h = L.kor_from_layout_ex(dt, lay.k, _ptr(stems), stems.size, _ptr(lb), lb.size,
+                                 _ptr(ex), ex.shape[0], lay.max_stem_level, lay.size,
+                                 lay.max_leaf_len, getattr(lay, "block_height", 0))
+        if not h:
+            raise ValueError("unsupported dtype/dimension for this oracle library")
+        return cls(h, lay.dtype, lay.k, L)
 
     def __del__(self):
-        if getattr(self, "_h", None) and _lib is not None:
-            _lib.kor_free(self._h)
+        if getattr(self, "_h", None) and getattr(self, "_L", None) is not None:
+            self._L.kor_free(self._h)
             self._h = None
 
     def layout(self) -> Layout:
         info = np.zeros(7, dtype=np.int64)
-        lib().kor_layout_info(self._h, _ptr(info))
+        self._L.kor_layout_info(self._h, _ptr(info))
         stems = np.empty(int(info[0]), dtype=self.dtype)
         lb = np.empty(int(info[1]), dtype=np.uint8)
         ex = np.empty((int(info[2]), 2), dtype=np.uint64)
-        lib().kor_copy_layout(self._h, _ptr(stems), _ptr(lb), _ptr(ex))
+        self._L.kor_copy_layout(self._h, _ptr(stems), _ptr(lb), _ptr(ex))
         return Layout(self.dtype, self.k, stems, lb, ex, info[3], info[4], info[5], info[6])
 
     def iter(self):
@@ -157,13 +225,22 @@ class OracleTree:
         items = np.empty(n, dtype=np.uint32)
         pts = np.empty((n, self.k), dtype=self.dtype)
         if n:
-            lib().kor_iter(self._h, _ptr(items), _ptr(pts))
+            self._L.kor_iter(self._h, _ptr(items), _ptr(pts))
         return items, pts
 
     def _q(self, queries):
         q = np.ascontiguousarray(queries, dtype=self.dtype)
         assert q.ndim == 2 and q.shape[1] == self.k
         return q
+
+    def _radii(self, radius, nq):
+        """(scalar radius, per-query radii array or None): an array-like
+        radius gives every query its own radius, in the tree's dtype."""
+        if np.ndim(radius) == 0:
+            return float(radius), None
+        r = np.ascontiguousarray(radius, dtype=self.dtype).reshape(-1)
+        assert r.size == nq, "one radius per query"
+        return 0.0, r
 
     def _box(self, box):
         if box is None:
@@ -181,9 +258,10 @@ class OracleTree:
         st = np.zeros(3, dtype=np.uint64) if stats else None
         nth = threads if threads > 0 else (os.cpu_count() or 1)
         bx = self._box(box)
-        rc = lib().kor_query_fixed(self._h, family, METRICS[metric], _ptr(q), nq, kk,
-                                   float(radius), int(exclusive), int(sorted), _ptr(bx), _ptr(d),
-                                   _ptr(it), _ptr(c), nth, _ptr(st))
+        r0, rr = self._radii(radius, nq)
+        rc = self._L.kor_query_fixed_r(self._h, family, METRICS[metric], _ptr(q), nq, kk, r0,
+                                     _ptr(rr), int(exclusive), int(sorted), _ptr(bx), _ptr(d),
+                                     _ptr(it), _ptr(c), nth, _ptr(st))
         if rc != 0:
             raise ValueError("query family not supported on this tree by the oracle")
         out = (d.reshape(nq, kk), it.reshape(nq, kk), c)
@@ -196,16 +274,17 @@ class OracleTree:
         st = np.zeros(3, dtype=np.uint64) if stats else None
         nth = threads if threads > 0 else (os.cpu_count() or 1)
         bx = self._box(box)
-        r = lib().kor_query_radius(self._h, family, METRICS[metric], _ptr(q), nq, float(radius),
-                                   int(exclusive), int(sorted), _ptr(bx), nth, _ptr(st))
+        r0, rr = self._radii(radius, nq)
+        r = self._L.kor_query_radius_r(self._h, family, METRICS[metric], _ptr(q), nq, r0, _ptr(rr),
+                                     int(exclusive), int(sorted), _ptr(bx), nth, _ptr(st))
         if not r:
             raise ValueError("query family not supported on this tree by the oracle")
-        total = lib().kor_radius_total(r)
+        total = self._L.kor_radius_total(r)
         off = np.empty(nq + 1, dtype=np.uint64)
         d = np.empty(total, dtype=self.dtype)
         it = np.empty(total, dtype=np.uint32)
-        lib().kor_radius_copy(r, _ptr(off), _ptr(d), _ptr(it))
-        lib().kor_radius_free(r)
+        self._L.kor_radius_copy(r, _ptr(off), _ptr(d), _ptr(it))
+        self._L.kor_radius_free(r)
         out = (off, d, it)
         return out + (st,) if stats else out
 

@@ -78,7 +78,7 @@ struct StatsAcc {
 
 template <typename A, int K, typename M>
 int query_fixed_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq, uint32_t k,
-                  A radius, int exclusive, int sorted, const A* box, A* out_d,
+                  A radius0, const A* radii, int exclusive, int sorted, const A* box, A* out_d,
                   uint32_t* out_i, uint32_t* out_c, int nthreads, uint64_t* stats3) {
   StatsAcc acc;
   const bool want_stats = stats3 != nullptr;
@@ -86,6 +86,7 @@ int query_fixed_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq
     Stats s;
     Stats* sp = want_stats ? &s : nullptr;
     const A* q = queries + qi * K;
+    const A radius = radii ? radii[qi] : radius0;  // one radius per query, or one for all
     switch (family) {
       case FAM_NEAREST_ONE: {
         auto r = nearest_one<A, K, M>(t, q, sp);
@@ -144,8 +145,8 @@ int query_fixed_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq
 
 template <typename A, int K, typename M>
 RadiusResult* query_radius_t(const Tree<A, K>& t, int family, const A* queries, uint64_t nq,
-                             A radius, int exclusive, int sorted, const A* box, int nthreads,
-                             uint64_t* stats3) {
+                             A radius0, const A* radii, int exclusive, int sorted, const A* box,
+                             int nthreads, uint64_t* stats3) {
   std::vector<std::vector<Hit<A>>> per(nq);
   StatsAcc acc;
   const bool want_stats = stats3 != nullptr;
@@ -153,6 +154,7 @@ RadiusResult* query_radius_t(const Tree<A, K>& t, int family, const A* queries, 
     Stats s;
     Stats* sp = want_stats ? &s : nullptr;
     const A* q = queries + qi * K;
+    const A radius = radii ? radii[qi] : radius0;
     if (family == FAM_WITHIN)
       per[qi] = within<A, K, M>(t, q, radius, exclusive, sorted, sp);
     else if constexpr (M::kPeriodic)
@@ -189,6 +191,14 @@ RadiusResult* query_radius_t(const Tree<A, K>& t, int family, const A* queries, 
 template <typename F>
 auto dispatch(int dtype, int k, F&& f) -> decltype(f(float(), std::integral_constant<int, 3>())) {
   using R = decltype(f(float(), std::integral_constant<int, 3>()));
+#ifdef KOR_TIMING_BUILD
+  // the timed CPU baseline needs 3-D trees only; fewer instantiations keep its
+  // -O3 -march=native build short enough to run on the host being timed
+  if (k == 3) {
+    if (dtype == 0) return f(float(), std::integral_constant<int, 3>());
+    if (dtype == 1) return f(double(), std::integral_constant<int, 3>());
+  }
+#else
   if (dtype == 0) {
     switch (k) {
       case 1: return f(float(), std::integral_constant<int, 1>());
@@ -204,6 +214,7 @@ auto dispatch(int dtype, int k, F&& f) -> decltype(f(float(), std::integral_cons
       case 4: return f(double(), std::integral_constant<int, 4>());
     }
   }
+#endif
   return R();
 }
 
@@ -331,74 +342,78 @@ void kor_copy_layout(void* hp, void* stems_out, uint8_t* bytes_out, uint64_t* ex
 // metric: 0 SquaredEuclidean, 1 Manhattan, 2 Chebyshev, 3 / 4 Minkowski<3> /
 // Minkowski<4> (the last three not periodic: -2 / nullptr).  Outputs are dense [nq * k]
 // (k = 1 for the nearest-one families); unused slots hold +inf / 0xFFFFFFFF.
-int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint64_t nq,
-                    uint32_t k, double radius, int exclusive, int sorted, const void* box,
-                    void* out_d, uint32_t* out_i, uint32_t* out_c, int nthreads,
-                    uint64_t* stats3) {
+// radii: one radius per query in the tree's dtype, or nullptr for `radius` on every query.
+int kor_query_fixed_r(void* hp, int family, int metric, const void* queries, uint64_t nq,
+                      uint32_t k, double radius, const void* radii, int exclusive, int sorted,
+                      const void* box, void* out_d, uint32_t* out_i, uint32_t* out_c,
+                      int nthreads, uint64_t* stats3) {
   auto* b = static_cast<TreeBase*>(hp);
   return dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
     using A = decltype(a);
     constexpr int K = decltype(kk)::value;
     auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
-    const A r = A(radius);
-    if (t.stem_strategy == 1 && (family == FAM_PERIODIC_NEAREST_ONE ||
-                                 family == FAM_PERIODIC_NEAREST_N))
+    const bool periodic = family == FAM_PERIODIC_NEAREST_ONE || family == FAM_PERIODIC_NEAREST_N;
+    if (t.stem_strategy == 1 && periodic)
       return -2;  // the periodic restatement follows the Eytzinger traversal only
-    if (metric == 0)
-      return query_fixed_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, k,
-                                              r, exclusive, sorted,
-                                              static_cast<const A*>(box), static_cast<A*>(out_d),
-                                              out_i, out_c, nthreads, stats3);
-    if (metric >= 2) {
-      if (family == FAM_PERIODIC_NEAREST_ONE || family == FAM_PERIODIC_NEAREST_N) return -2;
-      auto run = [&](auto m) {
-        return query_fixed_t<A, K, decltype(m)>(t, family, static_cast<const A*>(queries), nq, k,
-                                                r, exclusive, sorted, static_cast<const A*>(box),
-                                                static_cast<A*>(out_d), out_i, out_c, nthreads,
-                                                stats3);
-      };
-      if (metric == 2) return run(Chebyshev());
-      if (metric == 3) return run(Minkowski<3>());
-      if (metric == 4) return run(Minkowski<4>());
-      return -1;
-    }
-    return query_fixed_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, k, r,
-                                          exclusive, sorted, static_cast<const A*>(box),
-                                          static_cast<A*>(out_d), out_i, out_c, nthreads,
-                                          stats3);
+    auto run = [&](auto m) -> int {
+      return query_fixed_t<A, K, decltype(m)>(
+          t, family, static_cast<const A*>(queries), nq, k, A(radius),
+          static_cast<const A*>(radii), exclusive, sorted, static_cast<const A*>(box),
+          static_cast<A*>(out_d), out_i, out_c, nthreads, stats3);
+    };
+    if (metric == 0) return run(SqEuclidean());
+#ifndef KOR_TIMING_BUILD
+    if (metric == 1) return run(Manhattan());
+    if (periodic) return -2;
+    if (metric == 2) return run(Chebyshev());
+    if (metric == 3) return run(Minkowski<3>());
+    if (metric == 4) return run(Minkowski<4>());
+#endif
+    return -1;
+  });
+}
+
+int kor_query_fixed(void* hp, int family, int metric, const void* queries, uint64_t nq,
+                    uint32_t k, double radius, int exclusive, int sorted, const void* box,
+                    void* out_d, uint32_t* out_i, uint32_t* out_c, int nthreads,
+                    uint64_t* stats3) {
+  return kor_query_fixed_r(hp, family, metric, queries, nq, k, radius, nullptr, exclusive,
+                           sorted, box, out_d, out_i, out_c, nthreads, stats3);
+}
+
+void* kor_query_radius_r(void* hp, int family, int metric, const void* queries, uint64_t nq,
+                         double radius, const void* radii, int exclusive, int sorted,
+                         const void* box, int nthreads, uint64_t* stats3) {
+  auto* b = static_cast<TreeBase*>(hp);
+  return dispatch(b->dtype, b->k, [&](auto a, auto kk) -> void* {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    const bool periodic = family == FAM_PERIODIC_WITHIN;
+    if (t.stem_strategy == 1 && periodic) return nullptr;
+    auto run = [&](auto m) -> void* {
+      return query_radius_t<A, K, decltype(m)>(
+          t, family, static_cast<const A*>(queries), nq, A(radius),
+          static_cast<const A*>(radii), exclusive, sorted, static_cast<const A*>(box), nthreads,
+          stats3);
+    };
+    if (metric == 0) return run(SqEuclidean());
+#ifndef KOR_TIMING_BUILD
+    if (metric == 1) return run(Manhattan());
+    if (periodic) return nullptr;
+    if (metric == 2) return run(Chebyshev());
+    if (metric == 3) return run(Minkowski<3>());
+    if (metric == 4) return run(Minkowski<4>());
+#endif
+    return nullptr;
   });
 }
 
 void* kor_query_radius(void* hp, int family, int metric, const void* queries, uint64_t nq,
                        double radius, int exclusive, int sorted, const void* box, int nthreads,
                        uint64_t* stats3) {
-  auto* b = static_cast<TreeBase*>(hp);
-  return dispatch(b->dtype, b->k, [&](auto a, auto kk) -> void* {
-    using A = decltype(a);
-    constexpr int K = decltype(kk)::value;
-    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
-    const A r = A(radius);
-    if (t.stem_strategy == 1 && family == FAM_PERIODIC_WITHIN) return nullptr;
-    if (metric == 0)
-      return query_radius_t<A, K, SqEuclidean>(t, family, static_cast<const A*>(queries), nq, r,
-                                               exclusive, sorted, static_cast<const A*>(box),
-                                               nthreads, stats3);
-    if (metric >= 2) {
-      if (family == FAM_PERIODIC_WITHIN) return nullptr;
-      auto run = [&](auto m) {
-        return query_radius_t<A, K, decltype(m)>(t, family, static_cast<const A*>(queries), nq, r,
-                                                 exclusive, sorted, static_cast<const A*>(box),
-                                                 nthreads, stats3);
-      };
-      if (metric == 2) return run(Chebyshev());
-      if (metric == 3) return run(Minkowski<3>());
-      if (metric == 4) return run(Minkowski<4>());
-      return nullptr;
-    }
-    return query_radius_t<A, K, Manhattan>(t, family, static_cast<const A*>(queries), nq, r,
-                                           exclusive, sorted, static_cast<const A*>(box),
-                                           nthreads, stats3);
-  });
+  return kor_query_radius_r(hp, family, metric, queries, nq, radius, nullptr, exclusive, sorted,
+                            box, nthreads, stats3);
 }
 
 // Test hook for the metric arithmetic (f64, K = 3): out[0] = dist(a, b),

@@ -1,6 +1,6 @@
 """Batched queries over many trees (one persistent launch with a device work
-queue) give the same bits as querying every tree on its own, which is pinned
-to the oracle; per-query radii are checked against the oracle directly."""
+queue) against the oracle tree each query names, bit for bit, for every
+family, with one radius for the batch or one per query."""
 import numpy as np
 import pytest
 
@@ -20,13 +20,18 @@ def _forest_data(rng, n_trees=9, dtype=np.float32):
     return pts
 
 
-@pytest.mark.parametrize("engine", [None, "warp"])
-def test_forest_matches_per_tree_queries(engine):
+@pytest.mark.parametrize("engine", [None, "warp", "thread"])
+@pytest.mark.parametrize("order", [None, True])
+def test_forest_fixed_families_match_oracle(engine, order):
+    """nearest_one, nearest_n(8) sorted and unsorted, nearest_n(8).within and
+    best_n_within(5) over 9 trees of 20 to 60,000 points in one launch: each
+    query's row against the oracle tree it names."""
     import torch
     rng = np.random.default_rng(8)
     pts = _forest_data(rng)
     items = [rng.permutation(len(p)).astype(np.uint32) for p in pts]
     trees = [kb.ImmutableKdTree.new_from_entries(it, p) for it, p in zip(items, pts)]
+    oracles = [oracle.OracleTree.build(p, it) for it, p in zip(items, pts)]
     forest = kb.Forest(trees)
     nq = 12000
     tree_of = rng.integers(0, len(trees), nq).astype(np.int32)
@@ -34,29 +39,30 @@ def test_forest_matches_per_tree_queries(engine):
     Q = (Q / np.linalg.norm(Q, axis=1, keepdims=True)).astype(np.float32)
     dq = torch.from_numpy(Q).cuda()
     dt = torch.from_numpy(tree_of).cuda()
-    for fam in ("nn1", "knn", "best"):
-        b = forest.query(dq, dt).with_engine(engine)
-        if fam == "nn1":
-            g = b.nearest_one(kb.SquaredEuclidean).execute_gpu()
-        elif fam == "knn":
-            g = b.nearest_n(kb.SquaredEuclidean, 8).execute_gpu()
-        else:
-            g = b.best_n_within(kb.SquaredEuclidean, 4e-4, 5).execute_gpu()
+    r = 4e-4
+    cases = {
+        "nn1": (lambda b: b.nearest_one(kb.SquaredEuclidean),
+                lambda o, q: o.nearest_one(q) + (np.ones(len(q), np.uint32),)),
+        "knn": (lambda b: b.nearest_n(kb.SquaredEuclidean, 8), lambda o, q: o.nearest_n(q, 8)),
+        "knn_unsorted": (lambda b: b.nearest_n(kb.SquaredEuclidean, 8).unsorted(),
+                         lambda o, q: o.nearest_n(q, 8, sorted=False)),
+        "knn_within": (lambda b: b.nearest_n(kb.SquaredEuclidean, 8).within(r),
+                       lambda o, q: o.nearest_n(q, 8, radius=r)),
+        "best": (lambda b: b.best_n_within(kb.SquaredEuclidean, r, 5),
+                 lambda o, q: o.best_n_within(q, r, 5)),
+    }
+    for fam, (make, ref) in cases.items():
+        g = make(forest.query(dq, dt).with_engine(engine).with_spatial_order(order)).execute_gpu()
+        gd = g.distances.cpu().numpy().reshape(nq, -1)
+        gi = g.items.cpu().numpy().view(np.uint32).reshape(nq, -1)
+        gc = np.ones(nq, np.uint32) if fam == "nn1" else g.counts.cpu().numpy()
         for t in range(len(trees)):
             sel = np.nonzero(tree_of == t)[0]
             if len(sel) == 0:
                 continue
-            bt = trees[t].query(Q[sel]).with_engine(engine)
-            if fam == "nn1":
-                r = bt.nearest_one(kb.SquaredEuclidean).execute_gpu()
-                assert np.array_equal(g.distances.cpu().numpy()[sel], r.distances)
-                assert np.array_equal(g.items.cpu().numpy().view(np.uint32)[sel], r.items)
-            else:
-                r = (bt.nearest_n(kb.SquaredEuclidean, 8) if fam == "knn" else
-                     bt.best_n_within(kb.SquaredEuclidean, 4e-4, 5)).execute_gpu()
-                assert_same_fixed(g.distances.cpu().numpy()[sel],
-                                  g.items.cpu().numpy().view(np.uint32)[sel],
-                                  g.counts.cpu().numpy()[sel], r.distances, r.items, r.counts, fam)
+            od, oi, oc = ref(oracles[t], Q[sel])
+            assert_same_fixed(gd[sel], gi[sel], gc[sel], np.asarray(od).reshape(len(sel), -1),
+                              np.asarray(oi).reshape(len(sel), -1), oc, f"{fam} tree {t}")
 
 
 @pytest.mark.parametrize("sorted_", [True, False])

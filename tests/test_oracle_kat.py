@@ -224,3 +224,29 @@ def test_donnelly_tree_matches_brute_force_and_eytzinger(bh, dtype):
         assert np.array_equal(b1[1], b2[1]) and np.array_equal(b1[2], b2[2])
         a1 = don.approx_nearest_one(Q)[0]
         assert np.all(a1 >= dd)
+
+
+def test_timing_build_matches_the_checker():
+    """The timed CPU baseline (the oracle's source at -O3 -march=native, built
+    on this host) answers the benchmarked families bit for bit like the -O2
+    checker, and builds the same tree; a mismatch would mean the timed code is
+    not the checked code."""
+    T = oracle.timing_lib()
+    rng = np.random.default_rng(77)
+    for dtype in (np.float32, np.float64):
+        P = np.concatenate([rng.random((30_000, 3)),
+                            np.floor(rng.random((5_000, 3)) * 8) / 8]).astype(dtype)
+        Q = np.concatenate([rng.random((4_000, 3)), P[:500]]).astype(dtype)
+        a = oracle.OracleTree.build(P)
+        b = oracle.OracleTree.build(P, L=T)
+        la, lb = a.layout(), b.layout()
+        assert np.array_equal(la.stems, lb.stems) and np.array_equal(la.leaf_bytes, lb.leaf_bytes)
+        for x, y in ((a.nearest_one(Q), b.nearest_one(Q)),
+                     (a.approx_nearest_one(Q), b.approx_nearest_one(Q)),
+                     (a.nearest_n(Q, 16), b.nearest_n(Q, 16)),
+                     (a.periodic_nearest_n(Q, np.ones(3), 32, radius=0.01),
+                      b.periodic_nearest_n(Q, np.ones(3), 32, radius=0.01)),
+                     (a.best_n_within(Q, 1e-3, 5), b.best_n_within(Q, 1e-3, 5)),
+                     (a.within(Q, 1e-3), b.within(Q, 1e-3))):
+            for u, v in zip(x, y):
+                assert np.array_equal(u, v)

@@ -105,13 +105,16 @@ def test_projection_ordering_rules_on_the_host():
     off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
     n = int(off[-1])
     dist = np.floor(rng.random(n) * 6).astype(np.float32)  # many ties
-    ranks = rng.permutation(1 << 20)[:n].astype(np.int32)
+    # ranks are uint32 held in int32: include some at 2^31 and above (negative as int32)
+    ranks_u = rng.permutation(1 << 20)[:n].astype(np.uint32)
+    ranks_u[::7] = rng.integers(1 << 31, (1 << 32) - 1, len(ranks_u[::7]), dtype=np.uint64)
+    ranks = ranks_u.view(np.int32)
     rows = np.repeat(np.arange(60), counts)
     got = kb._csr_order(torch.from_numpy(off), torch.from_numpy(ranks)).numpy()
-    assert np.array_equal(got, np.lexsort((ranks, rows)))
+    assert np.array_equal(got, np.lexsort((ranks_u, rows)))
     got = kb._csr_order(torch.from_numpy(off), torch.from_numpy(ranks),
                         torch.from_numpy(dist)).numpy()
-    assert np.array_equal(got, np.lexsort((ranks, dist, rows)))
+    assert np.array_equal(got, np.lexsort((ranks_u, dist, rows)))
     D = np.floor(rng.random((40, 12)) * 4).astype(np.float32)
     R = rng.integers(0, 1000, (40, 12)).astype(np.int32)
     D[:, 9:] = np.inf
@@ -120,3 +123,44 @@ def test_projection_ordering_rules_on_the_host():
     key = R.astype(np.int64) % (1 << 32)
     for j in range(40):
         assert np.array_equal(got[j], np.lexsort((key[j], D[j])))
+
+
+def test_nearest_one_projection_keeps_rows_without_hits():
+    """with_points().nearest_one on a query with a NaN coordinate: its radius
+    row is empty (NaN distances fail d <= r), and scan_projected_nearest_one
+    (builder.rs:2175-2212) keeps the first entry in iteration order at its own
+    NaN distance.  Empty rows in the middle and at the end, on CPU tensors."""
+    import torch
+    import kiddo_b200 as kb
+    from kiddo_b200 import _capi as C
+
+    class FakeTree:
+        def iter(self, stream=None):
+            return (torch.tensor([40, 41, 42], dtype=torch.int32),
+                    torch.tensor([[0.5, 0.5], [0.1, 0.2], [0.9, 0.9]], dtype=torch.float32))
+
+    class Res:
+        pass
+
+    r = Res()
+    r.offsets = torch.tensor([0, 2, 2, 3, 3], dtype=torch.int64)  # rows 1 and 3 empty
+    r.distances = torch.tensor([0.25, 0.25, 0.01], dtype=torch.float32)
+    r.items = torch.tensor([42, 41, 40], dtype=torch.int32)
+    ranks = torch.tensor([2, 1, 0], dtype=torch.int32)
+    pts = torch.tensor([[0.9, 0.9], [0.1, 0.2], [0.5, 0.5]], dtype=torch.float32)
+    q = torch.tensor([[0.4, 0.4], [float("nan"), 0.3], [0.5, 0.6], [0.2, float("nan")]],
+                     dtype=torch.float32)
+    out = kb._first_by_rank(r, ranks, pts, q, C.SQUARED_EUCLIDEAN, FakeTree(), None)
+    assert out.items.tolist() == [41, 40, 40, 40]
+    d = out.distances.numpy()
+    assert d[0] == np.float32(0.25) and d[2] == np.float32(0.01)
+    assert np.isnan(d[1]) and np.isnan(d[3])
+    assert np.array_equal(out.points.numpy(), np.array([[0.1, 0.2], [0.5, 0.5], [0.5, 0.5],
+                                                        [0.5, 0.5]], dtype=np.float32))
+    # the NaN rows agree with the oracle's restatement of the scan
+    import oracle
+    P = np.array([[0.5, 0.5], [0.1, 0.2], [0.9, 0.9]], dtype=np.float32)
+    o = oracle.OracleTree.build(P)
+    items, ipts = o.iter()
+    od, oi, op, orank = oracle.projected_nearest_one(o, q[1].numpy())
+    assert orank == 0 and np.isnan(od) and oi == int(items[0])

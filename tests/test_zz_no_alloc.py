@@ -26,7 +26,7 @@ def _desc(radius, family=C.WITHIN, flags=0):
     d.family = family
     d.metric = C.SQUARED_EUCLIDEAN
     d.radius = radius
-    d.sorted = 1
+    d.sorted = 1 if family == C.WITHIN else 0
     d.flags = flags
     return d
 
@@ -38,25 +38,93 @@ def _count(fn, tree, d, dq, nq, offsets):
               ctypes.c_void_p(offsets.data_ptr()), st)
 
 
-def test_noalloc_count_matches_the_allocating_count_on_two_calls_in_a_row():
+def _default_pool_usage():
+    """(bytes in use, high-water mark, bytes held) of the device's default
+    stream-ordered pool, read through the CUDA runtime bindings."""
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    assert err == rt.cudaError_t.cudaSuccess
+    out = []
+    for a in (rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent,
+              rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
+              rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent):
+        err, v = rt.cudaMemPoolGetAttribute(pool, a)
+        assert err == rt.cudaError_t.cudaSuccess
+        out.append(int(v))
+    return tuple(out), pool
+
+
+def _reset_default_pool_high(pool):
+    from cuda.bindings import runtime as rt
+    err, = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
+                                      rt.cuuint64_t(0))
+    assert err == rt.cudaError_t.cudaSuccess
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("block_height", [0, 4])
+@pytest.mark.parametrize("family", [C.WITHIN, C.WITHIN_UNSORTED])
+def test_noalloc_count_matches_the_allocating_count_on_two_calls_in_a_row(dtype, block_height,
+                                                                        family):
     import torch
     L = C.lib()
     rng = np.random.default_rng(4)
-    P = rng.random((200_000, 3)).astype(np.float32)
-    tree = kb.ImmutableKdTree.new_from_slice(P).to_gpu()
-    # two different batches and radii back to back: the second call must not
-    # see anything the first left in the shared scratch
-    for nq, radius in ((300_000, 2e-4), (70_001, 5e-5)):
-        Q = rng.random((nq, 3)).astype(np.float32)
+    P = rng.random((200_000, 3)).astype(dtype)
+    tree = kb.ImmutableKdTree.new_from_slice(P, block_height=block_height).to_gpu()
+    # different batches and radii back to back: each call must not see
+    # anything the previous one left in the shared scratch (the sizes cover
+    # an empty batch, one query, exactly one scan tile and one past it)
+    for nq, radius in ((300_000, 2e-4), (70_001, 5e-5), (0, 1e-4), (1, 1e-3), (2048, 1e-4),
+                       (2049, 3e-4)):
+        Q = rng.random((max(nq, 1), 3)).astype(dtype)
         dq = torch.from_numpy(Q).cuda()
         ref = torch.empty(nq + 1, dtype=torch.int64, device="cuda")
         got = torch.full((nq + 1,), -1, dtype=torch.int64, device="cuda")
-        d = _desc(radius)
+        d = _desc(radius, family)
         C.check(_count(L.kgpu_query_radius_count, tree, d, dq, nq, ref))
+        torch.cuda.synchronize()
         C.check(_count(L.kgpu_query_radius_count_noalloc, tree, d, dq, nq, got))
         torch.cuda.synchronize()
-        assert torch.equal(got, ref)  # integer offsets: exact
-        assert int(got[-1]) > 0
+        assert torch.equal(got, ref), (nq, radius)  # integer offsets: exact
+        if nq >= 2048:
+            assert int(got[-1]) > 0
+
+
+def test_noalloc_count_allocates_nothing():
+    """Neither the library's scratch pool, nor the device's default pool, nor
+    torch's allocator gains a byte (not even transiently: the high-water marks
+    are reset first) across two calls."""
+    import torch
+    L = C.lib()
+    rng = np.random.default_rng(6)
+    tree = kb.ImmutableKdTree.new_from_slice(rng.random((100_000, 3)).astype(np.float32)).to_gpu()
+    nq = 500_000
+    dq = torch.from_numpy(rng.random((nq, 3)).astype(np.float32)).cuda()
+    got = torch.empty(nq + 1, dtype=torch.int64, device="cuda")
+    ref = torch.empty(nq + 1, dtype=torch.int64, device="cuda")
+    d = _desc(2e-4)
+    C.check(_count(L.kgpu_query_radius_count_noalloc, tree, d, dq, nq, got))  # first-call set-up
+    torch.cuda.synchronize()
+    C.scratch_trim(0)
+    lib_before = C.scratch_stats(0)
+    default_before, pool = _default_pool_usage()
+    _reset_default_pool_high(pool)
+    default_before, _ = _default_pool_usage()
+    torch_before = (torch.cuda.memory_allocated(), torch.cuda.memory_reserved())
+    for _ in range(2):
+        C.check(_count(L.kgpu_query_radius_count_noalloc, tree, d, dq, nq, got))
+    torch.cuda.synchronize()
+    lib_after = C.scratch_stats(0)
+    default_after, _ = _default_pool_usage()
+    assert lib_after[0] == lib_before[0] and lib_after[2] == lib_before[2]
+    assert lib_after[1] == lib_before[1]  # high-water mark: no transient allocation
+    assert default_after == default_before
+    assert (torch.cuda.memory_allocated(), torch.cuda.memory_reserved()) == torch_before
+    # and the allocating count does use the library's pool, so the probe can see one
+    C.check(_count(L.kgpu_query_radius_count, tree, d, dq, nq, ref))
+    torch.cuda.synchronize()
+    assert C.scratch_stats(0)[1] > lib_before[1]
+    assert torch.equal(got, ref)
 
 
 def test_noalloc_count_rejects_host_buffers_and_oversized_batches():
