@@ -304,6 +304,8 @@ def l2_note(n, nq, itemsize):
 def kernel_name(fam, engine):
     if fam.startswith("periodic"):
         return "k_tperiodic_nn" if engine != "warp" else "k_periodic_fixed<nearest_n>"
+    if fam == "nearest_n" and engine == "coop":
+        return "k_tnn_coop"
     f = {"nearest_n": "nearest_n", "approx": "approx", "nearest_one": "nearest_one"}[fam]
     return f"k_tfixed<{f}>" if engine != "warp" else f"k_fixed<{f}>"
 
@@ -524,7 +526,7 @@ def main():
     ap.add_argument("--spatial-order", default=None, action="store_true",
                     help="force leaf-grouped processing (default: the library decides)")
     ap.add_argument("--no-spatial-order", dest="spatial_order", action="store_false")
-    ap.add_argument("--engine", default=None, choices=["warp", "thread"],
+    ap.add_argument("--engine", default=None, choices=["warp", "thread", "coop"],
                     help="force the kernel variant (default: the library chooses)")
     ap.add_argument("--points", type=int, default=0, help="override the tree size (profiling)")
     ap.add_argument("--queries", type=int, default=0, help="override the batch size (profiling)")

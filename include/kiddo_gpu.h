@@ -87,6 +87,8 @@ typedef enum kgpu_family {
 #define KGPU_FLAG_NO_SPATIAL_ORDER 0x10u /* process queries in the order given */
 #define KGPU_FLAG_ENGINE_WARP 0x4u   /* force one warp per query (same results) */
 #define KGPU_FLAG_ENGINE_THREAD 0x8u /* force one thread per query (same results) */
+#define KGPU_FLAG_ENGINE_COOP 0x20u  /* one walk per thread, each leaf scanned by the whole
+                                        warp (same results; nearest_n sorted, k <= 32) */
 
 /* Layout of one ImmutableKdTree as the reference stores it
  * (src/kd_tree/mod.rs:221-241, src/leaf_strategy/vec_of_arenas.rs:60-69). */

@@ -709,10 +709,12 @@ class QueryBuilder:
         return self
 
     def with_engine(self, engine: Optional[str]) -> "QueryBuilder":
-        """Force the kernel variant: "warp" (one warp per query) or "thread"
-        (one thread per query); None lets the library choose.  Same results."""
-        if engine not in (None, "warp", "thread"):
-            raise ValueError("engine must be None, 'warp' or 'thread'")
+        """Force the kernel variant: "warp" (one warp per query), "thread"
+        (one thread per query) or "coop" (one walk per thread, each leaf
+        scanned by the whole warp; sorted nearest_n with k <= 32, other
+        families as "thread"); None lets the library choose.  Same results."""
+        if engine not in (None, "warp", "thread", "coop"):
+            raise ValueError("engine must be None, 'warp', 'thread' or 'coop'")
         self.engine = engine
         return self
 
@@ -755,7 +757,8 @@ class QueryBuilder:
             C.FLAG_SPATIAL_ORDER if self.spatial_order else 0) | (
             C.FLAG_NO_SPATIAL_ORDER if self.spatial_order is False else 0) | (
             C.FLAG_ENGINE_WARP if self.engine == "warp" else 0) | (
-            C.FLAG_ENGINE_THREAD if self.engine == "thread" else 0)
+            C.FLAG_ENGINE_THREAD if self.engine == "thread" else 0) | (
+            C.FLAG_ENGINE_COOP if self.engine == "coop" else 0)
         return d
 
     def traversal_stats(self):

@@ -26,6 +26,7 @@ FLAG_HOST_BUFFERS = 0x1
 FLAG_SPATIAL_ORDER = 0x2
 FLAG_ENGINE_WARP = 0x4
 FLAG_ENGINE_THREAD = 0x8
+FLAG_ENGINE_COOP = 0x20
 FLAG_NO_SPATIAL_ORDER = 0x10
 
 # Every symbol include/kiddo_gpu.h declares.

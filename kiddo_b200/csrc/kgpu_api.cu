@@ -841,7 +841,7 @@ int32_t kgpu_query(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, 
   q.sorted = d->sorted != 0;
   q.nq = nq;
   apply_periodic(dt, d, q);
-  q.engine = (d->flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (d->flags & KGPU_FLAG_ENGINE_THREAD) ? 2 : 0;
+  q.engine = engine_of(d->flags);
   const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
   cudaError_t e = cudaSuccess;
   if (host) return query_host_pipelined(dt, d, q, queries, nq, w, out_dists, out_items, out_counts, s);
@@ -878,7 +878,7 @@ int32_t kgpu_query_radius_count(kgpu_tree* t, const kgpu_query_desc* d, const vo
   q.sorted = d->family == KGPU_WITHIN && d->sorted != 0;
   q.nq = nq;
   apply_periodic(dt, d, q);
-  q.engine = (d->flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (d->flags & KGPU_FLAG_ENGINE_THREAD) ? 2 : 0;
+  q.engine = engine_of(d->flags);
   q.stream = s;
   uint64_t* doff = offsets;
   if (host) {
@@ -946,7 +946,7 @@ int32_t kgpu_query_radius_fill(kgpu_tree* t, const kgpu_query_desc* d, const voi
   q.sorted = sorted;
   q.nq = nq;
   apply_periodic(dt, d, q);
-  q.engine = (d->flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (d->flags & KGPU_FLAG_ENGINE_THREAD) ? 2 : 0;
+  q.engine = engine_of(d->flags);
   q.stream = s;
   const uint64_t* doff = offsets;
   if (host) {
@@ -1029,7 +1029,7 @@ int32_t kgpu_query_stats(kgpu_tree* t, const kgpu_query_desc* d, const void* que
   q.sorted = d->sorted != 0;
   q.nq = nq;
   apply_periodic(dt, d, q);
-  q.engine = (d->flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (d->flags & KGPU_FLAG_ENGINE_THREAD) ? 2 : 0;
+  q.engine = engine_of(d->flags);
   q.queries = dq;
   q.out_d = bd.p;
   q.out_i = bi.as<uint32_t>();

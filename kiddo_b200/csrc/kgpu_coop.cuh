@@ -13,8 +13,9 @@
 // best_n_within the n smallest by (item, arrival) (kd_tree/query/
 // best_n_within.rs:88-196), within appends hits in arrival order
 // (kd_tree/query/within.rs:18-41).  (For nearest_n the per-candidate
-// insertions cost more warp instructions than a per-thread scan saves, so
-// nearest_one and nearest_n scan per thread.)
+// insertions are paid per candidate while a per-thread scan pays per point;
+// nearest_n scans per thread unless KGPU_FLAG_ENGINE_COOP asks for this form,
+// and nearest_one always scans per thread.)
 #pragma once
 
 #include "kgpu_device.cuh"
@@ -81,7 +82,7 @@ struct CBestN {
   __device__ __forceinline__ A max_dist() const { return radius; }
   __device__ __forceinline__ bool unbounded_start() const { return false; }
 
-  __device__ __forceinline__ void leaf(int o, const CoopLeaf<A, K>& L, int lane) {
+  __device__ __forceinline__ void leaf(int o, uint64_t, const CoopLeaf<A, K>& L, int lane) {
     int nn = __shfl_sync(FULL, n, o);
     uint32_t lk = shfl(last, o);
     const A orad = shfl(radius, o);
@@ -178,7 +179,10 @@ struct CNearestNRow {
 
   // Chunks with this many candidates are merged at once instead of inserted
   // one by one.
-  static constexpr int kMergeFrom = 6;
+#ifndef KGPU_COOP_MERGE_FROM
+#define KGPU_COOP_MERGE_FROM 6
+#endif
+  static constexpr int kMergeFrom = KGPU_COOP_MERGE_FROM;
 
   // All candidates of a chunk at once.  The candidates are bitonic-sorted by
   // (distance, lane) -- lane order is arrival order -- with non-candidates

@@ -93,7 +93,7 @@ int forest_launch(kgpu_forest* f, const kgpu_query_desc* d, const void* queries,
   q.total_leaves = f->total_leaves;
   q.radii = radii;
   apply_periodic(f->meta, d, q);
-  q.engine = (d->flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (d->flags & KGPU_FLAG_ENGINE_THREAD) ? 2 : 0;
+  q.engine = engine_of(d->flags);
   return KGPU_OK;
 }
 

@@ -284,12 +284,12 @@ struct LaneFeeder {
 #ifndef KGPU_REFILL_MIN_IDLE
 #define KGPU_REFILL_MIN_IDLE 24
 #endif
-template <typename A>
+template <typename A, int MIN_IDLE = KGPU_REFILL_MIN_IDLE>
 __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, bool& active,
                                              bool& fresh, uint64_t& qi) {
   const unsigned lane = threadIdx.x & 31;
   unsigned need = __ballot_sync(FULL, !active);
-  if (need != FULL && __popc(need) < KGPU_REFILL_MIN_IDLE) return true;
+  if (need != FULL && __popc(need) < MIN_IDLE) return true;
   while (need) {
     if (fd.next >= fd.end && !fd.advance(b)) break;
     const uint64_t avail = fd.end - fd.next;
@@ -315,6 +315,11 @@ __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, 
 //   whether the query needs a walk at all; finish(o, qi) runs on the whole
 //   warp for lane o's finished query.
 // ---------------------------------------------------------------------------
+// Lanes refilled together in the cooperative driver: an idle lane costs
+// walk-phase slots only there (leaf scans loop over the active lanes).
+#ifndef KGPU_COOP_REFILL_MIN_IDLE
+#define KGPU_COOP_REFILL_MIN_IDLE KGPU_REFILL_MIN_IDLE
+#endif
 template <typename A, int K, typename M, typename Walk, typename Pol, typename Start,
           typename Finish>
 __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Walk& wk,
@@ -339,7 +344,7 @@ __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A
       const int o = __ffs(fm) - 1;
       finish(o, shfl64(qi, o));
     }
-    if (!refill_lanes(b, fd, active, fresh, qi)) break;
+    if (!refill_lanes<A, KGPU_COOP_REFILL_MIN_IDLE>(b, fd, active, fresh, qi)) break;
     bool bounded = true, empty = false;
     if (fresh) {
       fresh = false;
@@ -370,7 +375,7 @@ __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A
     }
     for (unsigned lm = __ballot_sync(FULL, active); lm; lm &= lm - 1) {
       const int o = __ffs(lm) - 1;
-      pol.leaf(o, coop_leaf<A, K>(o, lb, len, q), lane);
+      pol.leaf(o, shfl64(qi, o), coop_leaf<A, K>(o, lb, len, q), lane);
     }
   }
 }
@@ -533,6 +538,39 @@ __global__ void __launch_bounds__(256, tfixed_min_blocks<FAM, A>())
         },
         [&](int o, uint64_t qo) { pol.finish(o, qo, threadIdx.x & 31, out_d, out_i, out_c); });
   }
+  if (stats) flush_stats(stats, st);
+}
+
+// nearest_n / nearest_n().within with sorted output, k <= 32: per-thread
+// walks with lane refill (coop_drive), every leaf scanned by the whole warp
+// for its owner (lane p on point p: one coalesced load of the leaf's rows),
+// the owner's list kept sorted in its own output row (CNearestNRow: inserts
+// by ballot and shuffle, or a bitonic merge of a chunk's candidates).  Same
+// list as the per-thread scan: the k smallest by (distance, arrival).
+// Shared memory: the walk's per-level columns only.
+#ifndef KGPU_TNN_COOP_MIN_BLOCKS
+#define KGPU_TNN_COOP_MIN_BLOCKS 4
+#endif
+template <typename A, int K, typename M, bool EXCL, int STEMS = 0>
+__global__ void __launch_bounds__(256, KGPU_TNN_COOP_MIN_BLOCKS)
+    k_tnn_coop(TreeView<A> tv0, Batch<A> b, int levels, int k, A radius0,
+               A* __restrict__ out_d, uint32_t* __restrict__ out_i, uint32_t* __restrict__ out_c,
+               unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  const int stride = blockDim.x;
+  const int lane = threadIdx.x & 31;
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  auto wk = WalkOf<A, K, M, STEMS>::make(tsmem, levels, stride);
+  TravStats st;
+  CNearestNRow<A, K, M, EXCL, CartesianDist<A, K, M>> pol(out_d, out_i, k,
+                                                          CartesianDist<A, K, M>());
+  coop_drive<A, K, M>(
+      tv0, b, wk, pol, slot, stride, st,
+      [&](uint64_t qi, const TreeView<A>&) {
+        pol.reset(b.radius(radius0, qi));
+        return true;
+      },
+      [&](int o, uint64_t qo) { pol.finish(o, qo, lane, out_c); });
   if (stats) flush_stats(stats, st);
 }
 

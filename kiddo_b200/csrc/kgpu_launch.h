@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/kiddo_gpu.h"
+
 namespace kgpu {
 
 struct DeviceTree {
@@ -48,7 +50,8 @@ struct QueryLaunch {
   uint32_t* out_i = nullptr;
   uint32_t* out_c = nullptr;
   unsigned long long* stats = nullptr;  // optional [stems, leaves, points] totals
-  int engine = 0;                 // 0 auto, 1 warp per query, 2 thread per query
+  int engine = 0;                 // 0 auto, 1 warp per query, 2 thread per query,
+                                  // 3 thread walks with warp-cooperative leaf scans
   bool periodic = false;          // periodic boundary conditions
   double box[4] = {0, 0, 0, 0};   // periodic box (converted to A)
   // batches over many trees (see kgpu_forest_*): device arrays, or null
@@ -66,6 +69,12 @@ struct QueryLaunch {
 
 // process-wide count of kernel launches made by this library
 extern std::atomic<uint64_t> g_launches;
+
+// QueryLaunch::engine from a query's KGPU_FLAG_ENGINE_* bits.
+inline int engine_of(uint32_t flags) {
+  return (flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (flags & KGPU_FLAG_ENGINE_THREAD) ? 2
+         : (flags & KGPU_FLAG_ENGINE_COOP) ? 3 : 0;
+}
 
 // Fixed-size families: dispatches to the thread engine (2-D/3-D trees) or the
 // warp engine (everything else, periodic included).

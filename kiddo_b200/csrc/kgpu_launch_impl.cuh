@@ -226,6 +226,19 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
               return runt(k_tfixed<A, K, M, KF_APPROX, false, 0>);
             case KGPU_NEAREST_N:
             case KGPU_NEAREST_N_WITHIN:
+              if (q.engine == 3 && q.sorted && q.k <= kMaxK) {
+                // warp-cooperative leaf scans, lists in the output rows
+                const size_t csmem = size_t(levels) * 256 * (STEMS ? 2 * sizeof(A) + 4 : sizeof(A));
+                auto kern = k_tnn_coop<A, K, M, EX, STEMS>;
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(csmem));
+                const int grid = grid_for(kern, csmem, (q.nq + 31) / 32);
+                kern<<<grid, 256, csmem, q.stream>>>(tv, b, levels, q.k, radius,
+                                                     static_cast<A*>(q.out_d), q.out_i, q.out_c,
+                                                     q.stats);
+                g_launches++;
+                return cudaGetLastError();
+              }
               return runt(k_tfixed<A, K, M, KF_NEAREST_N, EX, STEMS>);
             case KGPU_BEST_N_WITHIN:
               return runt(k_tfixed<A, K, M, KF_BEST_N, EX, STEMS>);

@@ -106,7 +106,7 @@ extern "C" int32_t kgpu_query_radius_count_noalloc(kgpu_tree* t, const kgpu_quer
   q.sorted = d->family == KGPU_WITHIN && d->sorted != 0;
   q.nq = nq;
   apply_periodic(dt, d, q);
-  q.engine = (d->flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (d->flags & KGPU_FLAG_ENGINE_THREAD) ? 2 : 0;
+  q.engine = engine_of(d->flags);
   q.queries = queries;
   q.stream = s;
   if (nq) {

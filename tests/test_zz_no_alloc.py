@@ -55,9 +55,9 @@ def _default_pool_usage():
 
 
 def _reset_default_pool_high(pool):
-    from cuda.bindings import runtime as rt
+    from cuda.bindings import driver, runtime as rt
     err, = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
-                                      rt.cuuint64_t(0))
+                                      driver.cuuint64_t(0))
     assert err == rt.cudaError_t.cudaSuccess
 
 
