@@ -210,6 +210,51 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* desc, void* stream, kgpu_tree** o
  * on the host as VecOfArenas tiles and uploaded as kgpu_tree_create does. */
 int32_t kgpu_tree_create_vecofarrays(const kgpu_vecofarrays_desc* desc, void* stream,
                                      kgpu_tree** out);
+/* ---- upload from an rkyv archive -----------------------------------------
+ * Replaces `rkyv::access::<ArchivedKdTree<A, u32, SS, VecOfArenas<..>, K, 32>>`
+ * followed by the per-query `.execute()` on the archived tree
+ * (src/kd_tree/mod.rs:282-372, src/rkyv/adapters.rs:114-237,
+ * src/rkyv/query.rs): the archive's stems and leaf arena are uploaded straight
+ * from `bytes` (for example a read-only mmap of the archive file; registering
+ * that mapping with cudaHostRegister lets the copies run at bus speed), with
+ * no deserialisation.  The archive carries no type information, so `fmt`
+ * names the tree's type parameters and rkyv's format features. */
+typedef struct kgpu_archive_format {
+  uint32_t abi_version;   /* KGPU_ABI_VERSION */
+  int32_t dtype;          /* kgpu_dtype of A */
+  uint32_t dims;          /* K, 1..4 */
+  int32_t stem_strategy;  /* kgpu_stem_strategy of SS */
+  uint32_t block_height;  /* Donnelly BH; 0 for Eytzinger */
+  uint32_t pointer_width; /* bytes of rkyv's archived usize and relative offsets: 2, 4
+                             (rkyv's default, pointer_width_32) or 8 */
+  uint32_t big_endian;    /* 0 (rkyv's default little_endian); big-endian is refused */
+  uint32_t reserved0;
+} kgpu_archive_format;
+
+/* What kgpu_archive_inspect reads off an archive (offsets are byte positions
+ * in the buffer). */
+typedef struct kgpu_archive_info {
+  uint64_t root_offset;
+  uint64_t stems_offset, stem_count;
+  uint64_t extents_offset, leaf_count;
+  uint64_t leaf_bytes_offset, leaf_bytes_len;
+  int32_t resolution;     /* a kgpu_resolution value: Arithmetic, Pristine or Mapped */
+  int32_t max_stem_level;
+  uint64_t stems_depth, resolution_leaf_count; /* Arithmetic / Pristine fields */
+  uint64_t size, leaves_size, max_leaf_len;
+} kgpu_archive_info;
+
+/* Checks an archive's structure (every relative pointer and length inside the
+ * buffer) and reports its fields; touches no device. */
+int32_t kgpu_archive_inspect(const void* bytes, uint64_t len, const kgpu_archive_format* fmt,
+                             kgpu_archive_info* info);
+/* kgpu_tree_create over an archive in place.  Mapped resolution (a mutated
+ * MutableKdTree) returns KGPU_EUNSUPPORTED; Pristine resolves arithmetically.
+ * `bytes` is only read during the call. */
+int32_t kgpu_tree_create_from_archive(const void* bytes, uint64_t len,
+                                      const kgpu_archive_format* fmt, void* stream,
+                                      kgpu_tree** out);
+
 /* Uploads a tree whose leaves use the FlatVec strategy (KdTree<A, u32, SS,
  * FlatVec<A, u32, K, 32>, K, 32>, src/leaf_strategy/flat_vec.rs:20-26): its
  * stems as in kgpu_tree_desc, its K point columns, items and (start, end)

@@ -307,6 +307,66 @@ class GpuTree:
                                                  ctypes.byref(h)))
         return cls(None, _handle=h, dtype=dt, dims=len(cols))
 
+    @staticmethod
+    def _archive_format(dtype, dims, block_height, pointer_width):
+        f = C.ArchiveFormat()
+        f.abi_version = C.ABI_VERSION
+        f.dtype = C.F32 if np.dtype(dtype) == np.float32 else C.F64
+        f.dims = int(dims)
+        f.stem_strategy = C.STEM_DONNELLY if block_height else C.STEM_EYTZINGER
+        f.block_height = int(block_height)
+        f.pointer_width = int(pointer_width)
+        f.big_endian = 0
+        return f
+
+    @staticmethod
+    def _archive_bytes(source):
+        """(buffer, address, length, keepalive) of a path (mapped read-only)
+        or a bytes-like object."""
+        import mmap
+        import os as _os
+        if isinstance(source, (str, _os.PathLike)):
+            with open(source, "rb") as fh:
+                size = _os.fstat(fh.fileno()).st_size
+                if size == 0:
+                    raise ValueError("empty archive file")
+                mm = mmap.mmap(fh.fileno(), 0, access=mmap.ACCESS_READ)
+            arr = np.frombuffer(mm, dtype=np.uint8)
+            return arr, arr.ctypes.data, size, (mm, arr)
+        arr = np.frombuffer(source, dtype=np.uint8)
+        return arr, arr.ctypes.data if arr.size else None, arr.size, (source, arr)
+
+    @classmethod
+    def inspect_archive(cls, source, dtype, dims, block_height=0, pointer_width=4) -> dict:
+        """The fields of an rkyv archive of a KdTree (kgpu_archive_inspect),
+        read in place; no device work."""
+        arr, addr, n, keep = cls._archive_bytes(source)
+        f = cls._archive_format(dtype, dims, block_height, pointer_width)
+        info = C.ArchiveInfo()
+        C.check(C.lib().kgpu_archive_inspect(addr, n, ctypes.byref(f), ctypes.byref(info)))
+        del keep
+        return {name: getattr(info, name) for name, _ in C.ArchiveInfo._fields_}
+
+    @classmethod
+    def from_archive(cls, source, dtype, dims, block_height=0, pointer_width=4,
+                     stream=None) -> "GpuTree":
+        """A tree uploaded straight from an rkyv 0.8 archive of
+        `KdTree<dtype, u32, SS, VecOfArenas<..>, dims, 32>` (what kiddo writes
+        with `rkyv::to_bytes(&tree)` and reads with `rkyv::access`,
+        src/kd_tree/mod.rs:282-372, src/rkyv/adapters.rs:114-237): `source` is
+        a file path, mapped read-only, or a bytes-like object.  The archive
+        has no type information, so the caller names the coordinate dtype,
+        dims, the Donnelly block height (0 for Eytzinger) and rkyv's pointer
+        width in bytes (4 unless the crate was built with rkyv's
+        pointer_width_16 or _64 feature) (kgpu_tree_create_from_archive)."""
+        arr, addr, n, keep = cls._archive_bytes(source)
+        f = cls._archive_format(dtype, dims, block_height, pointer_width)
+        h = ctypes.c_void_p()
+        C.check(C.lib().kgpu_tree_create_from_archive(addr, n, ctypes.byref(f),
+                                                      _stream_ptr(stream), ctypes.byref(h)))
+        del keep
+        return cls(None, _handle=h, dtype=np.dtype(dtype), dims=dims)
+
     @classmethod
     def from_vec_of_arrays(cls, stems, content_points, content_items, sizes, max_stem_level,
                            block_height=0, stream=None) -> "GpuTree":

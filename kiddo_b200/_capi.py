@@ -41,7 +41,8 @@ EXPORTED_SYMBOLS = [
     "kgpu_forest_query_radius_count", "kgpu_forest_query_radius_fill", "kgpu_graph_begin",
     "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy", "kgpu_chamfer_loss",
     "kgpu_chamfer_backward", "kgpu_tree_create_flatvec", "kgpu_tree_create_vecofarrays",
-    "kgpu_scratch_stats", "kgpu_scratch_trim",
+    "kgpu_scratch_stats", "kgpu_scratch_trim", "kgpu_archive_inspect",
+    "kgpu_tree_create_from_archive",
 ]
 
 
@@ -80,6 +81,25 @@ class VecOfArraysDesc(ctypes.Structure):
         ("content_items", ctypes.c_void_p), ("sizes", ctypes.c_void_p),
         ("leaf_count", ctypes.c_uint64),
     ]
+
+
+class ArchiveFormat(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32), ("dtype", ctypes.c_int32), ("dims", ctypes.c_uint32),
+        ("stem_strategy", ctypes.c_int32), ("block_height", ctypes.c_uint32),
+        ("pointer_width", ctypes.c_uint32), ("big_endian", ctypes.c_uint32),
+        ("reserved0", ctypes.c_uint32)]
+
+
+class ArchiveInfo(ctypes.Structure):
+    _fields_ = [
+        ("root_offset", ctypes.c_uint64), ("stems_offset", ctypes.c_uint64),
+        ("stem_count", ctypes.c_uint64), ("extents_offset", ctypes.c_uint64),
+        ("leaf_count", ctypes.c_uint64), ("leaf_bytes_offset", ctypes.c_uint64),
+        ("leaf_bytes_len", ctypes.c_uint64), ("resolution", ctypes.c_int32),
+        ("max_stem_level", ctypes.c_int32), ("stems_depth", ctypes.c_uint64),
+        ("resolution_leaf_count", ctypes.c_uint64), ("size", ctypes.c_uint64),
+        ("leaves_size", ctypes.c_uint64), ("max_leaf_len", ctypes.c_uint64)]
 
 
 class QueryDesc(ctypes.Structure):
@@ -173,6 +193,12 @@ def lib():
     L.kgpu_graph_destroy.argtypes = [vp]
     L.kgpu_chamfer_loss.restype = i32
     L.kgpu_chamfer_loss.argtypes = [vp, vp, u64, u32, ctypes.c_double, vp, vp, vp]
+    L.kgpu_archive_inspect.restype = i32
+    L.kgpu_archive_inspect.argtypes = [vp, u64, ctypes.POINTER(ArchiveFormat),
+                                       ctypes.POINTER(ArchiveInfo)]
+    L.kgpu_tree_create_from_archive.restype = i32
+    L.kgpu_tree_create_from_archive.argtypes = [vp, u64, ctypes.POINTER(ArchiveFormat), vp,
+                                                ctypes.POINTER(vp)]
     L.kgpu_scratch_stats.restype = i32
     L.kgpu_scratch_stats.argtypes = [ctypes.c_int32, vp]
     L.kgpu_scratch_trim.restype = i32

@@ -35,7 +35,7 @@ CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kgpu_forest.cu"
               "kernels_f64_thread.cu",
               "kernels_f64_radius.cu",
               ]
-CXX_SOURCES = ["layout_build.cpp"]
+CXX_SOURCES = ["layout_build.cpp", "archive.cpp"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 
 
