@@ -34,6 +34,8 @@ CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kgpu_forest.cu"
               "kernels_f64_warp.cu",
               "kernels_f64_thread.cu",
               "kernels_f64_radius.cu",
+              "kernels_f32_rows.cu",
+              "kernels_f64_rows.cu",
               ]
 CXX_SOURCES = ["layout_build.cpp", "archive.cpp"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))

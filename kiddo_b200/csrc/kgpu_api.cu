@@ -600,9 +600,6 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
   if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
   if (d->metric < KGPU_SQUARED_EUCLIDEAN || d->metric > KGPU_MINKOWSKI4)
     return set_error(KGPU_EINVAL, "unknown metric");
-  if (d->metric >= KGPU_CHEBYSHEV && d->periodic_box)
-    return set_error(KGPU_EUNSUPPORTED,
-                     "periodic queries take SquaredEuclidean or Manhattan");
   const int f = d->family;
   if (radius_family) {
     if (f != KGPU_WITHIN && f != KGPU_WITHIN_UNSORTED)
@@ -613,14 +610,18 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
       return set_error(KGPU_EINVAL, "family is not a fixed-size family");
     if (f == KGPU_NEAREST_N || f == KGPU_NEAREST_N_WITHIN || f == KGPU_BEST_N_WITHIN) {
       if (d->max_qty == 0) return set_error(KGPU_EINVAL, "max_qty must be >= 1");
-      // k (nearest_n) and n (best_n_within) up to 256; above 32 on the warp
-      // engine, so for Eytzinger trees and Cartesian queries
-      const bool big = !t->dt.bh && !d->periodic_box;
-      if (d->max_qty > uint32_t(big ? kMaxBigK : kMaxK))
+      // The reference's collectors are unbounded (BinaryHeap above its
+      // ThresholdVec range).  2-D and 3-D trees hold lists of any length up
+      // to kMaxRowK in the output rows; the warp engine of 1-D and 4-D trees
+      // keeps them in shared memory, up to kMaxBigK entries, Cartesian only.
+      const bool rows = t->dt.dims == 2 || t->dt.dims == 3;
+      if (d->max_qty > uint32_t(kMaxRowK))
+        return set_error(KGPU_EUNSUPPORTED, "max_qty above 1,048,576 is not supported");
+      if (!rows && d->max_qty > uint32_t(d->periodic_box ? kMaxK : kMaxBigK))
         return set_error(KGPU_EUNSUPPORTED,
-                         big ? "max_qty above 256 is not supported"
-                             : "max_qty above 32 is not supported for Donnelly trees and "
-                               "periodic queries");
+                         d->periodic_box
+                             ? "periodic max_qty above 32 is served for 2-D and 3-D trees"
+                             : "max_qty above 256 is served for 2-D and 3-D trees");
     }
   }
   if (t->dt.bh) {
@@ -648,6 +649,13 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
   return KGPU_OK;
 }
 
+// Whether nearest_n rows come out sorted by distance.  An unsorted request
+// keeps arrival order only where the reference's collector is a ThresholdVec
+// (max_qty <= MAX_UNSORTED_VEC_RESULT_SIZE = 24, nearest_n_within.rs:27); above
+// that it collects into a BinaryHeap, whose into_vec order is unspecified, and
+// the rows come out sorted (as the oracle restates it).
+bool rows_sorted(const kgpu_query_desc* d) { return d->sorted != 0 || d->max_qty > 24; }
+
 // Leaf-grouped processing order: forced on or off by the flags, otherwise on
 // for batches large enough to share leaves (it never changes results).
 bool want_spatial_order(uint32_t flags, uint64_t nq, uint64_t leaves) {
@@ -673,10 +681,16 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   // at k = 33 on C2's data, 42M against 36M at 64); larger k (the warp engine
   // was faster from k = 100), and best_n_within above 32, run on the warp
   // engine's shared-memory lists
+  // Lists beyond those ranges live in the output rows (launch_trow): above
+  // 256 entries, periodic nearest_n above 32, and Donnelly trees above 32.
   const bool nn = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN;
-  const bool big_k = q.k > kMaxK && (q.family == KGPU_BEST_N_WITHIN ||
-                                     (nn && (q.k > kMaxThreadK || q.periodic)));
-  const bool thread = (t.bh || q.engine != 1) && (t.dims == 2 || t.dims == 3) &&
+  const bool best = q.family == KGPU_BEST_N_WITHIN;
+  const bool two_three = t.dims == 2 || t.dims == 3;
+  if ((nn || best) && two_three && q.k > kMaxK &&
+      (q.k > kMaxBigK || (nn && q.periodic) || t.bh))
+    return launch_trow<A>(t, q);
+  const bool big_k = q.k > kMaxK && (best || (nn && (q.k > kMaxThreadK || q.periodic)));
+  const bool thread = (t.bh || q.engine != 1) && two_three &&
                       (!q.periodic || q.family != KGPU_NEAREST_ONE) && !big_k;
   return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);
 }
@@ -838,7 +852,7 @@ int32_t kgpu_query(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, 
   q.k = w;
   q.radius = (d->family == KGPU_NEAREST_N) ? __builtin_inf() : d->radius;
   q.exclusive = d->exclusive != 0;
-  q.sorted = d->sorted != 0;
+  q.sorted = rows_sorted(d);
   q.nq = nq;
   apply_periodic(dt, d, q);
   q.engine = engine_of(d->flags);

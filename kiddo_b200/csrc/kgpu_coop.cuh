@@ -334,6 +334,131 @@ struct CNearestNRow {
 };
 
 // ---------------------------------------------------------------------------
+// Lists of any length, kept in the query's own output row: nearest_n (the k
+// smallest by (distance, arrival), the reference's ThresholdVec or, above its
+// range, BinaryHeap collector with the same distance multiset,
+// results/result_collection.rs:136-215, 365-560) or best_n_within (`BEST`, a
+// run-time choice: the n smallest items by (item, arrival),
+// result_collection.rs:463-560).  A leaf is
+// scanned by the whole warp for its owner; each candidate, in leaf order, finds
+// its place with one ballot per 32 held entries (after the entries whose key is
+// not above its own, which arrived first) and the entries behind it move up
+// one place, 32 at a time from the top; a full list drops its last entry.
+// Output rows are always sorted (by distance, or by item for best_n).
+// ---------------------------------------------------------------------------
+template <typename A, int K, typename M, bool kExclusive, typename Dist>
+struct CRowList {
+  static constexpr bool kPruneOnEqual = kExclusive;
+  bool BEST;  // best_n_within (by item) rather than nearest_n (by distance)
+  A* __restrict__ out_d;
+  uint32_t* __restrict__ out_i;
+  int k;
+  int n;
+  A radius, kth;
+  uint32_t last;  // best_n: the last item once full
+  Dist dist;
+  __device__ CRowList(bool best, A* d, uint32_t* i, int k_, Dist ds)
+      : BEST(best), out_d(d), out_i(i), k(k_), n(0), radius(A(0)), kth(inf_of<A>()), last(0),
+        dist(ds) {}
+  __device__ __forceinline__ void reset(A r) {
+    n = 0;
+    radius = r;
+    kth = inf_of<A>();
+    last = 0;
+  }
+  __device__ __forceinline__ A max_dist() const {
+    if (BEST) return radius;
+    return (n == k && kth < radius) ? kth : radius;
+  }
+  __device__ __forceinline__ bool unbounded_start() const {
+    return !BEST && radius == inf_of<A>();
+  }
+
+  __device__ __forceinline__ void leaf(int o, uint64_t qo, const CoopLeaf<A, K>& L, int lane) {
+    int nn = __shfl_sync(FULL, n, o);
+    A kk = shfl(kth, o);
+    uint32_t lk = shfl(last, o);
+    const A orad = shfl(radius, o);
+    const bool full_at_entry = nn == k;
+    const uint32_t thr_item = lk;
+    // the leaf filter's bound: max_dist() at leaf start
+    const A bound = (!BEST && nn == k && kk < orad) ? kk : orad;
+    A* rd = out_d + qo * uint64_t(k);
+    uint32_t* ri = out_i + qo * uint64_t(k);
+    for (uint32_t c0 = 0; c0 < L.len; c0 += 32) {
+      const uint32_t p = c0 + lane;
+      A d = inf_of<A>();
+      uint32_t it = 0;
+      bool pass = false;
+      if (p < L.len) {
+        d = coop_point<A, K>(L, p, it, dist);
+        pass = kExclusive ? (d < bound) : (d <= bound);
+        if (BEST) pass = pass && !(full_at_entry && it >= thr_item) && (nn < k || it < lk);
+        else pass = pass && (nn < k || d < kk);
+      }
+      unsigned m = __ballot_sync(FULL, pass);
+      while (m) {
+        const int c = __ffs(m) - 1;
+        m &= m - 1;
+        const A dc = shfl(d, c);
+        const uint32_t ic = shfl(it, c);
+        if (nn == k && (BEST ? !(ic < lk) : !(dc < kk))) continue;
+        int pos = 0;  // held entries whose key is not above the candidate's
+        for (int j0 = 0; j0 < nn; j0 += 32) {
+          const int j = j0 + lane;
+          bool le = false;
+          if (j < nn) le = BEST ? !(ri[j] > ic) : !(rd[j] > dc);
+          pos += __popc(__ballot_sync(FULL, le));
+        }
+        const int top = nn < k ? nn - 1 : k - 2;  // entries pos..top move up one
+        for (int j0 = top & ~31; top >= pos && j0 >= (pos & ~31); j0 -= 32) {
+          const int j = j0 + lane;
+          const bool mv = j >= pos && j <= top;
+          A vd = A(0);
+          uint32_t vi = 0;
+          if (mv) {
+            vd = rd[j];
+            vi = ri[j];
+          }
+          __syncwarp();
+          if (mv) {
+            rd[j + 1] = vd;
+            ri[j + 1] = vi;
+          }
+          __syncwarp();
+        }
+        if (lane == 0) {
+          rd[pos] = dc;
+          ri[pos] = ic;
+        }
+        __syncwarp();
+        if (nn < k) ++nn;
+        if (nn == k) {
+          if (BEST) lk = ri[k - 1];
+          else kk = rd[k - 1];
+        }
+      }
+    }
+    if (lane == o) {
+      n = nn;
+      kth = kk;
+      last = lk;
+    }
+  }
+
+  // The held entries are in place; the rest of the row is (+inf, u32::MAX).
+  __device__ __forceinline__ void finish(int o, uint64_t qo, int lane,
+                                         uint32_t* __restrict__ out_c) const {
+    const int on = __shfl_sync(FULL, n, o);
+    for (int j = on + lane; j < k; j += 32) {
+      out_d[qo * uint64_t(k) + j] = inf_of<A>();
+      out_i[qo * uint64_t(k) + j] = 0xffffffffu;
+    }
+    if (lane == 0 && out_c) out_c[qo] = uint32_t(on);
+  }
+};
+
+// ---------------------------------------------------------------------------
 // within: counting pass (no output) or filling pass (hits written in arrival
 // order into the query's CSR segment, `cap` long); a leaf's hits are one
 // coalesced store.

@@ -68,13 +68,18 @@ __device__ __forceinline__ void put(A (&v)[K], int d, A x) {
     if (d == j) v[j] = x;
 }
 
+// Every metric runs periodic queries (periodic.rs is generic over the
+// metric: combine_component over min-image components, and the metric's own
+// rect_dist_after_update over the interval offsets).
 // The additive metrics: combine_component is acc + component, and the
 // rectangle distance after one axis offset changes is the O(1) update of
-// rect() (distance_metric_core.rs:38-44, 86-96).  These also run periodic
-// queries.
+// rect() (distance_metric_core.rs:38-44, 86-96).  kPacked marks the two whose
+// point pairs take the packed f32x2 subtract/multiply path.
 template <typename Self>
 struct Additive {
   static constexpr bool kPeriodic = true;
+  static constexpr bool kAdditive = true;
+  static constexpr bool kPacked = false;
   template <typename A> __device__ __forceinline__ static A combine(A acc, A comp) {
     return add_rn(acc, comp);
   }
@@ -85,6 +90,7 @@ struct Additive {
 };
 
 struct SqEuclidean : Additive<SqEuclidean> {
+  static constexpr bool kPacked = true;
   // dist1(a, b) = (a - b)^2   (dist/squared_euclidean/mod.rs:35-38)
   template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
     const A d = sub_rn(a, b);
@@ -97,6 +103,7 @@ struct SqEuclidean : Additive<SqEuclidean> {
 };
 
 struct Manhattan : Additive<Manhattan> {
+  static constexpr bool kPacked = true;
   // |a - b|   (dist/manhattan/mod.rs:35-38)
   template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
     return abs_val(sub_rn(a, b));
@@ -111,11 +118,10 @@ struct Manhattan : Additive<Manhattan> {
 // without the final root.  Rust's powi is llvm.powi, expanded by binary
 // exponentiation (result times the running square, low bit first), so
 // x^3 = x * (x * x) and x^4 = (x * x) * (x * x), each product rounded.  P = 3
-// and 4; periodic queries take SquaredEuclidean and Manhattan.
+// and 4.
 template <int P>
 struct Minkowski : Additive<Minkowski<P>> {
   static_assert(P == 3 || P == 4, "Minkowski<3> and Minkowski<4>");
-  static constexpr bool kPeriodic = false;
   template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
     const A x = abs_val(sub_rn(a, b));
     const A x2 = mul_rn(x, x);
@@ -130,9 +136,11 @@ struct Minkowski : Additive<Minkowski<P>> {
 // combine_component keeps the larger value (a component that is not greater,
 // NaN included, leaves the accumulator as it is), and the rectangle distance
 // is re-scanned from zero over every axis offset, the changed axis taking its
-// new offset.  Periodic queries take the additive metrics only.
+// new offset.
 struct Chebyshev {
-  static constexpr bool kPeriodic = false;
+  static constexpr bool kPeriodic = true;
+  static constexpr bool kAdditive = false;
+  static constexpr bool kPacked = false;
   template <typename A> __device__ __forceinline__ static A dist1(A a, A b) {
     return abs_val(sub_rn(a, b));
   }
@@ -284,7 +292,7 @@ __device__ __forceinline__ void load_point(const uint8_t* __restrict__ leaf, uin
 // exact and is left out.
 template <typename M, typename A, int K>
 __device__ __forceinline__ A point_dist(const A (&c)[K], const A (&q)[K]) {
-  if constexpr (M::kPeriodic) {
+  if constexpr (M::kAdditive) {
     A acc = M::template dist1<A>(c[0], q[0]);
 #pragma unroll
     for (int d = 1; d < K; ++d) acc = M::combine(acc, M::template dist1<A>(c[d], q[d]));
@@ -350,7 +358,7 @@ struct CartesianDist {
 
 // Minimum-image distance of the periodic leaf scan (periodic.rs:272-284,
 // 357-400): per axis delta = |q - c|, replaced by L - delta when smaller, then
-// acc += dist1(delta, 0).
+// combine_component(acc, dist1(delta, 0)) from zero.
 template <typename A, int K, typename M>
 struct PeriodicDist {
   A box[K];
@@ -361,7 +369,7 @@ struct PeriodicDist {
       const A delta = abs_val(sub_rn(q[d], c[d]));
       const A wrapped = sub_rn(box[d], delta);
       const A m = wrapped < delta ? wrapped : delta;
-      acc = add_rn(acc, M::template dist1<A>(m, A(0)));
+      acc = M::combine(acc, M::template dist1<A>(m, A(0)));
     }
     return acc;
   }
@@ -1088,9 +1096,8 @@ __device__ __forceinline__ void warp_periodic_query(const TreeView<A>& tv, const
       const A far_hi = is_right ? minup : old_hi;
       const A near_off = periodic_interval_distance(qd, near_lo, near_hi, Ld);
       const A far_off = periodic_interval_distance(qd, far_lo, far_hi, Ld);
-      const A oo = sel(off, dim);
-      const A near_rd = M::template rect<A>(rd, oo, near_off);
-      const A far_rd = M::template rect<A>(rd, oo, far_off);
+      const A near_rd = M::template rect_k<A, K>(rd, off, dim, near_off);
+      const A far_rd = M::template rect_k<A, K>(rd, off, dim, far_off);
       const A thr = pol.max_dist();
       const bool near_pruned = near_rd > thr || (P::kPruneOnEqual && near_rd == thr);
       const bool far_pruned = far_rd > thr || (P::kPruneOnEqual && far_rd == thr);
@@ -1165,7 +1172,7 @@ __device__ __forceinline__ void warp_periodic_nearest_one(const TreeView<A>& tv,
       wq[c][a] = w;
       // periodic_image_axis_offset (periodic.rs:29-37)
       const A o = w < A(0) ? abs_val(sub_rn(w, A(0))) : (w > L ? abs_val(sub_rn(w, L)) : A(0));
-      acc = add_rn(acc, M::template dist1<A>(o, A(0)));
+      acc = M::combine(acc, M::template dist1<A>(o, A(0)));
     }
     lb[c] = acc;
     valid[c] = j < NI && nonzero && acc < best;

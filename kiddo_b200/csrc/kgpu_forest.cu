@@ -83,7 +83,7 @@ int forest_launch(kgpu_forest* f, const kgpu_query_desc* d, const void* queries,
                                                                                 : int(d->max_qty);
   q.radius = d->family == KGPU_NEAREST_N ? __builtin_inf() : d->radius;
   q.exclusive = d->exclusive != 0;
-  q.sorted = d->sorted != 0;
+  q.sorted = rows_sorted(d);
   q.nq = nq;
   q.queries = queries;
   q.forest = f->views;

@@ -12,6 +12,7 @@ namespace kgpu {
 constexpr int kMaxDims = 4;
 constexpr int kMaxK = 32;          // largest max_qty served by the register top-k lists
 constexpr int kMaxBigK = 256;      // largest nearest_n k (shared-memory lists, warp engine)
+constexpr int kMaxRowK = 1 << 20;  // largest k with the lists in the output rows
 constexpr int kMaxThreadK = 64;    // largest nearest_n k on the thread engine (128-thread blocks)
 constexpr int kMaxStemLevel = 30;  // 31 levels: one continuation slot per lane, u32 stem index
 

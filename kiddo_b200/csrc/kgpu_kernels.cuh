@@ -574,6 +574,36 @@ __global__ void __launch_bounds__(256, KGPU_TNN_COOP_MIN_BLOCKS)
   if (stats) flush_stats(stats, st);
 }
 
+// nearest_n (sorted rows) and best_n_within with lists of any length held in
+// the output rows (CRowList): per-thread walks over Eytzinger (STEMS == 0) or
+// Donnelly (STEMS == 1) stems with lane refill, each leaf scanned by the whole
+// warp for its owner.  The path for lists beyond the shared-memory kernels'
+// range and for Donnelly trees above 32 entries.  Shared memory: the walk's
+// per-level columns only.
+template <typename A, int K, typename M, bool EXCL, int STEMS = 0>
+__global__ void __launch_bounds__(256) k_trow(TreeView<A> tv0, Batch<A> b, int levels, int k,
+                                              int best_n, A radius0, A* __restrict__ out_d,
+                                              uint32_t* __restrict__ out_i,
+                                              uint32_t* __restrict__ out_c,
+                                              unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  const int stride = blockDim.x;
+  const int lane = threadIdx.x & 31;
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  auto wk = WalkOf<A, K, M, STEMS>::make(tsmem, levels, stride);
+  TravStats st;
+  CRowList<A, K, M, EXCL, CartesianDist<A, K, M>> pol(best_n != 0, out_d, out_i, k,
+                                                      CartesianDist<A, K, M>());
+  coop_drive<A, K, M>(
+      tv0, b, wk, pol, slot, stride, st,
+      [&](uint64_t qi, const TreeView<A>&) {
+        pol.reset(b.radius(radius0, qi));
+        return true;
+      },
+      [&](int o, uint64_t qo) { pol.finish(o, qo, lane, out_c); });
+  if (stats) flush_stats(stats, st);
+}
+
 // Counting pass (offsets == nullptr) or filling pass of the radius families.
 template <typename A, int K, typename M, bool EXCL, int STEMS = 0>
 __global__ void __launch_bounds__(256) k_twithin(TreeView<A> tv0, Batch<A> b, A radius0,
@@ -708,6 +738,33 @@ __global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_nn
 #pragma unroll
   for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
   CNearestNRow<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(out_d, out_i, k, pd);
+  periodic_drive<A, K, M>(
+      tv0, b, box.v, pol, slot, blockDim.x, st,
+      [&](uint64_t qi) {
+        pol.reset(b.radius(radius0, qi));
+        return true;
+      },
+      [&](int o, uint64_t qo) { pol.finish(o, qo, lane, out_c); });
+  if (stats) flush_stats(stats, st);
+}
+
+// Periodic nearest_n lists of any length in the output rows (CRowList with the
+// minimum-image distance); sorted rows, periodic.rs into_sorted_vec.
+template <typename A, int K, typename M, bool EXCL>
+__global__ void __launch_bounds__(256) k_tperiodic_row(TreeView<A> tv0, Batch<A> b,
+                                                       BoxArg<A, K> box, int k, A radius0,
+                                                       A* __restrict__ out_d,
+                                                       uint32_t* __restrict__ out_i,
+                                                       uint32_t* __restrict__ out_c,
+                                                       unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  TravStats st;
+  PeriodicDist<A, K, M> pd;
+#pragma unroll
+  for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
+  CRowList<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(false, out_d, out_i, k, pd);
   periodic_drive<A, K, M>(
       tv0, b, box.v, pol, slot, blockDim.x, st,
       [&](uint64_t qi) {

@@ -81,6 +81,8 @@ inline int engine_of(uint32_t flags) {
 template <typename A> cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q);
+// Lists of any length held in the output rows (kernels_*_rows.cu).
+template <typename A> cudaError_t launch_trow(const DeviceTree& t, const QueryLaunch& q);
 // Donnelly-stem kernels, defined in their own translation units
 // (kernels_f32_donnelly.cu, kernels_f64_donnelly.cu); the last argument only
 // selects the coordinate type.

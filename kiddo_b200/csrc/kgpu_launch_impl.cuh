@@ -256,6 +256,61 @@ cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
   return launch_tfixed_stems<A, 0>(t, q);
 }
 
+// Lists in the output rows (k_trow, k_tperiodic_row): nearest_n and
+// best_n_within of any length on 2-D and 3-D trees, either stem order;
+// periodic nearest_n on Eytzinger trees.
+template <typename A>
+cudaError_t launch_trow(const DeviceTree& t, const QueryLaunch& q) {
+  const TreeView<A> tv = make_view<A>(t);
+  const Batch<A> b = make_batch<A>(q);
+  const A radius = A(q.radius);
+  const int levels = t.max_stem_level + 2;
+  const bool best = q.family == KGPU_BEST_N_WITHIN;
+  return with_dims(t.dims, [&](auto kk) -> cudaError_t {
+    constexpr int K = decltype(kk)::value;
+    if constexpr (!thread_engine_dims(K)) {
+      return cudaErrorInvalidValue;
+    } else {
+      return with_metric(q.metric, [&](auto m) {
+        using M = decltype(m);
+        return with_excl(q.exclusive, [&](auto ex) -> cudaError_t {
+          constexpr bool EX = decltype(ex)::value;
+          if (q.periodic) {
+            if constexpr (M::kPeriodic) {
+              if (best || t.bh) return cudaErrorInvalidValue;
+              const auto box = make_box<A, K>(q);
+              const size_t smem = thread_smem<A>(t);
+              auto kern = k_tperiodic_row<A, K, M, EX>;
+              cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+              const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+              kern<<<grid, 256, smem, q.stream>>>(tv, b, box, q.k, radius,
+                                                  static_cast<A*>(q.out_d), q.out_i, q.out_c,
+                                                  q.stats);
+              g_launches++;
+              return cudaGetLastError();
+            } else {
+              return cudaErrorInvalidValue;
+            }
+          }
+          auto run = [&](auto kern, int stems) {
+            const size_t smem =
+                size_t(levels) * 256 * (stems ? 2 * sizeof(A) + 4 : sizeof(A));
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+            kern<<<grid, 256, smem, q.stream>>>(tv, b, levels, q.k, best ? 1 : 0, radius,
+                                                static_cast<A*>(q.out_d), q.out_i, q.out_c,
+                                                q.stats);
+            g_launches++;
+            return cudaGetLastError();
+          };
+          if (t.bh) return run(k_trow<A, K, M, EX, 1>, 1);
+          return run(k_trow<A, K, M, EX, 0>, 0);
+        });
+      });
+    }
+  });
+}
+
 // Counting (offsets == nullptr, counts set) or filling pass of the radius
 // families.
 template <typename A, int STEMS>
@@ -424,6 +479,11 @@ cudaError_t launch_spatial_order(const DeviceTree& t, const QueryLaunch& q, uint
                                      const uint64_t* offsets, A) {                               \
     return launch_within_pass_stems<A, 1>(t, q, counts, offsets);                                \
   }                                                                                              \
+  }
+
+#define KGPU_INSTANTIATE_ROWS(A)                                                                 \
+  namespace kgpu {                                                                               \
+  template cudaError_t launch_trow<A>(const DeviceTree&, const QueryLaunch&);                    \
   }
 
 #define KGPU_INSTANTIATE_RADIUS(A)                                                               \

@@ -459,9 +459,8 @@ struct PeriodicWalk {
       const A far_hi = is_right ? minup : old_hi;
       const A near_off = periodic_interval_distance(qd, near_lo, near_hi, Ld);
       const A far_off = periodic_interval_distance(qd, far_lo, far_hi, Ld);
-      const A oo = sel(off, dim);
-      const A near_rd = M::template rect<A>(rd, oo, near_off);
-      const A far_rd = M::template rect<A>(rd, oo, far_off);
+      const A near_rd = M::template rect_k<A, K>(rd, off, dim, near_off);
+      const A far_rd = M::template rect_k<A, K>(rd, off, dim, far_off);
       const A thr = pol.max_dist();
       const bool near_pruned = near_rd > thr || (P::kPruneOnEqual && near_rd == thr);
       const bool far_pruned = far_rd > thr || (P::kPruneOnEqual && far_rd == thr);
@@ -502,7 +501,7 @@ struct CartesianQ {
   // Both points of an f32 pair (v[d] = {axis d of point 0, of point 1}):
   // dist1 packed, the sum scalar in the order of point_dist.
   __device__ __forceinline__ void pair(const float2 (&v)[K], float& d0, float& d1) const {
-    if constexpr (!M::kPeriodic) {
+    if constexpr (!M::kPacked) {
       float c0[K], c1[K];
 #pragma unroll
       for (int d = 0; d < K; ++d) {

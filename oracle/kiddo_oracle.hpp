@@ -415,7 +415,7 @@ struct Manhattan : Additive<Manhattan> {
 // rectangle distance is re-scanned from zero over every axis offset, the
 // changed axis taking its new offset.
 struct Chebyshev {
-  static constexpr bool kPeriodic = false;  // periodic queries are restated for + metrics only
+  static constexpr bool kPeriodic = true;
   template <typename A> static A dist1(A a, A b) { return std::fabs(a - b); }
   template <typename A> static A combine(A acc, A component) {
     return component > acc ? component : acc;
@@ -432,8 +432,7 @@ struct Chebyshev {
 // sum of powered differences without the final root.  Rust's powi is LLVM's
 // llvm.powi, which is expanded by binary exponentiation (result times the
 // running square, low bit first): x^3 = x * (x * x), x^4 = (x * x) * (x * x).
-// Restated for P = 3 and 4; periodic queries are restated for the other
-// metrics.
+// Restated for P = 3 and 4.
 template <int P>
 inline double powi_binary(double x) {
   double res = 1.0, cur = x;
@@ -462,7 +461,6 @@ inline float powi_binary(float x) {
 }
 template <int P>
 struct Minkowski : Additive<Minkowski<P>> {
-  static constexpr bool kPeriodic = false;
   template <typename A> static A dist1(A a, A b) { return powi_binary<P>(std::fabs(a - b)); }
   template <typename A> static A rect_after_update(A rd, A old_off, A new_off) {
     return (rd - dist1(old_off, A(0))) + dist1(new_off, A(0));
@@ -896,8 +894,7 @@ void image_candidates_rec(const A* q, const A* box, int axis, A* wrapped, bool n
     A w = shift == -1 ? original - L : (shift == 0 ? original : original + L);
     wrapped[axis] = w;
     A offset = image_axis_offset(w, L);
-    A next = lb;
-    next += M::template dist1<A>(offset, A(0));
+    A next = M::combine(lb, M::template dist1<A>(offset, A(0)));
     if (!(next < limit)) continue;  // boundary_accepts(Exclusive, next, limit)
     image_candidates_rec<A, K, M>(q, box, axis + 1, wrapped, nonzero || shift != 0, next, limit,
                                   out);
@@ -1003,8 +1000,8 @@ void periodic_query(const Tree<A, K>& t, const A* q, const A* box, Ctx& ctx, Lea
       else { near_lo = old_lower; near_hi = minup; far_lo = maxlo; far_hi = old_upper; }
       const A near_off = periodic_interval_distance_1d(q[dim], near_lo, near_hi, box[dim]);
       const A far_off = periodic_interval_distance_1d(q[dim], far_lo, far_hi, box[dim]);
-      const A near_rd = M::rect_after_update(rd, off[dim], near_off);
-      const A far_rd = M::rect_after_update(rd, off[dim], far_off);
+      const A near_rd = M::template rect_k<A, K>(rd, off, dim, near_off);
+      const A far_rd = M::template rect_k<A, K>(rd, off, dim, far_off);
       const A thr = ctx.max_dist();
       const bool poe = ctx.prune_on_equal();
       const bool near_pruned = near_rd > thr || (poe && near_rd == thr);
@@ -1030,13 +1027,14 @@ void periodic_query(const Tree<A, K>& t, const A* q, const A* box, Ctx& ctx, Lea
   }
 }
 
-// periodic leaf distance (process_periodic_leaf_arena, periodic.rs:357-400)
+// periodic leaf distance (process_periodic_leaf_arena, periodic.rs:357-400):
+// combine_component over the min-image components, from zero
 template <typename A, int K, typename M>
 inline A periodic_point_dist(const A* c, const A* q, const A* box) {
   A acc = A(0);
   for (int d = 0; d < K; ++d) {
     A delta = min_image_delta(q[d], c[d], box[d]);
-    acc += M::template dist1<A>(delta, A(0));
+    acc = M::combine(acc, M::template dist1<A>(delta, A(0)));
   }
   return acc;
 }

@@ -340,7 +340,7 @@ void kor_copy_layout(void* hp, void* stems_out, uint8_t* bytes_out, uint64_t* ex
 }
 
 // metric: 0 SquaredEuclidean, 1 Manhattan, 2 Chebyshev, 3 / 4 Minkowski<3> /
-// Minkowski<4> (the last three not periodic: -2 / nullptr).  Outputs are dense [nq * k]
+// Minkowski<4>; every metric also periodic (Eytzinger trees).  Outputs are dense [nq * k]
 // (k = 1 for the nearest-one families); unused slots hold +inf / 0xFFFFFFFF.
 // radii: one radius per query in the tree's dtype, or nullptr for `radius` on every query.
 int kor_query_fixed_r(void* hp, int family, int metric, const void* queries, uint64_t nq,
@@ -364,7 +364,6 @@ int kor_query_fixed_r(void* hp, int family, int metric, const void* queries, uin
     if (metric == 0) return run(SqEuclidean());
 #ifndef KOR_TIMING_BUILD
     if (metric == 1) return run(Manhattan());
-    if (periodic) return -2;
     if (metric == 2) return run(Chebyshev());
     if (metric == 3) return run(Minkowski<3>());
     if (metric == 4) return run(Minkowski<4>());
@@ -400,7 +399,6 @@ void* kor_query_radius_r(void* hp, int family, int metric, const void* queries, 
     if (metric == 0) return run(SqEuclidean());
 #ifndef KOR_TIMING_BUILD
     if (metric == 1) return run(Manhattan());
-    if (periodic) return nullptr;
     if (metric == 2) return run(Chebyshev());
     if (metric == 3) return run(Minkowski<3>());
     if (metric == 4) return run(Minkowski<4>());

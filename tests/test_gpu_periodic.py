@@ -22,7 +22,8 @@ def _data(dtype, dims, rng, n):
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("dims", [2, 3])
-@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan"])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev", "minkowski3",
+                                    "minkowski4"])
 def test_periodic_families(dtype, dims, metric):
     rng = np.random.default_rng(dims * 10 + (metric == "manhattan"))
     P = _data(dtype, dims, rng, 20000)
@@ -31,11 +32,14 @@ def test_periodic_families(dtype, dims, metric):
     box = np.ones(dims, dtype=dtype)
     t = kb.ImmutableKdTree.new_from_slice(P)
     o = oracle.OracleTree.build(P)
-    M = kb.SquaredEuclidean if metric == "sqeuclidean" else kb.Manhattan
+    M = {"sqeuclidean": kb.SquaredEuclidean, "manhattan": kb.Manhattan,
+         "chebyshev": kb.Chebyshev, "minkowski3": kb.Minkowski(3),
+         "minkowski4": kb.Minkowski(4)}[metric]
     g = t.query(Q).periodic_boundary_condition(box).nearest_one(M).execute_gpu()
     od, oi = o.periodic_nearest_one(Q, box, metric=metric)
     assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "pnn1")
-    r = 1e-4 if metric == "sqeuclidean" else 0.02
+    r = {"sqeuclidean": 1e-4, "manhattan": 0.02, "chebyshev": 0.008, "minkowski3": 1e-6,
+         "minkowski4": 1e-8}[metric]
     for k in (1, 8, 32):
         for radius in (None, r):
             for excl in ((False, True) if radius else (False,)):
@@ -95,15 +99,3 @@ def test_periodic_rejections():
     q = np.zeros((1, 3))
     with pytest.raises(TypeError):
         t.query(q).periodic_boundary_condition(np.ones(3)).nearest_one(kb.SquaredEuclidean).approx()
-
-
-def test_periodic_rejects_chebyshev():
-    """Periodic queries take the additive metrics (SquaredEuclidean,
-    Manhattan); a Chebyshev periodic query is refused with a status."""
-    rng = np.random.default_rng(3)
-    t = kb.ImmutableKdTree.new_from_slice(rng.random((2000, 3)))
-    Q = rng.random((10, 3))
-    with pytest.raises(kb.KiddoGpuError):
-        t.query(Q).periodic_boundary_condition(np.ones(3)).nearest_one(kb.Chebyshev).execute_gpu()
-    with pytest.raises(kb.KiddoGpuError):
-        t.query(Q).periodic_boundary_condition(np.ones(3)).within(kb.Chebyshev, 0.01).execute_gpu()

@@ -250,3 +250,48 @@ def test_timing_build_matches_the_checker():
                      (a.within(Q, 1e-3), b.within(Q, 1e-3))):
             for u, v in zip(x, y):
                 assert np.array_equal(u, v)
+
+
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev", "minkowski3",
+                                    "minkowski4"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_periodic_families_match_min_image_brute_force(metric, dtype):
+    """periodic.rs is generic over the metric: the plural families scan leaves
+    with combine_component over min-image components (periodic.rs:272-284,
+    357-400), so their results equal a brute-force min-image scan; nearest_one
+    (home query plus shifted images, :156-214) agrees up to the rounding of
+    the shifted query."""
+    rng = np.random.default_rng(len(metric) + (dtype == np.float64))
+    P = rng.random((3000, 3)).astype(dtype)
+    Q = np.concatenate([rng.random((150, 3)), rng.random((40, 3)) * 0.01,
+                        1 - rng.random((40, 3)) * 0.01]).astype(dtype)
+    box = np.ones(3, dtype)
+    o = oracle.OracleTree.build(P)
+
+    def min_image(q):
+        acc = np.zeros(len(P), dtype)
+        for d in range(3):
+            delta = np.abs((q[d] - P[:, d]).astype(dtype))
+            w = (box[d] - delta).astype(dtype)
+            m = np.where(w < delta, w, delta)
+            if metric == "chebyshev":
+                acc = np.where(m > acc, m, acc).astype(dtype)
+            elif metric == "sqeuclidean":
+                acc = (acc + m * m).astype(dtype)
+            elif metric == "manhattan":
+                acc = (acc + m).astype(dtype)
+            else:
+                x2 = (m * m).astype(dtype)
+                acc = (acc + ((m * x2) if metric == "minkowski3" else (x2 * x2))).astype(dtype)
+        return acc
+
+    d, i, c = o.periodic_nearest_n(Q, box, 10, metric=metric)
+    nd, ni = o.periodic_nearest_one(Q, box, metric=metric)
+    r = {"chebyshev": 0.05, "minkowski3": 1e-4, "minkowski4": 1e-5, "sqeuclidean": 2e-3,
+         "manhattan": 0.08}[metric]
+    off, wd, wi = o.periodic_within(Q, box, r, metric=metric)
+    for j, q in enumerate(Q):
+        bd = min_image(q)
+        assert np.array_equal(np.sort(bd)[:10], d[j])
+        assert abs(float(nd[j]) - float(bd.min())) <= 1e-5 * float(bd.min()) + 1e-7
+        assert set(wi[off[j]:off[j + 1]].tolist()) == set(np.nonzero(bd <= r)[0].tolist())
