@@ -154,8 +154,10 @@ typedef struct kgpu_query_desc {
   uint32_t abi_version;   /* KGPU_ABI_VERSION */
   int32_t family;         /* kgpu_family */
   int32_t metric;         /* kgpu_metric */
-  uint32_t max_qty;       /* k for nearest_n*, n for best_n_within: 1..256 (above 32
-                             only for Eytzinger trees and Cartesian queries) */
+  uint32_t max_qty;       /* k for nearest_n*, n for best_n_within: 1..1,048,576 on 2-D
+                             and 3-D trees (lists above 256, Donnelly lists above 32 and
+                             periodic lists above 32 in the output rows); 1..256 on 1-D
+                             and 4-D trees (periodic: 1..32) */
   double radius;          /* metric units (squared distance for SquaredEuclidean); cast to A */
   int32_t exclusive;      /* .exclusive_boundaries(): strict `< radius` */
   int32_t sorted;         /* 1 = default sorted output, 0 = .unsorted() */
@@ -365,8 +367,8 @@ int32_t kgpu_query_stats(kgpu_tree* tree, const kgpu_query_desc* desc, const voi
                          uint64_t nq, uint64_t* stats, void* stream);
 
 /* ---- batches over many trees --------------------------------------------
- * A forest groups uploaded trees of one dtype and dimensionality (the trees
- * must outlive it).  Forest queries take device pointers only: queries
+ * A forest groups uploaded trees of one dtype, dimensionality and stem order
+ * (Eytzinger, or Donnelly of one block height; the trees must outlive it).  Forest queries take device pointers only: queries
  * [nq, dims], tree_of[nq] (index into the forest; a query naming no tree gets
  * empty results) and optionally radii[nq] (one radius per query, type A;
  * NULL = desc->radius).  One persistent launch answers the whole batch, its

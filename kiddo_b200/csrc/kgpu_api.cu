@@ -631,8 +631,6 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
       return set_error(KGPU_EUNSUPPORTED, "Donnelly trees are served for 2-D and 3-D points");
     if (d->flags & KGPU_FLAG_ENGINE_WARP)
       return set_error(KGPU_EUNSUPPORTED, "Donnelly trees run on the thread engine");
-    if (d->periodic_box)
-      return set_error(KGPU_EUNSUPPORTED, "periodic queries need an Eytzinger tree");
   }
   if (d->periodic_box) {
     // builder.rs: periodic queries support nearest_one, nearest_n(.within) and
@@ -691,7 +689,7 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
     return launch_trow<A>(t, q);
   const bool big_k = q.k > kMaxK && (best || (nn && (q.k > kMaxThreadK || q.periodic)));
   const bool thread = (t.bh || q.engine != 1) && two_three &&
-                      (!q.periodic || q.family != KGPU_NEAREST_ONE) && !big_k;
+                      (!q.periodic || q.family != KGPU_NEAREST_ONE || t.bh) && !big_k;
   return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);
 }
 template cudaError_t launch_fixed<float>(const DeviceTree&, const QueryLaunch&);

@@ -59,7 +59,7 @@ void fill_views(const std::vector<kgpu_tree*>& trees, std::vector<uint8_t>& out)
     v.leaf_count = t.leaf_count;
     v.size = t.size;
     v.stem_count = t.stem_count;
-    v.bh = 0;
+    v.bh = t.bh;
     std::memcpy(out.data() + i * sizeof(TreeView<A>), &v, sizeof(v));
   }
 }
@@ -135,8 +135,10 @@ int32_t kgpu_forest_create(kgpu_tree* const* trees, uint32_t n_trees, void* stre
     if (!t) return set_error(KGPU_EINVAL, "NULL tree in the forest");
     if (t->dt.dtype != ts[0]->dt.dtype || t->dt.dims != ts[0]->dt.dims)
       return set_error(KGPU_EINVAL, "forest trees must share dtype and dims");
-    if (t->dt.bh)
-      return set_error(KGPU_EUNSUPPORTED, "forests hold Eytzinger trees (ImmutableKdTree)");
+    // one stem order per forest: the kernels walk Eytzinger stems, or
+    // Donnelly stems of one block height
+    if (t->dt.bh != ts[0]->dt.bh)
+      return set_error(KGPU_EINVAL, "forest trees must share the stem order (and block height)");
     if (t->dt.device != cur) return set_error(KGPU_EINVAL, "forest trees must be on the current device");
   }
   auto* f = new (std::nothrow) kgpu_forest();
@@ -147,6 +149,7 @@ int32_t kgpu_forest_create(kgpu_tree* const* trees, uint32_t n_trees, void* stre
   f->meta.device = cur;
   f->meta.max_stem_level = -1;
   f->meta.size = 1;
+  f->meta.bh = ts[0]->dt.bh;
   std::vector<uint64_t> base(n_trees);
   uint64_t total = 0;
   for (uint32_t i = 0; i < n_trees; ++i) {

@@ -661,13 +661,23 @@ struct BoxArg {
 // Periodic families, one query per thread: PeriodicWalk with lane refill,
 // leaves scanned warp-cooperatively.  Each iteration: finish the lanes whose
 // walks ended, refill, take every active walk to its next leaf, scan those.
-template <typename A, int K, typename M, typename Pol, typename Start, typename Finish>
+// Shared memory: the rd slot column ((max_stem_level + 2) * blockDim values
+// of A); Donnelly stems (STEMS == 1) add one u32 column of path stem indices
+// after it (periodic_smem).
+template <typename A, int K, typename M, int STEMS, typename Pol, typename Start,
+          typename Finish>
 __device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Batch<A>& b,
                                                const A (&box)[K], Pol& pol, A* __restrict__ slot,
                                                int stride, TravStats& st, Start&& start,
                                                Finish&& finish) {
   const int lane = threadIdx.x & 31;
-  PeriodicWalk<A, K, M> wk;
+  uint32_t* path = nullptr;
+  if constexpr (STEMS) {
+    extern __shared__ __align__(16) unsigned char psmem[];
+    path = reinterpret_cast<uint32_t*>(psmem + size_t(tv0.max_stem_level + 2) * stride *
+                                                   sizeof(A)) + threadIdx.x;
+  }
+  PeriodicWalk<A, K, M, STEMS> wk(path, stride);
   wk.init(box);
   LaneFeeder fd;
   fd.start();
@@ -700,7 +710,7 @@ __device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Bat
     uint32_t len = 0;
     if (active) {
       const uint32_t leaf = wk.next(tv, q, box, pol, slot, stride, st);
-      if (leaf == PeriodicWalk<A, K, M>::kDone) {
+      if (leaf == PeriodicWalk<A, K, M, STEMS>::kDone) {
         done = true;
         active = false;
       } else {
@@ -723,7 +733,7 @@ __device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Bat
 #ifndef KGPU_TPERIODIC_MIN_BLOCKS
 #define KGPU_TPERIODIC_MIN_BLOCKS 3
 #endif
-template <typename A, int K, typename M, bool EXCL>
+template <typename A, int K, typename M, bool EXCL, int STEMS = 0>
 __global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_nn(TreeView<A> tv0, Batch<A> b,
                                                       BoxArg<A, K> box, int k, A radius0,
                                                       A* __restrict__ out_d,
@@ -738,7 +748,7 @@ __global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_nn
 #pragma unroll
   for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
   CNearestNRow<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(out_d, out_i, k, pd);
-  periodic_drive<A, K, M>(
+  periodic_drive<A, K, M, STEMS>(
       tv0, b, box.v, pol, slot, blockDim.x, st,
       [&](uint64_t qi) {
         pol.reset(b.radius(radius0, qi));
@@ -748,9 +758,106 @@ __global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_nn
   if (stats) flush_stats(stats, st);
 }
 
+// Periodic nearest_one with per-thread walks (periodic.rs:156-214): the home
+// query, then each shifted image whose lower bound beats the home result, in
+// stable lower-bound order, skipping those that no longer beat the best so
+// far.  Image j of the 3^K shifts has shift digit (j / 3^(K-1-a)) % 3 - 1 on
+// axis a, the generation order of periodic_image_candidates (:45-142).  The
+// path for Donnelly stems (the warp engine's home and image queries walk
+// Eytzinger stems).  Shared memory: the walk's per-level columns.
+template <typename A, int K, typename M, int STEMS>
+__global__ void __launch_bounds__(256) k_tperiodic_nn1(TreeView<A> tv0, Batch<A> b,
+                                                       BoxArg<A, K> box, int levels,
+                                                       A* __restrict__ out_d,
+                                                       uint32_t* __restrict__ out_i,
+                                                       uint32_t* __restrict__ out_c,
+                                                       unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char tsmem[];
+  const int stride = blockDim.x;
+  A* slot = reinterpret_cast<A*>(tsmem) + threadIdx.x;
+  auto wk = WalkOf<A, K, M, STEMS>::make(tsmem, levels, stride);
+  TravStats st;
+  for_each_query_thread(b, [&](uint64_t qi) {
+    const TreeView<A> tv = b.tree(tv0, qi);
+    A q[K];
+    b.query(qi, q);
+    // one full nearest_one traversal (the reference's scalar/arithmetic walk)
+    auto nearest = [&](const A (&qq)[K], A& best, uint32_t& item) {
+      TNearestOne<A, K, M> pol;
+      if (tv.size != 0) {
+        wk.init();
+        uint32_t leaf = wk.descend(tv, qq, pol, !pol.unbounded_start(), slot, stride, st);
+        st.points += pol.leaf(tv, leaf, qq);
+        ++st.leaves;
+        while (wk.backtrack(tv, qq, pol, slot, stride)) {
+          leaf = wk.descend(tv, qq, pol, true, slot, stride, st);
+          st.points += pol.leaf(tv, leaf, qq);
+          ++st.leaves;
+        }
+      }
+      best = pol.best;
+      item = pol.item;
+    };
+    A best;
+    uint32_t item;
+    nearest(q, best, item);
+    constexpr int NI = pow3(K);
+    A lb[NI];
+    uint32_t valid = 0;  // bit j: image j is a candidate (nonzero shift, lb < home best)
+#pragma unroll
+    for (int j = 0; j < NI; ++j) {
+      bool nonzero = false;
+      A acc = A(0);
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        int div = 1;
+        for (int c = a + 1; c < K; ++c) div *= 3;
+        const int digit = (j / div) % 3;
+        const A L = box.v[a];
+        const A w = digit == 0 ? sub_rn(q[a], L) : (digit == 1 ? q[a] : add_rn(q[a], L));
+        nonzero |= digit != 1;
+        // periodic_image_axis_offset (periodic.rs:29-37)
+        const A o = w < A(0) ? abs_val(sub_rn(w, A(0))) : (w > L ? abs_val(sub_rn(w, L)) : A(0));
+        acc = M::combine(acc, M::template dist1<A>(o, A(0)));
+      }
+      lb[j] = acc;
+      if (nonzero && acc < best) valid |= 1u << j;
+    }
+    while (valid) {
+      // the next candidate in stable lower-bound order
+      int pick = -1;
+      for (int j = 0; j < NI; ++j)
+        if ((valid >> j) & 1u)
+          if (pick < 0 || lb[j] < lb[pick]) pick = j;
+      valid &= ~(1u << pick);
+      if (!(lb[pick] < best)) continue;
+      A img[K];
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        int div = 1;
+        for (int c = a + 1; c < K; ++c) div *= 3;
+        const int digit = (pick / div) % 3;
+        const A L = box.v[a];
+        img[a] = digit == 0 ? sub_rn(q[a], L) : (digit == 1 ? q[a] : add_rn(q[a], L));
+      }
+      A d;
+      uint32_t it;
+      nearest(img, d, it);
+      if (d < best) {
+        best = d;
+        item = it;
+      }
+    }
+    out_d[qi] = best;
+    out_i[qi] = item;
+    if (out_c) out_c[qi] = 1;
+  });
+  if (stats) flush_stats(stats, st);
+}
+
 // Periodic nearest_n lists of any length in the output rows (CRowList with the
 // minimum-image distance); sorted rows, periodic.rs into_sorted_vec.
-template <typename A, int K, typename M, bool EXCL>
+template <typename A, int K, typename M, bool EXCL, int STEMS = 0>
 __global__ void __launch_bounds__(256) k_tperiodic_row(TreeView<A> tv0, Batch<A> b,
                                                        BoxArg<A, K> box, int k, A radius0,
                                                        A* __restrict__ out_d,
@@ -765,7 +872,7 @@ __global__ void __launch_bounds__(256) k_tperiodic_row(TreeView<A> tv0, Batch<A>
 #pragma unroll
   for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
   CRowList<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(false, out_d, out_i, k, pd);
-  periodic_drive<A, K, M>(
+  periodic_drive<A, K, M, STEMS>(
       tv0, b, box.v, pol, slot, blockDim.x, st,
       [&](uint64_t qi) {
         pol.reset(b.radius(radius0, qi));
@@ -776,7 +883,7 @@ __global__ void __launch_bounds__(256) k_tperiodic_row(TreeView<A> tv0, Batch<A>
 }
 
 // Periodic within: counting pass (offsets == nullptr) or filling pass.
-template <typename A, int K, typename M, bool EXCL>
+template <typename A, int K, typename M, bool EXCL, int STEMS = 0>
 __global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_within(
     TreeView<A> tv0, Batch<A> b, BoxArg<A, K> box, A radius0, uint64_t* __restrict__ counts,
     const uint64_t* __restrict__ offsets, uint64_t capacity, A* __restrict__ out_d,
@@ -791,7 +898,7 @@ __global__ void __launch_bounds__(256, KGPU_TPERIODIC_MIN_BLOCKS) k_tperiodic_wi
   for (int d = 0; d < K; ++d) pd.box[d] = box.v[d];
   CWithin<A, K, M, EXCL, PeriodicDist<A, K, M>> pol(pd);
   uint64_t o = 0;  // this lane's segment start (filling pass)
-  periodic_drive<A, K, M>(
+  periodic_drive<A, K, M, STEMS>(
       tv0, b, box.v, pol, slot, blockDim.x, st,
       [&](uint64_t qi) {
         pol.radius = b.radius(radius0, qi);

@@ -90,6 +90,13 @@ inline size_t thread_smem(const DeviceTree& t) {
   return size_t(t.max_stem_level + 2) * 256 * sizeof(A);
 }
 
+// Dynamic shared memory of the periodic per-thread walks: the rd slots, plus
+// for Donnelly stems a column of path stem indices.
+template <typename A>
+inline size_t periodic_smem(const DeviceTree& t, int stems) {
+  return thread_smem<A>(t) + (stems ? size_t(t.max_stem_level + 2) * 256 * sizeof(uint32_t) : 0);
+}
+
 // 2-D and 3-D trees have thread-per-query kernels; other dimensionalities use
 // the warp kernels (same results).
 constexpr bool thread_engine_dims(int K) { return K == 2 || K == 3; }
@@ -196,12 +203,29 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
         return with_excl(q.exclusive, [&](auto ex) {
           constexpr bool EX = decltype(ex)::value;
           if (!M::kPeriodic && q.periodic) return cudaErrorInvalidValue;
-          if constexpr (M::kPeriodic) if (STEMS == 0 && q.periodic) {
+          if constexpr (M::kPeriodic) if (q.periodic) {
+            const auto box = make_box<A, K>(q);
+            if constexpr (STEMS == 1) {
+              if (q.family == KGPU_NEAREST_ONE) {
+                // home query plus images, per-thread walks over Donnelly stems
+                const size_t nsmem = size_t(levels) * 256 * (2 * sizeof(A) + 4);
+                auto kern = k_tperiodic_nn1<A, K, M, STEMS>;
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(nsmem));
+                const int grid = grid_for(kern, nsmem, (q.nq + 31) / 32);
+                kern<<<grid, 256, nsmem, q.stream>>>(tv, b, box, levels,
+                                                     static_cast<A*>(q.out_d), q.out_i, q.out_c,
+                                                     q.stats);
+                g_launches++;
+                return cudaGetLastError();
+              }
+            }
+            if (q.family != KGPU_NEAREST_N && q.family != KGPU_NEAREST_N_WITHIN)
+              return cudaErrorInvalidValue;
             // periodic nearest_n: per-thread walk, cooperative leaf scans,
             // lists in the output rows
-            const auto box = make_box<A, K>(q);
-            const size_t psmem = thread_smem<A>(t);
-            auto kern = k_tperiodic_nn<A, K, M, EX>;
+            const size_t psmem = periodic_smem<A>(t, STEMS);
+            auto kern = k_tperiodic_nn<A, K, M, EX, STEMS>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(psmem));
             const int grid = grid_for(kern, psmem, (q.nq + 31) / 32);
             kern<<<grid, 256, psmem, q.stream>>>(tv, b, box, q.k, radius,
@@ -277,17 +301,22 @@ cudaError_t launch_trow(const DeviceTree& t, const QueryLaunch& q) {
           constexpr bool EX = decltype(ex)::value;
           if (q.periodic) {
             if constexpr (M::kPeriodic) {
-              if (best || t.bh) return cudaErrorInvalidValue;
+              if (best) return cudaErrorInvalidValue;
               const auto box = make_box<A, K>(q);
-              const size_t smem = thread_smem<A>(t);
-              auto kern = k_tperiodic_row<A, K, M, EX>;
-              cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-              const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
-              kern<<<grid, 256, smem, q.stream>>>(tv, b, box, q.k, radius,
-                                                  static_cast<A*>(q.out_d), q.out_i, q.out_c,
-                                                  q.stats);
-              g_launches++;
-              return cudaGetLastError();
+              const int stems = t.bh ? 1 : 0;
+              const size_t smem = periodic_smem<A>(t, stems);
+              auto launch = [&](auto kern) {
+                cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(smem));
+                const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
+                kern<<<grid, 256, smem, q.stream>>>(tv, b, box, q.k, radius,
+                                                    static_cast<A*>(q.out_d), q.out_i, q.out_c,
+                                                    q.stats);
+                g_launches++;
+                return cudaGetLastError();
+              };
+              return stems ? launch(k_tperiodic_row<A, K, M, EX, 1>)
+                           : launch(k_tperiodic_row<A, K, M, EX, 0>);
             } else {
               return cudaErrorInvalidValue;
             }
@@ -327,10 +356,10 @@ cudaError_t launch_within_pass_stems(const DeviceTree& t, const QueryLaunch& q, 
         constexpr bool EX = decltype(ex)::value;
         if (!M::kPeriodic && q.periodic) return cudaErrorInvalidValue;
         if constexpr (thread_engine_dims(K) && M::kPeriodic) {
-          if (q.periodic && q.engine != 1) {
+          if (q.periodic && (q.engine != 1 || STEMS)) {
             const auto box = make_box<A, K>(q);
-            const size_t smem = thread_smem<A>(t);
-            auto kern = k_tperiodic_within<A, K, M, EX>;
+            const size_t smem = periodic_smem<A>(t, STEMS);
+            auto kern = k_tperiodic_within<A, K, M, EX, STEMS>;
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             const int grid = grid_for(kern, smem, (q.nq + 31) / 32);
             kern<<<grid, 256, smem, q.stream>>>(tv, b, box, radius, counts, offsets, q.capacity,

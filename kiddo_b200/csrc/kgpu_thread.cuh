@@ -351,15 +351,24 @@ struct DonnellyWalk {
 //    ancestor step split axis d (bit L of `split`), else 0.
 // Both are exactly what the reference's step computed from the same inputs,
 // so the rebuilt state equals the frame it replaces.
-template <typename A, int K, typename M>
+// STEMS == 0: Eytzinger stems, where an ancestor's index is the current
+// index shifted right.  STEMS == 1: Donnelly<bh> stems, where the walk keeps
+// the stem index of each level of its path in a column (path[L * stride])
+// and the leaf index in `leaf`, one path bit per level; the traversal is the
+// same (periodic.rs drives both stem orders through the StemStrategy trait).
+template <typename A, int K, typename M, int STEMS = 0>
 struct PeriodicWalk {
   static constexpr uint32_t kDone = 0xffffffffu;
   A lo[K], hi[K], off[K];
   A rd;
-  uint32_t stem_idx;
+  uint32_t stem_idx, leaf;
   int level;
   uint32_t frames, split, lo_set, hi_set;
   bool at_leaf;
+  uint32_t* __restrict__ path;  // Donnelly: this thread's column of path stem indices
+  int pstride;
+
+  __device__ explicit PeriodicWalk(uint32_t* p = nullptr, int ps = 0) : path(p), pstride(ps) {}
 
   __device__ __forceinline__ static uint32_t axis_levels(int d) {
     uint32_t m = 0;
@@ -375,10 +384,18 @@ struct PeriodicWalk {
       off[d] = A(0);
     }
     rd = A(0);
-    stem_idx = 1;
+    stem_idx = STEMS ? 0u : 1u;
+    leaf = 0;
     level = 0;
     frames = split = lo_set = hi_set = 0;
     at_leaf = false;
+  }
+
+  // Stem index of the path's node at level L <= P, where `parent` is the
+  // node at level P.
+  __device__ __forceinline__ uint32_t ancestor(uint32_t parent, int P, int L) const {
+    if constexpr (STEMS) return path[L * pstride];
+    else return parent >> (P - L);
   }
 
   // Pops the deepest pending frame (the reference's stack.pop()); false when
@@ -389,14 +406,14 @@ struct PeriodicWalk {
     const int FL = 31 - __clz(frames);
     frames &= ~(1u << FL);
     const int P = FL - 1;
-    const uint32_t parent = stem_idx >> (level - P);
+    const uint32_t parent = STEMS ? path[P * pstride] : stem_idx >> (level - P);
     const uint32_t below = (1u << P) - 1u;
 #pragma unroll
     for (int d = 0; d < K; ++d) {
       const uint32_t am = axis_levels(d) & below;
       const uint32_t ml = lo_set & am, mh = hi_set & am;
-      lo[d] = ml ? __ldg(tv.stems + (parent >> (P - (31 - __clz(ml))))) : A(0);
-      hi[d] = mh ? __ldg(tv.stems + (parent >> (P - (31 - __clz(mh))))) : box[d];
+      lo[d] = ml ? __ldg(tv.stems + ancestor(parent, P, 31 - __clz(ml))) : A(0);
+      hi[d] = mh ? __ldg(tv.stems + ancestor(parent, P, 31 - __clz(mh))) : box[d];
       off[d] = (split & am) ? periodic_interval_distance(q[d], lo[d], hi[d], box[d]) : A(0);
     }
     const int dP = P % K;
@@ -418,7 +435,14 @@ struct PeriodicWalk {
     split |= 1u << P;
     if (!is_right && pivot > old_lo) lo_set |= 1u << P;   // far = right child: lower = maxlo
     if (is_right && !(old_hi < pivot)) hi_set |= 1u << P;  // far = left child: upper = minup
-    stem_idx = parent * 2u + (is_right ? 0u : 1u);
+    if constexpr (STEMS) {
+      uint32_t l, r;
+      donnelly_children(parent, uint32_t(P) % tv.bh, tv.bh, l, r);
+      stem_idx = is_right ? l : r;
+      leaf = ((leaf >> (level - P)) << 1) | (is_right ? 0u : 1u);
+    } else {
+      stem_idx = parent * 2u + (is_right ? 0u : 1u);
+    }
     level = FL;
     return true;
   }
@@ -438,12 +462,20 @@ struct PeriodicWalk {
     for (;;) {
       if (level > msl) {
         at_leaf = true;
-        return stem_idx & ~(1u << level);
+        return STEMS ? leaf : (stem_idx & ~(1u << level));
       }
       ++st.stems;
       const A pivot = stem_idx < tv.stem_count ? __ldg(tv.stems + stem_idx) : INF;
+      if constexpr (STEMS) path[level * pstride] = stem_idx;
       if (!(pivot < INF)) {
-        stem_idx *= 2u;
+        if constexpr (STEMS) {
+          uint32_t l, r;
+          donnelly_children(stem_idx, uint32_t(level) % tv.bh, tv.bh, l, r);
+          stem_idx = l;
+          leaf <<= 1;
+        } else {
+          stem_idx *= 2u;
+        }
         ++level;
         dim = dim + 1 == K ? 0 : dim + 1;
         continue;
@@ -481,7 +513,14 @@ struct PeriodicWalk {
       put(hi, dim, near_hi);
       put(off, dim, near_off);
       rd = near_rd;
-      stem_idx = stem_idx * 2u + (is_right ? 1u : 0u);
+      if constexpr (STEMS) {
+        uint32_t l, r;
+        donnelly_children(stem_idx, uint32_t(level) % tv.bh, tv.bh, l, r);
+        stem_idx = is_right ? r : l;
+        leaf = (leaf << 1) | (is_right ? 1u : 0u);
+      } else {
+        stem_idx = stem_idx * 2u + (is_right ? 1u : 0u);
+      }
       ++level;
       dim = dim + 1 == K ? 0 : dim + 1;
     }

@@ -148,6 +148,19 @@ struct EytzingerCursor {
     r.level = level;
     return r;
   }
+  // the arithmetic leaf index: stem_idx without its leading bit
+  size_t leaf_idx() const { return size_t(stem_idx & ~(uint32_t(1) << level)); }
+  void traverse(bool is_right) {
+    stem_idx = stem_idx * 2 + (is_right ? 1u : 0u);
+    ++level;
+  }
+  // self -> near child, returns the far one (traits/stem_strategy.rs:110-118)
+  EytzingerCursor branch_relative(bool is_right) {
+    EytzingerCursor far = *this;
+    far.traverse(!is_right);
+    traverse(is_right);
+    return far;
+  }
 };
 
 // DonnellyCore<BH> (stem_strategy/donnelly/core.rs:35-154, 254-290, 400-428):
@@ -954,16 +967,23 @@ inline A min_image_delta(A q, A c, A L) {
   return wrapped < delta ? wrapped : delta;
 }
 
+template <int K>
+inline size_t cursor_leaf(const EytzingerCursor<K>& c) { return c.leaf_idx(); }
+template <int K>
+inline size_t cursor_leaf(const DonnellyCursor<K>& c) { return size_t(c.leaf_idx); }
+
 // periodic_backtracking_query (periodic.rs:455-619) driving a collector
-// through `max_dist()`, `prune_on_equal()` and `leaf(leaf_idx)`.
-template <typename A, int K, typename M, typename Ctx, typename Leaf>
-void periodic_query(const Tree<A, K>& t, const A* q, const A* box, Ctx& ctx, Leaf&& leaf_fn,
-                    Stats* st) {
+// through `max_dist()`, `prune_on_equal()` and `leaf(leaf_idx)`, over the
+// stem order of cursor C (EytzingerCursor or DonnellyCursor: periodic.rs
+// drives both through the StemStrategy trait).  A far child is pushed unless pruned when it is
+// generated; popped frames are not tested again.
+template <typename A, int K, typename M, typename C, typename Ctx, typename Leaf>
+void periodic_query_c(const Tree<A, K>& t, C root, const A* q, const A* box, Ctx& ctx,
+                      Leaf&& leaf_fn, Stats* st) {
   if (t.size == 0) return;
-  struct Frame { uint32_t stem_idx; int level; A lower[K]; A upper[K]; A off[K]; A rd; };
+  struct Frame { C s; A lower[K]; A upper[K]; A off[K]; A rd; };
   std::vector<Frame> stack;
-  uint32_t stem_idx = 1;
-  int level = 0;
+  C s = root;
   A lower[K], upper[K], off[K];
   for (int d = 0; d < K; ++d) { lower[d] = A(0); upper[d] = box[d]; off[d] = A(0); }
   A rd = A(0);
@@ -972,27 +992,26 @@ void periodic_query(const Tree<A, K>& t, const A* q, const A* box, Ctx& ctx, Lea
     if (stack.empty()) return false;
     Frame f = stack.back();
     stack.pop_back();
-    stem_idx = f.stem_idx; level = f.level; rd = f.rd;
+    s = f.s; rd = f.rd;
     for (int d = 0; d < K; ++d) { lower[d] = f.lower[d]; upper[d] = f.upper[d]; off[d] = f.off[d]; }
     return true;
   };
   for (;;) {
     bool finished = false;
     for (;;) {
-      if (level > t.max_stem_level) {
-        size_t leaf = size_t(stem_idx & ~(uint32_t(1) << level));
+      if (s.level > t.max_stem_level) {
+        const size_t leaf = cursor_leaf(s);
         if (st) { st->leaf_visits++; st->points_scanned += t.leaf_len(leaf); }
         leaf_fn(leaf);
         break;
       }
       if (st) st->stem_visits++;
-      const int dim = level % K;
-      const A pivot = stem_idx < t.stems.size() ? t.stems[stem_idx] : INF;
-      if (pivot >= INF) { stem_idx = stem_idx * 2; ++level; continue; }
+      const int dim = s.dim();
+      const A pivot = s.stem_idx < t.stems.size() ? t.stems[s.stem_idx] : INF;
+      if (pivot >= INF) { s.traverse(false); continue; }
       const A old_lower = lower[dim], old_upper = upper[dim];
       const bool is_right = q[dim] >= pivot;
-      const uint32_t near_idx = stem_idx * 2 + (is_right ? 1u : 0u);
-      const uint32_t far_idx = stem_idx * 2 + (is_right ? 0u : 1u);
+      C far = s.branch_relative(is_right);
       const A minup = old_upper < pivot ? old_upper : pivot;
       const A maxlo = std::max(old_lower, pivot);
       A near_lo, near_hi, far_lo, far_hi;
@@ -1008,7 +1027,7 @@ void periodic_query(const Tree<A, K>& t, const A* q, const A* box, Ctx& ctx, Lea
       const bool far_pruned = far_rd > thr || (poe && far_rd == thr);
       if (!far_pruned) {
         Frame f;
-        f.stem_idx = far_idx; f.level = level + 1; f.rd = far_rd;
+        f.s = far; f.rd = far_rd;
         for (int d = 0; d < K; ++d) { f.lower[d] = lower[d]; f.upper[d] = upper[d]; f.off[d] = off[d]; }
         f.lower[dim] = far_lo; f.upper[dim] = far_hi; f.off[dim] = far_off;
         stack.push_back(f);
@@ -1019,11 +1038,22 @@ void periodic_query(const Tree<A, K>& t, const A* q, const A* box, Ctx& ctx, Lea
         break;
       }
       lower[dim] = near_lo; upper[dim] = near_hi; off[dim] = near_off; rd = near_rd;
-      stem_idx = near_idx;
-      ++level;
     }
     if (finished) return;
     if (!pop()) return;
+  }
+}
+
+// periodic_query over the tree's own stem order.
+template <typename A, int K, typename M, typename Ctx, typename Leaf>
+void periodic_query(const Tree<A, K>& t, const A* q, const A* box, Ctx& ctx, Leaf&& leaf_fn,
+                    Stats* st) {
+  if (t.stem_strategy == 1) {
+    DonnellyCursor<K> root;
+    root.bh = t.bh;
+    periodic_query_c<A, K, M>(t, root, q, box, ctx, leaf_fn, st);
+  } else {
+    periodic_query_c<A, K, M>(t, EytzingerCursor<K>(), q, box, ctx, leaf_fn, st);
   }
 }
 

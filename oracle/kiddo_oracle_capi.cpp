@@ -340,7 +340,7 @@ void kor_copy_layout(void* hp, void* stems_out, uint8_t* bytes_out, uint64_t* ex
 }
 
 // metric: 0 SquaredEuclidean, 1 Manhattan, 2 Chebyshev, 3 / 4 Minkowski<3> /
-// Minkowski<4>; every metric also periodic (Eytzinger trees).  Outputs are dense [nq * k]
+// Minkowski<4>; every metric and stem order also periodic.  Outputs are dense [nq * k]
 // (k = 1 for the nearest-one families); unused slots hold +inf / 0xFFFFFFFF.
 // radii: one radius per query in the tree's dtype, or nullptr for `radius` on every query.
 int kor_query_fixed_r(void* hp, int family, int metric, const void* queries, uint64_t nq,
@@ -352,9 +352,6 @@ int kor_query_fixed_r(void* hp, int family, int metric, const void* queries, uin
     using A = decltype(a);
     constexpr int K = decltype(kk)::value;
     auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
-    const bool periodic = family == FAM_PERIODIC_NEAREST_ONE || family == FAM_PERIODIC_NEAREST_N;
-    if (t.stem_strategy == 1 && periodic)
-      return -2;  // the periodic restatement follows the Eytzinger traversal only
     auto run = [&](auto m) -> int {
       return query_fixed_t<A, K, decltype(m)>(
           t, family, static_cast<const A*>(queries), nq, k, A(radius),
@@ -388,8 +385,6 @@ void* kor_query_radius_r(void* hp, int family, int metric, const void* queries, 
     using A = decltype(a);
     constexpr int K = decltype(kk)::value;
     auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
-    const bool periodic = family == FAM_PERIODIC_WITHIN;
-    if (t.stem_strategy == 1 && periodic) return nullptr;
     auto run = [&](auto m) -> void* {
       return query_radius_t<A, K, decltype(m)>(
           t, family, static_cast<const A*>(queries), nq, A(radius),

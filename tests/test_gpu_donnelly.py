@@ -160,11 +160,90 @@ def test_donnelly_explicit_items_and_rejections():
     Q = rng.random((500, 3)).astype(np.float32)
     g = t.query(Q).best_n_within(kb.SquaredEuclidean, 0.01, 4).execute_gpu()
     assert_same_fixed(g.distances, g.items, g.counts, *o.best_n_within(Q, 0.01, 4), "best_n")
-    # periodic queries and the warp engine need Eytzinger stems
-    with pytest.raises(Exception):
-        t.query(Q).periodic_boundary_condition(np.ones(3)).nearest_one(
-            kb.SquaredEuclidean).execute_gpu()
+    # the warp engine walks Eytzinger stems only; a forest takes one stem order
     with pytest.raises(Exception):
         t.query(Q).with_engine("warp").nearest_one(kb.SquaredEuclidean).execute_gpu()
     with pytest.raises(Exception):
-        kb.Forest([t])
+        kb.Forest([t, kb.ImmutableKdTree.new_from_slice(P)])
+    with pytest.raises(Exception):
+        kb.Forest([t, kb.ImmutableKdTree.new_from_slice(P, block_height=3)])
+
+
+@pytest.mark.parametrize("bh", [3, 4])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("dims", [2, 3])
+@pytest.mark.parametrize("metric", ["sqeuclidean", "manhattan", "chebyshev", "minkowski4"])
+def test_periodic_families_donnelly(bh, dtype, dims, metric):
+    """periodic_backtracking_query over Donnelly stems (periodic.rs:455-619 is
+    generic over the stem strategy) and periodic nearest_one as home plus
+    image queries over the scalar backtracking (periodic.rs:156-214)."""
+    rng = np.random.default_rng(zlib.crc32(f"pdon{bh}{dims}{metric}".encode()))
+    c = rng.random((32, dims))
+    P = np.concatenate([(c[rng.integers(0, 32, 8000)] + rng.normal(0, 0.01, (8000, dims))) % 1.0,
+                        rng.random((8000, dims))]).astype(dtype)
+    Q = np.concatenate([rng.random((800, dims)), rng.random((200, dims)) * 0.01,
+                        1 - rng.random((200, dims)) * 0.01, P[:100]]).astype(dtype)
+    box = np.ones(dims, dtype=dtype)
+    t, o = _pair(P, bh)
+    M = _metric(metric)
+    g = t.query(Q).periodic_boundary_condition(box).nearest_one(M).execute_gpu()
+    od, oi = o.periodic_nearest_one(Q, box, metric=metric)
+    assert_same_fixed(g.distances, g.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "pnn1")
+    r = {"sqeuclidean": 2e-4, "manhattan": 0.03, "chebyshev": 0.01, "minkowski4": 1e-8}[metric]
+    for k in (1, 8, 32, 70):
+        for radius in (None, r):
+            b = t.query(Q).periodic_boundary_condition(box).nearest_n(M, k)
+            if radius is not None:
+                b = b.within(radius)
+            g = b.execute_gpu()
+            ref = o.periodic_nearest_n(Q, box, k, radius=np.inf if radius is None else radius,
+                                       metric=metric)
+            assert_same_fixed(g.distances, g.items, g.counts, *ref, f"pnn{k} r={radius}")
+    for sorted_ in (True, False):
+        b = t.query(Q).periodic_boundary_condition(box).within(M, r)
+        if not sorted_:
+            b = b.unsorted()
+        g = b.execute_gpu()
+        ref = o.periodic_within(Q, box, r, metric=metric, sorted=sorted_)
+        assert_same_csr((g.offsets, g.distances, g.items), ref, f"pwithin sorted={sorted_}")
+
+
+@pytest.mark.parametrize("bh", [3, 4])
+def test_donnelly_forest_matches_the_oracle(bh):
+    """Many Donnelly trees of one block height in one launch: every family,
+    one radius per query for the radius families, each row against the
+    oracle tree it names."""
+    import torch
+    rng = np.random.default_rng(40 + bh)
+    sizes = [20, 700, 5000, 30000]
+    pts = [rng.random((n, 3)).astype(np.float32) for n in sizes]
+    trees = [kb.ImmutableKdTree.new_from_slice(p, block_height=bh) for p in pts]
+    oracles = [oracle.OracleTree.build(p, block_height=bh) for p in pts]
+    forest = kb.Forest(trees)
+    nq = 6000
+    tree_of = rng.integers(0, len(pts), nq).astype(np.int32)
+    Q = rng.random((nq, 3)).astype(np.float32)
+    radii = (np.exp(rng.uniform(np.log(1e-4), np.log(1e-2), nq))).astype(np.float32)
+    dq, dt, dr = (torch.from_numpy(x).cuda() for x in (Q, tree_of, radii))
+    g1 = forest.query(dq, dt).nearest_one(kb.SquaredEuclidean).execute_gpu()
+    g16 = forest.query(dq, dt).nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
+    gb = forest.query(dq, dt, dr).best_n_within(kb.SquaredEuclidean, 0.0, 5).execute_gpu()
+    gw = forest.query(dq, dt, dr).within(kb.SquaredEuclidean, 0.0).execute_gpu()
+    off = gw.offsets.cpu().numpy()
+    wd, wi = gw.distances.cpu().numpy(), gw.items.cpu().numpy().view(np.uint32)
+    for t in range(len(pts)):
+        sel = np.nonzero(tree_of == t)[0]
+        od, oi = oracles[t].nearest_one(Q[sel])
+        assert_same_fixed(g1.distances.cpu().numpy()[sel], g1.items.cpu().numpy()[sel],
+                          np.ones(len(sel)), od, oi, np.ones(len(sel)), f"nn1 tree {t}")
+        assert_same_fixed(g16.distances.cpu().numpy()[sel], g16.items.cpu().numpy()[sel],
+                          g16.counts.cpu().numpy()[sel], *oracles[t].nearest_n(Q[sel], 16),
+                          f"knn tree {t}")
+        assert_same_fixed(gb.distances.cpu().numpy()[sel], gb.items.cpu().numpy()[sel],
+                          gb.counts.cpu().numpy()[sel],
+                          *oracles[t].best_n_within(Q[sel], radii[sel], 5), f"best tree {t}")
+        oo, od, oi = oracles[t].within(Q[sel], radii[sel])
+        got_d = np.concatenate([wd[off[j]:off[j + 1]] for j in sel])
+        got_i = np.concatenate([wi[off[j]:off[j + 1]] for j in sel])
+        assert np.array_equal(np.diff(off)[sel], np.diff(oo).astype(np.int64))
+        assert np.array_equal(got_d, od) and np.array_equal(got_i, oi), f"within tree {t}"
