@@ -212,6 +212,31 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* desc, void* stream, kgpu_tree** o
  * on the host as VecOfArenas tiles and uploaded as kgpu_tree_create does. */
 int32_t kgpu_tree_create_vecofarrays(const kgpu_vecofarrays_desc* desc, void* stream,
                                      kgpu_tree** out);
+/* ---- Mapped stem/leaf resolution (MutableKdTree) -------------------------
+ * OwnedStemLeafResolution::Mapped (src/kd_tree/stem_leaf_resolution.rs:53-66,
+ * 77-120): a terminal stem maps straight to a leaf, so leaves may sit at any
+ * depth.  kiddo's MutableKdTree (KdTree<A, u32, Eytzinger, VecOfArrays<..>>,
+ * src/lib.rs:274-275) uses it from bulk construction on (hard buckets,
+ * construction.rs:413-539, 695-864, 972-1009) and keeps it through leaf
+ * splits (:19-130).  Queries walk such trees with the reference's scalar
+ * backtracking (orchestrator/mod.rs:214-345, 607-669), either stem order;
+ * 2-D and 3-D trees.  The map is checked at upload: every walk from the root
+ * must end at a mapped terminal stem. */
+typedef struct kgpu_leaf_map {
+  const uint64_t* leaf_idx_map; /* `len` entries: leaf index of stem min_stem_leaf_idx + i,
+                                   or UINT64_MAX for None (not terminal) */
+  uint64_t len;
+  uint64_t min_stem_leaf_idx;
+} kgpu_leaf_map;
+/* kgpu_tree_create for desc->resolution == KGPU_RES_MAPPED. */
+int32_t kgpu_tree_create_mapped(const kgpu_tree_desc* desc, const kgpu_leaf_map* map,
+                                void* stream, kgpu_tree** out);
+/* kgpu_tree_create_vecofarrays with a Mapped resolution: a MutableKdTree's
+ * own leaves and map. */
+int32_t kgpu_tree_create_vecofarrays_mapped(const kgpu_vecofarrays_desc* desc,
+                                            const kgpu_leaf_map* map, void* stream,
+                                            kgpu_tree** out);
+
 /* ---- upload from an rkyv archive -----------------------------------------
  * Replaces `rkyv::access::<ArchivedKdTree<A, u32, SS, VecOfArenas<..>, K, 32>>`
  * followed by the per-query `.execute()` on the archived tree
@@ -244,14 +269,16 @@ typedef struct kgpu_archive_info {
   int32_t max_stem_level;
   uint64_t stems_depth, resolution_leaf_count; /* Arithmetic / Pristine fields */
   uint64_t size, leaves_size, max_leaf_len;
+  uint64_t map_offset, map_len, min_stem_leaf_idx; /* Mapped fields (leaf_idx_map) */
 } kgpu_archive_info;
 
 /* Checks an archive's structure (every relative pointer and length inside the
  * buffer) and reports its fields; touches no device. */
 int32_t kgpu_archive_inspect(const void* bytes, uint64_t len, const kgpu_archive_format* fmt,
                              kgpu_archive_info* info);
-/* kgpu_tree_create over an archive in place.  Mapped resolution (a mutated
- * MutableKdTree) returns KGPU_EUNSUPPORTED; Pristine resolves arithmetically.
+/* kgpu_tree_create over an archive in place (kgpu_tree_create_mapped for a
+ * Mapped resolution, whose leaf_idx_map entries equal to the all-ones usize
+ * are None, src/rkyv/adapters.rs:168-237); Pristine resolves arithmetically.
  * `bytes` is only read during the call. */
 int32_t kgpu_tree_create_from_archive(const void* bytes, uint64_t len,
                                       const kgpu_archive_format* fmt, void* stream,

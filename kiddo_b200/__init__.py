@@ -367,14 +367,45 @@ class GpuTree:
         del keep
         return cls(None, _handle=h, dtype=np.dtype(dtype), dims=dims)
 
+    @staticmethod
+    def _leaf_map(leaf_idx_map, min_stem_leaf_idx):
+        m = np.ascontiguousarray(leaf_idx_map, dtype=np.uint64).reshape(-1)
+        lm = C.LeafMap()
+        lm.leaf_idx_map = m.ctypes.data if m.size else None
+        lm.len = m.size
+        lm.min_stem_leaf_idx = int(min_stem_leaf_idx)
+        return lm, m
+
+    @classmethod
+    def from_mapped_layout(cls, dtype, dims, stems, leaf_bytes, extents, max_stem_level, size,
+                           max_leaf_len, leaf_idx_map, min_stem_leaf_idx=0, block_height=0,
+                           stream=None) -> "GpuTree":
+        """A tree with Mapped stem/leaf resolution (OwnedStemLeafResolution::
+        Mapped, src/kd_tree/stem_leaf_resolution.rs:53-66), as a MutableKdTree
+        holds it: the layout arrays of ``ImmutableKdTree.from_layout`` plus the
+        leaf index of each terminal stem (``leaf_idx_map[i]`` for stem
+        ``min_stem_leaf_idx + i``, 2^64 - 1 for None) (kgpu_tree_create_mapped)."""
+        host = ImmutableKdTree.from_layout(dtype, dims, stems, leaf_bytes, extents,
+                                           max_stem_level, size, max_leaf_len, block_height)
+        host._desc.resolution = C.RES_MAPPED
+        lm, keep = cls._leaf_map(leaf_idx_map, min_stem_leaf_idx)
+        h = ctypes.c_void_p()
+        C.check(C.lib().kgpu_tree_create_mapped(ctypes.byref(host._desc), ctypes.byref(lm),
+                                                _stream_ptr(stream), ctypes.byref(h)))
+        del keep
+        return cls(None, _handle=h, dtype=np.dtype(dtype), dims=dims)
+
     @classmethod
     def from_vec_of_arrays(cls, stems, content_points, content_items, sizes, max_stem_level,
-                           block_height=0, stream=None) -> "GpuTree":
+                           block_height=0, stream=None, leaf_idx_map=None,
+                           min_stem_leaf_idx=0) -> "GpuTree":
         """A tree whose leaves use the VecOfArrays strategy
         (src/leaf_strategy/vec_of_arrays.rs:51-97): `stems` in the stem order of
         the strategy, each leaf's `content_points` ([leaf_count, K, B]) and
         `content_items` ([leaf_count, B], uint32) and its live-entry count in
-        `sizes` ([leaf_count]) (kgpu_tree_create_vecofarrays)."""
+        `sizes` ([leaf_count]) (kgpu_tree_create_vecofarrays); with
+        `leaf_idx_map`, a MutableKdTree's Mapped resolution
+        (kgpu_tree_create_vecofarrays_mapped)."""
         pts = np.ascontiguousarray(content_points)
         if pts.dtype not in (np.float32, np.float64) or pts.ndim != 3:
             raise TypeError("content_points must be a float32 or float64 [leaf_count, K, B] array")
@@ -397,8 +428,17 @@ class GpuTree:
         d.sizes = sz.ctypes.data if sz.size else None
         d.leaf_count = L_
         h = ctypes.c_void_p()
-        C.check(C.lib().kgpu_tree_create_vecofarrays(ctypes.byref(d), _stream_ptr(stream),
-                                                     ctypes.byref(h)))
+        if leaf_idx_map is None:
+            C.check(C.lib().kgpu_tree_create_vecofarrays(ctypes.byref(d), _stream_ptr(stream),
+                                                         ctypes.byref(h)))
+        else:
+            # a MutableKdTree's own leaves and Mapped resolution
+            lm, keep = cls._leaf_map(leaf_idx_map, min_stem_leaf_idx)
+            C.check(C.lib().kgpu_tree_create_vecofarrays_mapped(ctypes.byref(d),
+                                                                ctypes.byref(lm),
+                                                                _stream_ptr(stream),
+                                                                ctypes.byref(h)))
+            del keep
         return cls(None, _handle=h, dtype=pts.dtype, dims=K)
 
     @classmethod

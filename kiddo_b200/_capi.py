@@ -42,7 +42,8 @@ EXPORTED_SYMBOLS = [
     "kgpu_graph_end", "kgpu_graph_launch", "kgpu_graph_destroy", "kgpu_chamfer_loss",
     "kgpu_chamfer_backward", "kgpu_tree_create_flatvec", "kgpu_tree_create_vecofarrays",
     "kgpu_scratch_stats", "kgpu_scratch_trim", "kgpu_archive_inspect",
-    "kgpu_tree_create_from_archive",
+    "kgpu_tree_create_from_archive", "kgpu_tree_create_mapped",
+    "kgpu_tree_create_vecofarrays_mapped",
 ]
 
 
@@ -83,6 +84,11 @@ class VecOfArraysDesc(ctypes.Structure):
     ]
 
 
+class LeafMap(ctypes.Structure):
+    _fields_ = [("leaf_idx_map", ctypes.c_void_p), ("len", ctypes.c_uint64),
+                ("min_stem_leaf_idx", ctypes.c_uint64)]
+
+
 class ArchiveFormat(ctypes.Structure):
     _fields_ = [
         ("abi_version", ctypes.c_uint32), ("dtype", ctypes.c_int32), ("dims", ctypes.c_uint32),
@@ -99,7 +105,9 @@ class ArchiveInfo(ctypes.Structure):
         ("leaf_bytes_len", ctypes.c_uint64), ("resolution", ctypes.c_int32),
         ("max_stem_level", ctypes.c_int32), ("stems_depth", ctypes.c_uint64),
         ("resolution_leaf_count", ctypes.c_uint64), ("size", ctypes.c_uint64),
-        ("leaves_size", ctypes.c_uint64), ("max_leaf_len", ctypes.c_uint64)]
+        ("leaves_size", ctypes.c_uint64), ("max_leaf_len", ctypes.c_uint64),
+        ("map_offset", ctypes.c_uint64), ("map_len", ctypes.c_uint64),
+        ("min_stem_leaf_idx", ctypes.c_uint64)]
 
 
 class QueryDesc(ctypes.Structure):
@@ -193,6 +201,13 @@ def lib():
     L.kgpu_graph_destroy.argtypes = [vp]
     L.kgpu_chamfer_loss.restype = i32
     L.kgpu_chamfer_loss.argtypes = [vp, vp, u64, u32, ctypes.c_double, vp, vp, vp]
+    L.kgpu_tree_create_mapped.restype = i32
+    L.kgpu_tree_create_mapped.argtypes = [ctypes.POINTER(TreeDesc), ctypes.POINTER(LeafMap), vp,
+                                          ctypes.POINTER(vp)]
+    L.kgpu_tree_create_vecofarrays_mapped.restype = i32
+    L.kgpu_tree_create_vecofarrays_mapped.argtypes = [ctypes.POINTER(VecOfArraysDesc),
+                                                      ctypes.POINTER(LeafMap), vp,
+                                                      ctypes.POINTER(vp)]
     L.kgpu_archive_inspect.restype = i32
     L.kgpu_archive_inspect.argtypes = [vp, u64, ctypes.POINTER(ArchiveFormat),
                                        ctypes.POINTER(ArchiveInfo)]

@@ -15,7 +15,10 @@
 //     leaf_bytes            ArchivedBox<AlignedArchiveSlice<[u8]>> rel. offset, len
 //     size                  usize
 //   stem_leaf_resolution  enum, u8 tag (0 Arithmetic, 1 Pristine, 2 Mapped),
-//                         then the variant's fields (stem_leaf_resolution.rs:28-68)
+//                         then the variant's fields (stem_leaf_resolution.rs:28-68):
+//                         Arithmetic / Pristine { stems_depth, leaf_count },
+//                         Mapped { min_stem_leaf_idx, leaf_idx_map: vec of usize,
+//                         all-ones = None (rkyv/adapters.rs:168-237) }
 //   size                  usize
 //   max_stem_level        i32
 //   max_leaf_len          usize
@@ -170,6 +173,15 @@ int32_t kgpu_archive_inspect(const void* bytes, uint64_t len, const kgpu_archive
   if (tag < 2) {
     info->stems_depth = r.u(root + L.resolution + r.w, r.w);
     info->resolution_leaf_count = r.u(root + L.resolution + 2 * r.w, r.w);
+  } else {
+    // Mapped { min_stem_leaf_idx: usize, leaf_idx_map: Vec<usize with the
+    // all-ones sentinel for None> }
+    info->min_stem_leaf_idx = r.u(root + L.resolution + r.w, r.w);
+    if ((st = rel_slice(r, root + L.resolution + 2 * r.w, r.w, r.w, "leaf_idx_map", &pos, &n)) !=
+        KGPU_OK)
+      return st;
+    info->map_offset = pos;
+    info->map_len = n;
   }
   info->size = r.u(root + L.size, r.w);
   info->leaves_size = r.u(root + L.leaves_size, r.w);
@@ -191,10 +203,21 @@ int32_t kgpu_tree_create_from_archive(const void* bytes, uint64_t len,
   kgpu_archive_info info;
   int st = kgpu_archive_inspect(bytes, len, fmt, &info);
   if (st != KGPU_OK) return st;
-  if (info.resolution == KGPU_RES_MAPPED)
-    return set_error(KGPU_EUNSUPPORTED,
-                     "archive holds a Mapped stem/leaf resolution (a mutated MutableKdTree)");
   const Reader r{static_cast<const uint8_t*>(bytes), len, fmt->pointer_width};
+  const bool mapped = info.resolution == KGPU_RES_MAPPED;
+  std::vector<uint64_t> map;
+  if (mapped) {
+    try {
+      map.resize(info.map_len);
+    } catch (const std::bad_alloc&) {
+      return set_error(KGPU_ENOMEM, "host allocation failed");
+    }
+    const uint64_t none = r.w == 8 ? ~uint64_t(0) : (uint64_t(1) << (8 * r.w)) - 1;
+    for (uint64_t i = 0; i < info.map_len; ++i) {
+      const uint64_t v = r.u(info.map_offset + i * r.w, r.w);
+      map[i] = v == none ? ~uint64_t(0) : v;
+    }
+  }
   std::vector<uint64_t> ex;
   try {
     ex.resize(2 * info.leaf_count);
@@ -214,7 +237,7 @@ int32_t kgpu_tree_create_from_archive(const void* bytes, uint64_t len,
   d.bucket_size = 32;
   d.stem_strategy = fmt->stem_strategy;
   d.block_height = fmt->block_height;
-  d.resolution = KGPU_RES_ARITHMETIC;  // Pristine resolves arithmetically too
+  d.resolution = mapped ? KGPU_RES_MAPPED : KGPU_RES_ARITHMETIC;  // Pristine: arithmetic
   const uint8_t* base = static_cast<const uint8_t*>(bytes);
   d.stems = info.stem_count ? base + info.stems_offset : nullptr;
   d.stem_count = info.stem_count;
@@ -226,7 +249,13 @@ int32_t kgpu_tree_create_from_archive(const void* bytes, uint64_t len,
   d.size = info.size;
   d.max_leaf_len = info.max_leaf_len;
   // kgpu_tree_create checks the layout itself (extents inside the arena,
-  // leaf count against the stem depth, sizes) before it touches the device
+  // leaf count against the stem depth or every walk against the leaf map,
+  // sizes) before it touches the device
+  if (mapped) {
+    const kgpu_leaf_map lm{map.empty() ? nullptr : map.data(), map.size(),
+                           info.min_stem_leaf_idx};
+    return kgpu_tree_create_mapped(&d, &lm, stream, out);
+  }
   return kgpu_tree_create(&d, stream, out);
 }
 

@@ -148,6 +148,8 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t s) {
 }
 
 void release_tree_arrays(DeviceTree& dt) {
+  cudaFree(dt.leaf_map);
+  dt.leaf_map = nullptr;
   cudaFree(dt.iter_points);
   cudaFree(dt.sorted_items);
   cudaFree(dt.sorted_ranks);
@@ -316,7 +318,45 @@ int32_t kgpu_layout_free(kgpu_layout* lay) {
 }
 
 // ---- device trees -----------------------------------------------------------
-int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out) {
+}  // extern "C"
+
+namespace kgpu {
+namespace {
+
+// The stem index of a child in the tree's stem order (host side).
+uint32_t host_child(uint32_t bh, uint32_t stem, int level, bool right) {
+  if (!bh) return stem * 2u + (right ? 1u : 0u);
+  const uint32_t minor = uint32_t(level) % bh;
+  const uint32_t mask = (1u << bh) - 1u, min_idx = stem & mask, base = (stem & ~mask) + 1u;
+  const uint32_t l = minor + 1u == bh ? (base + ((min_idx - minor - 1u) << 1)) << bh
+                                      : base + (min_idx << 1);
+  return right ? (minor + 1u == bh ? l + (1u << bh) : l + 1u) : l;
+}
+
+// Checks a Mapped resolution against its stems: every walk from the root ends
+// at a terminal stem (resolve_terminal_stem) naming a leaf, at the latest just
+// past max_stem_level, where the reference would otherwise panic
+// (stem_leaf_resolution.rs:176-200).  A stem without a split continues to its
+// left child only (traverse(false)).
+bool mapped_walks_end_in_leaves(const kgpu_tree_desc* d, const std::vector<uint32_t>& map,
+                                uint64_t map_min, uint32_t bh, uint32_t stem, int level) {
+  const uint64_t mi = uint64_t(stem) - map_min;
+  if (stem >= map_min && mi < map.size() && map[mi] != 0xffffffffu) return true;
+  if (level > d->max_stem_level) return false;
+  double pivot = __builtin_inf();
+  if (stem < d->stem_count)
+    pivot = d->dtype == KGPU_F64 ? static_cast<const double*>(d->stems)[stem]
+                                 : double(static_cast<const float*>(d->stems)[stem]);
+  if (!mapped_walks_end_in_leaves(d, map, map_min, bh, host_child(bh, stem, level, false),
+                                  level + 1))
+    return false;
+  return !(pivot < __builtin_inf()) ||
+         mapped_walks_end_in_leaves(d, map, map_min, bh, host_child(bh, stem, level, true),
+                                    level + 1);
+}
+
+int create_tree(const kgpu_tree_desc* d, const kgpu_leaf_map* m, void* stream,
+                kgpu_tree** out) {
   if (!d || !out) return set_error(KGPU_EINVAL, "NULL argument");
   *out = nullptr;
   if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
@@ -331,14 +371,45 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
     return set_error(KGPU_EINVAL, "unknown stem strategy");
   if (donnelly && d->block_height != 3 && d->block_height != 4)
     return set_error(KGPU_EUNSUPPORTED, "Donnelly block height must be 3 or 4");
-  if (d->resolution != KGPU_RES_ARITHMETIC)
-    return set_error(KGPU_EUNSUPPORTED,
-                     "only arithmetic stem/leaf resolution (soft immutable trees) is accepted");
+  const bool mapped = m != nullptr;
+  if (mapped ? d->resolution != KGPU_RES_MAPPED
+             : (d->resolution != KGPU_RES_ARITHMETIC && d->resolution != KGPU_RES_PRISTINE))
+    return set_error(KGPU_EINVAL,
+                     mapped ? "a leaf map comes with KGPU_RES_MAPPED"
+                            : "Mapped resolution needs its leaf map (kgpu_tree_create_mapped)");
   if (d->max_stem_level < -1 || d->max_stem_level > kMaxStemLevel)
     return set_error(KGPU_EUNSUPPORTED, "max_stem_level must be -1..30");
   const size_t sa = d->dtype == KGPU_F64 ? 8 : 4;
   const int K = int(d->dims);
-  if (!donnelly) {
+  std::vector<uint32_t> lmap;
+  if (mapped) {
+    // the leaf map, as u32 leaf indices (0xffffffff: not terminal)
+    if (m->len && !m->leaf_idx_map) return set_error(KGPU_EINVAL, "leaf_idx_map is NULL");
+    if (m->len > 0xffffffffull || m->min_stem_leaf_idx > 0xffffffffull)
+      return set_error(KGPU_EOVERFLOW, "leaf map beyond 32-bit stem indices");
+    if (d->stem_count > 0xFFFFFFFFull)
+      return set_error(KGPU_EOVERFLOW, "stem indices beyond 32 bits");
+    if (d->max_stem_level >= 0 && !d->stems) return set_error(KGPU_EINVAL, "stems is NULL");
+    try {
+      lmap.resize(m->len);
+    } catch (const std::bad_alloc&) {
+      return set_error(KGPU_ENOMEM, "host allocation failed");
+    }
+    for (uint64_t i = 0; i < m->len; ++i) {
+      const uint64_t v = m->leaf_idx_map[i];
+      if (v == ~uint64_t(0)) {
+        lmap[i] = 0xffffffffu;
+      } else if (v >= d->leaf_count) {
+        return set_error(KGPU_EINVAL, "leaf map names a leaf beyond leaf_count");
+      } else {
+        lmap[i] = uint32_t(v);
+      }
+    }
+    if (d->size && !mapped_walks_end_in_leaves(d, lmap, m->min_stem_leaf_idx,
+                                               donnelly ? d->block_height : 0, donnelly ? 0u : 1u,
+                                               0))
+      return set_error(KGPU_EINVAL, "a walk of the Mapped tree reaches no leaf");
+  } else if (!donnelly) {
     const uint64_t expect_leaves =
         d->max_stem_level >= 0 ? (uint64_t(1) << (d->max_stem_level + 1)) : (d->size ? 1 : 0);
     if (d->leaf_count != expect_leaves)
@@ -478,7 +549,16 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
   if (e == cudaSuccess && moved)
     e = cudaMemcpyAsync(dt.src_extents, ex.data(), ex.size() * 4, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && rows) e = convert_leaf_layout(dt, tiles.as<uint8_t>(), dt.arena, true, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // `ex` is a local
+  if (e == cudaSuccess && mapped) {
+    dt.map_min = m->min_stem_leaf_idx;
+    dt.map_len = uint32_t(lmap.size());
+    if ((e = cudaMalloc(reinterpret_cast<void**>(&dt.leaf_map),
+                        std::max<size_t>(16, lmap.size() * 4))) == cudaSuccess &&
+        !lmap.empty())
+      e = cudaMemcpyAsync(dt.leaf_map, lmap.data(), lmap.size() * 4, cudaMemcpyHostToDevice, s);
+    dt.device_bytes += lmap.size() * 4;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // `ex` and `lmap` are locals
   if (e != cudaSuccess) {
     kgpu_tree_destroy(t);
     return cuda_fail(e, "uploading the tree");
@@ -487,7 +567,27 @@ int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out)
   return KGPU_OK;
 }
 
-int32_t kgpu_tree_create_flatvec(const kgpu_flatvec_desc* d, void* stream, kgpu_tree** out) {
+}  // namespace
+}  // namespace kgpu
+
+extern "C" {
+
+int32_t kgpu_tree_create(const kgpu_tree_desc* d, void* stream, kgpu_tree** out) {
+  return create_tree(d, nullptr, stream, out);
+}
+
+int32_t kgpu_tree_create_mapped(const kgpu_tree_desc* d, const kgpu_leaf_map* map, void* stream,
+                                kgpu_tree** out) {
+  if (!map) return set_error(KGPU_EINVAL, "NULL leaf map");
+  return create_tree(d, map, stream, out);
+}
+
+}  // extern "C"
+
+namespace kgpu {
+namespace {
+int create_flatvec(const kgpu_flatvec_desc* d, const kgpu_leaf_map* map, void* stream,
+                   kgpu_tree** out) {
   if (!d || !out) return set_error(KGPU_EINVAL, "NULL argument");
   *out = nullptr;
   if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
@@ -504,7 +604,7 @@ int32_t kgpu_tree_create_flatvec(const kgpu_flatvec_desc* d, void* stream, kgpu_
   td.bucket_size = 32;
   td.stem_strategy = d->stem_strategy;
   td.block_height = d->block_height;
-  td.resolution = KGPU_RES_ARITHMETIC;
+  td.resolution = map ? KGPU_RES_MAPPED : KGPU_RES_ARITHMETIC;
   td.stems = d->stems;
   td.stem_count = d->stem_count;
   td.leaf_bytes = L.leaf_bytes.data();
@@ -514,11 +614,11 @@ int32_t kgpu_tree_create_flatvec(const kgpu_flatvec_desc* d, void* stream, kgpu_
   td.max_stem_level = d->max_stem_level;
   td.size = d->size;
   td.max_leaf_len = L.max_leaf_len;
-  return kgpu_tree_create(&td, stream, out);
+  return create_tree(&td, map, stream, out);
 }
 
-int32_t kgpu_tree_create_vecofarrays(const kgpu_vecofarrays_desc* d, void* stream,
-                                     kgpu_tree** out) {
+int create_vecofarrays(const kgpu_vecofarrays_desc* d, const kgpu_leaf_map* map, void* stream,
+                       kgpu_tree** out) {
   if (!d || !out) return set_error(KGPU_EINVAL, "NULL argument");
   *out = nullptr;
   if (d->abi_version != KGPU_ABI_VERSION) return set_error(KGPU_EINVAL, "abi_version mismatch");
@@ -567,7 +667,27 @@ int32_t kgpu_tree_create_vecofarrays(const kgpu_vecofarrays_desc* d, void* strea
   f.extents = ext.data();
   f.leaf_count = d->leaf_count;
   f.size = n;
-  return kgpu_tree_create_flatvec(&f, stream, out);
+  return create_flatvec(&f, map, stream, out);
+}
+}  // namespace
+}  // namespace kgpu
+
+extern "C" {
+
+int32_t kgpu_tree_create_flatvec(const kgpu_flatvec_desc* d, void* stream, kgpu_tree** out) {
+  return create_flatvec(d, nullptr, stream, out);
+}
+
+int32_t kgpu_tree_create_vecofarrays(const kgpu_vecofarrays_desc* d, void* stream,
+                                     kgpu_tree** out) {
+  return create_vecofarrays(d, nullptr, stream, out);
+}
+
+int32_t kgpu_tree_create_vecofarrays_mapped(const kgpu_vecofarrays_desc* d,
+                                            const kgpu_leaf_map* map, void* stream,
+                                            kgpu_tree** out) {
+  if (!map) return set_error(KGPU_EINVAL, "NULL leaf map");
+  return create_vecofarrays(d, map, stream, out);
 }
 
 int32_t kgpu_tree_destroy(kgpu_tree* t) {
@@ -624,13 +744,14 @@ int check_query_desc(const kgpu_tree* t, const kgpu_query_desc* d, bool radius_f
                              : "max_qty above 256 is served for 2-D and 3-D trees");
     }
   }
-  if (t->dt.bh) {
-    // Donnelly stems run on the thread engine (2-D and 3-D trees), Cartesian
-    // families only.
+  if (t->dt.scalar_walk()) {
+    // Donnelly stems and Mapped resolution run the scalar backtracking walk
+    // of the thread engine (2-D and 3-D trees).
     if (t->dt.dims != 2 && t->dt.dims != 3)
-      return set_error(KGPU_EUNSUPPORTED, "Donnelly trees are served for 2-D and 3-D points");
+      return set_error(KGPU_EUNSUPPORTED,
+                       "Donnelly and Mapped trees are served for 2-D and 3-D points");
     if (d->flags & KGPU_FLAG_ENGINE_WARP)
-      return set_error(KGPU_EUNSUPPORTED, "Donnelly trees run on the thread engine");
+      return set_error(KGPU_EUNSUPPORTED, "Donnelly and Mapped trees run on the thread engine");
   }
   if (d->periodic_box) {
     // builder.rs: periodic queries support nearest_one, nearest_n(.within) and
@@ -685,11 +806,11 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   const bool best = q.family == KGPU_BEST_N_WITHIN;
   const bool two_three = t.dims == 2 || t.dims == 3;
   if ((nn || best) && two_three && q.k > kMaxK &&
-      (q.k > kMaxBigK || (nn && q.periodic) || t.bh))
+      (q.k > kMaxBigK || (nn && q.periodic) || t.scalar_walk()))
     return launch_trow<A>(t, q);
   const bool big_k = q.k > kMaxK && (best || (nn && (q.k > kMaxThreadK || q.periodic)));
-  const bool thread = (t.bh || q.engine != 1) && two_three &&
-                      (!q.periodic || q.family != KGPU_NEAREST_ONE || t.bh) && !big_k;
+  const bool thread = (t.scalar_walk() || q.engine != 1) && two_three &&
+                      (!q.periodic || q.family != KGPU_NEAREST_ONE || t.scalar_walk()) && !big_k;
   return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);
 }
 template cudaError_t launch_fixed<float>(const DeviceTree&, const QueryLaunch&);

@@ -169,7 +169,31 @@ struct TreeView {
   uint64_t size;
   uint64_t stem_count;
   uint32_t bh;  // 0: Eytzinger stem order; 3 or 4: Donnelly<bh>
+  // OwnedStemLeafResolution::Mapped (stem_leaf_resolution.rs:53-66): the leaf
+  // of each terminal stem index from map_min on (0xffffffff: not terminal),
+  // or null for arithmetic resolution
+  const uint32_t* __restrict__ leaf_map;
+  uint64_t map_min;
+  uint32_t map_len;
 };
+
+// resolve_terminal_stem (orchestrator/mod.rs:183-192) for Mapped trees: the
+// leaf `stem` maps to, if it is a terminal stem.
+template <typename A>
+__device__ __forceinline__ bool terminal_leaf(const TreeView<A>& tv, uint32_t stem,
+                                              uint32_t& leaf) {
+  if (!tv.leaf_map || stem < tv.map_min || uint64_t(stem) - tv.map_min >= tv.map_len) return false;
+  const uint32_t l = __ldg(tv.leaf_map + (stem - tv.map_min));
+  if (l == 0xffffffffu) return false;
+  leaf = l;
+  return true;
+}
+
+// The two children of a stem at level `level` in the tree's stem order:
+// Eytzinger 2i and 2i + 1, Donnelly<bh> as donnelly_children.
+template <typename A>
+__device__ __forceinline__ void stem_children(const TreeView<A>& tv, uint32_t stem, int level,
+                                              uint32_t& l, uint32_t& r);
 
 // Children of a Donnelly<bh> stem (stem_strategy/donnelly/core.rs:400-428):
 // inside a minor triangle of bh levels the children of heap slot m of the
@@ -474,8 +498,35 @@ __device__ __forceinline__ void warp_arith_query(const TreeView<A>& tv, const A 
 }
 
 // Straight descent for approx (traits/stem_strategy.rs:182-200).
+template <typename A>
+__device__ __forceinline__ void stem_children(const TreeView<A>& tv, uint32_t stem, int level,
+                                              uint32_t& l, uint32_t& r) {
+  if (tv.bh) {
+    donnelly_children(stem, uint32_t(level) % tv.bh, tv.bh, l, r);
+  } else {
+    l = stem * 2u;
+    r = l + 1u;
+  }
+}
+
 template <typename A, int K>
 __device__ __forceinline__ uint32_t straight_leaf(const TreeView<A>& tv, const A (&q)[K]) {
+  if (tv.leaf_map) {
+    // get_leaf_idx_mapped (orchestrator/mod.rs:160-178): a terminal stem ends
+    // the descent; past max_stem_level the stem maps to its leaf
+    uint32_t stem = tv.bh ? 0u : 1u, leaf = 0;
+    int dim = 0;
+    for (int level = 0; level <= tv.max_stem_level; ++level) {
+      if (terminal_leaf(tv, stem, leaf)) return leaf;
+      const A pivot = stem < tv.stem_count ? __ldg(tv.stems + stem) : inf_of<A>();
+      uint32_t l, r;
+      stem_children(tv, stem, level, l, r);
+      stem = sel(q, dim) >= pivot ? r : l;
+      dim = dim + 1 == K ? 0 : dim + 1;
+    }
+    terminal_leaf(tv, stem, leaf);  // every terminal is mapped (checked at upload)
+    return leaf;
+  }
   if (tv.bh) {
     // StemStrategy::get_leaf_idx over Donnelly stems (traits/stem_strategy.rs:
     // 182-200): the leaf index accumulates the path bits.

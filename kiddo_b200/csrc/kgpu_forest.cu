@@ -60,6 +60,9 @@ void fill_views(const std::vector<kgpu_tree*>& trees, std::vector<uint8_t>& out)
     v.size = t.size;
     v.stem_count = t.stem_count;
     v.bh = t.bh;
+    v.leaf_map = t.leaf_map;
+    v.map_min = t.map_min;
+    v.map_len = t.map_len;
     std::memcpy(out.data() + i * sizeof(TreeView<A>), &v, sizeof(v));
   }
 }
@@ -139,6 +142,9 @@ int32_t kgpu_forest_create(kgpu_tree* const* trees, uint32_t n_trees, void* stre
     // Donnelly stems of one block height
     if (t->dt.bh != ts[0]->dt.bh)
       return set_error(KGPU_EINVAL, "forest trees must share the stem order (and block height)");
+    if ((t->dt.leaf_map != nullptr) != (ts[0]->dt.leaf_map != nullptr))
+      return set_error(KGPU_EINVAL,
+                       "forest trees must share the stem/leaf resolution (Mapped or arithmetic)");
     if (t->dt.device != cur) return set_error(KGPU_EINVAL, "forest trees must be on the current device");
   }
   auto* f = new (std::nothrow) kgpu_forest();
@@ -150,6 +156,8 @@ int32_t kgpu_forest_create(kgpu_tree* const* trees, uint32_t n_trees, void* stre
   f->meta.max_stem_level = -1;
   f->meta.size = 1;
   f->meta.bh = ts[0]->dt.bh;
+  // routes the forest to the scalar walk; each query reads its own tree's map
+  f->meta.leaf_map = ts[0]->dt.leaf_map;
   std::vector<uint64_t> base(n_trees);
   uint64_t total = 0;
   for (uint32_t i = 0; i < n_trees; ++i) {

@@ -24,6 +24,14 @@ struct DeviceTree {
   uint64_t max_leaf_len = 0;
   size_t device_bytes = 0;
   uint32_t bh = 0;             // 0: Eytzinger stems; 3 or 4: Donnelly<bh>
+  // Mapped stem/leaf resolution: u32 leaf of each stem index from map_min
+  // (0xffffffff: not terminal) on the device, or null (arithmetic)
+  uint32_t* leaf_map = nullptr;
+  uint64_t map_min = 0;
+  uint32_t map_len = 0;
+  // the kernels' scalar backtracking walk (Donnelly stems or Mapped resolution)
+  // rather than the Eytzinger arithmetic DFS
+  bool scalar_walk() const { return bh != 0 || leaf_map != nullptr; }
   bool pooled = false;         // arrays from the stream-ordered pool (device-built trees)
   // f64 3-D leaves are 32-byte rows with offsets of their own: the reference
   // layout's extents, uint2 (offset / 8, len), for read-back; null otherwise

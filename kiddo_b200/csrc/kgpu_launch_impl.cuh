@@ -21,6 +21,9 @@ inline TreeView<A> make_view(const DeviceTree& t) {
   v.size = t.size;
   v.stem_count = t.stem_count;
   v.bh = t.bh;
+  v.leaf_map = t.leaf_map;
+  v.map_min = t.map_min;
+  v.map_len = t.map_len;
   return v;
 }
 
@@ -276,7 +279,7 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
 
 template <typename A>
 cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q) {
-  if (t.bh) return launch_tfixed_donnelly(t, q, A());
+  if (t.scalar_walk()) return launch_tfixed_donnelly(t, q, A());
   return launch_tfixed_stems<A, 0>(t, q);
 }
 
@@ -303,7 +306,7 @@ cudaError_t launch_trow(const DeviceTree& t, const QueryLaunch& q) {
             if constexpr (M::kPeriodic) {
               if (best) return cudaErrorInvalidValue;
               const auto box = make_box<A, K>(q);
-              const int stems = t.bh ? 1 : 0;
+              const int stems = t.scalar_walk() ? 1 : 0;
               const size_t smem = periodic_smem<A>(t, stems);
               auto launch = [&](auto kern) {
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -332,7 +335,7 @@ cudaError_t launch_trow(const DeviceTree& t, const QueryLaunch& q) {
             g_launches++;
             return cudaGetLastError();
           };
-          if (t.bh) return run(k_trow<A, K, M, EX, 1>, 1);
+          if (t.scalar_walk()) return run(k_trow<A, K, M, EX, 1>, 1);
           return run(k_trow<A, K, M, EX, 0>, 0);
         });
       });
@@ -415,14 +418,14 @@ cudaError_t launch_within_pass_stems(const DeviceTree& t, const QueryLaunch& q, 
 
 template <typename A>
 cudaError_t launch_within_count(const DeviceTree& t, const QueryLaunch& q, uint64_t* counts) {
-  if (t.bh) return launch_within_donnelly(t, q, counts, nullptr, A());
+  if (t.scalar_walk()) return launch_within_donnelly(t, q, counts, nullptr, A());
   return launch_within_pass_stems<A, 0>(t, q, counts, nullptr);
 }
 
 template <typename A>
 cudaError_t launch_within_fill(const DeviceTree& t, const QueryLaunch& q,
                                const uint64_t* offsets) {
-  if (t.bh) return launch_within_donnelly(t, q, nullptr, offsets, A());
+  if (t.scalar_walk()) return launch_within_donnelly(t, q, nullptr, offsets, A());
   return launch_within_pass_stems<A, 0>(t, q, nullptr, offsets);
 }
 

@@ -250,9 +250,10 @@ struct ThreadWalk {
   }
 };
 
-// Per-thread scalar backtracking over Donnelly<bh> stems, the reference's
-// path for strategies with BLOCK_SIZE != 1 (kd_tree/orchestrator/mod.rs:
-// 265-345, 607-669; traits/stem_strategy.rs:209-325).  The reference's stack
+// Per-thread scalar backtracking, the reference's path for Donnelly<bh>
+// stems (BLOCK_SIZE != 1) and for Mapped resolution over either stem order
+// (kd_tree/orchestrator/mod.rs:214-345, 607-669; traits/stem_strategy.rs:
+// 209-325): a Mapped tree's terminal stems end a descent at their leaf.  The reference's stack
 // holds frames at strictly increasing levels, so the frame of the far child at
 // level FL lives in slot FL of three shared-memory columns (its rd, the off
 // value to put on its parent's axis, its stem index) with a bit in `pending`;
@@ -287,14 +288,17 @@ struct DonnellyWalk {
     const A INF = inf_of<A>();
     const A best = pol.max_dist();
     const int msl = tv.max_stem_level;
-    const uint32_t bh = tv.bh;
+    if (!tv.bh && stem == 0) stem = 1;  // a fresh walk starts at the Eytzinger root
     int dim = level % K;
-    uint32_t minor = uint32_t(level) % bh;
+    uint32_t tl;
     while (level <= msl) {
+      // a Mapped tree's terminal stem is a leaf (traverse_to_leaf,
+      // orchestrator/mod.rs:624-631)
+      if (terminal_leaf(tv, stem, tl)) return tl;
       ++st.stems;
       const A pivot = stem < tv.stem_count ? __ldg(tv.stems + stem) : INF;
       uint32_t l, r;
-      donnelly_children(stem, minor, bh, l, r);
+      stem_children(tv, stem, level, l, r);
       if (pivot < INF) {
         const A qd = sel(q, dim);
         const bool is_right = qd >= pivot;
@@ -315,8 +319,8 @@ struct DonnellyWalk {
       }
       ++level;
       dim = dim + 1 == K ? 0 : dim + 1;
-      minor = minor + 1u == bh ? 0u : minor + 1u;
     }
+    if (tv.leaf_map && terminal_leaf(tv, stem, tl)) return tl;
     return leaf;
   }
 
@@ -352,7 +356,8 @@ struct DonnellyWalk {
 // Both are exactly what the reference's step computed from the same inputs,
 // so the rebuilt state equals the frame it replaces.
 // STEMS == 0: Eytzinger stems, where an ancestor's index is the current
-// index shifted right.  STEMS == 1: Donnelly<bh> stems, where the walk keeps
+// index shifted right.  STEMS == 1: Donnelly<bh> stems or Mapped resolution
+// (either stem order, terminal stems ending a descent), where the walk keeps
 // the stem index of each level of its path in a column (path[L * stride])
 // and the leaf index in `leaf`, one path bit per level; the traversal is the
 // same (periodic.rs drives both stem orders through the StemStrategy trait).
@@ -437,7 +442,7 @@ struct PeriodicWalk {
     if (is_right && !(old_hi < pivot)) hi_set |= 1u << P;  // far = left child: upper = minup
     if constexpr (STEMS) {
       uint32_t l, r;
-      donnelly_children(parent, uint32_t(P) % tv.bh, tv.bh, l, r);
+      stem_children(tv, parent, P, l, r);
       stem_idx = is_right ? l : r;
       leaf = ((leaf >> (level - P)) << 1) | (is_right ? 0u : 1u);
     } else {
@@ -458,10 +463,17 @@ struct PeriodicWalk {
     }
     const A INF = inf_of<A>();
     const int msl = tv.max_stem_level;
+    if (STEMS && !tv.bh && level == 0 && stem_idx == 0) stem_idx = 1;  // Eytzinger root
     int dim = level % K;
     for (;;) {
+      uint32_t tl;
+      if (STEMS && terminal_leaf(tv, stem_idx, tl)) {  // resolve_terminal_stem (periodic.rs:496-500)
+        at_leaf = true;
+        return tl;
+      }
       if (level > msl) {
         at_leaf = true;
+        if (STEMS && tv.leaf_map && terminal_leaf(tv, stem_idx, tl)) return tl;
         return STEMS ? leaf : (stem_idx & ~(1u << level));
       }
       ++st.stems;
@@ -470,7 +482,7 @@ struct PeriodicWalk {
       if (!(pivot < INF)) {
         if constexpr (STEMS) {
           uint32_t l, r;
-          donnelly_children(stem_idx, uint32_t(level) % tv.bh, tv.bh, l, r);
+          stem_children(tv, stem_idx, level, l, r);
           stem_idx = l;
           leaf <<= 1;
         } else {
@@ -515,7 +527,7 @@ struct PeriodicWalk {
       rd = near_rd;
       if constexpr (STEMS) {
         uint32_t l, r;
-        donnelly_children(stem_idx, uint32_t(level) % tv.bh, tv.bh, l, r);
+        stem_children(tv, stem_idx, level, l, r);
         stem_idx = is_right ? r : l;
         leaf = (leaf << 1) | (is_right ? 1u : 0u);
       } else {

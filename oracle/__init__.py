@@ -113,6 +113,11 @@ def _declare(L):
     L.kor_from_layout_ex.argtypes = [i32, i32, vp, u64, vp, u64, vp, u64, ctypes.c_int32, u64,
                                      u64, ctypes.c_uint32]
     L.kor_free.argtypes = [vp]
+    L.kor_build_mapped.restype = vp
+    L.kor_build_mapped.argtypes = [i32, i32, vp, vp, u64, ctypes.c_uint32, i32, u64]
+    L.kor_leaf_map_info.argtypes = [vp, vp]
+    L.kor_copy_leaf_map.argtypes = [vp, vp]
+    L.kor_set_leaf_map.argtypes = [vp, vp, u64, u64]
     L.kor_iter.argtypes = [vp, vp, vp]
     L.kor_layout_info.argtypes = [vp, vp]
     L.kor_copy_layout.argtypes = [vp, vp, vp, vp]
@@ -157,6 +162,8 @@ class Layout:
         self.max_stem_level = int(max_stem_level)
         self.size = int(size)
         self.max_leaf_len = int(max_leaf_len)
+        self.leaf_map = None  # Mapped resolution: uint64 per stem index (2^64 - 1 = None)
+        self.map_min = 0
 
     @property
     def leaf_count(self):
@@ -189,6 +196,35 @@ class OracleTree:
         return cls(h, points.dtype, k, L)
 
     @classmethod
+    def build_mutable(cls, points, items=None, block_height=0, irregular_seed=None, L=None):
+        """A tree with hard buckets and Mapped stem/leaf resolution, as
+        MutableKdTree's bulk construction makes it (construction.rs:413-539,
+        695-864, 972-1009); with `irregular_seed`, a Mapped tree of random leaf
+        depths instead (Eytzinger stems), as leaf splits leave one."""
+        L = L if L is not None else lib()
+        points = np.ascontiguousarray(points)
+        n, k = points.shape
+        it = None if items is None else np.ascontiguousarray(items, dtype=np.uint32)
+        kind = 0 if irregular_seed is None else 1
+        h = L.kor_build_mapped(0 if points.dtype == np.float32 else 1, k, _ptr(points), _ptr(it),
+                               n, int(block_height), kind, int(irregular_seed or 0))
+        if not h:
+            raise ValueError("unsplittable bucket, or unsupported dtype/dimension")
+        return cls(h, points.dtype, k, L)
+
+    def leaf_map(self):
+        """(leaf_idx_map, min_stem_leaf_idx) of a Mapped tree (uint64, 2^64 - 1
+        for None), or None for arithmetic resolution."""
+        info = np.zeros(3, dtype=np.uint64)
+        self._L.kor_leaf_map_info(self._h, _ptr(info))
+        if not info[0]:
+            return None
+        m = np.empty(int(info[1]), dtype=np.uint64)
+        if m.size:
+            self._L.kor_copy_leaf_map(self._h, _ptr(m))
+        return m, int(info[2])
+
+    @classmethod
     def from_layout(cls, lay: Layout, L=None):
         L = L if L is not None else lib()
         dt = 0 if lay.dtype == np.float32 else 1
@@ -200,6 +236,9 @@ class OracleTree:
                                  lay.max_leaf_len, getattr(lay, "block_height", 0))
         if not h:
             raise ValueError("unsupported dtype/dimension for this oracle library")
+        if getattr(lay, "leaf_map", None) is not None:
+            m = np.ascontiguousarray(lay.leaf_map, dtype=np.uint64)
+            L.kor_set_leaf_map(h, _ptr(m), m.size, int(getattr(lay, "map_min", 0)))
         return cls(h, lay.dtype, lay.k, L)
 
     def __del__(self):
@@ -214,7 +253,11 @@ class OracleTree:
         lb = np.empty(int(info[1]), dtype=np.uint8)
         ex = np.empty((int(info[2]), 2), dtype=np.uint64)
         self._L.kor_copy_layout(self._h, _ptr(stems), _ptr(lb), _ptr(ex))
-        return Layout(self.dtype, self.k, stems, lb, ex, info[3], info[4], info[5], info[6])
+        lay = Layout(self.dtype, self.k, stems, lb, ex, info[3], info[4], info[5], info[6])
+        lm = self.leaf_map()
+        if lm is not None:
+            lay.leaf_map, lay.map_min = lm
+        return lay
 
     def iter(self):
         """(items[size], points[size, K]) in KdTreeIter order

@@ -33,6 +33,7 @@
 #pragma once
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -71,8 +72,32 @@ struct Tree {
   uint32_t stems_depth = 0;
   int stem_strategy = 0;  // 0 Eytzinger, 1 Donnelly<bh>
   uint32_t bh = 0;        // Donnelly block height
+  // OwnedStemLeafResolution::Mapped (stem_leaf_resolution.rs:53-66): stem
+  // index -> leaf index for terminal stems (kNoLeaf = None), from
+  // min_stem_leaf_idx on.  Arithmetic resolution when `mapped` is false.
+  static constexpr uint64_t kNoLeaf = ~uint64_t(0);
+  bool mapped = false;
+  std::vector<uint64_t> leaf_map;
+  uint64_t map_min = 0;
 
   size_t leaf_count() const { return extents.size() / 2; }
+  // is_terminal_stem_idx + resolve_terminal_stem_idx (stem_leaf_resolution.rs:
+  // 77-120): the stem maps straight to a leaf (Mapped trees only)
+  bool terminal(uint64_t stem, size_t* leaf) const {
+    if (!mapped || stem < map_min || stem - map_min >= leaf_map.size()) return false;
+    const uint64_t l = leaf_map[stem - map_min];
+    if (l == kNoLeaf) return false;
+    *leaf = size_t(l);
+    return true;
+  }
+  // the leaf of a walk that passed max_stem_level: the map for Mapped trees
+  // (which must hold it: the reference panics otherwise), else the arithmetic
+  // index
+  size_t resolve(uint64_t stem, size_t arithmetic_leaf) const {
+    size_t l = arithmetic_leaf;
+    if (mapped && !terminal(stem, &l)) return ~size_t(0);
+    return l;
+  }
   uint64_t leaf_offset(size_t l) const { return extents[2 * l]; }
   uint64_t leaf_len(size_t l) const { return extents[2 * l + 1]; }
 
@@ -339,6 +364,183 @@ struct Builder {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Construction: hard-bucket bulk build for mutable leaf strategies
+// (MutableKdTree = KdTree<A, u32, Eytzinger, VecOfArrays<A, u32, K, 32>, K, 32>,
+// lib.rs:274-275; construction.rs:413-539, 695-864, 972-1009, 1039-1085)
+// ---------------------------------------------------------------------------
+// calc_pivot (construction.rs:1039-1085) for hard buckets: the left part is
+// filled up to a multiple of B, at least B where the chunk allows; a split
+// that would leave everything on the left (and more than B there) puts
+// max(right_capacity, B) on the right instead.
+inline size_t hard_calc_pivot(size_t len, size_t right_capacity) {
+  auto next_multiple = [](size_t x) { return (x + kBucket - 1) / kBucket * kBucket; };
+  const size_t sat = len > right_capacity ? len - right_capacity : 0;
+  size_t result = std::min(next_multiple(sat), len);
+  if (len > 0) result = std::max(result, std::min(kBucket, len));
+  if (result >= len && result > kBucket) {
+    const size_t rc = std::max(right_capacity, kBucket);
+    const size_t sat2 = len > rc ? len - rc : 0;
+    result = std::min(next_multiple(sat2), len);
+  }
+  return result;
+}
+
+template <typename A, int K>
+struct HardBuilder {
+  Builder<A, K>& b;
+  Tree<A, K>& t;
+  std::vector<uint64_t> terminals;  // terminal stem index of each leaf, in leaf order
+  bool unsplittable = false;
+
+  // populate_recursive_hard (construction.rs:695-864)
+  template <typename Cursor>
+  void populate(size_t* idx, size_t len, Cursor cur, int max_stem_level, size_t capacity) {
+    if (unsplittable || len == 0) return;
+    if (len <= kBucket) {
+      t.max_leaf_len = std::max<uint64_t>(t.max_leaf_len, len);
+      append_leaf(t, b.pts, b.items, idx, len);
+      terminals.push_back(cur.stem_idx);
+      return;
+    }
+    const int levels_below = std::max(max_stem_level - cur.level, 0);
+    const size_t left_capacity =
+        std::min(levels_below >= 60 ? capacity : (size_t(1) << levels_below) * kBucket, capacity);
+    const size_t right_capacity = capacity > left_capacity ? capacity - left_capacity : 0;
+    const uint32_t stem_index = cur.stem_idx;
+    t.max_stem_level = std::max(t.max_stem_level, cur.level);
+    if (stem_index >= t.stems.size()) t.stems.resize(stem_index + 1, inf_value<A>());
+    const int dim = cur.dim();
+    size_t pivot = hard_calc_pivot(len, right_capacity);
+    if (pivot < len) {
+      pivot = b.update_pivot(idx, len, dim, pivot);
+      if (pivot >= len) {  // ConstructionError::UnsplittableBucket (construction.rs:1146-1148)
+        unsplittable = true;
+        return;
+      }
+      b.stable_split(idx, len, dim, pivot);
+      A m = b.coord(idx[pivot], dim);
+      for (size_t i = pivot; i < len; ++i) m = std::min(m, b.coord(idx[i], dim));
+      t.stems[stem_index] = m;
+    }
+    Cursor right = cur.branch();
+    populate(idx, pivot, cur, max_stem_level, left_capacity);
+    if (len > pivot) populate(idx + pivot, len - pivot, right, max_stem_level, right_capacity);
+  }
+};
+
+// new_from_source_with for a mutable, hard-bucket leaf strategy: the stem
+// tree sized by walking to leaf leaf_node_count - 1 below the root
+// (construction.rs:448-469), populate_recursive_hard, then Mapped resolution
+// from the terminal stems in leaf order (mapped_stem_leaf_resolution_from_
+// terminals, :972-1009); a tree of fewer than two leaves has no stems and maps
+// the root stem to its leaf (build_mapped_stem_leaf_resolution,
+// traits/leaf_strategy.rs:30-76).  Returns false for an unsplittable bucket.
+template <typename A, int K>
+bool build_hard(Tree<A, K>& t, const A* pts, const uint32_t* items, size_t n, uint32_t bh = 0) {
+  t = Tree<A, K>();
+  t.size = n;
+  t.stem_strategy = bh ? 1 : 0;
+  t.bh = bh;
+  t.mapped = true;
+  t.map_min = 0;
+  const size_t leaf_node_count = (n + kBucket - 1) / kBucket;
+  std::vector<size_t> idx(n);
+  std::iota(idx.begin(), idx.end(), size_t(0));
+  if (leaf_node_count < 2) {
+    t.max_stem_level = -1;
+    if (n == 0) return true;
+    t.max_leaf_len = n;
+    append_leaf(t, pts, items, idx.data(), n);
+    const uint64_t root = bh ? 0 : 1;
+    t.leaf_map.assign(root + 1, Tree<A, K>::kNoLeaf);
+    t.leaf_map[root] = 0;
+    return true;
+  }
+  uint32_t depth = 0;
+  while ((size_t(1) << depth) < leaf_node_count) ++depth;
+  Builder<A, K> b{pts, items, &t, {}};
+  HardBuilder<A, K> hb{b, t, {}, false};
+  t.max_stem_level = -1;
+  auto run = [&](auto root, uint32_t padded_depth) {
+    auto walk = root;
+    for (int bit = int(padded_depth) - 1; bit >= 1; --bit)
+      walk.traverse(((leaf_node_count - 1) >> bit) & 1u);
+    const size_t stem_node_count = size_t(walk.stem_idx) + 1;
+    t.stems.assign((stem_node_count + 7) / 8 * 8, inf_value<A>());
+    hb.populate(idx.data(), n, root, int(padded_depth) - 1, leaf_node_count * kBucket);
+  };
+  if (!bh) {
+    t.stems_depth = depth;
+    run(EytzingerCursor<K>{}, depth);
+  } else {
+    const uint32_t padding = depth % bh ? bh - depth % bh : 0;
+    depth += padding;
+    t.stems_depth = depth;
+    DonnellyCursor<K> root;
+    root.bh = bh;
+    for (uint32_t i = 0; i < padding; ++i) root.traverse(false);
+    run(root, depth);
+  }
+  if (hb.unsplittable) return false;
+  uint64_t max_terminal = 0;
+  for (uint64_t s : hb.terminals) max_terminal = std::max(max_terminal, s);
+  t.leaf_map.assign(max_terminal + 1, Tree<A, K>::kNoLeaf);
+  for (size_t l = 0; l < hb.terminals.size(); ++l) t.leaf_map[hb.terminals[l]] = l;
+  return true;
+}
+
+// A Mapped tree of irregular depth, as a MutableKdTree holds after leaf
+// splits (construction.rs:19-130): from each node, a chunk of at most B
+// points becomes a leaf with probability 1/2 (always once it has one point,
+// or cannot be split), a larger one is split at its median by the
+// reference's pivot rule.  Test data for the Mapped traversal, not a
+// restatement of the reference's mutation sequence.
+template <typename A, int K>
+void build_irregular(Tree<A, K>& t, const A* pts, const uint32_t* items, size_t n,
+                     uint64_t seed) {
+  t = Tree<A, K>();
+  t.size = n;
+  t.mapped = true;
+  t.max_stem_level = -1;
+  std::vector<size_t> idx(n);
+  std::iota(idx.begin(), idx.end(), size_t(0));
+  Builder<A, K> b{pts, items, &t, {}};
+  std::vector<uint64_t> terminals;
+  uint64_t rng = seed * 6364136223846793005ull + 1442695040888963407ull;
+  auto coin = [&]() {
+    rng = rng * 6364136223846793005ull + 1442695040888963407ull;
+    return (rng >> 33) & 1u;
+  };
+  std::function<void(size_t*, size_t, EytzingerCursor<K>)> rec = [&](size_t* ix, size_t len,
+                                                                     EytzingerCursor<K> cur) {
+    const int dim = cur.dim();
+    size_t pivot = len;
+    if (len > 1 && cur.level < 30 && (len > kBucket || coin()))
+      pivot = b.update_pivot(ix, len, dim, len / 2 ? len / 2 : 1);
+    if (pivot >= len || pivot == 0) {
+      t.max_leaf_len = std::max<uint64_t>(t.max_leaf_len, len);
+      append_leaf(t, pts, items, ix, len);
+      terminals.push_back(cur.stem_idx);
+      return;
+    }
+    t.max_stem_level = std::max(t.max_stem_level, cur.level);
+    if (cur.stem_idx >= t.stems.size()) t.stems.resize(cur.stem_idx + 1, inf_value<A>());
+    b.stable_split(ix, len, dim, pivot);
+    A m = b.coord(ix[pivot], dim);
+    for (size_t i = pivot; i < len; ++i) m = std::min(m, b.coord(ix[i], dim));
+    t.stems[cur.stem_idx] = m;
+    EytzingerCursor<K> right = cur.branch();
+    rec(ix, pivot, cur);
+    rec(ix + pivot, len - pivot, right);
+  };
+  if (n) rec(idx.data(), n, EytzingerCursor<K>{});
+  uint64_t max_terminal = 0;
+  for (uint64_t s : terminals) max_terminal = std::max(max_terminal, s);
+  t.leaf_map.assign(n ? max_terminal + 1 : 0, Tree<A, K>::kNoLeaf);
+  for (size_t l = 0; l < terminals.size(); ++l) t.leaf_map[terminals[l]] = l;
+}
+
 // KdTree::new_from_entries / new_from_slice -> new_from_source_with
 // (construction.rs:278-303, 403-409, 413-539, 540-589).  bh == 0 builds the
 // Eytzinger layout (ImmutableKdTree); bh > 0 builds Donnelly<bh>, whose stem
@@ -596,19 +798,26 @@ void arithmetic_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_
 // pushed when rd_far is not greater than max_dist() as read when the descent
 // started.  Only the popped frame's own dimension of `off` is reset, so
 // values set under deeper subtrees carry over, as in the reference.
-template <typename A, int K, typename M, typename Ctx, typename Leaf>
-void scalar_backtracking_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_leaf,
-                               Stats* st) {
+template <int K>
+inline size_t cursor_leaf(const EytzingerCursor<K>& c) { return c.leaf_idx(); }
+template <int K>
+inline size_t cursor_leaf(const DonnellyCursor<K>& c) { return size_t(c.leaf_idx); }
+
+// Over the stem order of cursor C (DonnellyCursor, or EytzingerCursor for a
+// Mapped Eytzinger tree), with the Mapped resolution's terminal-stem checks of
+// traverse_to_leaf (orchestrator/mod.rs:607-669): a stem that maps to a leaf
+// ends the descent there.
+template <typename A, int K, typename M, typename C, typename Ctx, typename Leaf>
+void scalar_backtracking_query_c(const Tree<A, K>& t, C root, const A* q, Ctx& ctx,
+                                 Leaf&& process_leaf, Stats* st) {
   if (t.size == 0) return;
   struct Frame {
-    DonnellyCursor<K> s;
+    C s;
     int restore_dim;  // -1: the popped state's own dimension
     A old_off;
     A rd;
   };
   std::vector<Frame> stack;
-  DonnellyCursor<K> root;
-  root.bh = t.bh;
   stack.push_back({root, -1, A(0), A(0)});
   A off[K];
   for (int d = 0; d < K; ++d) off[d] = A(0);
@@ -616,7 +825,7 @@ void scalar_backtracking_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&&
   while (!stack.empty()) {
     Frame f = stack.back();
     stack.pop_back();
-    DonnellyCursor<K> s = f.s;
+    C s = f.s;
     int dim = s.dim();
     const int restore_dim = f.restore_dim < 0 ? dim : f.restore_dim;
     const A md = ctx.max_dist();
@@ -624,12 +833,18 @@ void scalar_backtracking_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&&
     off[restore_dim] = f.old_off;
     const A best = ctx.max_dist();
     const A rd = f.rd;
-    while (s.level <= t.max_stem_level) {
+    size_t leaf;
+    for (;;) {
+      if (t.terminal(s.stem_idx, &leaf)) break;
+      if (s.level > t.max_stem_level) {
+        leaf = t.resolve(s.stem_idx, cursor_leaf(s));
+        break;
+      }
       if (st) st->stem_visits++;
       const A pivot = s.stem_idx < t.stems.size() ? t.stems[s.stem_idx] : INF;
       if (pivot < INF) {
         const bool is_right = q[dim] >= pivot;
-        DonnellyCursor<K> far = s.branch_relative(is_right);
+        C far = s.branch_relative(is_right);
         const A new_off = std::fabs(q[dim] - pivot);  // Axis::saturating_dist
         const A rd_far = M::template rect_k<A, K>(rd, off, dim, new_off);
         if (!(rd_far > best)) stack.push_back({far, dim, new_off, rd_far});
@@ -638,46 +853,56 @@ void scalar_backtracking_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&&
       }
       dim = s.dim();
     }
-    const size_t leaf = size_t(s.leaf_idx);
+    if (leaf >= t.leaf_count()) continue;  // an unmapped terminal (the reference panics)
     if (st) { st->leaf_visits++; st->points_scanned += t.leaf_len(leaf); }
     process_leaf(leaf);
   }
 }
 
-// The traversal the reference runs for this tree's strategy
-// (orchestrator/mod.rs:214-255): arithmetic DFS for Eytzinger, scalar
-// backtracking for Donnelly.
+template <typename A, int K, typename M, typename Ctx, typename Leaf>
+void scalar_backtracking_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_leaf,
+                               Stats* st) {
+  if (t.stem_strategy == 1) {
+    DonnellyCursor<K> root;
+    root.bh = t.bh;
+    scalar_backtracking_query_c<A, K, M>(t, root, q, ctx, process_leaf, st);
+  } else {
+    scalar_backtracking_query_c<A, K, M>(t, EytzingerCursor<K>(), q, ctx, process_leaf, st);
+  }
+}
+
+// The traversal the reference runs for this tree (orchestrator/mod.rs:
+// 214-255): arithmetic DFS for Eytzinger stems with arithmetic resolution,
+// scalar backtracking for Donnelly stems and for Mapped resolution.
 template <typename A, int K, typename M, typename Ctx, typename Leaf>
 void tree_query(const Tree<A, K>& t, const A* q, Ctx& ctx, Leaf&& process_leaf, Stats* st) {
-  if (t.stem_strategy == 1)
+  if (t.stem_strategy == 1 || t.mapped)
     scalar_backtracking_query<A, K, M>(t, q, ctx, process_leaf, st);
   else
     arithmetic_query<A, K, M>(t, q, ctx, process_leaf, st);
 }
 
-// Straight descent (orchestrator/mod.rs:143-151, traits/stem_strategy.rs:182-200)
+// Straight descent (orchestrator/mod.rs:133-178, traits/stem_strategy.rs:182-200);
+// Mapped trees stop at a terminal stem (get_leaf_idx_mapped).
+template <typename A, int K, typename C>
+size_t get_leaf_idx_c(const Tree<A, K>& t, C s, const A* q, Stats* st) {
+  size_t leaf;
+  while (s.level <= t.max_stem_level) {
+    if (t.terminal(s.stem_idx, &leaf)) return leaf;
+    if (st) st->stem_visits++;
+    const A pivot = s.stem_idx < t.stems.size() ? t.stems[s.stem_idx] : inf_value<A>();
+    s.traverse(q[s.dim()] >= pivot);
+  }
+  return t.resolve(s.stem_idx, cursor_leaf(s));
+}
 template <typename A, int K>
 size_t get_leaf_idx(const Tree<A, K>& t, const A* q, Stats* st) {
   if (t.stem_strategy == 1) {
     DonnellyCursor<K> s;
     s.bh = t.bh;
-    while (s.level <= t.max_stem_level) {
-      if (st) st->stem_visits++;
-      const A pivot = s.stem_idx < t.stems.size() ? t.stems[s.stem_idx] : inf_value<A>();
-      s.traverse(q[s.dim()] >= pivot);
-    }
-    return size_t(s.leaf_idx);
+    return get_leaf_idx_c(t, s, q, st);
   }
-  uint32_t stem_idx = 1;
-  int level = 0;
-  while (level <= t.max_stem_level) {
-    if (st) st->stem_visits++;
-    const A pivot = t.stems[stem_idx];
-    const bool is_right = q[level % K] >= pivot;
-    stem_idx = stem_idx * 2 + (is_right ? 1u : 0u);
-    ++level;
-  }
-  return size_t(stem_idx & ~(uint32_t(1) << level));
+  return get_leaf_idx_c(t, EytzingerCursor<K>(), q, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -761,6 +986,7 @@ std::pair<A, uint32_t> approx_nearest_one(const Tree<A, K>& t, const A* q, Stats
   uint32_t best_item = 0;
   if (t.leaf_count() == 0) return {best, best_item};
   size_t leaf = get_leaf_idx(t, q, st);
+  if (leaf >= t.leaf_count()) return {best, best_item};
   if (st) { st->leaf_visits++; st->points_scanned += t.leaf_len(leaf); }
   t.for_each_point(leaf, [&](const A* c, uint32_t item) {
     A d = point_dist<M, A, K>(c, q);
@@ -967,11 +1193,6 @@ inline A min_image_delta(A q, A c, A L) {
   return wrapped < delta ? wrapped : delta;
 }
 
-template <int K>
-inline size_t cursor_leaf(const EytzingerCursor<K>& c) { return c.leaf_idx(); }
-template <int K>
-inline size_t cursor_leaf(const DonnellyCursor<K>& c) { return size_t(c.leaf_idx); }
-
 // periodic_backtracking_query (periodic.rs:455-619) driving a collector
 // through `max_dist()`, `prune_on_equal()` and `leaf(leaf_idx)`, over the
 // stem order of cursor C (EytzingerCursor or DonnellyCursor: periodic.rs
@@ -999,10 +1220,18 @@ void periodic_query_c(const Tree<A, K>& t, C root, const A* q, const A* box, Ctx
   for (;;) {
     bool finished = false;
     for (;;) {
-      if (s.level > t.max_stem_level) {
-        const size_t leaf = cursor_leaf(s);
-        if (st) { st->leaf_visits++; st->points_scanned += t.leaf_len(leaf); }
-        leaf_fn(leaf);
+      // resolve_terminal_stem, then the walk past max_stem_level (periodic.rs:496-510)
+      size_t leaf;
+      bool at_leaf = t.terminal(s.stem_idx, &leaf);
+      if (!at_leaf && s.level > t.max_stem_level) {
+        leaf = t.resolve(s.stem_idx, cursor_leaf(s));
+        at_leaf = true;
+      }
+      if (at_leaf) {
+        if (leaf < t.leaf_count()) {
+          if (st) { st->leaf_visits++; st->points_scanned += t.leaf_len(leaf); }
+          leaf_fn(leaf);
+        }
         break;
       }
       if (st) st->stem_visits++;

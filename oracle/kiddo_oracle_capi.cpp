@@ -284,6 +284,76 @@ void* kor_from_layout(int dtype, int k, const void* stems, uint64_t stems_len,
                             max_stem_level, size, max_leaf_len, 0);
 }
 
+// MutableKdTree-style bulk build: hard buckets and Mapped resolution
+// (build_hard).  `kind` 0: the reference's construction; 1: an irregular
+// Mapped tree of random leaf depths (build_irregular, Eytzinger stems), with
+// `seed`.  nullptr for an unsplittable bucket or an unsupported shape.
+void* kor_build_mapped(int dtype, int k, const void* pts, const uint32_t* items, uint64_t n,
+                       uint32_t bh, int kind, uint64_t seed) {
+  if (bh != 0 && bh != 3 && bh != 4) return nullptr;
+  return dispatch(dtype, k, [&](auto a, auto kk) -> void* {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    std::vector<uint32_t> gen;
+    if (!items) {
+      gen.resize(n);
+      for (uint64_t i = 0; i < n; ++i) gen[i] = uint32_t(i);
+      items = gen.data();
+    }
+    auto* h = new TreeHolder<A, K>();
+    h->dtype = dtype;
+    h->k = K;
+    if (kind == 1) {
+      build_irregular<A, K>(h->t, static_cast<const A*>(pts), items, n, seed);
+    } else if (!build_hard<A, K>(h->t, static_cast<const A*>(pts), items, n, bh)) {
+      delete h;
+      return nullptr;
+    }
+    return static_cast<TreeBase*>(h);
+  });
+}
+
+// The Mapped resolution of a tree: out[0] = 1 if mapped, out[1] = map length,
+// out[2] = min_stem_leaf_idx; kor_copy_leaf_map writes the map (leaf index or
+// 2^64 - 1 = None per stem index from min_stem_leaf_idx on).
+void kor_leaf_map_info(void* hp, uint64_t* out) {
+  auto* b = static_cast<TreeBase*>(hp);
+  dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    out[0] = t.mapped ? 1 : 0;
+    out[1] = t.leaf_map.size();
+    out[2] = t.map_min;
+    return 0;
+  });
+}
+
+void kor_copy_leaf_map(void* hp, uint64_t* out) {
+  auto* b = static_cast<TreeBase*>(hp);
+  dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    std::memcpy(out, t.leaf_map.data(), t.leaf_map.size() * 8);
+    return 0;
+  });
+}
+
+// Gives a tree made by kor_from_layout_ex a Mapped resolution.
+void kor_set_leaf_map(void* hp, const uint64_t* map, uint64_t len, uint64_t min_stem_leaf_idx) {
+  auto* b = static_cast<TreeBase*>(hp);
+  dispatch(b->dtype, b->k, [&](auto a, auto kk) -> int {
+    using A = decltype(a);
+    constexpr int K = decltype(kk)::value;
+    auto& t = static_cast<TreeHolder<A, K>*>(b)->t;
+    t.mapped = true;
+    t.leaf_map.assign(map, map + len);
+    t.map_min = min_stem_leaf_idx;
+    return 0;
+  });
+}
+
 void kor_free(void* h) { delete static_cast<TreeBase*>(h); }
 
 // KdTreeIter::next (src/kd_tree/iter.rs:64-90): leaf 0 to leaf_count - 1,

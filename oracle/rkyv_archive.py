@@ -72,11 +72,14 @@ def root_layout(w: int):
 
 
 def write_archive(stems, leaf_bytes, extents, size, max_stem_level, max_leaf_len,
-                  pointer_width=4, resolution="arithmetic"):
+                  pointer_width=4, resolution="arithmetic", leaf_map=None, map_min=0):
     """The archive bytes of a tree layout.  `stems` is the stem array in the
     tree's dtype, `leaf_bytes` the VecOfArenas arena, `extents` [leaf_count, 2]
     (offset, len); `resolution` is "arithmetic" or "pristine" (tags 0 and 1,
-    fields stems_depth = max_stem_level + 1 and leaf_count)."""
+    fields stems_depth = max_stem_level + 1 and leaf_count), or "mapped" (tag
+    2: min_stem_leaf_idx, then leaf_idx_map as a vec of usize written after the
+    arena, None as the all-ones usize, OptionNonMaxUsizeAsUsize,
+    src/rkyv/adapters.rs:168-237)."""
     w = int(pointer_width)
     stems = np.ascontiguousarray(stems)
     leaf_bytes = np.ascontiguousarray(leaf_bytes, dtype=np.uint8)
@@ -95,6 +98,14 @@ def write_archive(stems, leaf_bytes, extents, size, max_stem_level, max_leaf_len
     _align(buf, CACHELINE)
     arena_pos = len(buf)
     buf.extend(leaf_bytes.tobytes())
+    # 3b. the Mapped resolution's leaf_idx_map
+    map_pos = 0
+    if resolution == "mapped":
+        _align(buf, w)
+        map_pos = len(buf)
+        none = (1 << (8 * w)) - 1
+        for v in np.asarray(leaf_map, dtype=np.uint64):
+            buf.extend(_uint(none if int(v) == (1 << 64) - 1 else int(v), w))
     # 4. the root, aligned for its type
     L = root_layout(w)
     _align(buf, L["align"])
@@ -109,9 +120,15 @@ def write_archive(stems, leaf_bytes, extents, size, max_stem_level, max_leaf_len
     put(L["leaf_bytes"], _int(arena_pos - (root + L["leaf_bytes"]), w) +
         _uint(leaf_bytes.size, w))
     put(L["leaves_size"], _uint(size, w))
-    tag = {"arithmetic": 0, "pristine": 1}[resolution]
+    tag = {"arithmetic": 0, "pristine": 1, "mapped": 2}[resolution]
     put(L["resolution"], bytes([tag]))
-    put(L["resolution"] + w, _uint(max_stem_level + 1, w) + _uint(extents.shape[0], w))
+    if tag == 2:
+        at = root + L["resolution"] + 2 * w
+        n = 0 if leaf_map is None else len(leaf_map)
+        put(L["resolution"] + w, _uint(map_min, w) + _int(map_pos - at if n else 0, w) +
+            _uint(n, w))
+    else:
+        put(L["resolution"] + w, _uint(max_stem_level + 1, w) + _uint(extents.shape[0], w))
     put(L["size"], _uint(size, w))
     put(L["max_stem_level"], struct.pack("<i", int(max_stem_level)))
     put(L["max_leaf_len"], _uint(max_leaf_len, w))
@@ -119,7 +136,10 @@ def write_archive(stems, leaf_bytes, extents, size, max_stem_level, max_leaf_len
     return bytes(buf)
 
 
-def write_layout(lay, pointer_width=4, resolution="arithmetic"):
-    """write_archive over an oracle.Layout."""
+def write_layout(lay, pointer_width=4, resolution=None):
+    """write_archive over an oracle.Layout (Mapped when the layout has a leaf map)."""
+    if resolution is None:
+        resolution = "mapped" if getattr(lay, "leaf_map", None) is not None else "arithmetic"
     return write_archive(lay.stems, lay.leaf_bytes, lay.extents, lay.size, lay.max_stem_level,
-                         lay.max_leaf_len, pointer_width, resolution)
+                         lay.max_leaf_len, pointer_width, resolution,
+                         getattr(lay, "leaf_map", None), getattr(lay, "map_min", 0))

@@ -69,7 +69,7 @@ def test_tree_create_rejects_bad_layouts_before_touching_the_device():
         ("item_size", 8, C.KGPU_EUNSUPPORTED),
         ("bucket_size", 16, C.KGPU_EUNSUPPORTED),
         ("stem_strategy", C.STEM_DONNELLY, C.KGPU_EUNSUPPORTED),
-        ("resolution", C.RES_MAPPED, C.KGPU_EUNSUPPORTED),
+        ("resolution", C.RES_MAPPED, C.KGPU_EINVAL),  # a Mapped tree needs its leaf map
         ("max_stem_level", 40, C.KGPU_EUNSUPPORTED),
         ("leaf_count", 5, C.KGPU_EINVAL),
         ("size", 999, C.KGPU_EINVAL),
@@ -246,3 +246,39 @@ def test_descriptor_layouts_match_the_header(tmp_path):
         cls = pairs[cname]
         want = ctypes.sizeof(cls) if fname == "sizeof" else getattr(cls, fname).offset
         assert int(value) == want, (cname, fname, int(value), want)
+
+
+def test_mapped_create_rejects_bad_leaf_maps_before_touching_the_device():
+    """kgpu_tree_create_mapped checks the map against the stems: leaf indices
+    inside leaf_count, and every walk from the root ending at a mapped
+    terminal stem (where the reference would panic)."""
+    import oracle
+    rng = np.random.default_rng(1)
+    o = oracle.OracleTree.build_mutable(rng.random((3000, 3)))
+    lay = o.layout()
+    m, mn = o.leaf_map()
+    t = kb.ImmutableKdTree.from_layout(np.float64, 3, lay.stems, lay.leaf_bytes, lay.extents,
+                                       lay.max_stem_level, lay.size, lay.max_leaf_len)
+
+    def create(mp):
+        d = _desc_of(t)
+        d.resolution = C.RES_MAPPED
+        lm = C.LeafMap()
+        mp = np.ascontiguousarray(mp, dtype=np.uint64)
+        lm.leaf_idx_map = mp.ctypes.data if mp.size else None
+        lm.len = mp.size
+        lm.min_stem_leaf_idx = mn
+        h = ctypes.c_void_p()
+        return C.lib().kgpu_tree_create_mapped(ctypes.byref(d), ctypes.byref(lm), None,
+                                               ctypes.byref(h))
+    bad = m.copy()
+    bad[np.nonzero(bad != 2 ** 64 - 1)[0][0]] = lay.leaf_count  # beyond the leaves
+    assert create(bad) == C.KGPU_EINVAL
+    bad = m.copy()
+    bad[np.nonzero(bad != 2 ** 64 - 1)[0][-1]] = 2 ** 64 - 1  # a walk with no leaf
+    assert create(bad) == C.KGPU_EINVAL
+    assert b"reaches no leaf" in C.lib().kgpu_last_error()
+    d = _desc_of(t)  # a map needs the Mapped resolution
+    lm = C.LeafMap()
+    assert C.lib().kgpu_tree_create_mapped(ctypes.byref(d), ctypes.byref(lm), None,
+                                           ctypes.byref(ctypes.c_void_p())) == C.KGPU_EINVAL

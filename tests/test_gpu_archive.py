@@ -56,11 +56,19 @@ def test_archive_upload_from_bytes_and_the_c2_shape():
     assert_same_fixed(r.distances, r.items, np.ones(len(Q)), od, oi, np.ones(len(Q)), "approx")
 
 
-def test_archive_with_mapped_resolution_is_refused():
-    lay = oracle.OracleTree.build(np.random.default_rng(1).random((2000, 3))).layout()
-    b = bytearray(ra.write_layout(lay, 4))
-    L = ra.root_layout(4)
-    b[len(b) - L["total"] + L["resolution"]] = 2  # Mapped (a mutated MutableKdTree)
-    with pytest.raises(kb.KiddoGpuError) as e:
-        kb.GpuTree.from_archive(bytes(b), np.float64, 3)
-    assert e.value.status == C.KGPU_EUNSUPPORTED
+@pytest.mark.parametrize("width", [4, 8])
+def test_archive_of_a_mutable_tree(width):
+    """A MutableKdTree archive (hard buckets, Mapped resolution with its
+    leaf_idx_map) uploads in place and answers like the oracle."""
+    rng = np.random.default_rng(width)
+    P = rng.random((30_000, 3))
+    Q = rng.random((2_000, 3))
+    o = oracle.OracleTree.build_mutable(P)
+    b = ra.write_layout(o.layout(), width)
+    info = kb.GpuTree.inspect_archive(b, np.float64, 3, pointer_width=width)
+    assert info["resolution"] == C.RES_MAPPED and info["map_len"] == o.leaf_map()[0].size
+    g = kb.GpuTree.from_archive(b, np.float64, 3, pointer_width=width)
+    r = g.query(Q).nearest_n(SE, 10).execute_gpu()
+    assert_same_fixed(r.distances, r.items, r.counts, *o.nearest_n(Q, 10), "knn10")
+    r = g.query(Q).within(SE, 5e-4).execute_gpu()
+    assert_same_csr((r.offsets, r.distances, r.items), o.within(Q, 5e-4), "within")
