@@ -163,8 +163,15 @@ typedef struct kgpu_query_desc {
   int32_t sorted;         /* 1 = default sorted output, 0 = .unsorted() */
   const void* periodic_box; /* host pointer to K values of A (each > 0), or NULL: Cartesian */
   uint32_t flags;         /* KGPU_FLAG_* */
-  uint32_t reserved0;
+  uint32_t tuning;        /* launch knobs, same results (0 = defaults): KGPU_TUNE_REFILL(n),
+                             KGPU_TUNE_CHUNK_LOG2(c) */
 } kgpu_query_desc;
+
+/* kgpu_query_desc::tuning: the lane-refilled kernels refill a warp's idle
+ * lanes once n of them (1..32; default 24) are idle, and hand queries to a
+ * warp 2^c at a time (c in 5..10; default 64 queries). */
+#define KGPU_TUNE_REFILL(n) ((uint32_t)(n) & 0x3fu)
+#define KGPU_TUNE_CHUNK_LOG2(c) (((uint32_t)(c) & 0xfu) << 8)
 
 typedef struct kgpu_layout kgpu_layout; /* host-side tree layout built by this library */
 typedef struct kgpu_tree kgpu_tree;     /* device-resident tree */

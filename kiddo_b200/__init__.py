@@ -677,6 +677,8 @@ class QueryBuilder:
         self.box = None
         self.spatial_order = None  # None: the library decides
         self.engine = None
+        self.refill = None  # idle lanes before a warp refills (None: 24)
+        self.chunk = None   # queries handed to a warp at a time (None: 64)
         self.stream = None
         self.points = False
         self.want_items = True
@@ -818,6 +820,21 @@ class QueryBuilder:
         self.engine = engine
         return self
 
+    def with_tuning(self, refill: Optional[int] = None, chunk: Optional[int] = None
+                    ) -> "QueryBuilder":
+        """Launch knobs of the lane-refilled kernels (kgpu_query_desc::tuning):
+        refill a warp's idle lanes once `refill` (1..32) are idle, hand queries
+        to a warp `chunk` (a power of two, 32..1024) at a time; None keeps the
+        defaults (24, 64).  Same results."""
+        if refill is not None and not 1 <= int(refill) <= 32:
+            raise ValueError("refill must be 1..32")
+        if chunk is not None and (int(chunk) < 32 or int(chunk) > 1024 or
+                                  int(chunk) & (int(chunk) - 1)):
+            raise ValueError("chunk must be a power of two in 32..1024")
+        self.refill = None if refill is None else int(refill)
+        self.chunk = None if chunk is None else int(chunk)
+        return self
+
     def autotuned(self, tune_if_missing: bool = True) -> "QueryBuilder":
         """Apply the cached autotuner choice of engine and processing order for
         this kind of query (kiddo_b200.autotune); tune on a sample of this batch
@@ -829,7 +846,9 @@ class QueryBuilder:
         if choice is None and tune_if_missing and _is_torch_cuda(self.queries):
             choice = autotune.tune(self)
         if choice is not None:
-            self.engine, self.spatial_order = choice
+            self.engine = choice["engine"]
+            self.spatial_order = choice["spatial_order"]
+            self.with_tuning(choice.get("refill"), choice.get("chunk"))
         return self
 
     def on_stream(self, stream) -> "QueryBuilder":
@@ -859,6 +878,8 @@ class QueryBuilder:
             C.FLAG_ENGINE_WARP if self.engine == "warp" else 0) | (
             C.FLAG_ENGINE_THREAD if self.engine == "thread" else 0) | (
             C.FLAG_ENGINE_COOP if self.engine == "coop" else 0)
+        d.tuning = (self.refill or 0) | ((int(self.chunk).bit_length() - 1) << 8
+                                         if self.chunk else 0)
         return d
 
     def traversal_stats(self):

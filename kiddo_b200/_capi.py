@@ -115,7 +115,7 @@ class QueryDesc(ctypes.Structure):
         ("abi_version", ctypes.c_uint32), ("family", ctypes.c_int32), ("metric", ctypes.c_int32),
         ("max_qty", ctypes.c_uint32), ("radius", ctypes.c_double), ("exclusive", ctypes.c_int32),
         ("sorted", ctypes.c_int32), ("periodic_box", ctypes.c_void_p), ("flags", ctypes.c_uint32),
-        ("reserved0", ctypes.c_uint32),
+        ("tuning", ctypes.c_uint32),
     ]
 
 

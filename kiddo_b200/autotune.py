@@ -1,18 +1,27 @@
 """Autotuner for the query kernels.
 
 Every knob it turns leaves results bit-identical, so it only ever measures
-time.  For a (GPU, dtype, dims, family, metric, k, tree-size) key it times, on
-a sample of the caller's own batch:
+time.  For a (GPU, dtype, dims, family, metric, k, tree-size, periodic) key it
+times, on a sample of the caller's own batch, in three stages (each stage
+keeps the best choice of the ones before it):
 
-* the engine: one warp per query (lanes scan a leaf side by side, per-level
-  continuation records in lane registers) or one thread per query
-  (continuation slots and the k-list in shared memory);
-* the processing order: as given, or bucketed by each query's straight-descent
-  leaf (KGPU_FLAG_SPATIAL_ORDER).
+1. the engine and the processing order:
+   * one warp per query (lanes scan a leaf side by side, per-level
+     continuation records in lane registers), one thread per query
+     (continuation slots and the k-list in shared memory), or, for sorted
+     nearest_n up to 32 entries, per-thread walks whose leaves the whole warp
+     scans (each leaf's rows loaded once, coalesced: the staged-leaf form);
+   * the queries as given, or bucketed by their straight-descent leaf
+     (KGPU_FLAG_SPATIAL_ORDER);
+2. the lane refill threshold of the per-thread engines: how many of a warp's
+   lanes must be idle before they take new queries (8, 16, 24, 32);
+3. the queries handed to a warp at a time (32, 64, 128, 256).
 
 The winner is cached in a JSON file (``KIDDO_B200_TUNE_CACHE`` or
 ``~/.cache/kiddo_b200/autotune.json``) and applied by
-``QueryBuilder.autotuned()``.
+``QueryBuilder.autotuned()``.  The reference's own benchmark sweeps the
+analogous knobs of its CPU path per dimensionality and query family
+(benches/v6_codspeed_queries.rs:51-70).
 """
 from __future__ import annotations
 
@@ -22,7 +31,8 @@ import os
 import threading
 
 _LOCK = threading.Lock()
-CANDIDATES = [("thread", True), ("thread", False), ("warp", True), ("warp", False)]
+REFILLS = (8, 16, 24, 32)
+CHUNKS = (32, 64, 128, 256)
 
 
 def cache_path() -> str:
@@ -60,43 +70,75 @@ def key_for(builder) -> str:
                                      k, size_bucket, builder.box is not None))
 
 
-def tune(builder, sample: int = 1 << 20, repeats: int = 3):
-    """Time every candidate on up to `sample` queries of the batch; cache and
-    return the best (engine, spatial_order)."""
+def engines_for(builder):
+    """The engines that serve this query (the cooperative scan for sorted
+    nearest_n with k <= 32, Cartesian)."""
+    from . import _capi as C
+    out = ["thread", "warp"]
+    if (builder.family in (C.NEAREST_N, C.NEAREST_N_WITHIN) and builder.sorted
+            and builder.max_qty <= 32 and builder.box is None):
+        out.append("coop")
+    return out
+
+
+def _time(builder, sub, repeats, engine, order, refill, chunk):
     import torch
+    b = _clone(builder, sub).with_engine(engine).with_spatial_order(order)
+    b.with_tuning(refill, chunk)
+    b.execute_gpu()  # warm up (first launch, allocator)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(repeats):
+        b.execute_gpu()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / repeats
+
+
+def tune(builder, sample: int = 1 << 20, repeats: int = 3):
+    """Time the candidates on up to `sample` queries of the batch, stage by
+    stage; cache and return the best {engine, spatial_order, refill, chunk}."""
     q = builder.queries
-    n = q.shape[0]
-    sub = q[: min(n, sample)]
-    best, best_ms = None, float("inf")
+    sub = q[: min(q.shape[0], sample)]
     timings = {}
-    for engine, order in CANDIDATES:
-        b = _clone(builder, sub).with_engine(engine).with_spatial_order(order)
-        b.execute_gpu()  # warm up (first launch, allocator)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(repeats):
-            b.execute_gpu()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / repeats
-        timings[f"{engine},{int(order)}"] = ms
-        if ms < best_ms:
-            best, best_ms = (engine, order), ms
+    best = None
+    for engine in engines_for(builder):
+        for order in (True, False):
+            ms = _time(builder, sub, repeats, engine, order, None, None)
+            timings[f"{engine},{int(order)}"] = ms
+            if best is None or ms < best[0]:
+                best = (ms, engine, order, None, None)
+    ms0, engine, order, _, _ = best
+    refill = chunk = None
+    if engine != "warp":  # the per-thread engines refill lanes
+        for r in REFILLS:
+            ms = _time(builder, sub, repeats, engine, order, r, None)
+            timings[f"{engine},{int(order)},refill={r}"] = ms
+            if ms < best[0]:
+                best = (ms, engine, order, r, None)
+        refill = best[3]
+    for c in CHUNKS:
+        ms = _time(builder, sub, repeats, engine, order, refill, c)
+        timings[f"{engine},{int(order)},refill={refill},chunk={c}"] = ms
+        if ms < best[0]:
+            best = (ms, engine, order, refill, c)
+    choice = {"engine": best[1], "spatial_order": bool(best[2]), "refill": best[3],
+              "chunk": best[4]}
     with _LOCK:
         db = _load()
-        db[key_for(builder)] = {"engine": best[0], "spatial_order": best[1], "ms": timings,
-                                "sample": int(sub.shape[0])}
+        db[key_for(builder)] = dict(choice, ms=timings, sample=int(sub.shape[0]))
         _store(db)
-    return best
+    return choice
 
 
 def lookup(builder):
     entry = _load().get(key_for(builder))
-    if entry is None:
+    if entry is None or "engine" not in entry:
         return None
-    return entry["engine"], bool(entry["spatial_order"])
+    return {"engine": entry["engine"], "spatial_order": bool(entry["spatial_order"]),
+            "refill": entry.get("refill"), "chunk": entry.get("chunk")}
 
 
 def _clone(builder, queries):

@@ -975,6 +975,7 @@ int32_t kgpu_query(kgpu_tree* t, const kgpu_query_desc* d, const void* queries, 
   q.nq = nq;
   apply_periodic(dt, d, q);
   q.engine = engine_of(d->flags);
+  apply_tuning(d->tuning, q);
   const bool host = (d->flags & KGPU_FLAG_HOST_BUFFERS) != 0;
   cudaError_t e = cudaSuccess;
   if (host) return query_host_pipelined(dt, d, q, queries, nq, w, out_dists, out_items, out_counts, s);
@@ -1012,6 +1013,7 @@ int32_t kgpu_query_radius_count(kgpu_tree* t, const kgpu_query_desc* d, const vo
   q.nq = nq;
   apply_periodic(dt, d, q);
   q.engine = engine_of(d->flags);
+  apply_tuning(d->tuning, q);
   q.stream = s;
   uint64_t* doff = offsets;
   if (host) {
@@ -1080,6 +1082,7 @@ int32_t kgpu_query_radius_fill(kgpu_tree* t, const kgpu_query_desc* d, const voi
   q.nq = nq;
   apply_periodic(dt, d, q);
   q.engine = engine_of(d->flags);
+  apply_tuning(d->tuning, q);
   q.stream = s;
   const uint64_t* doff = offsets;
   if (host) {
@@ -1163,6 +1166,7 @@ int32_t kgpu_query_stats(kgpu_tree* t, const kgpu_query_desc* d, const void* que
   q.nq = nq;
   apply_periodic(dt, d, q);
   q.engine = engine_of(d->flags);
+  apply_tuning(d->tuning, q);
   q.queries = dq;
   q.out_d = bd.p;
   q.out_i = bi.as<uint32_t>();

@@ -97,6 +97,7 @@ int forest_launch(kgpu_forest* f, const kgpu_query_desc* d, const void* queries,
   q.radii = radii;
   apply_periodic(f->meta, d, q);
   q.engine = engine_of(d->flags);
+  apply_tuning(d->tuning, q);
   return KGPU_OK;
 }
 

@@ -41,6 +41,10 @@ struct Batch {
   uint32_t n_trees;
   const A* __restrict__ radii;
   unsigned long long* __restrict__ work;
+  // lane-refilled drivers: queries handed to a warp at a time, and idle lanes
+  // a warp waits for before it refills them (kgpu_query_desc::tuning)
+  uint32_t chunk;
+  int refill;
 
   // A query naming no tree of the forest sees an empty tree (no results).
   __device__ __forceinline__ TreeView<A> tree(const TreeView<A>& tv, uint64_t qi) const {
@@ -238,12 +242,12 @@ __device__ __forceinline__ void flush_stats(unsigned long long* stats, const Tra
   }
 }
 
-// Queries handed out to the lanes of one warp in 64-query chunks: from the
-// batch's work counter when it has one, else chunks gw, gw + W, gw + 2W, ...
-// (gw = this warp, W = warps in the grid).  Interleaving spreads the costly
-// regions of a leaf-ordered batch evenly over the warps.
+// Queries handed out to the lanes of one warp in chunks of Batch::chunk
+// queries (64 unless tuned): from the batch's work counter when it has one,
+// else chunks gw, gw + W, gw + 2W, ... (gw = this warp, W = warps in the
+// grid).  Interleaving spreads the costly regions of a leaf-ordered batch
+// evenly over the warps.
 struct LaneFeeder {
-  static constexpr uint32_t kChunk = 64;
   uint64_t next, end, chunk, step;
   bool done;
 
@@ -259,12 +263,13 @@ struct LaneFeeder {
   __device__ __forceinline__ bool advance(const Batch<A>& b) {
     if (done) return false;
     uint64_t base;
+    const uint64_t n = b.chunk;
     if (b.work) {
       unsigned long long v = 0;
-      if ((threadIdx.x & 31) == 0) v = atomicAdd(b.work, (unsigned long long)kChunk);
+      if ((threadIdx.x & 31) == 0) v = atomicAdd(b.work, (unsigned long long)n);
       base = __shfl_sync(FULL, v, 0);
     } else {
-      base = chunk * kChunk;
+      base = chunk * n;
       chunk += step;
     }
     if (base >= b.nq) {
@@ -272,24 +277,21 @@ struct LaneFeeder {
       return false;
     }
     next = base;
-    end = base + kChunk < b.nq ? base + kChunk : b.nq;
+    end = base + n < b.nq ? base + n : b.nq;
     return true;
   }
 };
 
-// Warp-uniform: once at least KGPU_REFILL_MIN_IDLE lanes of the warp (or all
-// of them) have no query, gives each of them the next query of the batch
-// (lowest lanes first, so new queries start side by side); returns whether
-// any lane of the warp still has a query.
-#ifndef KGPU_REFILL_MIN_IDLE
-#define KGPU_REFILL_MIN_IDLE 24
-#endif
-template <typename A, int MIN_IDLE = KGPU_REFILL_MIN_IDLE>
+// Warp-uniform: once at least Batch::refill lanes of the warp (24 unless
+// tuned), or all of them, have no query, gives each of them the next query of
+// the batch (lowest lanes first, so new queries start side by side); returns
+// whether any lane of the warp still has a query.
+template <typename A>
 __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, bool& active,
                                              bool& fresh, uint64_t& qi) {
   const unsigned lane = threadIdx.x & 31;
   unsigned need = __ballot_sync(FULL, !active);
-  if (need != FULL && __popc(need) < MIN_IDLE) return true;
+  if (need != FULL && __popc(need) < b.refill) return true;
   while (need) {
     if (fd.next >= fd.end && !fd.advance(b)) break;
     const uint64_t avail = fd.end - fd.next;
@@ -315,11 +317,6 @@ __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, 
 //   whether the query needs a walk at all; finish(o, qi) runs on the whole
 //   warp for lane o's finished query.
 // ---------------------------------------------------------------------------
-// Lanes refilled together in the cooperative driver: an idle lane costs
-// walk-phase slots only there (leaf scans loop over the active lanes).
-#ifndef KGPU_COOP_REFILL_MIN_IDLE
-#define KGPU_COOP_REFILL_MIN_IDLE KGPU_REFILL_MIN_IDLE
-#endif
 template <typename A, int K, typename M, typename Walk, typename Pol, typename Start,
           typename Finish>
 __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Walk& wk,
@@ -344,7 +341,7 @@ __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A
       const int o = __ffs(fm) - 1;
       finish(o, shfl64(qi, o));
     }
-    if (!refill_lanes<A, KGPU_COOP_REFILL_MIN_IDLE>(b, fd, active, fresh, qi)) break;
+    if (!refill_lanes(b, fd, active, fresh, qi)) break;
     bool bounded = true, empty = false;
     if (fresh) {
       fresh = false;

@@ -58,6 +58,8 @@ struct QueryLaunch {
   uint32_t* out_i = nullptr;
   uint32_t* out_c = nullptr;
   unsigned long long* stats = nullptr;  // optional [stems, leaves, points] totals
+  uint32_t chunk = 64;            // queries handed to a warp at a time (lane-refilled drivers)
+  int refill = 24;                // idle lanes a warp waits for before refilling them
   int engine = 0;                 // 0 auto, 1 warp per query, 2 thread per query,
                                   // 3 thread walks with warp-cooperative leaf scans
   bool periodic = false;          // periodic boundary conditions
@@ -82,6 +84,15 @@ extern std::atomic<uint64_t> g_launches;
 inline int engine_of(uint32_t flags) {
   return (flags & KGPU_FLAG_ENGINE_WARP) ? 1 : (flags & KGPU_FLAG_ENGINE_THREAD) ? 2
          : (flags & KGPU_FLAG_ENGINE_COOP) ? 3 : 0;
+}
+
+// The launch knobs of kgpu_query_desc::tuning (KGPU_TUNE_*); 0 fields keep
+// the defaults (24 idle lanes, 64-query chunks).
+inline void apply_tuning(uint32_t tuning, QueryLaunch& q) {
+  const uint32_t refill = tuning & 0x3fu;
+  const uint32_t chunk_log2 = (tuning >> 8) & 0xfu;
+  if (refill >= 1 && refill <= 32) q.refill = int(refill);
+  if (chunk_log2 >= 5 && chunk_log2 <= 10) q.chunk = 1u << chunk_log2;
 }
 
 // Fixed-size families: dispatches to the thread engine (2-D/3-D trees) or the

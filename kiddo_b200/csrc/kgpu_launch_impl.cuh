@@ -77,6 +77,8 @@ inline Batch<A> make_batch(const QueryLaunch& q) {
   b.n_trees = q.n_trees;
   b.radii = static_cast<const A*>(q.radii);
   b.work = q.work;
+  b.chunk = q.chunk;
+  b.refill = q.refill;
   return b;
 }
 

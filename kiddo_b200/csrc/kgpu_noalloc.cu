@@ -107,6 +107,7 @@ extern "C" int32_t kgpu_query_radius_count_noalloc(kgpu_tree* t, const kgpu_quer
   q.nq = nq;
   apply_periodic(dt, d, q);
   q.engine = engine_of(d->flags);
+  apply_tuning(d->tuning, q);
   q.queries = queries;
   q.stream = s;
   if (nq) {

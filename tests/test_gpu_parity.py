@@ -294,9 +294,35 @@ def test_autotuner_caches_a_choice_and_keeps_results(tmp_path, monkeypatch):
     t = kb.ImmutableKdTree.new_from_slice(P)
     plain = t.query(Q).nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
     b = t.query(Q).nearest_n(kb.SquaredEuclidean, 16).autotuned()
-    assert b.engine in ("warp", "thread")
+    assert b.engine in ("warp", "thread", "coop")
     tuned = b.execute_gpu()
     assert torch.equal(plain.distances, tuned.distances) and torch.equal(plain.items, tuned.items)
     import json
     db = json.loads((tmp_path / "tune.json").read_text())
-    assert len(db) == 1 and len(next(iter(db.values()))["ms"]) == 4
+    entry = next(iter(db.values()))
+    assert len(db) == 1 and {"engine", "spatial_order", "refill", "chunk"} <= set(entry)
+    # stage 1 covers 3 engines x 2 orders, then 4 refill and 4 chunk settings
+    assert len(entry["ms"]) >= 6 + 4
+    # a second builder of the same kind takes the cached choice
+    b2 = t.query(Q).nearest_n(kb.SquaredEuclidean, 16).autotuned(tune_if_missing=False)
+    assert (b2.engine, b2.refill, b2.chunk) == (entry["engine"], entry["refill"], entry["chunk"])
+
+
+@pytest.mark.parametrize("engine", ["thread", "coop", "warp"])
+def test_launch_knobs_keep_results(engine):
+    """The refill threshold and the chunk size change only the schedule."""
+    import torch
+    rng = np.random.default_rng(43)
+    P = gaussian_mixture(200_000, 64, 0.01, 0.2, rng)
+    Q = torch.from_numpy(gaussian_mixture(100_000, 64, 0.01, 0.2, rng)).cuda()
+    t, o = _pair(P)
+    ref = o.nearest_n(Q.cpu().numpy(), 16)
+    for refill, chunk in ((1, 32), (8, 256), (32, 1024), (None, 128)):
+        g = (t.query(Q).with_engine(engine).with_tuning(refill, chunk)
+             .nearest_n(kb.SquaredEuclidean, 16).execute_gpu())
+        assert_same_fixed(g.distances.cpu().numpy(), g.items.cpu().numpy(), g.counts.cpu().numpy(),
+                          *ref, f"refill={refill} chunk={chunk}")
+        g = (t.query(Q).with_engine(engine).with_tuning(refill, chunk)
+             .within(kb.SquaredEuclidean, 1e-4).execute_gpu())
+        assert_same_csr((g.offsets.cpu().numpy(), g.distances.cpu().numpy(),
+                         g.items.cpu().numpy()), o.within(Q.cpu().numpy(), 1e-4), "within")
