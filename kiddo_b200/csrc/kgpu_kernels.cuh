@@ -317,11 +317,12 @@ __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, 
 //   whether the query needs a walk at all; finish(o, qi) runs on the whole
 //   warp for lane o's finished query.
 // ---------------------------------------------------------------------------
-template <typename A, int K, typename M, typename Walk, typename Pol, typename Start,
-          typename Finish>
-__device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Walk& wk,
-                                           Pol& pol, A* __restrict__ slot, int stride,
-                                           TravStats& st, Start&& start, Finish&& finish) {
+template <typename A, int K, typename M, bool kForest, typename Walk, typename Pol,
+          typename Start, typename Finish>
+__device__ __forceinline__ void coop_drive_impl(const TreeView<A>& tv0, const Batch<A>& b,
+                                                Walk& wk, Pol& pol, A* __restrict__ slot,
+                                                int stride, TravStats& st, Start&& start,
+                                                Finish&& finish) {
   const int lane = threadIdx.x & 31;
   LaneFeeder fd;
   fd.start();
@@ -345,7 +346,7 @@ __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A
     bool bounded = true, empty = false;
     if (fresh) {
       fresh = false;
-      tv = b.tree(tv0, qi);
+      if constexpr (kForest) tv = b.tree(tv0, qi);
       b.query(qi, q);
       wk.init();
       if (!start(qi, tv)) {
@@ -364,7 +365,7 @@ __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A
     uint32_t len = 0;
     if (active) {
       const uint32_t leaf = wk.descend(tv, q, pol, bounded, slot, stride, st);
-      const uint2 ex = __ldg(tv.extents + leaf);
+      const uint2 ex = wk.leaf_extents(tv, leaf);
       lb = tv.arena + size_t(ex.x) * 8;
       len = ex.y;
       st.points += len;
@@ -377,13 +378,29 @@ __device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A
   }
 }
 
+// One copy of the driver for a batch over one tree, where every lane's tree
+// is the kernel's own argument (no per-lane tree state held in registers), and
+// one for a forest batch, where each query names its tree.
+template <typename A, int K, typename M, typename Walk, typename Pol, typename Start,
+          typename Finish>
+__device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Walk& wk,
+                                           Pol& pol, A* __restrict__ slot, int stride,
+                                           TravStats& st, Start&& start, Finish&& finish) {
+  if (b.forest)
+    coop_drive_impl<A, K, M, true>(tv0, b, wk, pol, slot, stride, st, start, finish);
+  else
+    coop_drive_impl<A, K, M, false>(tv0, b, wk, pol, slot, stride, st, start, finish);
+}
+
 // The per-thread driver: lane-refilled walks, each thread scanning its own
 // leaves (the list families keep their lists in shared-memory columns).
 //   finish(qi) writes a finished query's results from its own lane.
-template <typename A, int K, typename M, typename Walk, typename Pol, typename Finish>
-__device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch<A>& b, A radius0,
-                                             Walk& wk, Pol& pol, A* __restrict__ slot, int stride,
-                                             TravStats& st, Finish&& finish) {
+template <typename A, int K, typename M, bool kForest, typename Walk, typename Pol,
+          typename Finish>
+__device__ __forceinline__ void thread_drive_impl(const TreeView<A>& tv0, const Batch<A>& b,
+                                                  A radius0, Walk& wk, Pol& pol,
+                                                  A* __restrict__ slot, int stride, TravStats& st,
+                                                  Finish&& finish) {
   LaneFeeder fd;
   fd.start();
   TreeView<A> tv = tv0;
@@ -401,7 +418,7 @@ __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch
     bool bounded = true;
     if (fresh) {
       fresh = false;
-      tv = b.tree(tv0, qi);
+      if constexpr (kForest) tv = b.tree(tv0, qi);
       b.query(qi, q);
       pol.reset(b.radius(radius0, qi));
       wk.init();
@@ -412,10 +429,21 @@ __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch
       }
     }
     if (active) {
-      st.points += pol.leaf(tv, wk.descend(tv, q, pol, bounded, slot, stride, st), q);
+      const uint32_t leaf = wk.descend(tv, q, pol, bounded, slot, stride, st);
+      st.points += pol.leaf(tv, wk.leaf_extents(tv, leaf), q);
       ++st.leaves;
     }
   }
+}
+
+template <typename A, int K, typename M, typename Walk, typename Pol, typename Finish>
+__device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch<A>& b, A radius0,
+                                             Walk& wk, Pol& pol, A* __restrict__ slot, int stride,
+                                             TravStats& st, Finish&& finish) {
+  if (b.forest)
+    thread_drive_impl<A, K, M, true>(tv0, b, radius0, wk, pol, slot, stride, st, finish);
+  else
+    thread_drive_impl<A, K, M, false>(tv0, b, radius0, wk, pol, slot, stride, st, finish);
 }
 
 // The per-thread walk of a stem order: Eytzinger arithmetic DFS (STEMS == 0)
@@ -489,7 +517,7 @@ __global__ void __launch_bounds__(256, tfixed_min_blocks<FAM, A>())
       b.query(qi, q);
       TNearestOne<A, K, M> pol;
       if (tv.leaf_count > 0) {
-        st.points += pol.leaf(tv, straight_leaf<A, K>(tv, q), q);
+        st.points += pol.leaf(tv, __ldg(tv.extents + straight_leaf<A, K>(tv, q)), q);
         st.stems += uint32_t(tv.max_stem_level + 1);
         st.leaves += 1;
       }
@@ -661,20 +689,24 @@ struct BoxArg {
 // Shared memory: the rd slot column ((max_stem_level + 2) * blockDim values
 // of A); Donnelly stems (STEMS == 1) add one u32 column of path stem indices
 // after it (periodic_smem).
-template <typename A, int K, typename M, int STEMS, typename Pol, typename Start,
+template <typename A, int K, typename M, int STEMS, bool kForest, typename Pol, typename Start,
           typename Finish>
-__device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Batch<A>& b,
-                                               const A (&box)[K], Pol& pol, A* __restrict__ slot,
-                                               int stride, TravStats& st, Start&& start,
-                                               Finish&& finish) {
+__device__ __forceinline__ void periodic_drive_impl(const TreeView<A>& tv0, const Batch<A>& b,
+                                                    const A (&box)[K], Pol& pol,
+                                                    A* __restrict__ slot, int stride,
+                                                    TravStats& st, Start&& start,
+                                                    Finish&& finish) {
   const int lane = threadIdx.x & 31;
+  // after the rd slots: for Donnelly stems the path column, then the walk's
+  // 2K cell-bound columns (periodic_smem)
+  extern __shared__ __align__(16) unsigned char psmem[];
+  size_t o = size_t(tv0.max_stem_level + 2) * stride * sizeof(A);
   uint32_t* path = nullptr;
   if constexpr (STEMS) {
-    extern __shared__ __align__(16) unsigned char psmem[];
-    path = reinterpret_cast<uint32_t*>(psmem + size_t(tv0.max_stem_level + 2) * stride *
-                                                   sizeof(A)) + threadIdx.x;
+    path = reinterpret_cast<uint32_t*>(psmem + o) + threadIdx.x;
+    o += size_t(tv0.max_stem_level + 2) * stride * sizeof(uint32_t);
   }
-  PeriodicWalk<A, K, M, STEMS> wk(path, stride);
+  PeriodicWalk<A, K, M, STEMS> wk(path, reinterpret_cast<A*>(psmem + o) + threadIdx.x, stride);
   wk.init(box);
   LaneFeeder fd;
   fd.start();
@@ -693,7 +725,7 @@ __device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Bat
     if (!refill_lanes(b, fd, active, fresh, qi)) break;
     if (fresh) {
       fresh = false;
-      tv = b.tree(tv0, qi);
+      if constexpr (kForest) tv = b.tree(tv0, qi);
       b.query(qi, q);
       wk.init(box);
       if (!start(qi)) {
@@ -723,6 +755,18 @@ __device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Bat
       pol.leaf(o, shfl64(qi, o), coop_leaf<A, K>(o, lb, len, q), lane);
     }
   }
+}
+
+template <typename A, int K, typename M, int STEMS, typename Pol, typename Start,
+          typename Finish>
+__device__ __forceinline__ void periodic_drive(const TreeView<A>& tv0, const Batch<A>& b,
+                                               const A (&box)[K], Pol& pol, A* __restrict__ slot,
+                                               int stride, TravStats& st, Start&& start,
+                                               Finish&& finish) {
+  if (b.forest)
+    periodic_drive_impl<A, K, M, STEMS, true>(tv0, b, box, pol, slot, stride, st, start, finish);
+  else
+    periodic_drive_impl<A, K, M, STEMS, false>(tv0, b, box, pol, slot, stride, st, start, finish);
 }
 
 // Periodic nearest_n / nearest_n().within (always sorted, periodic.rs
@@ -784,11 +828,11 @@ __global__ void __launch_bounds__(256) k_tperiodic_nn1(TreeView<A> tv0, Batch<A>
       if (tv.size != 0) {
         wk.init();
         uint32_t leaf = wk.descend(tv, qq, pol, !pol.unbounded_start(), slot, stride, st);
-        st.points += pol.leaf(tv, leaf, qq);
+        st.points += pol.leaf(tv, wk.leaf_extents(tv, leaf), qq);
         ++st.leaves;
         while (wk.backtrack(tv, qq, pol, slot, stride)) {
           leaf = wk.descend(tv, qq, pol, true, slot, stride, st);
-          st.points += pol.leaf(tv, leaf, qq);
+          st.points += pol.leaf(tv, wk.leaf_extents(tv, leaf), qq);
           ++st.leaves;
         }
       }

@@ -95,11 +95,13 @@ inline size_t thread_smem(const DeviceTree& t) {
   return size_t(t.max_stem_level + 2) * 256 * sizeof(A);
 }
 
-// Dynamic shared memory of the periodic per-thread walks: the rd slots, plus
-// for Donnelly stems a column of path stem indices.
+// Dynamic shared memory of the periodic per-thread walks: the rd slots, for
+// Donnelly stems a column of path stem indices, then 2K columns of cell
+// bounds per thread.
 template <typename A>
 inline size_t periodic_smem(const DeviceTree& t, int stems) {
-  return thread_smem<A>(t) + (stems ? size_t(t.max_stem_level + 2) * 256 * sizeof(uint32_t) : 0);
+  return thread_smem<A>(t) + (stems ? size_t(t.max_stem_level + 2) * 256 * sizeof(uint32_t) : 0) +
+         size_t(2 * t.dims) * 256 * sizeof(A);
 }
 
 // 2-D and 3-D trees have thread-per-query kernels; other dimensionalities use

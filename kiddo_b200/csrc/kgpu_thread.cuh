@@ -32,10 +32,9 @@ namespace kgpu {
 // both points of a pair go through one call site of f, so the policy's
 // insertion code is emitted once.
 template <typename A, int K, typename D, typename P, typename F>
-__device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint32_t leaf,
+__device__ __forceinline__ uint32_t thread_for_each_point(const TreeView<A>& tv, uint2 ex,
                                                           const D& dist, P&& pass, F&& f) {
   constexpr uint32_t per = K * sizeof(A) + sizeof(uint32_t);
-  const uint2 ex = __ldg(tv.extents + leaf);
   const uint8_t* base = tv.arena + size_t(ex.x) * 8;
   if constexpr (RowLeaves<A, K>::value) {
     // rows: one row per step, the leaf's lines requested up front
@@ -248,6 +247,10 @@ struct ThreadWalk {
     }
     return false;
   }
+
+  __device__ __forceinline__ uint2 leaf_extents(const TreeView<A>& tv, uint32_t l) const {
+    return __ldg(tv.extents + l);
+  }
 };
 
 // Per-thread scalar backtracking, the reference's path for Donnelly<bh>
@@ -272,6 +275,10 @@ struct DonnellyWalk {
   uint32_t* __restrict__ stem_slot;
 
   __device__ DonnellyWalk(A* offs, uint32_t* stems) : off_slot(offs), stem_slot(stems) {}
+
+  __device__ __forceinline__ uint2 leaf_extents(const TreeView<A>& tv, uint32_t l) const {
+    return __ldg(tv.extents + l);
+  }
 
   __device__ __forceinline__ void init() {
 #pragma unroll
@@ -361,19 +368,28 @@ struct DonnellyWalk {
 // the stem index of each level of its path in a column (path[L * stride])
 // and the leaf index in `leaf`, one path bit per level; the traversal is the
 // same (periodic.rs drives both stem orders through the StemStrategy trait).
+// The cell bounds (lower and upper of every axis) live in 2K shared-memory
+// columns of the thread (`bnd`: lower of axis d at d * pstride, upper at
+// (K + d) * pstride), so they hold no registers while the warp scans leaves.
 template <typename A, int K, typename M, int STEMS = 0>
 struct PeriodicWalk {
   static constexpr uint32_t kDone = 0xffffffffu;
-  A lo[K], hi[K], off[K];
+  A off[K];
   A rd;
   uint32_t stem_idx, leaf;
   int level;
   uint32_t frames, split, lo_set, hi_set;
   bool at_leaf;
   uint32_t* __restrict__ path;  // Donnelly: this thread's column of path stem indices
+  A* __restrict__ bnd;          // this thread's cell-bound columns
   int pstride;
 
-  __device__ explicit PeriodicWalk(uint32_t* p = nullptr, int ps = 0) : path(p), pstride(ps) {}
+  __device__ PeriodicWalk(uint32_t* p, A* bounds, int ps) : path(p), bnd(bounds), pstride(ps) {}
+
+  __device__ __forceinline__ A lo(int d) const { return bnd[d * pstride]; }
+  __device__ __forceinline__ A hi(int d) const { return bnd[(K + d) * pstride]; }
+  __device__ __forceinline__ void set_lo(int d, A v) { bnd[d * pstride] = v; }
+  __device__ __forceinline__ void set_hi(int d, A v) { bnd[(K + d) * pstride] = v; }
 
   __device__ __forceinline__ static uint32_t axis_levels(int d) {
     uint32_t m = 0;
@@ -384,8 +400,8 @@ struct PeriodicWalk {
   __device__ __forceinline__ void init(const A (&box)[K]) {
 #pragma unroll
     for (int d = 0; d < K; ++d) {
-      lo[d] = A(0);
-      hi[d] = box[d];
+      set_lo(d, A(0));
+      set_hi(d, box[d]);
       off[d] = A(0);
     }
     rd = A(0);
@@ -414,24 +430,31 @@ struct PeriodicWalk {
     const uint32_t parent = STEMS ? path[P * pstride] : stem_idx >> (level - P);
     const uint32_t below = (1u << P) - 1u;
 #pragma unroll
+    const int dP = P % K;
+    A old_lo = A(0), old_hi = A(0);
+#pragma unroll
     for (int d = 0; d < K; ++d) {
       const uint32_t am = axis_levels(d) & below;
       const uint32_t ml = lo_set & am, mh = hi_set & am;
-      lo[d] = ml ? __ldg(tv.stems + ancestor(parent, P, 31 - __clz(ml))) : A(0);
-      hi[d] = mh ? __ldg(tv.stems + ancestor(parent, P, 31 - __clz(mh))) : box[d];
-      off[d] = (split & am) ? periodic_interval_distance(q[d], lo[d], hi[d], box[d]) : A(0);
+      const A l = ml ? __ldg(tv.stems + ancestor(parent, P, 31 - __clz(ml))) : A(0);
+      const A h = mh ? __ldg(tv.stems + ancestor(parent, P, 31 - __clz(mh))) : box[d];
+      set_lo(d, l);
+      set_hi(d, h);
+      off[d] = (split & am) ? periodic_interval_distance(q[d], l, h, box[d]) : A(0);
+      if (d == dP) {
+        old_lo = l;
+        old_hi = h;
+      }
     }
-    const int dP = P % K;
     const A pivot = __ldg(tv.stems + parent);
     const A qd = sel(q, dP);
     const bool is_right = qd >= pivot;
-    const A old_lo = sel(lo, dP), old_hi = sel(hi, dP);
     const A minup = old_hi < pivot ? old_hi : pivot;
     const A maxlo = max_ref(old_lo, pivot);
     const A far_lo = is_right ? old_lo : maxlo;
     const A far_hi = is_right ? minup : old_hi;
-    put(lo, dP, far_lo);
-    put(hi, dP, far_hi);
+    set_lo(dP, far_lo);
+    set_hi(dP, far_hi);
     put(off, dP, periodic_interval_distance(qd, far_lo, far_hi, sel(box, dP)));
     rd = slot[FL * stride];
     split &= below;
@@ -492,7 +515,7 @@ struct PeriodicWalk {
         dim = dim + 1 == K ? 0 : dim + 1;
         continue;
       }
-      const A old_lo = sel(lo, dim), old_hi = sel(hi, dim);
+      const A old_lo = lo(dim), old_hi = hi(dim);
       const A qd = sel(q, dim), Ld = sel(box, dim);
       const bool is_right = qd >= pivot;
       const A minup = old_hi < pivot ? old_hi : pivot;
@@ -521,8 +544,8 @@ struct PeriodicWalk {
       split |= bit;
       if (is_right && pivot > old_lo) lo_set |= bit;
       if (!is_right && !(old_hi < pivot)) hi_set |= bit;
-      put(lo, dim, near_lo);
-      put(hi, dim, near_hi);
+      set_lo(dim, near_lo);
+      set_hi(dim, near_hi);
       put(off, dim, near_off);
       rd = near_rd;
       if constexpr (STEMS) {
@@ -588,10 +611,10 @@ struct TNearestOne {
   __device__ __forceinline__ void reset(A) { best = inf_of<A>(); item = 0; }
   __device__ __forceinline__ A max_dist() const { return best; }
   __device__ __forceinline__ bool unbounded_start() const { return true; }
-  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint2 ex, const A (&q)[K]) {
     const CartesianQ<A, K, M> dist{q};
     return thread_for_each_point<A, K>(
-        tv, l, dist, [&](A d) { return d < best; },
+        tv, ex, dist, [&](A d) { return d < best; },
         [&](A d, uint32_t it) {
           if (d < best) { best = d; item = it; }
         });
@@ -717,7 +740,7 @@ struct TNearestN {
   // order together, each re-read from L1 and re-tested against the current
   // kth.  The add() calls are the sequential ones minus those add() would
   // reject, so the list is the same.
-  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint2 ex, const A (&q)[K]) {
     // The mark "d within the leaf-start bound, and below kth when the list
     // started full" as one test d <= gate: strict comparisons become <= on
     // the next value down.
@@ -730,7 +753,6 @@ struct TNearestN {
       gate = kth <= radius ? below(kth) : radius;
     }
     const CartesianQ<A, K, M> dist{q};
-    const uint2 ex = __ldg(tv.extents + l);
     const uint8_t* base = tv.arena + size_t(ex.x) * 8;
     const uint32_t len = ex.y;
     // every 128-byte line of the leaf's rows requested up front, so the scan's
@@ -824,12 +846,12 @@ struct TBestN {
     ld[j * stride] = d;
     li[j * stride] = it;
   }
-  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint32_t l, const A (&q)[K]) {
+  __device__ __forceinline__ uint32_t leaf(const TreeView<A>& tv, uint2 ex, const A (&q)[K]) {
     const bool full_at_entry = n == k;
     const uint32_t thr_item = full_at_entry ? li[(k - 1) * stride] : 0u;
     const CartesianQ<A, K, M> dist{q};
     return thread_for_each_point<A, K>(
-        tv, l, dist, [&](A d) { return kExclusive ? (d < radius) : (d <= radius); },
+        tv, ex, dist, [&](A d) { return kExclusive ? (d < radius) : (d <= radius); },
         [&](A d, uint32_t it) {
           if (!(kExclusive ? (d < radius) : (d <= radius))) return;
           if (full_at_entry && it >= thr_item) return;
