@@ -317,12 +317,11 @@ __device__ __forceinline__ bool refill_lanes(const Batch<A>& b, LaneFeeder& fd, 
 //   whether the query needs a walk at all; finish(o, qi) runs on the whole
 //   warp for lane o's finished query.
 // ---------------------------------------------------------------------------
-template <typename A, int K, typename M, bool kForest, typename Walk, typename Pol,
-          typename Start, typename Finish>
-__device__ __forceinline__ void coop_drive_impl(const TreeView<A>& tv0, const Batch<A>& b,
-                                                Walk& wk, Pol& pol, A* __restrict__ slot,
-                                                int stride, TravStats& st, Start&& start,
-                                                Finish&& finish) {
+template <typename A, int K, typename M, typename Walk, typename Pol, typename Start,
+          typename Finish>
+__device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Walk& wk,
+                                           Pol& pol, A* __restrict__ slot, int stride,
+                                           TravStats& st, Start&& start, Finish&& finish) {
   const int lane = threadIdx.x & 31;
   LaneFeeder fd;
   fd.start();
@@ -346,7 +345,7 @@ __device__ __forceinline__ void coop_drive_impl(const TreeView<A>& tv0, const Ba
     bool bounded = true, empty = false;
     if (fresh) {
       fresh = false;
-      if constexpr (kForest) tv = b.tree(tv0, qi);
+      tv = b.tree(tv0, qi);
       b.query(qi, q);
       wk.init();
       if (!start(qi, tv)) {
@@ -378,19 +377,6 @@ __device__ __forceinline__ void coop_drive_impl(const TreeView<A>& tv0, const Ba
   }
 }
 
-// One copy of the driver for a batch over one tree, where every lane's tree
-// is the kernel's own argument (no per-lane tree state held in registers), and
-// one for a forest batch, where each query names its tree.
-template <typename A, int K, typename M, typename Walk, typename Pol, typename Start,
-          typename Finish>
-__device__ __forceinline__ void coop_drive(const TreeView<A>& tv0, const Batch<A>& b, Walk& wk,
-                                           Pol& pol, A* __restrict__ slot, int stride,
-                                           TravStats& st, Start&& start, Finish&& finish) {
-  if (b.forest)
-    coop_drive_impl<A, K, M, true>(tv0, b, wk, pol, slot, stride, st, start, finish);
-  else
-    coop_drive_impl<A, K, M, false>(tv0, b, wk, pol, slot, stride, st, start, finish);
-}
 
 // The per-thread driver: lane-refilled walks, each thread scanning its own
 // leaves (the list families keep their lists in shared-memory columns).
@@ -436,6 +422,11 @@ __device__ __forceinline__ void thread_drive_impl(const TreeView<A>& tv0, const 
   }
 }
 
+// One copy of the driver for a batch over one tree, where every lane's tree
+// is the kernel's own argument (no per-lane tree state held in registers), and
+// one for a forest batch, where each query names its tree.  (The cooperative
+// driver keeps one copy: with two, the 256-catalogue forest's radius queries
+// ran 8% slower.)
 template <typename A, int K, typename M, typename Walk, typename Pol, typename Finish>
 __device__ __forceinline__ void thread_drive(const TreeView<A>& tv0, const Batch<A>& b, A radius0,
                                              Walk& wk, Pol& pol, A* __restrict__ slot, int stride,
@@ -698,7 +689,7 @@ __device__ __forceinline__ void periodic_drive_impl(const TreeView<A>& tv0, cons
                                                     Finish&& finish) {
   const int lane = threadIdx.x & 31;
   // after the rd slots: for Donnelly stems the path column, then the walk's
-  // 2K cell-bound columns (periodic_smem)
+  // 3K cell-state columns (periodic_smem)
   extern __shared__ __align__(16) unsigned char psmem[];
   size_t o = size_t(tv0.max_stem_level + 2) * stride * sizeof(A);
   uint32_t* path = nullptr;

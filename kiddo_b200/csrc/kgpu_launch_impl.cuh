@@ -96,12 +96,12 @@ inline size_t thread_smem(const DeviceTree& t) {
 }
 
 // Dynamic shared memory of the periodic per-thread walks: the rd slots, for
-// Donnelly stems a column of path stem indices, then 2K columns of cell
-// bounds per thread.
+// Donnelly stems a column of path stem indices, then 3K columns of cell state
+// (bounds and offsets) per thread.
 template <typename A>
 inline size_t periodic_smem(const DeviceTree& t, int stems) {
   return thread_smem<A>(t) + (stems ? size_t(t.max_stem_level + 2) * 256 * sizeof(uint32_t) : 0) +
-         size_t(2 * t.dims) * 256 * sizeof(A);
+         size_t(3 * t.dims) * 256 * sizeof(A);
 }
 
 // 2-D and 3-D trees have thread-per-query kernels; other dimensionalities use

@@ -368,13 +368,13 @@ struct DonnellyWalk {
 // the stem index of each level of its path in a column (path[L * stride])
 // and the leaf index in `leaf`, one path bit per level; the traversal is the
 // same (periodic.rs drives both stem orders through the StemStrategy trait).
-// The cell bounds (lower and upper of every axis) live in 2K shared-memory
-// columns of the thread (`bnd`: lower of axis d at d * pstride, upper at
-// (K + d) * pstride), so they hold no registers while the warp scans leaves.
+// The cell state (lower bound, upper bound and interval offset of every
+// axis) lives in 3K shared-memory columns of the thread (`bnd`: lower of axis
+// d at d * pstride, upper at (K + d) * pstride, offset at (2K + d) * pstride),
+// so it holds no registers while the warp scans leaves.
 template <typename A, int K, typename M, int STEMS = 0>
 struct PeriodicWalk {
   static constexpr uint32_t kDone = 0xffffffffu;
-  A off[K];
   A rd;
   uint32_t stem_idx, leaf;
   int level;
@@ -390,6 +390,19 @@ struct PeriodicWalk {
   __device__ __forceinline__ A hi(int d) const { return bnd[(K + d) * pstride]; }
   __device__ __forceinline__ void set_lo(int d, A v) { bnd[d * pstride] = v; }
   __device__ __forceinline__ void set_hi(int d, A v) { bnd[(K + d) * pstride] = v; }
+  __device__ __forceinline__ A off(int d) const { return bnd[(2 * K + d) * pstride]; }
+  __device__ __forceinline__ void set_off(int d, A v) { bnd[(2 * K + d) * pstride] = v; }
+  // the metric's rect_dist_after_update with axis `dim`'s offset replaced
+  __device__ __forceinline__ A rect_after(int dim, A new_off) const {
+    if constexpr (M::kAdditive) {
+      return M::template rect<A>(rd, off(dim), new_off);
+    } else {
+      A o[K];
+#pragma unroll
+      for (int d = 0; d < K; ++d) o[d] = off(d);
+      return M::template rect_k<A, K>(rd, o, dim, new_off);
+    }
+  }
 
   __device__ __forceinline__ static uint32_t axis_levels(int d) {
     uint32_t m = 0;
@@ -402,7 +415,7 @@ struct PeriodicWalk {
     for (int d = 0; d < K; ++d) {
       set_lo(d, A(0));
       set_hi(d, box[d]);
-      off[d] = A(0);
+      set_off(d, A(0));
     }
     rd = A(0);
     stem_idx = STEMS ? 0u : 1u;
@@ -429,7 +442,6 @@ struct PeriodicWalk {
     const int P = FL - 1;
     const uint32_t parent = STEMS ? path[P * pstride] : stem_idx >> (level - P);
     const uint32_t below = (1u << P) - 1u;
-#pragma unroll
     const int dP = P % K;
     A old_lo = A(0), old_hi = A(0);
 #pragma unroll
@@ -440,7 +452,7 @@ struct PeriodicWalk {
       const A h = mh ? __ldg(tv.stems + ancestor(parent, P, 31 - __clz(mh))) : box[d];
       set_lo(d, l);
       set_hi(d, h);
-      off[d] = (split & am) ? periodic_interval_distance(q[d], l, h, box[d]) : A(0);
+      set_off(d, (split & am) ? periodic_interval_distance(q[d], l, h, box[d]) : A(0));
       if (d == dP) {
         old_lo = l;
         old_hi = h;
@@ -455,7 +467,7 @@ struct PeriodicWalk {
     const A far_hi = is_right ? minup : old_hi;
     set_lo(dP, far_lo);
     set_hi(dP, far_hi);
-    put(off, dP, periodic_interval_distance(qd, far_lo, far_hi, sel(box, dP)));
+    set_off(dP, periodic_interval_distance(qd, far_lo, far_hi, sel(box, dP)));
     rd = slot[FL * stride];
     split &= below;
     lo_set &= below;
@@ -526,8 +538,8 @@ struct PeriodicWalk {
       const A far_hi = is_right ? minup : old_hi;
       const A near_off = periodic_interval_distance(qd, near_lo, near_hi, Ld);
       const A far_off = periodic_interval_distance(qd, far_lo, far_hi, Ld);
-      const A near_rd = M::template rect_k<A, K>(rd, off, dim, near_off);
-      const A far_rd = M::template rect_k<A, K>(rd, off, dim, far_off);
+      const A near_rd = rect_after(dim, near_off);
+      const A far_rd = rect_after(dim, far_off);
       const A thr = pol.max_dist();
       const bool near_pruned = near_rd > thr || (P::kPruneOnEqual && near_rd == thr);
       const bool far_pruned = far_rd > thr || (P::kPruneOnEqual && far_rd == thr);
@@ -546,7 +558,7 @@ struct PeriodicWalk {
       if (!is_right && !(old_hi < pivot)) hi_set |= bit;
       set_lo(dim, near_lo);
       set_hi(dim, near_hi);
-      put(off, dim, near_off);
+      set_off(dim, near_off);
       rd = near_rd;
       if constexpr (STEMS) {
         uint32_t l, r;
