@@ -450,7 +450,10 @@ def run_tree_workload(args, workload, rank, world, steps, warmup, points=0, quer
 
     w = k if fam in ("nearest_n", "periodic_nearest_n_within") else 1
     h2d = nq * 3 * Q.itemsize
-    d2h = nq * w * (Q.itemsize + 4) + (nq * 4 if w > 1 else 0)
+    # per-row counts cross the bus only where they vary (nearest_n without a
+    # radius has min(k, size) in every row, written on the host)
+    d2h = nq * w * (Q.itemsize + 4) + (nq * 4 if w > 1 and fam != "nearest_n" else 0)
+    out_bytes = nq * w * (Q.itemsize + 4) + (nq * 4 if w > 1 else 0)  # written to HBM
     value = world * nq * steps / (total_ms_max / 1e3)
     e2e_val = world * nq * e2e_steps / (e2e_ms / 1e3)
     kern_ms = total_ms / steps
@@ -459,7 +462,7 @@ def run_tree_workload(args, workload, rank, world, steps, warmup, points=0, quer
     traffic = profile_traffic(workload)
     # compulsory bytes: the whole tree once, the queries once, the results once
     tree_bytes = sum(a.nbytes for a in (tree.stems(), tree.leaf_bytes(), tree.leaf_extents()))
-    compulsory = tree_bytes + h2d + d2h
+    compulsory = tree_bytes + h2d + out_bytes
     comp_gbs = compulsory / (kern_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,

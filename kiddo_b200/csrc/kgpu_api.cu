@@ -10,6 +10,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -843,6 +844,19 @@ int out_width(const kgpu_query_desc* d) {
              : int(d->max_qty);
 }
 
+// Counts the rows of a nearest_n chunk holding fewer than `full` entries
+// (min(k, size); a row falls short only when its query's distances are NaN,
+// which no candidate passes, or the tree's points hold NaN).
+__global__ void k_short_rows(const uint32_t* __restrict__ counts, uint64_t n, uint32_t full,
+                             uint32_t* __restrict__ out) {
+  uint32_t m = 0;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x)
+    m += counts[i] != full ? 1u : 0u;
+  m = __reduce_add_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(out, m);
+}
+
 #ifndef KGPU_HOST_SLOTS
 #define KGPU_HOST_SLOTS 3
 #endif
@@ -869,8 +883,33 @@ int query_host_pipelined(const DeviceTree& dt, const kgpu_query_desc* d, const Q
   const uint64_t chunk = std::min<uint64_t>(nq, uint64_t(1) << KGPU_HOST_CHUNK_LOG2);
   const int nslots = int(std::min<uint64_t>(kSlots, (nq + chunk - 1) / chunk));
   cudaStream_t st[kSlots] = {};
+  // nearest_n without a radius fills min(k, size) entries in every row whose
+  // query has comparable distances, so those counts are written on the host
+  // while the device works instead of crossing the bus.  The rows' counts stay
+  // on the device (all_counts), a small kernel counts each chunk's rows short
+  // of that, and only chunks with such rows are copied back at the end.
+  uint32_t* const host_counts = out_counts;
+  const bool counts_known = out_counts && d->family == KGPU_NEAREST_N;
+  const uint32_t full = uint32_t(std::min<uint64_t>(uint64_t(w), dt.size));
+  const uint64_t edge = std::max<uint64_t>(1, chunk / KGPU_HOST_EDGE_DIV);
+  const uint64_t max_chunks = (nq + edge - 1) / edge + 1;
+  DevBuf all_counts, short_rows;
+  std::vector<std::pair<uint64_t, uint64_t>> spans;  // (first query, length) per chunk
+  cudaError_t e = cudaSuccess;
+  if (counts_known) {
+    out_counts = nullptr;
+    if ((e = all_counts.alloc(nq * 4, s)) == cudaSuccess &&
+        (e = short_rows.alloc(max_chunks * 4, s)) == cudaSuccess)
+      e = cudaMemsetAsync(short_rows.p, 0, max_chunks * 4, s);
+  }
+  auto count_short_rows = [&](uint64_t c0, uint64_t nc, uint64_t ci, cudaStream_t ss) {
+    k_short_rows<<<148 * 2, 256, 0, ss>>>(all_counts.as<uint32_t>() + c0, nc, full,
+                                          short_rows.as<uint32_t>() + ci);
+    ++g_launches;
+    return cudaGetLastError();
+  };
   cudaEvent_t ready = nullptr;
-  cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventRecord(ready, s);
   for (int i = 0; i < nslots && e == cudaSuccess; ++i) {
     e = cudaStreamCreateWithFlags(&st[i], cudaStreamNonBlocking);
@@ -892,7 +931,6 @@ int query_host_pipelined(const DeviceTree& dt, const kgpu_query_desc* d, const Q
     // chunk's kernel runs before any result can leave, and the last chunk's
     // results leave after every kernel, so shorter ends shorten the
     // unoverlapped head and tail (kNN16 over 16M queries: 50.9 -> 47.1 ms).
-    const uint64_t edge = std::max<uint64_t>(1, chunk / KGPU_HOST_EDGE_DIV);
     auto chunk_len = [&](uint64_t c0) -> uint64_t {
       const uint64_t rem = nq - c0;
       if (nslots == 1 || rem <= edge) return rem;
@@ -910,7 +948,8 @@ int query_host_pipelined(const DeviceTree& dt, const kgpu_query_desc* d, const Q
       q.queries = bq[slot].p;
       q.out_d = bd[slot].p;
       q.out_i = bi[slot].as<uint32_t>();
-      q.out_c = out_counts ? bc[slot].as<uint32_t>() : nullptr;
+      q.out_c = counts_known ? all_counts.as<uint32_t>() + c0
+                             : out_counts ? bc[slot].as<uint32_t>() : nullptr;
       q.stream = ss;
       const char* what = nullptr;
       if ((e = cudaMemcpyAsync(bq[slot].p, static_cast<const uint8_t*>(queries) + c0 * dt.dims * sa,
@@ -928,6 +967,8 @@ int query_host_pipelined(const DeviceTree& dt, const kgpu_query_desc* d, const Q
         else if ((e = dt.dtype == KGPU_F64 ? run_fixed<double>(dt, q) : run_fixed<float>(dt, q)) !=
                  cudaSuccess)
           what = "launching the query kernel";
+        else if (counts_known && (e = count_short_rows(c0, nc, ci, ss)) != cudaSuccess)
+          what = "checking the rows' counts";
         else if ((e = cudaMemcpyAsync(static_cast<uint8_t*>(out_dists) + c0 * w * sa, bd[slot].p,
                                       nc * w * sa, cudaMemcpyDeviceToHost, ss)) != cudaSuccess ||
                  (e = cudaMemcpyAsync(out_items + c0 * w, bi[slot].p, nc * w * 4,
@@ -937,10 +978,22 @@ int query_host_pipelined(const DeviceTree& dt, const kgpu_query_desc* d, const Q
           what = "copying results to the host";
       }
       if (what) status = cuda_fail(e, what);
+      spans.emplace_back(c0, nc);
     }
+    if (counts_known && status == KGPU_OK) std::fill(host_counts, host_counts + nq, full);
     for (int i = 0; i < nslots; ++i)
       if (st[i] && (e = cudaStreamSynchronize(st[i])) != cudaSuccess && status == KGPU_OK)
         status = cuda_fail(e, "query execution");
+    if (counts_known && status == KGPU_OK) {
+      // the chunks with short rows, if any, bring their counts back
+      std::vector<uint32_t> shorts(spans.size());
+      e = cudaMemcpy(shorts.data(), short_rows.p, spans.size() * 4, cudaMemcpyDeviceToHost);
+      for (size_t i = 0; i < spans.size() && e == cudaSuccess; ++i)
+        if (shorts[i])
+          e = cudaMemcpy(host_counts + spans[i].first, all_counts.as<uint32_t>() + spans[i].first,
+                         spans[i].second * 4, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) status = cuda_fail(e, "copying results to the host");
+    }
   }  // device buffers are released on their streams here
   for (int i = 0; i < nslots; ++i)
     if (st[i]) {

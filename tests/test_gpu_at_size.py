@@ -64,6 +64,15 @@ def test_host_pipeline_multi_chunk(nq):
     g = t.query(Q).nearest_n(SE, 16).execute_gpu()
     assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Q, 16), "host knn16")
     del g
+    # rows whose query holds a NaN find no candidate (count 0): the pipeline
+    # fills nearest_n's counts on the host and brings back the chunks with
+    # short rows, here the first chunk and a later one
+    Qn = Q.copy()
+    Qn[[3, 17, nq - 5, nq // 2]] = np.nan
+    g = t.query(Qn).nearest_n(SE, 16).execute_gpu()
+    assert_same_fixed(g.distances, g.items, g.counts, *o.nearest_n(Qn, 16), "host knn16 nan rows")
+    assert (g.counts == 0).sum() == 4
+    del g, Qn
     g = t.query(Q).nearest_one(SE).execute_gpu()
     od, oi = o.nearest_one(Q)
     assert_same_fixed(g.distances, g.items, np.ones(nq), od, oi, np.ones(nq), "host nn1")

@@ -198,6 +198,15 @@ def test_device_buffers_match_host_buffers():
     torch.cuda.synchronize()
     assert np.array_equal(d.distances.cpu().numpy(), h.distances)
     assert np.array_equal(d.items.cpu().numpy().view(np.uint32), h.items)
+    # host buffers fill nearest_n's counts as min(k, size) on the host and
+    # copy back only chunks with shorter rows (NaN queries find nothing)
+    assert np.array_equal(d.counts.cpu().numpy().view(np.uint32), h.counts)
+    Qn = Q.copy()
+    Qn[::997] = np.nan
+    hn = t.query(Qn).nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
+    dn = t.query(torch.from_numpy(Qn).cuda()).nearest_n(kb.SquaredEuclidean, 16).execute_gpu()
+    assert np.array_equal(dn.counts.cpu().numpy().view(np.uint32), hn.counts)
+    assert np.all(hn.counts[::997] == 0) and (hn.counts == 16).sum() == len(Q) - len(Q[::997])
     hw = t.query(Q).within(kb.SquaredEuclidean, 1e-4).execute_gpu()
     dw = t.query(dq).within(kb.SquaredEuclidean, 1e-4).execute_gpu()
     assert np.array_equal(dw.offsets.cpu().numpy().astype(np.uint64), hw.offsets)
