@@ -23,6 +23,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-f
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]
 
 CU_SOURCES = ["kgpu_api.cu", "kgpu_scan.cu", "kgpu_noalloc.cu", "kgpu_forest.cu",
+              "kgpu_periodic_fast.cu",
               "kgpu_build.cu",
               "kgpu_chamfer.cu",
               "kgpu_points.cu",

@@ -836,7 +836,11 @@ cudaError_t maybe_spatial_order(const DeviceTree& dt, const kgpu_query_desc* d, 
 }
 
 template <typename A>
-cudaError_t run_fixed(const DeviceTree& dt, QueryLaunch& q) { return launch_fixed<A>(dt, q); }
+cudaError_t run_fixed(const DeviceTree& dt, QueryLaunch& q) {
+  bool handled = false;
+  const cudaError_t e = periodic_fast<A>(dt, q, handled);
+  return handled ? e : launch_fixed<A>(dt, q);
+}
 
 int out_width(const kgpu_query_desc* d) {
   return (d->family == KGPU_NEAREST_ONE || d->family == KGPU_APPROX_NEAREST_ONE)

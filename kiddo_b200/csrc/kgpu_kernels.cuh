@@ -45,6 +45,9 @@ struct Batch {
   // a warp waits for before it refills them (kgpu_query_desc::tuning)
   uint32_t chunk;
   int refill;
+  // when set, a device count that bounds nq (a compacted `order` list whose
+  // length the host has not read)
+  const unsigned long long* nq_dev = nullptr;
 
   // A query naming no tree of the forest sees an empty tree (no results).
   __device__ __forceinline__ TreeView<A> tree(const TreeView<A>& tv, uint64_t qi) const {
@@ -272,12 +275,17 @@ struct LaneFeeder {
       base = chunk * n;
       chunk += step;
     }
-    if (base >= b.nq) {
+    uint64_t nq = b.nq;
+    if (b.nq_dev) {
+      const uint64_t m = *b.nq_dev;
+      nq = m < nq ? m : nq;
+    }
+    if (base >= nq) {
       done = true;
       return false;
     }
     next = base;
-    end = base + n < b.nq ? base + n : b.nq;
+    end = base + n < nq ? base + n : nq;
     return true;
   }
 };

@@ -42,6 +42,11 @@ struct DeviceTree {
   uint32_t* sorted_items = nullptr;
   uint32_t* sorted_ranks = nullptr;
   int items_distinct = -1;     // -1: not checked yet; 0: two entries share an item; 1: distinct
+  // per-axis bounds of the stored points, measured on first use by periodic
+  // queries (kgpu_periodic_fast.cu): -1 not measured, 0 unusable (no points,
+  // or a NaN coordinate), 1 measured
+  mutable int point_bounds = -1;
+  mutable double point_lo[4] = {0, 0, 0, 0}, point_hi[4] = {0, 0, 0, 0};
 };
 
 struct QueryLaunch {
@@ -72,6 +77,7 @@ struct QueryLaunch {
   uint64_t total_leaves = 0;             // leaves of all trees (spatial order)
   const void* radii = nullptr;           // per-query radius (A), or null
   unsigned long long* work = nullptr;    // work-queue counter (zeroed), or null
+  const unsigned long long* nq_dev = nullptr;  // device count bounding nq (lane-refilled drivers)
   uint64_t capacity = ~uint64_t(0);      // fill pass: hits that fit the output
   int* status = nullptr;                 // fill pass: set to KGPU_EOVERFLOW on mismatch
   cudaStream_t stream = nullptr;
@@ -98,6 +104,13 @@ inline void apply_tuning(uint32_t tuning, QueryLaunch& q) {
 // Fixed-size families: dispatches to the thread engine (2-D/3-D trees) or the
 // warp engine (everything else, periodic included).
 template <typename A> cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q);
+
+// Periodic sorted nearest_n over one tree through a plain walk where the box's
+// faces cannot change a row, and the periodic walk for the other rows
+// (kgpu_periodic_fast.cu).  `handled` is false, with nothing launched, where
+// it does not apply; the caller then launches the periodic walk itself.
+template <typename A>
+cudaError_t periodic_fast(const DeviceTree& t, const QueryLaunch& q, bool& handled);
 template <typename A> cudaError_t launch_wfixed(const DeviceTree& t, const QueryLaunch& q);
 template <typename A> cudaError_t launch_tfixed(const DeviceTree& t, const QueryLaunch& q);
 // Lists of any length held in the output rows (kernels_*_rows.cu).

@@ -79,6 +79,7 @@ inline Batch<A> make_batch(const QueryLaunch& q) {
   b.work = q.work;
   b.chunk = q.chunk;
   b.refill = q.refill;
+  b.nq_dev = q.nq_dev;
   return b;
 }
 
@@ -257,8 +258,13 @@ cudaError_t launch_tfixed_stems(const DeviceTree& t, const QueryLaunch& q) {
               return runt(k_tfixed<A, K, M, KF_APPROX, false, 0>);
             case KGPU_NEAREST_N:
             case KGPU_NEAREST_N_WITHIN:
-              if (q.engine == 3 && q.sorted && q.k <= kMaxK) {
-                // warp-cooperative leaf scans, lists in the output rows
+              // warp-cooperative leaf scans with lists in the output rows: on
+              // request, and by default for f64 lists above 20 entries, where
+              // per-thread lists in shared memory cut the blocks per SM (16M
+              // queries, f64, k = 24: 95 against 101 ms; k = 32: 115 against
+              // 261 ms; f32 up to k = 32 and f64 up to 16 stay per thread)
+              if ((q.engine == 3 || (q.engine == 0 && sizeof(A) == 8 && q.k > 20)) && q.sorted &&
+                  q.k <= kMaxK) {
                 const size_t csmem = size_t(levels) * 256 * (STEMS ? 2 * sizeof(A) + 4 : sizeof(A));
                 auto kern = k_tnn_coop<A, K, M, EX, STEMS>;
                 cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
