@@ -303,7 +303,10 @@ def l2_note(n, nq, itemsize):
 
 def kernel_name(fam, engine):
     if fam.startswith("periodic"):
-        return "k_tperiodic_nn" if engine != "warp" else "k_periodic_fixed<nearest_n>"
+        # rows away from the box's faces: the plain cooperative pass; the rest
+        # (a few percent) take the periodic walk
+        return ("k_tnn_coop (plain pass) + k_tperiodic_nn (rows near the faces)"
+                if engine != "warp" else "k_periodic_fixed<nearest_n>")
     if fam == "nearest_n" and engine == "coop":
         return "k_tnn_coop"
     f = {"nearest_n": "nearest_n", "approx": "approx", "nearest_one": "nearest_one"}[fam]
