@@ -49,6 +49,13 @@ struct Batch {
   // length the host has not read)
   const unsigned long long* nq_dev = nullptr;
 
+  // the number of queries to process: nq, or less when nq_dev says so
+  __device__ __forceinline__ uint64_t count() const {
+    if (!nq_dev) return nq;
+    const uint64_t m = *nq_dev;
+    return m < nq ? m : nq;
+  }
+
   // A query naming no tree of the forest sees an empty tree (no results).
   __device__ __forceinline__ TreeView<A> tree(const TreeView<A>& tv, uint64_t qi) const {
     if (!forest) return tv;
@@ -70,37 +77,39 @@ struct Batch {
 // One query per warp: f(qi) with all 32 lanes.
 template <typename A, typename F>
 __device__ __forceinline__ void for_each_query_warp(const Batch<A>& b, F&& f) {
+  const uint64_t nq = b.count();
   if (b.work) {
     const int lane = threadIdx.x & 31;
     for (;;) {
       unsigned long long w = 0;
       if (lane == 0) w = atomicAdd(b.work, 1ull);
       w = __shfl_sync(FULL, w, 0);
-      if (w >= b.nq) break;
+      if (w >= nq) break;
       f(b.order ? uint64_t(b.order[w]) : uint64_t(w));
     }
   } else {
     const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t w = warp; w < b.nq; w += nwarps) f(b.order ? uint64_t(b.order[w]) : w);
+    for (uint64_t w = warp; w < nq; w += nwarps) f(b.order ? uint64_t(b.order[w]) : w);
   }
 }
 
 // One query per thread; with a work counter a warp takes 32 consecutive slots.
 template <typename A, typename F>
 __device__ __forceinline__ void for_each_query_thread(const Batch<A>& b, F&& f) {
+  const uint64_t nq = b.count();
   if (b.work) {
     const int lane = threadIdx.x & 31;
     for (;;) {
       unsigned long long base = 0;
       if (lane == 0) base = atomicAdd(b.work, 32ull);
       base = __shfl_sync(FULL, base, 0);
-      if (base >= b.nq) break;
+      if (base >= nq) break;
       const uint64_t w = base + lane;
-      if (w < b.nq) f(b.order ? uint64_t(b.order[w]) : w);
+      if (w < nq) f(b.order ? uint64_t(b.order[w]) : w);
     }
   } else {
-    for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < b.nq;
+    for (uint64_t w = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < nq;
          w += uint64_t(gridDim.x) * blockDim.x)
       f(b.order ? uint64_t(b.order[w]) : w);
   }
@@ -275,11 +284,7 @@ struct LaneFeeder {
       base = chunk * n;
       chunk += step;
     }
-    uint64_t nq = b.nq;
-    if (b.nq_dev) {
-      const uint64_t m = *b.nq_dev;
-      nq = m < nq ? m : nq;
-    }
+    const uint64_t nq = b.count();
     if (base >= nq) {
       done = true;
       return false;

@@ -24,7 +24,8 @@
 // So the batch runs the plain walk first, a small kernel lists the queries
 // whose bound comes within a safety margin of a face (or whose coordinates
 // are not inside the box), and the periodic walk runs on those alone,
-// overwriting their rows.  Unsorted lists are not taken this way (their order
+// overwriting their rows.  Batches that ask for the warp engine keep its
+// periodic walk for every row.  Unsorted lists are not taken this way (their order
 // after evictions depends on every insertion the walk made), nor are
 // traversal statistics (they count the reference's periodic walk).
 #include <algorithm>
@@ -199,7 +200,8 @@ cudaError_t periodic_fast(const DeviceTree& dt, const QueryLaunch& q, bool& hand
   handled = false;
   const bool nn = q.family == KGPU_NEAREST_N || q.family == KGPU_NEAREST_N_WITHIN;
   if (!q.periodic || !nn || !q.sorted || q.stats || q.forest || q.radii || q.nq_dev ||
-      dt.scalar_walk() || (dt.dims != 2 && dt.dims != 3) || q.nq < kFastMinBatch)
+      q.engine == 1 || dt.scalar_walk() || (dt.dims != 2 && dt.dims != 3) ||
+      q.nq < kFastMinBatch)
     return cudaSuccess;
   if (!point_bounds<A>(dt, q.stream)) return cudaSuccess;
   for (int d = 0; d < dt.dims; ++d) {

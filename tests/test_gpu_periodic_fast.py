@@ -114,3 +114,31 @@ def test_fast_path_launches_the_extra_kernels_only_for_large_batches():
 
     assert launches(small) == 1
     assert launches(large) == 3
+
+
+@pytest.mark.parametrize("k", [40, 100])
+def test_fast_path_with_lists_beyond_32(k):
+    """Lists above 32 entries: the periodic rows go through the row-list
+    kernel, the plain rows through the plain engines."""
+    rng = np.random.default_rng(k)
+    P = rng.random((150_000, 3))
+    Q = _queries(rng, 70_000, 3, np.float64)
+    box = np.ones(3)
+    t = kb.ImmutableKdTree.new_from_slice(P)
+    o = oracle.OracleTree.build(P)
+    g = t.query(Q).periodic_boundary_condition(box).nearest_n(kb.SquaredEuclidean, k).execute_gpu()
+    assert_same_fixed(g.distances, g.items, g.counts, *o.periodic_nearest_n(Q, box, k), f"pnn{k}")
+
+
+def test_warp_engine_batches_keep_the_periodic_walk():
+    """A large batch that asks for the warp engine takes its periodic walk for
+    every row, with the same rows as the oracle."""
+    rng = np.random.default_rng(21)
+    P = rng.random((80_000, 3))
+    Q = _queries(rng, 70_500, 3, np.float64)[:-500]  # without the NaN rows
+    box = np.ones(3)
+    t = kb.ImmutableKdTree.new_from_slice(P)
+    o = oracle.OracleTree.build(P)
+    g = (t.query(Q).with_engine("warp").periodic_boundary_condition(box)
+         .nearest_n(kb.SquaredEuclidean, 8).execute_gpu())
+    assert_same_fixed(g.distances, g.items, g.counts, *o.periodic_nearest_n(Q, box, 8), "warp")
