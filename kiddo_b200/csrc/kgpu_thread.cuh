@@ -772,6 +772,21 @@ struct TNearestN {
     if constexpr (RowLeaves<A, K>::value)
       for (uint32_t b = 0; b < len * row_bytes<A>(); b += 128u)
         asm volatile("prefetch.global.L1 [%0];" ::"l"(base + b));
+    if constexpr (RowLeaves<A, K>::value && sizeof(A) == 4) {
+      if (n == 0) {
+        // A leaf reached with an empty list (every query's first): each point
+        // that passes the gate is added, so one pass loads, measures and adds
+        // the points in leaf order instead of marking them first.
+        const float4* rows = reinterpret_cast<const float4*>(base);
+        for (uint32_t p = 0; p < len; ++p) {
+          const float4 v = __ldg(rows + p);
+          const A c[K] = {v.x, v.y, v.z};
+          const A d = dist(c);
+          if (d <= gate) add(d, __float_as_uint(v.w));
+        }
+        return len;
+      }
+    }
     for (uint32_t c0 = 0; c0 < len; c0 += 32) {
       uint32_t mask = leaf_chunk_mask<A, K>(base, len, c0, dist, [&](A d) { return d <= gate; });
       if constexpr (RowLeaves<A, K>::value && sizeof(A) == 4) {
