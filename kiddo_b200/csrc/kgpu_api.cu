@@ -792,6 +792,24 @@ void apply_periodic(const DeviceTree& dt, const kgpu_query_desc* d, QueryLaunch&
                                     : double(static_cast<const float*>(d->periodic_box)[a]);
 }
 
+// The lane-refilled kernels take their next chunk of queries from a device
+// counter when they are given one: a warp whose chunks finish early takes
+// more, where a fixed interleaved share of the batch left warps idle behind
+// the slowest (kNN16 over 16M queries: 471M against 531M queries/s).  Forest
+// batches bring their own counter; every other launch gets a fresh zeroed
+// one, so launches never share a count.
+template <typename F>
+cudaError_t with_work_counter(const QueryLaunch& q, F&& launch) {
+  if (q.work) return launch(q);
+  DevBuf w;
+  cudaError_t e = w.alloc(sizeof(unsigned long long), q.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(w.p, 0, sizeof(unsigned long long), q.stream);
+  if (e != cudaSuccess) return e;
+  QueryLaunch qw = q;
+  qw.work = w.as<unsigned long long>();
+  return launch(qw);
+}
+
 template <typename A>
 cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   // thread engine for 2-D/3-D trees; periodic nearest_one stays on the warp
@@ -808,11 +826,13 @@ cudaError_t launch_fixed(const DeviceTree& t, const QueryLaunch& q) {
   const bool two_three = t.dims == 2 || t.dims == 3;
   if ((nn || best) && two_three && q.k > kMaxK &&
       (q.k > kMaxBigK || (nn && q.periodic) || t.scalar_walk()))
-    return launch_trow<A>(t, q);
+    return with_work_counter(q, [&](const QueryLaunch& qw) { return launch_trow<A>(t, qw); });
   const bool big_k = q.k > kMaxK && (best || (nn && (q.k > kMaxThreadK || q.periodic)));
   const bool thread = (t.scalar_walk() || q.engine != 1) && two_three &&
                       (!q.periodic || q.family != KGPU_NEAREST_ONE || t.scalar_walk()) && !big_k;
-  return thread ? launch_tfixed<A>(t, q) : launch_wfixed<A>(t, q);
+  // the warp engine keeps its fixed shares: it takes one query at a time
+  if (!thread) return launch_wfixed<A>(t, q);
+  return with_work_counter(q, [&](const QueryLaunch& qw) { return launch_tfixed<A>(t, qw); });
 }
 template cudaError_t launch_fixed<float>(const DeviceTree&, const QueryLaunch&);
 template cudaError_t launch_fixed<double>(const DeviceTree&, const QueryLaunch&);
